@@ -1,0 +1,356 @@
+"""CP-ALS benchmark on the Zipf(1.1) 2M x 2M x 25k, 200M-nonzero, rank-32
+workload (plain FP64 form), one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one CP-ALS iteration: MTTKRP of all three modes, the R x R
+solves, factor updates, normalisation, Grams and the fit.  Prints one JSON
+line (rank 0).  Inputs (3.2 GB stream + 1 GB of factors) are larger than
+the 126 MB L2, so no flush is needed between steps.
+
+--impl reference times the reference's own CPU MTTKRP (mttkrp_alto_par from
+include/alto.hpp, compiled from the reference sources into oracle/_ref) on a
+bounded sample of the same workload with all host threads.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+WORKLOAD = dict(workload="cpals_zipf1.1_2Mx2Mx25k_nnz200M_r32", dims=[2_000_000, 2_000_000, 25_000],
+                nnz=200_000_000, rank=32, zipf=1.1, values="lognormal(0,1) fp32 summed over duplicates, fp64")
+METRIC = "CP-ALS ms/iter"
+
+
+def load_pkg():
+    import __graft_entry__ as ge
+    return ge._load()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def mttkrp_alg_bytes(dims, nnz, R, mode, s_idx=8, s_val=8, s_fac=8, s_out=8):
+    """Algorithmic bytes of one mode-t MTTKRP: the index/value stream once,
+    every input factor once and the output once."""
+    b = nnz * (s_idx + s_val) + dims[mode] * R * s_out
+    for m, d in enumerate(dims):
+        if m != mode:
+            b += d * R * s_fac
+    return b
+
+
+def traffic_from_profiles():
+    """DRAM bytes per MTTKRP launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "mttkrp_fp64_zipf_2Mx2Mx25k_r32.md")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.startswith("traffic_bytes_per_launch_full_size:"):
+                try:
+                    return float(line.split(":", 1)[1].strip())
+                except ValueError:
+                    return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip() == "Active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return dict(sm_mhz=statistics.median(sm), sm_max_mhz=mx, reasons=sorted(reasons), samples=len(sm))
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU MTTKRP on a bounded sample of the workload."""
+    if rank != 0:
+        return
+    import ctypes
+    import torch
+    import pyoracle as po
+    R = po.ref_lib()
+    if R is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libblco_ref.so not built"}))
+        return
+    pkg = load_pkg()
+    from blco_b200 import synth
+    sample = args.ref_sample
+    dims = WORKLOAD["dims"]
+    if torch.cuda.is_available():
+        X = synth.zipf_tensor_device(sample, dims, WORKLOAD["zipf"], seed=7)
+        cidx = np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]])
+        vals = X["vals"].cpu().numpy()
+    else:
+        X = synth.uniform_tensor_host(sample, dims, seed=7)
+        cidx, vals = X["cidx"], X["vals"]
+    rk = WORKLOAD["rank"]
+    nthreads = os.cpu_count() or 1
+    d64 = np.ascontiguousarray(dims, dtype=np.uint64)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    f64p = ctypes.POINTER(ctypes.c_double)
+    h = R.ref_alto_create(3, d64.ctypes.data_as(u64p), sample, np.ascontiguousarray(cidx).ctypes.data_as(u64p),
+                          np.ascontiguousarray(vals).ctypes.data_as(f64p), nthreads)
+    rng = np.random.default_rng(0)
+    fs = [rng.random((d, rk)) for d in dims]
+    ptrs = (ctypes.c_void_p * 3)(*[f.ctypes.data for f in fs])
+    step_ms = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for m in range(3):
+            R.ref_alto_mttkrp(h, m, rk, ptrs)
+        dt = (time.perf_counter() - t0) * 1e3
+        if s >= args.warmup:
+            step_ms.append(dt)
+    R.ref_alto_destroy(h, rk)
+    per_nnz = statistics.median(step_ms) / sample
+    value = per_nnz * WORKLOAD["nnz"]
+    desc = (f"reference mttkrp_alto_par (oracle/_ref) over all 3 modes, {sample} nonzeros of the same "
+            f"distribution and dims, {nthreads} threads, median of {args.steps} sweeps, scaled linearly "
+            f"to {WORKLOAD['nnz']} nonzeros; MTTKRP part of the iteration only")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "higher_is_better": False,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(workload=WORKLOAD["workload"], parallelism="cpu", l2="inputs larger than L2"),
+        "cpu_baseline": dict(value=value, unit="ms", cores=nthreads, kind="reference", sample=desc),
+        "e2e": dict(value=value, unit="ms", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+    }))
+
+
+def cpu_baseline_quick(args, dims, rk):
+    """Reference CPU MTTKRP on a bounded sample (rank 0, N=1 only)."""
+    import ctypes
+    import pyoracle as po
+    from blco_b200 import synth
+    R = po.ref_lib()
+    if R is None:
+        return None
+    sample = args.ref_sample
+    X = synth.zipf_tensor_device(sample, dims, WORKLOAD["zipf"], seed=7)
+    cidx = np.ascontiguousarray(np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]]))
+    vals = np.ascontiguousarray(X["vals"].cpu().numpy())
+    del X
+    nthreads = os.cpu_count() or 1
+    d64 = np.ascontiguousarray(dims, dtype=np.uint64)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    f64p = ctypes.POINTER(ctypes.c_double)
+    h = R.ref_alto_create(3, d64.ctypes.data_as(u64p), sample, cidx.ctypes.data_as(u64p),
+                          vals.ctypes.data_as(f64p), nthreads)
+    rng = np.random.default_rng(0)
+    fs = [rng.random((d, rk)) for d in dims]
+    ptrs = (ctypes.c_void_p * 3)(*[f.ctypes.data for f in fs])
+    for m in range(3):
+        R.ref_alto_mttkrp(h, m, rk, ptrs)
+    t0 = time.perf_counter()
+    reps = 2
+    for _ in range(reps):
+        for m in range(3):
+            R.ref_alto_mttkrp(h, m, rk, ptrs)
+    dt = (time.perf_counter() - t0) * 1e3 / reps
+    R.ref_alto_destroy(h, rk)
+    value = dt / sample * WORKLOAD["nnz"]
+    return dict(value=value, unit="ms", cores=nthreads, kind="reference",
+                sample=(f"reference mttkrp_alto_par (oracle/_ref), all 3 modes on {sample} nonzeros of the "
+                        f"same distribution and dims, {nthreads} threads, scaled linearly to "
+                        f"{WORKLOAD['nnz']} nonzeros; MTTKRP part of the iteration only"))
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    pkg = load_pkg()
+    from blco_b200 import synth
+    dims, nnz, rk = WORKLOAD["dims"], args.nnz, WORKLOAD["rank"]
+    X = synth.zipf_tensor_device(nnz, dims, WORKLOAD["zipf"], seed=args.seed + rank)
+    stream = torch.cuda.current_stream()
+    opts = pkg.make_opts(kernel=args.kernel, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"], 0, opts)
+    torch.cuda.synchronize()
+    encode_ms = (time.perf_counter() - e0) * 1e3
+    # host copies for the end-to-end leg (pinned)
+    h_cidx = [c.to(torch.int64).cpu().pin_memory() for c in X["cidx"]]
+    h_vals = X["vals"].cpu().pin_memory()
+    del X
+    g = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    fs0 = [torch.rand(d, rk, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    fs = [f.clone() for f in fs0]
+    lam = torch.ones(rk, dtype=torch.float64, device="cuda")
+    plan = pkg.CpalsPlan(t, fs, lam, opts)
+    plan.iterate(args.warmup, tol=-1.0)
+    ms0, calls0 = plan.mttkrp_ms()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    pkg.launch_count(reset=True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    fits = plan.iterate(args.steps, tol=-1.0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = pkg.launch_count(reset=True)
+    ck = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1)
+    ms1, calls1 = plan.mttkrp_ms()
+    mt_ms = (ms1 - ms0) / max(1, calls1 - calls0)  # per mode, per iteration
+    if dist:
+        tt = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = tt.item()
+    ms_per_step = elapsed / args.steps
+    plan.destroy()
+    del fs, lam
+
+    # end-to-end: the public C ABI from host buffers (COO in, factors out)
+    h_fs = [f.cpu().numpy().copy() for f in fs0]
+    e_iters = args.steps
+    h2d = sum(c.numel() * 8 for c in h_cidx) + h_vals.numel() * 8 + sum(f.nbytes for f in h_fs) + rk * 8
+    d2h = sum(f.nbytes for f in h_fs) + rk * 8 + e_iters * 8
+    cidx_np = [c.numpy().view(np.uint64) for c in h_cidx]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    import ctypes
+    L = pkg.lib()
+    ptrs = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in cidx_np])
+    h = ctypes.c_void_p()
+    o2 = pkg.make_opts(kernel=args.kernel, stream=0)
+    d64 = np.ascontiguousarray(dims, dtype=np.uint64)
+    st = L.blco_encode(3, d64.ctypes.data, nnz, ptrs, h_vals.numpy().ctypes.data, 0, ctypes.byref(o2),
+                       ctypes.byref(h))
+    if st != 0:
+        raise RuntimeError(L.blco_last_error().decode())
+    t2 = pkg.Tensor(h.value)
+    lam_h = np.ones(rk)
+    pkg.cpals(t2, h_fs, lam_h, e_iters, -1.0, o2)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e_iters
+    t2.free()
+    if dist:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = tt.item()
+
+    peak, peak_kind = peaks()
+    alg = [mttkrp_alg_bytes(dims, nnz, rk, m) for m in range(3)]
+    achieved = sum(alg) / (sum(mt_ms) * 1e-3) / 1e9  # GB/s averaged over the three launches
+    traffic = traffic_from_profiles()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_quick(args, dims, rk)
+    t.free()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ms_per_step, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload=WORKLOAD["workload"], dims=dims, nnz=nnz, rank=rk, zipf=WORKLOAD["zipf"],
+                           values=WORKLOAD["values"], precision="fp64 (plain form)", kernel=args.kernel,
+                           parallelism=("replicas" if world > 1 else "single"),
+                           l2="inputs larger than L2 (3.2 GB stream, 1 GB factors)"),
+            "mttkrp_ms_per_mode": [round(x, 4) for x in mt_ms],
+            "mttkrp_gbs": achieved, "encode_ms": encode_ms, "fit_last": fits[-1] if fits else None,
+            "roofline": dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                             traffic=traffic, peak_kind=peak_kind + " (hbm_gbs burst copy)",
+                             kernel="k_mttkrp_vec<3,32> (mean over the 3 modes)"),
+            "cpu_baseline": cpu,
+            "e2e": dict(value=e2e_ms, unit="ms", h2d_bytes_per_step=int(h2d / e_iters),
+                        d2h_bytes_per_step=int(d2h / e_iters),
+                        note=(f"blco_encode from pinned host COO + blco_cpals({e_iters} iters) with host "
+                              "factors; job time / iterations; bytes are per iteration")),
+            "gpu_launches": int(launches),
+            "clocks": ck,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nnz", type=int, default=WORKLOAD["nnz"])
+    ap.add_argument("--kernel", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--ref-sample", type=int, default=2_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,308 @@
+"""Python binding of libblco_b200 (ctypes over the C ABI in include/blco.h).
+
+The engine is the CUDA/C++ library lib/libblco_b200.so built for sm_100a by
+`make -C blocked-linearized-coordinate_b200`.  This module only marshals
+pointers: host arrays are numpy arrays, device arrays are torch CUDA tensors
+(torch is used for device memory and streams, nothing else).  Every call
+raises BlcoError when the library returns a non-zero status; there is no
+fallback path.
+
+Entry points mirror the reference's in-process interface
+(jeewhanchoi/blocked-linearized-coordinate):
+  encode / encode_device   gen_blcotensor_host<u64> (include/blco.hpp:196)
+  mttkrp / mttkrp_host     mttkrp_alto_dev_onemode (src/alto_dev.cu:1955)
+  cpals                    cpals_blco_dev (src/cpd_gpu.cu:21)
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libblco_b200.so")
+MAX_MODES = 5
+
+OK = 0
+ERR_INVALID = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_NOMEM = 4
+ERR_TIMEOUT = 5
+ERR_IO = 6
+ERR_STATE = 7
+
+KERNEL_AUTO = 10
+KERNEL_LVL1 = 1
+KERNEL_LVL2 = 2
+KERNEL_LVL3 = 3
+KERNEL_BATCHED = 11
+KERNEL_BATCHED_V2 = 12
+KERNEL_ATOMIC = 13
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+# Every symbol include/blco.h declares.
+EXPORTS = (
+    "blco_opts_init", "blco_status_string", "blco_last_error", "blco_version",
+    "blco_encode", "blco_encode_device", "blco_tensor_free", "blco_tensor_get_info",
+    "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_host",
+    "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
+    "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_launch_count",
+)
+
+
+class BlcoError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} [status {status}]")
+        self.status = status
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [
+        ("kernel", ctypes.c_int),
+        ("nprtn", ctypes.c_int),
+        ("thread_cf", ctypes.c_int),
+        ("stream_data", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("verbose", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("residency_bytes", ctypes.c_uint64),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+class TensorInfo(ctypes.Structure):
+    _fields_ = [
+        ("nmodes", ctypes.c_int),
+        ("dims", ctypes.c_uint64 * MAX_MODES),
+        ("nnz", ctypes.c_uint64),
+        ("block_count", ctypes.c_uint64),
+        ("max_block_size", ctypes.c_uint64),
+        ("mode_masks", ctypes.c_uint64 * MAX_MODES),
+        ("mode_pos", ctypes.c_int * MAX_MODES),
+        ("alto_masks", ctypes.c_uint64 * MAX_MODES),
+        ("alto_bits", ctypes.c_int),
+        ("device", ctypes.c_int),
+        ("resident", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load the library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is not built; run make -C {HERE}")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u64, i32, f64 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_double
+        L.blco_status_string.restype = ctypes.c_char_p
+        L.blco_last_error.restype = ctypes.c_char_p
+        L.blco_version.restype = ctypes.c_char_p
+        L.blco_launch_count.restype = u64
+        L.blco_launch_count.argtypes = [i32]
+        L.blco_opts_init.argtypes = [vp]
+        L.blco_encode.argtypes = [i32, vp, u64, vp, vp, u64, vp, vp]
+        L.blco_encode_device.argtypes = [i32, vp, u64, vp, vp, u64, vp, vp]
+        L.blco_tensor_free.argtypes = [vp]
+        L.blco_tensor_get_info.argtypes = [vp, vp]
+        L.blco_tensor_copy_out.argtypes = [vp, vp, vp, vp, vp]
+        L.blco_tensor_device_arrays.argtypes = [vp, vp, vp]
+        L.blco_mttkrp.argtypes = [vp, i32, i32, vp, vp, vp]
+        L.blco_mttkrp_host.argtypes = [vp, i32, i32, vp, vp, vp]
+        L.blco_cpals.argtypes = [vp, i32, vp, vp, i32, f64, vp, vp, vp, vp]
+        L.blco_cpals_plan_create.argtypes = [vp, i32, vp, vp, vp, vp]
+        L.blco_cpals_plan_iterate.argtypes = [vp, i32, f64, vp, vp]
+        L.blco_cpals_plan_mttkrp_ms.argtypes = [vp, vp, vp]
+        L.blco_cpals_plan_destroy.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != OK:
+        raise BlcoError(status, lib().blco_last_error().decode() or lib().blco_status_string(status).decode())
+
+
+def version():
+    return lib().blco_version().decode()
+
+
+def launch_count(reset=False):
+    return int(lib().blco_launch_count(1 if reset else 0))
+
+
+def make_opts(kernel=KERNEL_AUTO, nprtn=0, thread_cf=2, stream_data=False, precision=PRECISION_FP64,
+              verbose=False, device=0, residency_bytes=0, stream=None):
+    o = Opts()
+    lib().blco_opts_init(ctypes.byref(o))
+    o.kernel, o.nprtn, o.thread_cf = kernel, nprtn, thread_cf
+    o.stream_data, o.precision, o.verbose = int(stream_data), precision, int(verbose)
+    o.device, o.residency_bytes = device, residency_bytes
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                stream = torch.cuda.current_stream(device).cuda_stream
+        except ImportError:
+            stream = None
+    o.stream = stream
+    return o
+
+
+def _u64arr(a):
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def _ptrs(ptr_list):
+    return (ctypes.c_void_p * len(ptr_list))(*ptr_list)
+
+
+class Tensor:
+    """An encoded BLCO tensor owned by the library."""
+
+    def __init__(self, handle):
+        self._h = ctypes.c_void_p(handle)
+
+    @property
+    def handle(self):
+        return self._h
+
+    @classmethod
+    def encode(cls, dims, cidx, vals, max_block_size=0, opts=None):
+        """Encode host COO arrays: cidx is (nmodes, nnz) 0-based, vals (nnz,)."""
+        dims = _u64arr(dims)
+        cidx = _u64arr(cidx)
+        vals = np.ascontiguousarray(vals, dtype=np.float64)
+        nmodes, nnz = cidx.shape
+        ptrs = _ptrs([cidx[n].ctypes.data for n in range(nmodes)])
+        h = ctypes.c_void_p()
+        o = opts if opts is not None else make_opts()
+        _check(lib().blco_encode(nmodes, dims.ctypes.data, nnz, ptrs, vals.ctypes.data, max_block_size,
+                                 ctypes.byref(o), ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def encode_device(cls, dims, d_cidx, d_vals, max_block_size=0, opts=None):
+        """Encode COO arrays already on the GPU (torch int64/uint64 and float64)."""
+        dims = _u64arr(dims)
+        nmodes = len(d_cidx)
+        nnz = int(d_vals.numel())
+        ptrs = _ptrs([int(c.data_ptr()) for c in d_cidx])
+        h = ctypes.c_void_p()
+        o = opts if opts is not None else make_opts()
+        _check(lib().blco_encode_device(nmodes, dims.ctypes.data, nnz, ptrs, int(d_vals.data_ptr()),
+                                        max_block_size, ctypes.byref(o), ctypes.byref(h)))
+        return cls(h.value)
+
+    def info(self):
+        inf = TensorInfo()
+        _check(lib().blco_tensor_get_info(self._h, ctypes.byref(inf)))
+        n = inf.nmodes
+        return dict(nmodes=n, dims=list(inf.dims[:n]), nnz=inf.nnz, block_count=inf.block_count,
+                    max_block_size=inf.max_block_size, mode_masks=list(inf.mode_masks[:n]),
+                    mode_pos=list(inf.mode_pos[:n]), alto_masks=list(inf.alto_masks[:n]),
+                    alto_bits=inf.alto_bits, device=inf.device, resident=bool(inf.resident))
+
+    def copy_out(self):
+        inf = self.info()
+        nnz, nb, n = inf["nnz"], inf["block_count"], inf["nmodes"]
+        coords = np.zeros(nnz, dtype=np.uint64)
+        vals = np.zeros(nnz, dtype=np.float64)
+        offs = np.zeros(nb + 1, dtype=np.uint64)
+        bcoords = np.zeros(max(nb * n, 1), dtype=np.uint64)
+        _check(lib().blco_tensor_copy_out(self._h, coords.ctypes.data, vals.ctypes.data, offs.ctypes.data,
+                                          bcoords.ctypes.data))
+        return dict(coords=coords, vals=vals, block_offsets=offs, block_coords=bcoords[: nb * n].reshape(nb, n),
+                    **inf)
+
+    def free(self):
+        if self._h and self._h.value:
+            _check(lib().blco_tensor_free(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def mttkrp(t, mode, factors, out, opts=None):
+    """out (torch CUDA float64, dims[mode] x R) += MTTKRP; factors are torch
+    CUDA float64 row-major matrices (factors[mode] may be None)."""
+    rank = int(out.shape[1])
+    ptrs = _ptrs([int(f.data_ptr()) if f is not None else 0 for f in factors])
+    o = opts if opts is not None else make_opts()
+    _check(lib().blco_mttkrp(t.handle, mode, rank, ptrs, int(out.data_ptr()), ctypes.byref(o)))
+
+
+def mttkrp_host(t, mode, factors, out=None, opts=None):
+    """Host numpy version; returns out (+)= MTTKRP."""
+    factors = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    rank = factors[0].shape[1]
+    if out is None:
+        out = np.zeros((factors[mode].shape[0], rank), dtype=np.float64)
+    ptrs = _ptrs([f.ctypes.data for f in factors])
+    o = opts if opts is not None else make_opts()
+    _check(lib().blco_mttkrp_host(t.handle, mode, rank, ptrs, out.ctypes.data, ctypes.byref(o)))
+    return out
+
+
+def cpals(t, factors, lam, maxiter, tol, opts=None):
+    """CP-ALS with host numpy factors (updated in place).  Returns
+    (final_fit, per-iteration fits)."""
+    for f in factors:
+        if not (f.flags.c_contiguous and f.dtype == np.float64):
+            raise ValueError("factors must be C-contiguous float64")
+    rank = factors[0].shape[1]
+    fits = np.zeros(max(maxiter, 1), dtype=np.float64)
+    fit = ctypes.c_double()
+    iters = ctypes.c_int()
+    ptrs = _ptrs([f.ctypes.data for f in factors])
+    o = opts if opts is not None else make_opts()
+    _check(lib().blco_cpals(t.handle, rank, ptrs, lam.ctypes.data, maxiter, tol, ctypes.byref(o),
+                            ctypes.byref(fit), fits.ctypes.data, ctypes.byref(iters)))
+    return fit.value, list(fits[: iters.value])
+
+
+class CpalsPlan:
+    """Device-resident CP-ALS over torch CUDA factors (owned by the caller)."""
+
+    def __init__(self, t, factors, lam, opts=None):
+        self._t = t
+        self._keep = (factors, lam)
+        self.nmodes = len(factors)
+        ptrs = _ptrs([int(f.data_ptr()) for f in factors])
+        h = ctypes.c_void_p()
+        o = opts if opts is not None else make_opts()
+        self._opts = o
+        _check(lib().blco_cpals_plan_create(t.handle, int(factors[0].shape[1]), ptrs, int(lam.data_ptr()),
+                                            ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    def iterate(self, iters, tol=-1.0):
+        fits = np.zeros(max(iters, 1), dtype=np.float64)
+        done = ctypes.c_int()
+        _check(lib().blco_cpals_plan_iterate(self._h, iters, tol, fits.ctypes.data, ctypes.byref(done)))
+        return list(fits[: done.value])
+
+    def mttkrp_ms(self):
+        ms = np.zeros(self.nmodes, dtype=np.float64)
+        calls = ctypes.c_int()
+        _check(lib().blco_cpals_plan_mttkrp_ms(self._h, ms.ctypes.data, ctypes.byref(calls)))
+        return ms, calls.value
+
+    def destroy(self):
+        if self._h and self._h.value:
+            _check(lib().blco_cpals_plan_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

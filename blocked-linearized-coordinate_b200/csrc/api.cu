@@ -1,0 +1,393 @@
+// api.cu -- the extern "C" boundary of libblco_b200 (include/blco.h).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "internal.cuh"
+
+namespace blco {
+
+static thread_local std::string g_last_error;
+static thread_local uint64_t g_launches = 0;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+void count_launch() { g_launches++; }
+
+int fail(int status, const std::string& msg)
+{
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line)
+{
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    g_last_error = buf;
+    return e == cudaErrorMemoryAllocation ? BLCO_ERR_NOMEM : BLCO_ERR_CUDA;
+}
+
+int device_info(int device, DeviceInfo* out)
+{
+    static std::mutex mu;
+    static DeviceInfo cache[64];
+    static bool have[64] = {};
+    if (device < 0 || device >= 64) return fail(BLCO_ERR_INVALID, "bad device ordinal");
+    std::lock_guard<std::mutex> g(mu);
+    if (!have[device]) {
+        DeviceInfo d;
+        d.device = device;
+        BLCO_CUDA(cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, device));
+        int optin = 0;
+        BLCO_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        d.smem_optin = (size_t)optin;
+        int major = 0;
+        BLCO_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+        if (major != 10)
+            return fail(BLCO_ERR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+        cache[device] = d;
+        have[device] = true;
+    }
+    *out = cache[device];
+    return BLCO_OK;
+}
+
+cudaStream_t pick_stream(const blco_tensor* t, const blco_opts* opts)
+{
+    if (opts && opts->stream) return (cudaStream_t)opts->stream;
+    if (t && t->own_stream) return t->own_stream;
+    if (t) {
+        blco_tensor* tm = const_cast<blco_tensor*>(t);
+        if (cudaStreamCreateWithFlags(&tm->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_error("cudaStreamCreate failed");
+            return nullptr;
+        }
+        return tm->own_stream;
+    }
+    return nullptr;
+}
+
+// Streamed MTTKRP: the blocks stay in pinned host memory; they are copied
+// into a ring of device buffers on a copy stream while the compute stream
+// runs the kernel on the previous block (the --stream-data path,
+// src/alto_dev.cu:1979-2012, with events instead of one stream per block).
+static int mttkrp_streamed(blco_tensor* t, const MttkrpArgs& base, const blco_opts* opts, cudaStream_t s)
+{
+    const uint64_t B = t->max_block_size ? t->max_block_size : t->nnz;
+    uint64_t budget = (opts && opts->residency_bytes) ? opts->residency_bytes : (8ull << 30);
+    int nbuf = (int)std::max<uint64_t>(2, std::min<uint64_t>(8, budget / std::max<uint64_t>(1, B * 16)));
+    nbuf = (int)std::min<uint64_t>((uint64_t)nbuf, std::max<uint64_t>(1, t->block_count));
+    std::vector<uint64_t*> dc(nbuf, nullptr);
+    std::vector<double*> dv(nbuf, nullptr);
+    std::vector<cudaEvent_t> copied(nbuf, nullptr), consumed(nbuf, nullptr);
+    cudaStream_t cs = nullptr;
+    int st = BLCO_OK;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(s);
+        if (cs) cudaStreamSynchronize(cs);
+        for (int i = 0; i < nbuf; i++) {
+            cudaFree(dc[i]);
+            cudaFree(dv[i]);
+            if (copied[i]) cudaEventDestroy(copied[i]);
+            if (consumed[i]) cudaEventDestroy(consumed[i]);
+        }
+        if (cs) cudaStreamDestroy(cs);
+    };
+#define SC(call)                                                               \
+    do {                                                                       \
+        cudaError_t _e = (call);                                               \
+        if (_e != cudaSuccess) {                                               \
+            st = cuda_fail(_e, #call, __FILE__, __LINE__);                     \
+            cleanup();                                                         \
+            return st;                                                         \
+        }                                                                      \
+    } while (0)
+    SC(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    for (int i = 0; i < nbuf; i++) {
+        SC(cudaMalloc(&dc[i], B * 8));
+        SC(cudaMalloc(&dv[i], B * 8));
+        SC(cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming));
+        SC(cudaEventCreateWithFlags(&consumed[i], cudaEventDisableTiming));
+    }
+    // The copy stream must not overwrite the caller's pending work order:
+    // make it wait for everything already queued on s.
+    SC(cudaEventRecord(consumed[0], s));
+    SC(cudaStreamWaitEvent(cs, consumed[0], 0));
+    for (uint64_t b = 0; b < t->block_count; b++) {
+        const int k = (int)(b % nbuf);
+        const uint64_t beg = b * B, n = std::min(B, t->nnz - beg);
+        if (b >= (uint64_t)nbuf) SC(cudaStreamWaitEvent(cs, consumed[k], 0));
+        SC(cudaMemcpyAsync(dc[k], t->h_coords + beg, n * 8, cudaMemcpyHostToDevice, cs));
+        SC(cudaMemcpyAsync(dv[k], t->h_values + beg, n * 8, cudaMemcpyHostToDevice, cs));
+        SC(cudaEventRecord(copied[k], cs));
+        SC(cudaStreamWaitEvent(s, copied[k], 0));
+        MttkrpArgs a = base;
+        a.coords = dc[k];
+        a.vals = dv[k];
+        a.nnz = n;
+        st = mttkrp_launch(t, a, s);
+        if (st != BLCO_OK) {
+            cleanup();
+            return st;
+        }
+        SC(cudaEventRecord(consumed[k], s));
+    }
+#undef SC
+    cleanup();
+    return BLCO_OK;
+}
+
+} // namespace blco
+
+using namespace blco;
+
+extern "C" {
+
+void blco_opts_init(blco_opts* o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->kernel = BLCO_KERNEL_AUTO;
+    o->nprtn = 0;
+    o->thread_cf = 2;
+    o->precision = BLCO_PRECISION_FP64;
+}
+
+const char* blco_status_string(int s)
+{
+    switch (s) {
+    case BLCO_OK: return "ok";
+    case BLCO_ERR_INVALID: return "invalid argument";
+    case BLCO_ERR_UNSUPPORTED: return "unsupported";
+    case BLCO_ERR_CUDA: return "CUDA error";
+    case BLCO_ERR_NOMEM: return "out of memory";
+    case BLCO_ERR_TIMEOUT: return "device wait timed out";
+    case BLCO_ERR_IO: return "I/O error";
+    case BLCO_ERR_STATE: return "invalid state";
+    default: return "unknown status";
+    }
+}
+
+const char* blco_last_error(void) { return blco::last_error(); }
+
+const char* blco_version(void) { return "blco_b200 0.1.0 (sm_100a)"; }
+
+uint64_t blco_launch_count(int reset)
+{
+    uint64_t v = blco::g_launches;
+    if (reset) blco::g_launches = 0;
+    return v;
+}
+
+int blco_encode_device(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* d_cidx,
+                       const double* d_vals, uint64_t max_block_size, const blco_opts* opts, blco_tensor** out)
+{
+    if (!out) return fail(BLCO_ERR_INVALID, "null output handle");
+    return encode_impl(nmodes, dims, nnz, d_cidx, d_vals, max_block_size, opts, out);
+}
+
+int blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* cidx, const double* vals,
+                uint64_t max_block_size, const blco_opts* opts, blco_tensor** out)
+{
+    if (!out) return fail(BLCO_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    if (nmodes < 1 || nmodes > BLCO_MAX_MODES) return fail(BLCO_ERR_INVALID, "nmodes must be 1..5");
+    if (!dims || (nnz && (!cidx || !vals))) return fail(BLCO_ERR_INVALID, "null argument");
+    int device = opts ? opts->device : 0;
+    BLCO_CUDA(cudaSetDevice(device));
+    DeviceInfo di;
+    BLCO_TRY(device_info(device, &di));
+    const uint64_t n_alloc = nnz ? nnz : 1;
+    uint64_t* dc[BLCO_MAX_MODES] = {};
+    double* dv = nullptr;
+    int st = BLCO_OK;
+    cudaStream_t s = opts && opts->stream ? (cudaStream_t)opts->stream : nullptr;
+    auto cleanup = [&]() {
+        if (s) cudaStreamSynchronize(s);
+        else cudaDeviceSynchronize();
+        for (int n = 0; n < nmodes; n++) cudaFree(dc[n]);
+        cudaFree(dv);
+    };
+    for (int n = 0; n < nmodes && st == BLCO_OK; n++) {
+        if (nnz && !cidx[n]) st = fail(BLCO_ERR_INVALID, "null coordinate array");
+        cudaError_t e = cudaMalloc(&dc[n], n_alloc * 8);
+        if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(dc[n], cidx[n], nnz * 8, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess && st == BLCO_OK) st = cuda_fail(e, "coordinate upload", __FILE__, __LINE__);
+    }
+    if (st == BLCO_OK) {
+        cudaError_t e = cudaMalloc(&dv, n_alloc * 8);
+        if (e == cudaSuccess && nnz) e = cudaMemcpyAsync(dv, vals, nnz * 8, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) st = cuda_fail(e, "value upload", __FILE__, __LINE__);
+    }
+    if (st == BLCO_OK) {
+        if (s) st = cudaStreamSynchronize(s) == cudaSuccess ? BLCO_OK : fail(BLCO_ERR_CUDA, "upload sync failed");
+        else st = cudaDeviceSynchronize() == cudaSuccess ? BLCO_OK : fail(BLCO_ERR_CUDA, "upload sync failed");
+    }
+    if (st == BLCO_OK) st = encode_impl(nmodes, dims, nnz, dc, dv, max_block_size, opts, out);
+    cleanup();
+    return st;
+}
+
+int blco_tensor_free(blco_tensor* t)
+{
+    if (!t) return BLCO_OK;
+    cudaSetDevice(t->device);
+    if (t->own_stream) cudaStreamSynchronize(t->own_stream);
+    cudaFree(t->d_coords);
+    cudaFree(t->d_values);
+    cudaFree(t->d_values_f32);
+    if (t->h_coords) cudaFreeHost(t->h_coords);
+    if (t->h_values) cudaFreeHost(t->h_values);
+    for (int n = 0; n < BLCO_MAX_MODES; n++) {
+        cudaFree(t->hot[n].d_keys);
+        cudaFree(t->hot[n].d_slot);
+        cudaFree(t->hot[n].d_rows);
+    }
+    if (t->own_stream) cudaStreamDestroy(t->own_stream);
+    delete t;
+    return BLCO_OK;
+}
+
+int blco_tensor_get_info(const blco_tensor* t, blco_tensor_info* info)
+{
+    if (!t || !info) return fail(BLCO_ERR_INVALID, "null argument");
+    memset(info, 0, sizeof(*info));
+    info->nmodes = t->layout.nmodes;
+    for (int n = 0; n < t->layout.nmodes; n++) {
+        info->dims[n] = t->layout.dims[n];
+        info->mode_masks[n] = t->layout.mode_masks[n];
+        info->mode_pos[n] = t->layout.mode_pos[n];
+        info->alto_masks[n] = t->layout.alto_masks[n];
+    }
+    info->nnz = t->nnz;
+    info->block_count = t->block_count;
+    info->max_block_size = t->max_block_size;
+    info->alto_bits = t->layout.alto_bits;
+    info->device = t->device;
+    info->resident = t->resident ? 1 : 0;
+    return BLCO_OK;
+}
+
+int blco_tensor_copy_out(const blco_tensor* t, uint64_t* coords, double* values, uint64_t* block_offsets,
+                         uint64_t* block_coords)
+{
+    if (!t) return fail(BLCO_ERR_INVALID, "null tensor");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    if (t->nnz) {
+        if (t->resident) {
+            if (coords) BLCO_CUDA(cudaMemcpy(coords, t->d_coords, t->nnz * 8, cudaMemcpyDeviceToHost));
+            if (values) BLCO_CUDA(cudaMemcpy(values, t->d_values, t->nnz * 8, cudaMemcpyDeviceToHost));
+        } else {
+            if (coords) memcpy(coords, t->h_coords, t->nnz * 8);
+            if (values) memcpy(values, t->h_values, t->nnz * 8);
+        }
+    }
+    const uint64_t B = t->max_block_size ? t->max_block_size : t->nnz;
+    if (block_offsets) {
+        for (uint64_t b = 0; b < t->block_count; b++) block_offsets[b] = b * B;
+        block_offsets[t->block_count] = t->nnz;
+    }
+    if (block_coords) memset(block_coords, 0, t->block_count * t->layout.nmodes * sizeof(uint64_t));
+    return BLCO_OK;
+}
+
+int blco_tensor_device_arrays(const blco_tensor* t, const uint64_t** d_coords, const double** d_values)
+{
+    if (!t) return fail(BLCO_ERR_INVALID, "null tensor");
+    if (!t->resident) return fail(BLCO_ERR_STATE, "tensor blocks are streamed from host memory");
+    if (d_coords) *d_coords = t->d_coords;
+    if (d_values) *d_values = t->d_values;
+    return BLCO_OK;
+}
+
+int blco_mttkrp(blco_tensor* t, int mode, int rank, const double* const* d_factors, double* d_out,
+                const blco_opts* opts)
+{
+    if (!t || !d_factors || !d_out) return fail(BLCO_ERR_INVALID, "null argument");
+    if (mode < 0 || mode >= t->layout.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
+    if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
+    if (opts && opts->precision != BLCO_PRECISION_FP64)
+        return fail(BLCO_ERR_UNSUPPORTED, "blco_mttkrp takes FP64 factors; use the mixed-precision entry point");
+    for (int m = 0; m < t->layout.nmodes; m++)
+        if (m != mode && !d_factors[m]) return fail(BLCO_ERR_INVALID, "null factor matrix");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    cudaStream_t s = pick_stream(t, opts);
+    if (!s) return BLCO_ERR_CUDA;
+    MttkrpArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nnz = t->nnz;
+    a.mode = mode;
+    a.rank = rank;
+    for (int m = 0; m < t->layout.nmodes; m++) a.factors[m] = d_factors[m];
+    a.out = d_out;
+    a.kernel = opts ? opts->kernel : BLCO_KERNEL_AUTO;
+    a.thread_cf = opts ? opts->thread_cf : 2;
+    if (!t->resident) return mttkrp_streamed(t, a, opts, s);
+    a.coords = t->d_coords;
+    a.vals = t->d_values;
+    return mttkrp_launch(t, a, s);
+}
+
+int blco_mttkrp_host(blco_tensor* t, int mode, int rank, const double* const* factors, double* out,
+                     const blco_opts* opts)
+{
+    if (!t || !factors || !out) return fail(BLCO_ERR_INVALID, "null argument");
+    if (mode < 0 || mode >= t->layout.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
+    if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    cudaStream_t s = pick_stream(t, opts);
+    if (!s) return BLCO_ERR_CUDA;
+    const int N = t->layout.nmodes;
+    double* df[BLCO_MAX_MODES] = {};
+    int st = BLCO_OK;
+    for (int m = 0; m < N && st == BLCO_OK; m++) {
+        size_t b = t->layout.dims[m] * (size_t)rank * sizeof(double);
+        cudaError_t e = cudaMalloc(&df[m], b);
+        const double* src = m == mode ? out : factors[m];
+        if (e == cudaSuccess && src) e = cudaMemcpyAsync(df[m], src, b, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) st = cuda_fail(e, "factor upload", __FILE__, __LINE__);
+    }
+    if (st == BLCO_OK) st = blco_mttkrp(t, mode, rank, df, df[mode], opts);
+    if (st == BLCO_OK) {
+        cudaError_t e = cudaMemcpyAsync(out, df[mode], t->layout.dims[mode] * (size_t)rank * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "MTTKRP download", __FILE__, __LINE__);
+    }
+    cudaStreamSynchronize(s);
+    for (int m = 0; m < N; m++) cudaFree(df[m]);
+    return st;
+}
+
+int blco_cpals(blco_tensor* t, int rank, double* const* factors, double* lambda, int maxiter, double tol,
+               const blco_opts* opts, double* fit_out, double* fits, int* iters_out)
+{
+    if (!t) return fail(BLCO_ERR_INVALID, "null tensor");
+    if (maxiter < 0) return fail(BLCO_ERR_INVALID, "maxiter must be >= 0");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    return cpals_host(t, rank, factors, lambda, maxiter, tol, opts, fit_out, fits, iters_out);
+}
+
+int blco_cpals_plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_lambda,
+                           const blco_opts* opts, blco_cpals_plan** out)
+{
+    if (!out) return fail(BLCO_ERR_INVALID, "null output handle");
+    if (!t) return fail(BLCO_ERR_INVALID, "null tensor");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    return plan_create(t, rank, d_factors, d_lambda, opts, out);
+}
+
+int blco_cpals_plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* iters_done)
+{
+    if (!p) return fail(BLCO_ERR_INVALID, "null plan");
+    return plan_iterate(p, iters, tol, fits, iters_done, false);
+}
+
+int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls) { return plan_mttkrp_ms(p, ms, calls); }
+
+int blco_cpals_plan_destroy(blco_cpals_plan* p) { return plan_destroy(p); }
+
+} // extern "C"

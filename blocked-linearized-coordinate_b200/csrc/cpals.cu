@@ -1,0 +1,716 @@
+// cpals.cu -- CP-ALS on the GPU (plain FP64 form).
+//
+// Keeps the arithmetic of cpals_blco_dev (src/cpd_gpu.cu:21-242) but runs
+// every step as this library's own kernels on one stream, with no host
+// round trip inside a mode update (the reference synchronises the host
+// about eight times per mode and calls cuBLAS/cuSOLVER):
+//   per mode n (descending length order, src/cpd_gpu.cu:137-139)
+//     M      = MTTKRP(n)                                  (mttkrp.cu)
+//     P      = pinv( hadamard_{m != n} Gram_m )           (k_solve: Cholesky
+//              inverse, falling back to a Jacobi eigen pseudoinverse with the
+//              reference cut-off n*ulp(s_max), src/cpd_gpu.cu:452-532)
+//     U_n    = M P^T, column sums of squares fused         (k_update)
+//     lambda = sqrt(lambda + colsq); U_n /= lambda, Gram_n (k_lambda,
+//              k_scale_gram; lambda is never reset, src/cpd_gpu.cu:244-291)
+//   fit as kruskal_fit_gpu (src/cpd_gpu.cu:331-384)        (k_iprod, k_fit)
+// Reductions over rows use per-block partials summed in a fixed order, so
+// a given launch shape gives the same bits on every run (the MTTKRP's FP64
+// atomics are the one non-deterministic step).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "internal.cuh"
+
+namespace blco {
+namespace {
+
+constexpr int DN_THREADS = 256;
+constexpr int MAX_SOLVE_R = 96; // k_solve keeps two R x R FP64 buffers in shared memory
+
+// ---------------------------------------------------------------- Gram --
+// Partial Gram of rows [beg, end) of a row-major I x R matrix, optionally
+// scaling the rows by inv[c] first and writing the scaled rows back.
+// Thread tile: TS x TS entries of the R x R result (TS = 4 up to R = 64,
+// 8 up to R = 128, so that 256 threads cover the result).
+constexpr int GR_CH = 32; // rows staged per step
+
+template <bool SCALE, int TS>
+__global__ __launch_bounds__(DN_THREADS) void k_gram(double* __restrict__ U, uint64_t I, int R,
+                                                     const double* __restrict__ inv, double* __restrict__ partials)
+{
+    extern __shared__ __align__(16) double gs[];
+    double* tile = gs;                 // GR_CH x R
+    double* red = gs + GR_CH * R;      // R x R reduction buffer
+    const int tpr = (R + TS - 1) / TS; // tiles per row of the result
+    const int ntile = tpr * tpr;
+    const int groups = max(1, DN_THREADS / ntile);
+    const int tid = threadIdx.x;
+    const int g = tid / ntile, e = tid % ntile;
+    const bool active = g < groups && tid < groups * ntile;
+    const int a0 = (e / tpr) * TS, b0 = (e % tpr) * TS;
+    double acc[TS][TS];
+#pragma unroll
+    for (int x = 0; x < TS; x++)
+#pragma unroll
+        for (int y = 0; y < TS; y++) acc[x][y] = 0.0;
+
+    const uint64_t per = (I + gridDim.x - 1) / gridDim.x;
+    const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
+    for (uint64_t r0 = beg; r0 < end; r0 += GR_CH) {
+        const int nr = (int)min((uint64_t)GR_CH, end - r0);
+        __syncthreads();
+        for (int k = tid; k < nr * R; k += DN_THREADS) {
+            double v = U[r0 * R + k];
+            if (SCALE) {
+                v *= inv[k % R];
+                U[r0 * R + k] = v;
+            }
+            tile[k] = v;
+        }
+        __syncthreads();
+        if (active) {
+            // Tiles that reach past R read columns clamped to R-1 and are
+            // discarded at the end.
+            for (int r = g; r < nr; r += groups) {
+                const double* row = tile + r * R;
+                double va[TS], vb[TS];
+#pragma unroll
+                for (int x = 0; x < TS; x++) {
+                    va[x] = row[min(a0 + x, R - 1)];
+                    vb[x] = row[min(b0 + x, R - 1)];
+                }
+#pragma unroll
+                for (int x = 0; x < TS; x++)
+#pragma unroll
+                    for (int y = 0; y < TS; y++) acc[x][y] += va[x] * vb[y];
+            }
+        }
+    }
+    // Reduce the row groups in a fixed order.
+    for (int k = tid; k < R * R; k += DN_THREADS) red[k] = 0.0;
+    __syncthreads();
+    for (int gg = 0; gg < groups; gg++) {
+        if (active && g == gg) {
+#pragma unroll
+            for (int x = 0; x < TS; x++)
+#pragma unroll
+                for (int y = 0; y < TS; y++)
+                    if (a0 + x < R && b0 + y < R) red[(a0 + x) * R + b0 + y] += acc[x][y];
+        }
+        __syncthreads();
+    }
+    for (int k = tid; k < R * R; k += DN_THREADS) partials[(size_t)blockIdx.x * R * R + k] = red[k];
+}
+
+// out[k] = sum_b partials[b][k], b ascending.
+__global__ void k_sum_partials(const double* __restrict__ partials, int nblocks, int len, double* __restrict__ out)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < len; k += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s += partials[(size_t)b * len + k];
+        out[k] = s;
+    }
+}
+
+// -------------------------------------------------------------- update --
+// U[i][c] = sum_k M[i][k] * P[c][k] (the cublasDgemm of src/cpd_gpu.cu:175
+// applied to the column-major pseudoinverse), plus per-block column sums of
+// squares of U.  A warp computes a row; lane c owns columns c, c+32, ...
+constexpr int UP_MAXC = 4; // R <= 128
+
+__global__ __launch_bounds__(DN_THREADS) void k_update(const double* __restrict__ M, const double* __restrict__ P,
+                                                       double* __restrict__ U, uint64_t I, int R,
+                                                       double* __restrict__ colsq_partials)
+{
+    extern __shared__ __align__(16) double us[];
+    double* PT = us;              // PT[k][c] = P[c][k]
+    double* csq = us + R * R;     // [warps][R]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = DN_THREADS / 32;
+    for (int k = tid; k < R * R; k += DN_THREADS) {
+        int c = k / R, kk = k % R;
+        PT[kk * R + c] = P[k];
+    }
+    __syncthreads();
+    double sq[UP_MAXC];
+#pragma unroll
+    for (int j = 0; j < UP_MAXC; j++) sq[j] = 0.0;
+    const uint64_t per = (I + gridDim.x - 1) / gridDim.x;
+    const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
+    for (uint64_t i = beg + warp; i < end; i += nw) {
+        const double* mrow = M + i * R;
+        double mreg[UP_MAXC];
+#pragma unroll
+        for (int j = 0; j < UP_MAXC; j++) mreg[j] = (lane + 32 * j < R) ? mrow[lane + 32 * j] : 0.0;
+        double acc[UP_MAXC];
+#pragma unroll
+        for (int j = 0; j < UP_MAXC; j++) acc[j] = 0.0;
+#pragma unroll
+        for (int kb = 0; kb < UP_MAXC; kb++) {
+            if (32 * kb >= R) break;
+            const int kn = min(32, R - 32 * kb);
+            for (int kk = 0; kk < kn; kk++) {
+                const int k = 32 * kb + kk;
+                double mk = __shfl_sync(0xffffffffu, mreg[kb], kk);
+#pragma unroll
+                for (int j = 0; j < UP_MAXC; j++) {
+                    int c = lane + 32 * j;
+                    if (c < R) acc[j] += mk * PT[k * R + c];
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < UP_MAXC; j++) {
+            int c = lane + 32 * j;
+            if (c < R) {
+                U[i * R + c] = acc[j];
+                sq[j] += acc[j] * acc[j];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < UP_MAXC; j++) {
+        int c = lane + 32 * j;
+        if (c < R) csq[warp * R + c] = sq[j];
+    }
+    __syncthreads();
+    for (int c = tid; c < R; c += DN_THREADS) {
+        double s = 0.0;
+        for (int w = 0; w < nw; w++) s += csq[w * R + c];
+        colsq_partials[(size_t)blockIdx.x * R + c] = s;
+    }
+}
+
+// lambda_c = sqrt(lambda_c + sum_b colsq[b][c]); inv_c = 1/lambda_c (0 if 0).
+__global__ void k_lambda(const double* __restrict__ colsq_partials, int nblocks, int R, double* __restrict__ lambda,
+                         double* __restrict__ inv)
+{
+    for (int c = threadIdx.x; c < R; c += blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s += colsq_partials[(size_t)b * R + c];
+        double l = sqrt(lambda[c] + s);
+        lambda[c] = l;
+        inv[c] = l == 0.0 ? 0.0 : 1.0 / l;
+    }
+}
+
+// --------------------------------------------------------------- solve --
+struct GramPtrs {
+    const double* g[BLCO_MAX_MODES];
+};
+
+// P = pinv(V), V = hadamard of the Grams of every mode except `skip`.
+// One CTA.  Cholesky V = L L^T; P = L^-T L^-1.  If a pivot is not clearly
+// positive, the pseudoinverse is taken from a cyclic Jacobi
+// eigen-decomposition V = Q diag(w) Q^T instead, dropping |w| <= R*ulp(max|w|)
+// as the reference does for its SVD.
+__global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, int skip, int R,
+                                                      double* __restrict__ Pout, int* __restrict__ used_eigen)
+{
+    extern __shared__ __align__(16) double ss[];
+    double* A = ss;          // R x R
+    double* W = ss + R * R;  // R x R
+    __shared__ double fw[MAX_SOLVE_R];
+    __shared__ int bad;
+    __shared__ double maxdiag;
+    const int tid = threadIdx.x, RR = R * R;
+    for (int k = tid; k < RR; k += DN_THREADS) {
+        double v = 1.0;
+        for (int m = 0; m < nmodes; m++)
+            if (m != skip) v *= gp.g[m][k];
+        A[k] = v;
+    }
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    if (tid == 0) {
+        double md = 0.0;
+        for (int i = 0; i < R; i++) md = fmax(md, fabs(A[i * R + i]));
+        maxdiag = md;
+    }
+    __syncthreads();
+    const double piv_tol = 64.0 * R * 2.220446049250313e-16 * maxdiag;
+    for (int k = 0; k < R; k++) {
+        if (tid == 0) {
+            double d = A[k * R + k];
+            if (!(d > piv_tol)) bad = 1;
+            A[k * R + k] = sqrt(fmax(d, 0.0));
+        }
+        __syncthreads();
+        if (bad) break;
+        const double dk = A[k * R + k];
+        for (int i = k + 1 + tid; i < R; i += DN_THREADS) A[i * R + k] /= dk;
+        __syncthreads();
+        const int n = R - k - 1;
+        for (int e = tid; e < n * n; e += DN_THREADS) {
+            int i = k + 1 + e / n, j = k + 1 + e % n;
+            if (j <= i) A[i * R + j] -= A[i * R + k] * A[j * R + k];
+        }
+        __syncthreads();
+    }
+    if (!bad) {
+        // W = L^-1 (lower), column j by forward substitution.
+        for (int j = tid; j < R; j += DN_THREADS) {
+            for (int i = 0; i < j; i++) W[i * R + j] = 0.0;
+            for (int i = j; i < R; i++) {
+                double s = (i == j) ? 1.0 : 0.0;
+                for (int k = j; k < i; k++) s -= A[i * R + k] * W[k * R + j];
+                W[i * R + j] = s / A[i * R + i];
+            }
+        }
+        __syncthreads();
+        for (int e = tid; e < RR; e += DN_THREADS) {
+            int a = e / R, b = e % R, k0 = max(a, b);
+            double s = 0.0;
+            for (int k = k0; k < R; k++) s += W[k * R + a] * W[k * R + b];
+            Pout[e] = s;
+        }
+        if (tid == 0) *used_eigen = 0;
+        return;
+    }
+    // ---- Jacobi eigen fallback: A <- V (recomputed), W <- I.
+    __syncthreads();
+    for (int e = tid; e < RR; e += DN_THREADS) {
+        double v = 1.0;
+        for (int m = 0; m < nmodes; m++)
+            if (m != skip) v *= gp.g[m][e];
+        A[e] = v;
+        W[e] = (e / R == e % R) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    __shared__ double off_s, tot_s;
+    for (int sweep = 0; sweep < 60; sweep++) {
+        if (tid == 0) {
+            double off = 0.0, tot = 0.0;
+            for (int e = 0; e < RR; e++) {
+                double v = A[e] * A[e];
+                tot += v;
+                if (e / R != e % R) off += v;
+            }
+            off_s = off;
+            tot_s = tot;
+        }
+        __syncthreads();
+        if (off_s <= 1e-30 * tot_s || off_s == 0.0) break;
+        for (int pi = 0; pi < R - 1; pi++) {
+            for (int qi = pi + 1; qi < R; qi++) {
+                const double apq = A[pi * R + qi];
+                if (apq == 0.0) continue; // uniform across threads (read before any write)
+                const double app = A[pi * R + pi], aqq = A[qi * R + qi];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                __syncthreads();
+                for (int k = tid; k < R; k += DN_THREADS) {
+                    double akp = A[k * R + pi], akq = A[k * R + qi];
+                    A[k * R + pi] = c * akp - s * akq;
+                    A[k * R + qi] = s * akp + c * akq;
+                    double qkp = W[k * R + pi], qkq = W[k * R + qi];
+                    W[k * R + pi] = c * qkp - s * qkq;
+                    W[k * R + qi] = s * qkp + c * qkq;
+                }
+                __syncthreads();
+                for (int k = tid; k < R; k += DN_THREADS) {
+                    double apk = A[pi * R + k], aqk = A[qi * R + k];
+                    A[pi * R + k] = c * apk - s * aqk;
+                    A[qi * R + k] = s * apk + c * aqk;
+                }
+                __syncthreads();
+            }
+        }
+    }
+    __shared__ double smax;
+    if (tid == 0) {
+        double m = 0.0;
+        for (int i = 0; i < R; i++) m = fmax(m, fabs(A[i * R + i]));
+        smax = m;
+    }
+    __syncthreads();
+    const double tol = R * (nextafter(smax, smax + 1.0) - smax);
+    for (int i = tid; i < R; i += DN_THREADS) {
+        double w = A[i * R + i];
+        fw[i] = fabs(w) > tol ? 1.0 / w : 0.0;
+    }
+    __syncthreads();
+    for (int e = tid; e < RR; e += DN_THREADS) {
+        int a = e / R, b = e % R;
+        double s = 0.0;
+        for (int k = 0; k < R; k++) s += W[a * R + k] * fw[k] * W[b * R + k];
+        Pout[e] = s;
+    }
+    if (tid == 0) *used_eigen = 1;
+}
+
+// ----------------------------------------------------------------- fit --
+// Per-block column sums of U[i][c] * M[i][c] (columnwise_inner_product,
+// src/cpd_gpu.cu:307-330).
+__global__ __launch_bounds__(DN_THREADS) void k_iprod(const double* __restrict__ U, const double* __restrict__ M,
+                                                      uint64_t I, int R, double* __restrict__ partials)
+{
+    extern __shared__ __align__(16) double ip[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = DN_THREADS / 32;
+    double s[UP_MAXC];
+#pragma unroll
+    for (int j = 0; j < UP_MAXC; j++) s[j] = 0.0;
+    const uint64_t per = (I + gridDim.x - 1) / gridDim.x;
+    const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
+    for (uint64_t i = beg + warp; i < end; i += nw) {
+#pragma unroll
+        for (int j = 0; j < UP_MAXC; j++) {
+            int c = lane + 32 * j;
+            if (c < R) s[j] += U[i * R + c] * M[i * R + c];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < UP_MAXC; j++) {
+        int c = lane + 32 * j;
+        if (c < R) ip[warp * R + c] = s[j];
+    }
+    __syncthreads();
+    for (int c = tid; c < R; c += DN_THREADS) {
+        double t = 0.0;
+        for (int w = 0; w < nw; w++) t += ip[w * R + c];
+        partials[(size_t)blockIdx.x * R + c] = t;
+    }
+}
+
+// fit = 1 - sqrt(| ||A||^2 - 2 <X,A> + ||X||^2 |) / ||X|| (src/cpd_gpu.cu:331-384)
+__global__ void k_fit(const double* __restrict__ ipart, int nblocks, GramPtrs gp, int nmodes, int R,
+                      const double* __restrict__ lambda, double xnorm, double* __restrict__ fit_out)
+{
+    __shared__ double red[DN_THREADS];
+    const int tid = threadIdx.x;
+    // iprod
+    double ip = 0.0;
+    for (int c = tid; c < R; c += blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s += ipart[(size_t)b * R + c];
+        ip += s * lambda[c];
+    }
+    red[tid] = ip;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+        if (tid < o) red[tid] += red[tid + o];
+        __syncthreads();
+    }
+    const double iprod = red[0];
+    __syncthreads();
+    double na = 0.0;
+    for (int e = tid; e < R * R; e += blockDim.x) {
+        double v = lambda[e / R] * lambda[e % R];
+        for (int m = 0; m < nmodes; m++) v *= gp.g[m][e];
+        na += v;
+    }
+    red[tid] = na;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o; o >>= 1) {
+        if (tid < o) red[tid] += red[tid + o];
+        __syncthreads();
+    }
+    if (tid == 0) {
+        double norm_a = sqrt(fabs(red[0]));
+        double fit = norm_a * norm_a - 2.0 * iprod;
+        if (xnorm != 0.0) {
+            fit = sqrt(fabs(fit + xnorm * xnorm));
+            fit = 1.0 - fit / xnorm;
+        }
+        fit_out[0] = fit;
+    }
+}
+
+int grid_rows(uint64_t I, int sm)
+{
+    uint64_t g = (I + 63) / 64;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(g, (uint64_t)sm * 2));
+}
+
+} // namespace
+} // namespace blco
+
+struct blco_cpals_plan {
+    blco_tensor* t = nullptr;
+    int R = 0, N = 0;
+    double* U[BLCO_MAX_MODES] = {};
+    double* lambda = nullptr;
+    double* M = nullptr;
+    double* grams[BLCO_MAX_MODES] = {};
+    double* P = nullptr;
+    double* partials = nullptr; // max(grid) * R * R
+    double* inv = nullptr;      // R
+    double* fit = nullptr;      // 1
+    int* used_eigen = nullptr;
+    int order[BLCO_MAX_MODES] = {};
+    double xnorm = 0.0;
+    double fit_old = 0.0;
+    int iters_run = 0;
+    blco_opts opts;
+    cudaStream_t s = nullptr;
+    int sm = 148;
+    cudaEvent_t ev[2 * BLCO_MAX_MODES] = {};
+    double mttkrp_ms[BLCO_MAX_MODES] = {};
+    int mttkrp_calls = 0;
+    bool mixed = false;
+};
+
+namespace blco {
+namespace {
+
+int plan_free(blco_cpals_plan* p)
+{
+    if (!p) return BLCO_OK;
+    if (p->s) cudaStreamSynchronize(p->s);
+    cudaFree(p->M);
+    for (int n = 0; n < BLCO_MAX_MODES; n++) cudaFree(p->grams[n]);
+    cudaFree(p->P);
+    cudaFree(p->partials);
+    cudaFree(p->inv);
+    cudaFree(p->fit);
+    cudaFree(p->used_eigen);
+    for (auto& e : p->ev)
+        if (e) cudaEventDestroy(e);
+    delete p;
+    return BLCO_OK;
+}
+
+int gram_launch(blco_cpals_plan* p, double* U, uint64_t I, const double* inv, double* G)
+{
+    const int R = p->R;
+    int grid = grid_rows(I, p->sm);
+    size_t smem = (size_t)(GR_CH * R + R * R) * sizeof(double);
+    void (*fn)(double*, uint64_t, int, const double*, double*);
+    if (R <= 64) fn = inv ? k_gram<true, 4> : k_gram<false, 4>;
+    else fn = inv ? k_gram<true, 8> : k_gram<false, 8>;
+    BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fn<<<grid, DN_THREADS, smem, p->s>>>(U, I, R, inv, p->partials);
+    BLCO_CHECK_LAUNCH("k_gram");
+    k_sum_partials<<<(R * R + 255) / 256, 256, 0, p->s>>>(p->partials, grid, R * R, G);
+    BLCO_CHECK_LAUNCH("k_sum_partials");
+    return BLCO_OK;
+}
+
+int mode_update(blco_cpals_plan* p, int n)
+{
+    blco_tensor* t = p->t;
+    const int R = p->R, N = p->N;
+    const uint64_t I = t->layout.dims[n];
+    BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
+    MttkrpArgs a;
+    memset(&a, 0, sizeof(a));
+    a.coords = t->d_coords;
+    a.vals = t->d_values;
+    a.nnz = t->nnz;
+    a.mode = n;
+    a.rank = R;
+    for (int m = 0; m < N; m++) a.factors[m] = p->U[m];
+    a.out = p->M;
+    a.kernel = p->opts.kernel;
+    a.thread_cf = p->opts.thread_cf;
+    BLCO_CUDA(cudaEventRecord(p->ev[2 * n], p->s));
+    BLCO_TRY(mttkrp_launch(t, a, p->s));
+    BLCO_CUDA(cudaEventRecord(p->ev[2 * n + 1], p->s));
+
+    GramPtrs gp;
+    memset(&gp, 0, sizeof(gp));
+    for (int m = 0; m < N; m++) gp.g[m] = p->grams[m];
+    size_t ssmem = 2 * (size_t)R * R * sizeof(double);
+    BLCO_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem));
+    k_solve<<<1, DN_THREADS, ssmem, p->s>>>(gp, N, n, R, p->P, p->used_eigen);
+    BLCO_CHECK_LAUNCH("k_solve");
+
+    int grid = grid_rows(I, p->sm);
+    size_t usmem = (size_t)(R * R + (DN_THREADS / 32) * R) * sizeof(double);
+    BLCO_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
+    k_update<<<grid, DN_THREADS, usmem, p->s>>>(p->M, p->P, p->U[n], I, R, p->partials);
+    BLCO_CHECK_LAUNCH("k_update");
+    k_lambda<<<1, 128, 0, p->s>>>(p->partials, grid, R, p->lambda, p->inv);
+    BLCO_CHECK_LAUNCH("k_lambda");
+    BLCO_TRY(gram_launch(p, p->U[n], I, p->inv, p->grams[n]));
+    return BLCO_OK;
+}
+
+int fit_launch(blco_cpals_plan* p)
+{
+    const int R = p->R, N = p->N;
+    const int lm = p->order[N - 1];
+    const uint64_t I = p->t->layout.dims[lm];
+    int grid = grid_rows(I, p->sm);
+    size_t smem = (size_t)(DN_THREADS / 32) * R * sizeof(double);
+    k_iprod<<<grid, DN_THREADS, smem, p->s>>>(p->U[lm], p->M, I, R, p->partials);
+    BLCO_CHECK_LAUNCH("k_iprod");
+    GramPtrs gp;
+    memset(&gp, 0, sizeof(gp));
+    for (int m = 0; m < N; m++) gp.g[m] = p->grams[m];
+    k_fit<<<1, DN_THREADS, 0, p->s>>>(p->partials, grid, gp, N, R, p->lambda, p->xnorm, p->fit);
+    BLCO_CHECK_LAUNCH("k_fit");
+    return BLCO_OK;
+}
+
+} // namespace
+
+int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_lambda, const blco_opts* opts,
+                blco_cpals_plan** out)
+{
+    *out = nullptr;
+    if (!t || !d_factors || !d_lambda) return fail(BLCO_ERR_INVALID, "null argument");
+    if (rank < 1 || rank > MAX_SOLVE_R) return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS rank must be 1..96");
+    if (!t->resident) return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS on a streamed tensor is not built yet");
+    blco_cpals_plan* p = new blco_cpals_plan();
+    p->t = t;
+    p->R = rank;
+    p->N = t->layout.nmodes;
+    p->lambda = d_lambda;
+    if (opts) p->opts = *opts;
+    else blco_opts_init(&p->opts);
+    DeviceInfo di;
+    int st = device_info(t->device, &di);
+    if (st != BLCO_OK) { plan_free(p); return st; }
+    p->sm = di.sm_count;
+    p->s = pick_stream(t, opts);
+    uint64_t maxdim = 0;
+    for (int n = 0; n < p->N; n++) {
+        p->U[n] = d_factors[n];
+        maxdim = std::max(maxdim, t->layout.dims[n]);
+    }
+    const int R = rank;
+    int gmax = std::max(grid_rows(maxdim, p->sm), 1);
+#define PC(call)                                                               \
+    do {                                                                       \
+        cudaError_t _e = (call);                                               \
+        if (_e != cudaSuccess) {                                               \
+            int _s = cuda_fail(_e, #call, __FILE__, __LINE__);                 \
+            plan_free(p);                                                      \
+            return _s;                                                         \
+        }                                                                      \
+    } while (0)
+    PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
+    for (int n = 0; n < p->N; n++) PC(cudaMalloc(&p->grams[n], (size_t)R * R * sizeof(double)));
+    PC(cudaMalloc(&p->P, (size_t)R * R * sizeof(double)));
+    PC(cudaMalloc(&p->partials, (size_t)gmax * R * R * sizeof(double)));
+    PC(cudaMalloc(&p->inv, (size_t)R * sizeof(double)));
+    PC(cudaMalloc(&p->fit, 2 * sizeof(double)));
+    PC(cudaMalloc(&p->used_eigen, sizeof(int)));
+    for (auto& e : p->ev) PC(cudaEventCreate(&e));
+#undef PC
+    p->xnorm = std::sqrt(t->norm_sq);
+    for (int n = 0; n < p->N; n++) {
+        st = gram_launch(p, p->U[n], t->layout.dims[n], nullptr, p->grams[n]);
+        if (st != BLCO_OK) { plan_free(p); return st; }
+    }
+    // Descending mode length, ties in natural order (src/cpd_gpu.cu:137-139).
+    for (int n = 0; n < p->N; n++) p->order[n] = n;
+    std::stable_sort(p->order, p->order + p->N,
+                     [&](int a, int b) { return t->layout.dims[a] > t->layout.dims[b]; });
+    cudaError_t e = cudaStreamSynchronize(p->s);
+    if (e != cudaSuccess) {
+        int s2 = cuda_fail(e, "plan setup", __FILE__, __LINE__);
+        plan_free(p);
+        return s2;
+    }
+    *out = p;
+    return BLCO_OK;
+}
+
+int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* iters_done, bool verbose)
+{
+    if (iters_done) *iters_done = 0;
+    int done = 0;
+    cudaEvent_t it0, it1;
+    BLCO_CUDA(cudaEventCreate(&it0));
+    BLCO_CUDA(cudaEventCreate(&it1));
+    int st = BLCO_OK;
+    for (int it = 0; it < iters; it++) {
+        cudaEventRecord(it0, p->s);
+        for (int k = 0; k < p->N && st == BLCO_OK; k++) st = mode_update(p, p->order[k]);
+        if (st == BLCO_OK) st = fit_launch(p);
+        if (st != BLCO_OK) break;
+        cudaEventRecord(it1, p->s);
+        double fit = 0.0;
+        cudaError_t e = cudaMemcpyAsync(&fit, p->fit, sizeof(double), cudaMemcpyDeviceToHost, p->s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(p->s);
+        if (e != cudaSuccess) { st = cuda_fail(e, "CP-ALS iteration", __FILE__, __LINE__); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, it0, it1);
+        for (int n = 0; n < p->N; n++) {
+            float m = 0.f;
+            cudaEventElapsedTime(&m, p->ev[2 * n], p->ev[2 * n + 1]);
+            p->mttkrp_ms[n] += m;
+        }
+        p->mttkrp_calls++;
+        if (fits) fits[it] = fit;
+        done++;
+        if (verbose)
+            printf("--> Iter %3d: f = %0.6f f-delta = %0.6f time = %0.6f, (s)\n", p->iters_run, fit, fit - p->fit_old,
+                   ms / 1000.0f);
+        p->iters_run++;
+        bool stop = std::fabs(fit - p->fit_old) < tol || std::isnan(fit);
+        p->fit_old = fit;
+        if (stop) break;
+    }
+    cudaEventDestroy(it0);
+    cudaEventDestroy(it1);
+    if (iters_done) *iters_done = done;
+    return st;
+}
+
+int plan_destroy(blco_cpals_plan* p) { return plan_free(p); }
+
+int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda, int maxiter, double tol,
+               const blco_opts* opts, double* fit_out, double* fits, int* iters_out)
+{
+    if (!t || !factors || !lambda) return fail(BLCO_ERR_INVALID, "null argument");
+    const int N = t->layout.nmodes;
+    cudaStream_t s = pick_stream(t, opts);
+    double* dU[BLCO_MAX_MODES] = {};
+    double* dl = nullptr;
+    int st = BLCO_OK;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(s);
+        for (int n = 0; n < N; n++) cudaFree(dU[n]);
+        cudaFree(dl);
+    };
+    for (int n = 0; n < N && st == BLCO_OK; n++) {
+        size_t b = t->layout.dims[n] * (size_t)rank * sizeof(double);
+        cudaError_t e = cudaMalloc(&dU[n], b);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dU[n], factors[n], b, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) st = cuda_fail(e, "factor upload", __FILE__, __LINE__);
+    }
+    if (st == BLCO_OK) {
+        cudaError_t e = cudaMalloc(&dl, rank * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dl, lambda, rank * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) st = cuda_fail(e, "lambda upload", __FILE__, __LINE__);
+    }
+    blco_cpals_plan* p = nullptr;
+    if (st == BLCO_OK) st = plan_create(t, rank, dU, dl, opts, &p);
+    const bool verbose = opts && opts->verbose;
+    if (st == BLCO_OK && verbose)
+        printf("Begin CP-ALS decomposition, rank=%d maxiter=%d tolerance=%f\n", rank, maxiter, tol);
+    int done = 0;
+    if (st == BLCO_OK) st = plan_iterate(p, maxiter, tol, fits, &done, verbose);
+    if (st == BLCO_OK) {
+        if (fit_out) *fit_out = p->fit_old;
+        if (verbose) printf("Final fit: %0.9f\n", p->fit_old);
+        for (int n = 0; n < N && st == BLCO_OK; n++) {
+            cudaError_t e = cudaMemcpyAsync(factors[n], dU[n], t->layout.dims[n] * (size_t)rank * sizeof(double),
+                                            cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) st = cuda_fail(e, "factor download", __FILE__, __LINE__);
+        }
+        cudaError_t e = cudaMemcpyAsync(lambda, dl, rank * sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess && st == BLCO_OK) st = cuda_fail(e, "lambda download", __FILE__, __LINE__);
+    }
+    if (iters_out) *iters_out = done;
+    plan_free(p);
+    cleanup();
+    return st;
+}
+
+int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls)
+{
+    if (!p) return fail(BLCO_ERR_INVALID, "null plan");
+    if (ms)
+        for (int n = 0; n < p->N; n++) ms[n] = p->mttkrp_ms[n];
+    if (calls) *calls = p->mttkrp_calls;
+    return BLCO_OK;
+}
+
+} // namespace blco

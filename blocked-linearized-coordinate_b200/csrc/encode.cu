@@ -1,0 +1,720 @@
+// encode.cu -- BLCO encoder on the GPU.
+//
+// Reproduces gen_blcotensor_host<uint64> (include/blco.hpp:196-331), which
+// runs gen_alto (include/alto.hpp:107-186) and sort_alto
+// (include/alto.hpp:704-754) on the host, as four device phases:
+//   1. linearize: key_i = OR_n pdep(c_n,i, alto_mask_n)      (k_alto_keys)
+//   2. sort (key, value) pairs by key: stable LSD radix sort, 8-bit digits,
+//      one pass per 8 significant key bits                   (k_rs_*)
+//   3. re-linearize in place: coord_i = OR_n pext(key_i, alto_mask_n)
+//      << mode_pos_n                                         (k_relinearize)
+//   4. block split: consecutive max_block_size slices (host arithmetic; the
+//      upper key half is always zero for 64-bit keys, so every nonzero is in
+//      histogram bucket 0, include/blco.hpp:249-321)
+// Then per-mode row statistics and heavy-row tables for the MTTKRP kernels.
+#include <algorithm>
+#include <cstring>
+
+#include "internal.cuh"
+
+namespace blco {
+
+int make_layout(int nmodes, const uint64_t* dims, Layout* L)
+{
+    if (nmodes < 1 || nmodes > BLCO_MAX_MODES) return fail(BLCO_ERR_INVALID, "nmodes must be 1..5");
+    memset(L, 0, sizeof(*L));
+    L->nmodes = nmodes;
+    int bits[BLCO_MAX_MODES], order[BLCO_MAX_MODES];
+    int total = 0, maxbits = 0;
+    for (int n = 0; n < nmodes; n++) {
+        if (dims[n] == 0) return fail(BLCO_ERR_INVALID, "mode length 0");
+        if (dims[n] > 0xffffffffull) return fail(BLCO_ERR_UNSUPPORTED, "mode length above 2^32-1");
+        L->dims[n] = dims[n];
+        // 64 - clz(dim - 1) (include/alto.hpp:613); dim == 1 -> 0 bits.
+        bits[n] = dims[n] <= 1 ? 0 : 64 - __builtin_clzll(dims[n] - 1);
+        total += bits[n];
+        maxbits = std::max(maxbits, bits[n]);
+        order[n] = n;
+    }
+    if (total > 64) return fail(BLCO_ERR_UNSUPPORTED, "coordinates need more than 64 bits (128-bit BLCO not built)");
+    // Shortest mode first, ties in natural order; LSB-first round robin over
+    // bit levels (include/alto.hpp:659-685).
+    std::stable_sort(order, order + nmodes, [&](int a, int b) { return bits[a] < bits[b]; });
+    int shift = 0;
+    for (int level = 0; level < maxbits; level++)
+        for (int k = 0; k < nmodes; k++)
+            if (level < bits[order[k]]) L->alto_masks[order[k]] |= 1ull << shift++;
+    for (int n = 0; n < nmodes; n++) {
+        L->mode_masks[n] = bits[n] >= 64 ? ~0ull : ((1ull << bits[n]) - 1);
+        L->mode_pos[n] = n == 0 ? 0 : L->mode_pos[n - 1] + bits[n - 1];
+    }
+    L->alto_bits = total;
+    return BLCO_OK;
+}
+
+namespace {
+
+struct CooPtrs {
+    const uint64_t* c[BLCO_MAX_MODES];
+};
+
+// Software bit deposit/extract over the set bits of a mask, LSB first
+// (the ALT_PEXT semantics of include/bitops.hpp:18-41).
+__device__ __forceinline__ uint64_t dev_pdep(uint64_t x, uint64_t m)
+{
+    uint64_t r = 0;
+    for (int j = 0; m; j++) {
+        int p = __ffsll((long long)m) - 1;
+        r |= ((x >> j) & 1ull) << p;
+        m &= m - 1;
+    }
+    return r;
+}
+
+__device__ __forceinline__ uint64_t dev_pext(uint64_t x, uint64_t m)
+{
+    uint64_t r = 0;
+    for (int j = 0; m; j++) {
+        int p = __ffsll((long long)m) - 1;
+        r |= ((x >> p) & 1ull) << j;
+        m &= m - 1;
+    }
+    return r;
+}
+
+__global__ void k_alto_keys(CooPtrs coo, const double* __restrict__ vals, uint64_t nnz, Layout L,
+                            uint64_t* __restrict__ keys, double* __restrict__ vout, int* __restrict__ bad)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t key = 0;
+        bool ok = true;
+#pragma unroll
+        for (int n = 0; n < BLCO_MAX_MODES; n++) {
+            if (n < L.nmodes) {
+                uint64_t c = coo.c[n][i];
+                ok &= c < L.dims[n];
+                key |= dev_pdep(c, L.alto_masks[n]);
+            }
+        }
+        if (!ok) atomicExch(bad, 1);
+        keys[i] = key;
+        vout[i] = vals[i];
+    }
+}
+
+__global__ void k_relinearize(uint64_t* __restrict__ keys, uint64_t nnz, Layout L)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t key = keys[i], c = 0;
+#pragma unroll
+        for (int n = 0; n < BLCO_MAX_MODES; n++)
+            if (n < L.nmodes) c |= (dev_pext(key, L.alto_masks[n]) & L.mode_masks[n]) << L.mode_pos[n];
+        keys[i] = c;
+    }
+}
+
+// ----------------------------------------------------------- radix sort --
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS; // 4096 keys per tile
+constexpr int RS_RADIX = 256;
+constexpr size_t RS_SMEM = RS_TILE * 16 + (RS_WARPS + 2) * RS_RADIX * 4;
+
+// Per-tile digit counts, digit-major: counts[d * ntiles + tile].
+__global__ __launch_bounds__(RS_THREADS) void k_rs_hist(const uint64_t* __restrict__ keys, uint64_t n, int shift,
+                                                        uint32_t* __restrict__ counts, uint32_t ntiles)
+{
+    __shared__ uint32_t h[RS_RADIX];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+#pragma unroll 4
+    for (int j = 0; j < RS_ITEMS; j++) {
+        uint64_t idx = base + (uint64_t)j * RS_THREADS + threadIdx.x;
+        uint32_t d = idx < n ? (uint32_t)((keys[idx] >> shift) & 255) : 256u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (d < 256 && (peers & ((1u << (threadIdx.x & 31)) - 1)) == 0) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    counts[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of a uint32 array in three kernels.
+constexpr int SC_THREADS = 256;
+constexpr int SC_ITEMS = 16;
+constexpr int SC_CHUNK = SC_THREADS * SC_ITEMS;
+
+__device__ __forceinline__ uint32_t block_excl_scan_256(uint32_t x, uint32_t* wsum, uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t z = lane < SC_THREADS / 32 ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += y;
+        }
+        if (lane < SC_THREADS / 32) wsum[lane] = z;
+    }
+    __syncthreads();
+    uint32_t excl = inc - x + (warp > 0 ? wsum[warp - 1] : 0);
+    if (total) *total = wsum[SC_THREADS / 32 - 1];
+    __syncthreads();
+    return excl;
+}
+
+__global__ __launch_bounds__(SC_THREADS) void k_scan_sums(const uint32_t* __restrict__ a, uint64_t n,
+                                                          uint32_t* __restrict__ sums)
+{
+    __shared__ uint32_t wsum[SC_THREADS / 32];
+    uint64_t base = (uint64_t)blockIdx.x * SC_CHUNK + (uint64_t)threadIdx.x * SC_ITEMS;
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < SC_ITEMS; j++)
+        if (base + j < n) s += a[base + j];
+    uint32_t total;
+    block_excl_scan_256(s, wsum, &total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ __launch_bounds__(SC_THREADS) void k_scan_top(uint32_t* __restrict__ sums, uint32_t nb)
+{
+    __shared__ uint32_t wsum[SC_THREADS / 32];
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < nb; base += SC_THREADS) {
+        uint32_t i = base + threadIdx.x;
+        uint32_t x = i < nb ? sums[i] : 0;
+        uint32_t total;
+        uint32_t e = block_excl_scan_256(x, wsum, &total);
+        if (i < nb) sums[i] = e + carry;
+        carry += total;
+    }
+}
+
+__global__ __launch_bounds__(SC_THREADS) void k_scan_apply(uint32_t* __restrict__ a, uint64_t n,
+                                                           const uint32_t* __restrict__ sums)
+{
+    __shared__ uint32_t wsum[SC_THREADS / 32];
+    uint64_t base = (uint64_t)blockIdx.x * SC_CHUNK + (uint64_t)threadIdx.x * SC_ITEMS;
+    uint32_t v[SC_ITEMS];
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < SC_ITEMS; j++) {
+        v[j] = base + j < n ? a[base + j] : 0;
+        s += v[j];
+    }
+    uint32_t run = block_excl_scan_256(s, wsum, nullptr) + sums[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < SC_ITEMS; j++) {
+        if (base + j < n) a[base + j] = run;
+        run += v[j];
+    }
+}
+
+// Stable scatter of one radix pass.  Warp w of a tile owns the 512
+// consecutive keys [tile*4096 + w*512, +512), read as 16 rounds of 32; the
+// rank of a key is (digit start in tile) + (keys of that digit in earlier
+// warps) + (earlier rounds and lower lanes of its own warp), which keeps the
+// input order of equal digits.  The tile is reordered in shared memory and
+// written out with per-digit global offsets.
+__global__ __launch_bounds__(RS_THREADS) void k_rs_scatter(const uint64_t* __restrict__ kin,
+                                                           const double* __restrict__ vin,
+                                                           uint64_t* __restrict__ kout, double* __restrict__ vout,
+                                                           uint64_t n, int shift, const uint32_t* __restrict__ offsets,
+                                                           uint32_t ntiles)
+{
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    uint64_t* skeys = reinterpret_cast<uint64_t*>(rs_smem);
+    double* svals = reinterpret_cast<double*>(skeys + RS_TILE);
+    uint32_t* whist = reinterpret_cast<uint32_t*>(svals + RS_TILE);
+    uint32_t* tstart = whist + RS_WARPS * RS_RADIX;
+    uint32_t* gbase = tstart + RS_RADIX;
+    __shared__ uint32_t wsum[SC_THREADS / 32];
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1;
+    for (int i = threadIdx.x; i < RS_WARPS * RS_RADIX; i += RS_THREADS) whist[i] = 0;
+    __syncthreads();
+
+    const uint64_t tile_base = (uint64_t)blockIdx.x * RS_TILE;
+    const uint64_t base = tile_base + (uint64_t)warp * (32 * RS_ITEMS);
+    uint64_t k[RS_ITEMS];
+    double v[RS_ITEMS];
+    uint32_t lp[RS_ITEMS];
+    uint32_t* wh = whist + warp * RS_RADIX;
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        uint64_t idx = base + (uint64_t)j * 32 + lane;
+        bool ok = idx < n;
+        k[j] = ok ? kin[idx] : 0;
+        v[j] = ok ? vin[idx] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        uint64_t idx = base + (uint64_t)j * 32 + lane;
+        uint32_t d = idx < n ? (uint32_t)((k[j] >> shift) & 255) : 256u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t prev = d < 256 ? wh[d] : 0;
+        lp[j] = prev + __popc(peers & lt);
+        __syncwarp();
+        if (d < 256 && (peers & lt) == 0) wh[d] = prev + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        const int d = threadIdx.x; // RS_THREADS == RS_RADIX
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < RS_WARPS; w++) {
+            uint32_t c = whist[w * RS_RADIX + d];
+            whist[w * RS_RADIX + d] = run;
+            run += c;
+        }
+        gbase[d] = offsets[(uint64_t)d * ntiles + blockIdx.x];
+        uint32_t ex = block_excl_scan_256(run, wsum, nullptr);
+        tstart[d] = ex;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; j++) {
+        uint64_t idx = base + (uint64_t)j * 32 + lane;
+        if (idx < n) {
+            uint32_t d = (uint32_t)((k[j] >> shift) & 255);
+            uint32_t sp = tstart[d] + wh[d] + lp[j];
+            skeys[sp] = k[j];
+            svals[sp] = v[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, n - tile_base);
+    for (uint32_t i = threadIdx.x; i < tile_n; i += RS_THREADS) {
+        uint64_t kk = skeys[i];
+        uint32_t d = (uint32_t)((kk >> shift) & 255);
+        uint64_t o = (uint64_t)gbase[d] + (i - tstart[d]);
+        kout[o] = kk;
+        vout[o] = svals[i];
+    }
+}
+
+int scan_u32(uint32_t* a, uint64_t n, uint32_t* sums, cudaStream_t s)
+{
+    uint32_t nb = (uint32_t)((n + SC_CHUNK - 1) / SC_CHUNK);
+    k_scan_sums<<<nb, SC_THREADS, 0, s>>>(a, n, sums);
+    BLCO_CHECK_LAUNCH("k_scan_sums");
+    k_scan_top<<<1, SC_THREADS, 0, s>>>(sums, nb);
+    BLCO_CHECK_LAUNCH("k_scan_top");
+    k_scan_apply<<<nb, SC_THREADS, 0, s>>>(a, n, sums);
+    BLCO_CHECK_LAUNCH("k_scan_apply");
+    return BLCO_OK;
+}
+
+// Sorts (k0, v0) by the low `bits` key bits; ping-pongs with (k1, v1).
+// *in_alt is set when the result ends up in (k1, v1).
+int radix_sort_pairs(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint64_t n, int bits,
+                     cudaStream_t s, bool* in_alt)
+{
+    *in_alt = false;
+    if (n <= 1 || bits <= 0) return BLCO_OK;
+    uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    uint64_t L = (uint64_t)RS_RADIX * ntiles;
+    uint32_t nsums = (uint32_t)((L + SC_CHUNK - 1) / SC_CHUNK);
+    uint32_t *counts = nullptr, *sums = nullptr;
+    BLCO_CUDA(cudaMallocAsync(&counts, L * sizeof(uint32_t), s));
+    BLCO_CUDA(cudaMallocAsync(&sums, (nsums + 1) * sizeof(uint32_t), s));
+    BLCO_CUDA(cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMEM));
+    uint64_t *ki = k0, *ko = k1;
+    double *vi = v0, *vo = v1;
+    int st = BLCO_OK;
+    for (int shift = 0; shift < bits; shift += 8) {
+        k_rs_hist<<<ntiles, RS_THREADS, 0, s>>>(ki, n, shift, counts, ntiles);
+        count_launch();
+        if ((st = scan_u32(counts, L, sums, s)) != BLCO_OK) break;
+        k_rs_scatter<<<ntiles, RS_THREADS, RS_SMEM, s>>>(ki, vi, ko, vo, n, shift, counts, ntiles);
+        count_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { st = cuda_fail(e, "k_rs_scatter", __FILE__, __LINE__); break; }
+        std::swap(ki, ko);
+        std::swap(vi, vo);
+        *in_alt = !*in_alt;
+    }
+    cudaFreeAsync(counts, s);
+    cudaFreeAsync(sums, s);
+    return st;
+}
+
+// ------------------------------------------------------ row statistics --
+
+constexpr int RC_THREADS = 256;
+constexpr int RC_HASH = 1024; // per mode, shared memory aggregation table
+
+__device__ __forceinline__ uint32_t hash_row(uint32_t r) { return (r * 2654435761u) >> 7; }
+
+struct CountPtrs {
+    uint32_t* c[BLCO_MAX_MODES];
+};
+
+// Nonzeros per row of every mode.  Rows are aggregated inside the warp
+// (match_any) and then in a per-block shared hash table before the global
+// atomics, so rows holding a large share of the nonzeros do not serialise
+// on one address.
+__global__ __launch_bounds__(RC_THREADS) void k_row_counts(const uint64_t* __restrict__ coords, uint64_t nnz,
+                                                           Layout L, CountPtrs counts)
+{
+    __shared__ uint32_t hkey[BLCO_MAX_MODES][RC_HASH];
+    __shared__ uint32_t hcnt[BLCO_MAX_MODES][RC_HASH];
+    for (int i = threadIdx.x; i < BLCO_MAX_MODES * RC_HASH; i += RC_THREADS) {
+        (&hkey[0][0])[i] = 0;
+        (&hcnt[0][0])[i] = 0;
+    }
+    __syncthreads();
+    const uint64_t per = (nnz + gridDim.x - 1) / gridDim.x;
+    const uint64_t beg = per * blockIdx.x, end = min(nnz, beg + per);
+    const int lane = threadIdx.x & 31;
+    for (uint64_t b0 = beg; b0 < end; b0 += RC_THREADS) {
+        uint64_t i = b0 + threadIdx.x;
+        bool ok = i < end;
+        uint64_t c = ok ? coords[i] : 0;
+        for (int n = 0; n < L.nmodes; n++) {
+            uint32_t row = ok ? (uint32_t)((c >> L.mode_pos[n]) & L.mode_masks[n]) : 0xffffffffu;
+            uint32_t peers = __match_any_sync(0xffffffffu, row);
+            if (!ok || (peers & ((1u << lane) - 1)) != 0) continue;
+            uint32_t cnt = __popc(peers);
+            uint32_t h = hash_row(row) & (RC_HASH - 1);
+            bool placed = false;
+            for (int probe = 0; probe < 8 && !placed; probe++) {
+                uint32_t slot = (h + probe) & (RC_HASH - 1);
+                uint32_t prev = atomicCAS(&hkey[n][slot], 0u, row + 1);
+                if (prev == 0u || prev == row + 1) {
+                    atomicAdd(&hcnt[n][slot], cnt);
+                    placed = true;
+                }
+            }
+            if (!placed) atomicAdd(&counts.c[n][row], cnt);
+        }
+    }
+    __syncthreads();
+    for (int n = 0; n < L.nmodes; n++)
+        for (int i = threadIdx.x; i < RC_HASH; i += RC_THREADS)
+            if (hkey[n][i]) atomicAdd(&counts.c[n][hkey[n][i] - 1], hcnt[n][i]);
+}
+
+struct StatOut {
+    unsigned long long hist[40];
+    unsigned long long nonempty;
+    unsigned long long maxc;
+};
+
+__global__ void k_row_stats(const uint32_t* __restrict__ counts, uint64_t rows, StatOut* out)
+{
+    __shared__ unsigned long long h[40];
+    __shared__ unsigned long long ne, mx;
+    if (threadIdx.x < 40) h[threadIdx.x] = 0;
+    if (threadIdx.x == 0) { ne = 0; mx = 0; }
+    __syncthreads();
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = counts[r];
+        if (c) {
+            atomicAdd(&h[31 - __clz(c)], 1ull);
+            atomicAdd(&ne, 1ull);
+            atomicMax(&mx, (unsigned long long)c);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 40 && h[threadIdx.x]) atomicAdd(&out->hist[threadIdx.x], h[threadIdx.x]);
+    if (threadIdx.x == 0) {
+        if (ne) atomicAdd(&out->nonempty, ne);
+        if (mx) atomicMax(&out->maxc, mx);
+    }
+}
+
+constexpr int HOT_CAND_MAX = 8192;
+constexpr int HOT_MAX = 2048;     // rows kept per mode
+constexpr int HOT_HASH = 4096;    // hash size (power of two, 2x HOT_MAX)
+constexpr uint32_t HOT_MIN_COUNT = 256;
+
+__global__ void k_collect_hot(const uint32_t* __restrict__ counts, uint64_t rows, uint32_t thresh,
+                              uint32_t* __restrict__ cand_row, uint32_t* __restrict__ cand_cnt,
+                              uint32_t* __restrict__ ncand)
+{
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = counts[r];
+        if (c >= thresh) {
+            uint32_t k = atomicAdd(ncand, 1u);
+            if (k < HOT_CAND_MAX) {
+                cand_row[k] = (uint32_t)r;
+                cand_cnt[k] = c;
+            }
+        }
+    }
+}
+
+__global__ void k_sumsq(const double* __restrict__ v, uint64_t n, double* __restrict__ partial)
+{
+    __shared__ double ws[32];
+    double s = 0.0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        s += v[i] * v[i];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < blockDim.x / 32 ? ws[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) partial[blockIdx.x] = s;
+    }
+}
+
+} // namespace
+
+uint32_t host_hash_row(uint32_t r) { return (r * 2654435761u) >> 7; }
+
+int build_hot_tables(blco_tensor* t, cudaStream_t s)
+{
+    const Layout& L = t->layout;
+    DeviceInfo di;
+    BLCO_TRY(device_info(t->device, &di));
+    CountPtrs cp;
+    memset(&cp, 0, sizeof(cp));
+    uint64_t total_rows = 0;
+    for (int n = 0; n < L.nmodes; n++) total_rows += L.dims[n];
+    uint32_t* counts = nullptr;
+    BLCO_CUDA(cudaMallocAsync(&counts, total_rows * sizeof(uint32_t), s));
+    BLCO_CUDA(cudaMemsetAsync(counts, 0, total_rows * sizeof(uint32_t), s));
+    uint64_t off = 0;
+    for (int n = 0; n < L.nmodes; n++) {
+        cp.c[n] = counts + off;
+        off += L.dims[n];
+    }
+    if (t->nnz) {
+        k_row_counts<<<di.sm_count * 4, RC_THREADS, 0, s>>>(t->d_coords, t->nnz, L, cp);
+        BLCO_CHECK_LAUNCH("k_row_counts");
+    }
+    StatOut* d_stats = nullptr;
+    uint32_t *cand = nullptr, *ncand = nullptr;
+    BLCO_CUDA(cudaMallocAsync(&d_stats, sizeof(StatOut) * L.nmodes, s));
+    BLCO_CUDA(cudaMemsetAsync(d_stats, 0, sizeof(StatOut) * L.nmodes, s));
+    BLCO_CUDA(cudaMallocAsync(&cand, sizeof(uint32_t) * 2 * HOT_CAND_MAX * L.nmodes, s));
+    BLCO_CUDA(cudaMallocAsync(&ncand, sizeof(uint32_t) * L.nmodes, s));
+    BLCO_CUDA(cudaMemsetAsync(ncand, 0, sizeof(uint32_t) * L.nmodes, s));
+    for (int n = 0; n < L.nmodes; n++) {
+        int grid = (int)std::min<uint64_t>((L.dims[n] + 255) / 256, (uint64_t)di.sm_count * 8);
+        k_row_stats<<<grid, 256, 0, s>>>(cp.c[n], L.dims[n], d_stats + n);
+        BLCO_CHECK_LAUNCH("k_row_stats");
+    }
+    std::vector<StatOut> hs(L.nmodes);
+    BLCO_CUDA(cudaMemcpyAsync(hs.data(), d_stats, sizeof(StatOut) * L.nmodes, cudaMemcpyDeviceToHost, s));
+    BLCO_CUDA(cudaStreamSynchronize(s));
+    std::vector<uint32_t> thresh(L.nmodes, 0);
+    for (int n = 0; n < L.nmodes; n++) {
+        ModeStats& ms = t->stats[n];
+        ms.max_row_nnz = hs[n].maxc;
+        ms.nonempty_rows = hs[n].nonempty;
+        for (int b = 0; b < 40; b++) ms.log2_hist[b] = hs[n].hist[b];
+        // Lowest power-of-two threshold with at most HOT_CAND_MAX rows above it.
+        uint64_t above = 0;
+        int bsel = 40;
+        for (int b = 39; b >= 0; b--) {
+            if (above + hs[n].hist[b] > (uint64_t)HOT_CAND_MAX) break;
+            above += hs[n].hist[b];
+            bsel = b;
+        }
+        uint64_t th = bsel >= 40 ? ~0u : (1ull << bsel);
+        thresh[n] = (uint32_t)std::max<uint64_t>(th, HOT_MIN_COUNT);
+    }
+    for (int n = 0; n < L.nmodes; n++) {
+        int grid = (int)std::min<uint64_t>((L.dims[n] + 255) / 256, (uint64_t)di.sm_count * 8);
+        k_collect_hot<<<grid, 256, 0, s>>>(cp.c[n], L.dims[n], thresh[n], cand + 2 * HOT_CAND_MAX * n,
+                                           cand + 2 * HOT_CAND_MAX * n + HOT_CAND_MAX, ncand + n);
+        BLCO_CHECK_LAUNCH("k_collect_hot");
+    }
+    std::vector<uint32_t> hc(2 * HOT_CAND_MAX * L.nmodes), hn(L.nmodes);
+    BLCO_CUDA(cudaMemcpyAsync(hc.data(), cand, hc.size() * 4, cudaMemcpyDeviceToHost, s));
+    BLCO_CUDA(cudaMemcpyAsync(hn.data(), ncand, hn.size() * 4, cudaMemcpyDeviceToHost, s));
+    BLCO_CUDA(cudaStreamSynchronize(s));
+    cudaFreeAsync(counts, s);
+    cudaFreeAsync(d_stats, s);
+    cudaFreeAsync(cand, s);
+    cudaFreeAsync(ncand, s);
+
+    for (int n = 0; n < L.nmodes; n++) {
+        HotTable& ht = t->hot[n];
+        uint32_t nc = std::min<uint32_t>(hn[n], HOT_CAND_MAX);
+        std::vector<std::pair<uint32_t, uint32_t>> rows; // (count, row)
+        for (uint32_t k = 0; k < nc; k++)
+            rows.push_back({hc[2 * HOT_CAND_MAX * n + HOT_CAND_MAX + k], hc[2 * HOT_CAND_MAX * n + k]});
+        std::sort(rows.begin(), rows.end(), [](auto& a, auto& b) {
+            return a.first != b.first ? a.first > b.first : a.second < b.second;
+        });
+        if (rows.size() > (size_t)HOT_MAX) rows.resize(HOT_MAX);
+        ht.nhot = (int)rows.size();
+        ht.hot_nnz = 0;
+        if (ht.nhot == 0) continue;
+        ht.hash_size = HOT_HASH;
+        std::vector<uint32_t> keys(HOT_HASH, 0), slots(HOT_HASH, 0);
+        for (int k = 0; k < ht.nhot; k++) {
+            uint32_t r = rows[k].second;
+            ht.hot_nnz += rows[k].first;
+            uint32_t h = host_hash_row(r) & (HOT_HASH - 1);
+            while (keys[h]) h = (h + 1) & (HOT_HASH - 1);
+            keys[h] = r + 1;
+            slots[h] = (uint32_t)k; // slots in descending heaviness
+        }
+        std::vector<uint32_t> rowlist(ht.nhot);
+        for (int k = 0; k < ht.nhot; k++) rowlist[k] = rows[k].second;
+        BLCO_CUDA(cudaMalloc(&ht.d_keys, HOT_HASH * sizeof(uint32_t)));
+        BLCO_CUDA(cudaMalloc(&ht.d_slot, HOT_HASH * sizeof(uint32_t)));
+        BLCO_CUDA(cudaMalloc(&ht.d_rows, ht.nhot * sizeof(uint32_t)));
+        BLCO_CUDA(cudaMemcpyAsync(ht.d_keys, keys.data(), HOT_HASH * 4, cudaMemcpyHostToDevice, s));
+        BLCO_CUDA(cudaMemcpyAsync(ht.d_slot, slots.data(), HOT_HASH * 4, cudaMemcpyHostToDevice, s));
+        BLCO_CUDA(cudaMemcpyAsync(ht.d_rows, rowlist.data(), ht.nhot * 4, cudaMemcpyHostToDevice, s));
+    }
+    BLCO_CUDA(cudaStreamSynchronize(s));
+    return BLCO_OK;
+}
+
+int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* d_cidx,
+                const double* d_vals, uint64_t max_block_size, const blco_opts* opts, blco_tensor** out)
+{
+    *out = nullptr;
+    if (!dims || !out || (nnz && (!d_cidx || !d_vals))) return fail(BLCO_ERR_INVALID, "null argument");
+    if (nnz >= 0xffffffffull) return fail(BLCO_ERR_UNSUPPORTED, "nnz must be below 2^32-1 for the device encoder");
+    blco_tensor* t = new blco_tensor();
+    int st = make_layout(nmodes, dims, &t->layout);
+    if (st != BLCO_OK) { delete t; return st; }
+    for (int n = 0; n < nmodes; n++)
+        if (nnz && !d_cidx[n]) { delete t; return fail(BLCO_ERR_INVALID, "null coordinate array"); }
+    t->device = opts ? opts->device : 0;
+    t->nnz = nnz;
+    t->max_block_size = max_block_size;
+    uint64_t B = max_block_size ? max_block_size : nnz;
+    t->block_count = nnz == 0 ? 0 : (nnz + B - 1) / B;
+    t->resident = !(opts && opts->stream_data);
+
+    auto cleanup_fail = [&](int s) { blco_tensor_free(t); return s; };
+    cudaError_t e = cudaSetDevice(t->device);
+    if (e != cudaSuccess) return cleanup_fail(cuda_fail(e, "cudaSetDevice", __FILE__, __LINE__));
+    cudaStream_t s = pick_stream(t, opts);
+    if (!s) return cleanup_fail(last_error()[0] ? BLCO_ERR_CUDA : BLCO_ERR_CUDA);
+
+    uint64_t n_alloc = nnz ? nnz : 1;
+    uint64_t *k0 = nullptr, *k1 = nullptr;
+    double *v0 = nullptr, *v1 = nullptr;
+    int* d_bad = nullptr;
+    auto free_tmp = [&]() {
+        cudaStreamSynchronize(s);
+        cudaFree(k1);
+        cudaFree(v1);
+        cudaFree(d_bad);
+        k1 = nullptr;
+        v1 = nullptr;
+        d_bad = nullptr;
+    };
+#define ENC_CUDA(call)                                                          \
+    do {                                                                        \
+        cudaError_t _e = (call);                                                \
+        if (_e != cudaSuccess) {                                                \
+            int _s = cuda_fail(_e, #call, __FILE__, __LINE__);                  \
+            free_tmp();                                                         \
+            cudaFree(k0);                                                       \
+            cudaFree(v0);                                                       \
+            return cleanup_fail(_s);                                            \
+        }                                                                       \
+    } while (0)
+    ENC_CUDA(cudaMalloc(&k0, n_alloc * 8));
+    ENC_CUDA(cudaMalloc(&v0, n_alloc * 8));
+    ENC_CUDA(cudaMalloc(&k1, n_alloc * 8));
+    ENC_CUDA(cudaMalloc(&v1, n_alloc * 8));
+    ENC_CUDA(cudaMalloc(&d_bad, sizeof(int)));
+    ENC_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+
+    DeviceInfo di;
+    if ((st = device_info(t->device, &di)) != BLCO_OK) {
+        free_tmp();
+        cudaFree(k0);
+        cudaFree(v0);
+        return cleanup_fail(st);
+    }
+    bool in_alt = false;
+    if (nnz) {
+        CooPtrs coo;
+        memset(&coo, 0, sizeof(coo));
+        for (int n = 0; n < nmodes; n++) coo.c[n] = d_cidx[n];
+        int grid = (int)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)di.sm_count * 16);
+        k_alto_keys<<<grid, 256, 0, s>>>(coo, d_vals, nnz, t->layout, k0, v0, d_bad);
+        count_launch();
+        ENC_CUDA(cudaGetLastError());
+        int bad = 0;
+        ENC_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        ENC_CUDA(cudaStreamSynchronize(s));
+        if (bad) {
+            free_tmp();
+            cudaFree(k0);
+            cudaFree(v0);
+            return cleanup_fail(fail(BLCO_ERR_INVALID, "a coordinate is not below its mode length"));
+        }
+        st = radix_sort_pairs(k0, v0, k1, v1, nnz, t->layout.alto_bits, s, &in_alt);
+        if (st != BLCO_OK) {
+            free_tmp();
+            cudaFree(k0);
+            cudaFree(v0);
+            return cleanup_fail(st);
+        }
+        if (in_alt) {
+            std::swap(k0, k1);
+            std::swap(v0, v1);
+        }
+        k_relinearize<<<grid, 256, 0, s>>>(k0, nnz, t->layout);
+        count_launch();
+        ENC_CUDA(cudaGetLastError());
+        double* partial = reinterpret_cast<double*>(k1); // k1 is free now
+        int g2 = std::min(grid, 1024);
+        k_sumsq<<<g2, 256, 0, s>>>(v0, nnz, partial);
+        count_launch();
+        ENC_CUDA(cudaGetLastError());
+        std::vector<double> hp(g2);
+        ENC_CUDA(cudaMemcpyAsync(hp.data(), partial, g2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ENC_CUDA(cudaStreamSynchronize(s));
+        double ss = 0.0;
+        for (double x : hp) ss += x;
+        t->norm_sq = ss;
+    }
+    free_tmp();
+    t->d_coords = k0;
+    t->d_values = v0;
+    k0 = nullptr;
+    v0 = nullptr;
+    ENC_CUDA(cudaStreamSynchronize(s));
+#undef ENC_CUDA
+    if ((st = build_hot_tables(t, s)) != BLCO_OK) return cleanup_fail(st);
+    if (!t->resident) {
+        // Streamed form: the encoded stream moves to pinned host memory and
+        // the device copy is released; blocks are copied back per use.
+        cudaError_t e1 = cudaMallocHost(&t->h_coords, n_alloc * 8);
+        cudaError_t e2 = cudaMallocHost(&t->h_values, n_alloc * 8);
+        if (e1 != cudaSuccess || e2 != cudaSuccess)
+            return cleanup_fail(fail(BLCO_ERR_NOMEM, "pinned host allocation for streamed blocks failed"));
+        BLCO_CUDA(cudaMemcpyAsync(t->h_coords, t->d_coords, nnz * 8, cudaMemcpyDeviceToHost, s));
+        BLCO_CUDA(cudaMemcpyAsync(t->h_values, t->d_values, nnz * 8, cudaMemcpyDeviceToHost, s));
+        BLCO_CUDA(cudaStreamSynchronize(s));
+        cudaFree(t->d_coords);
+        cudaFree(t->d_values);
+        t->d_coords = nullptr;
+        t->d_values = nullptr;
+    }
+    *out = t;
+    return BLCO_OK;
+}
+
+} // namespace blco

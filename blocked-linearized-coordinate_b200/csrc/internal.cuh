@@ -1,0 +1,148 @@
+// internal.cuh -- shared declarations of the BLCO engine (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "blco.h"
+
+namespace blco {
+
+// ---------------------------------------------------------------- errors --
+
+void set_error(const std::string& msg);
+const char* last_error();
+
+// Records a CUDA failure and yields BLCO_ERR_CUDA (or BLCO_ERR_NOMEM).
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define BLCO_CUDA(call)                                                        \
+    do {                                                                       \
+        cudaError_t _e = (call);                                               \
+        if (_e != cudaSuccess) return ::blco::cuda_fail(_e, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define BLCO_TRY(call)                                                         \
+    do {                                                                       \
+        int _s = (call);                                                       \
+        if (_s != BLCO_OK) return _s;                                          \
+    } while (0)
+
+#define BLCO_CHECK_LAUNCH(name)                                                \
+    do {                                                                       \
+        ::blco::count_launch();                                                \
+        cudaError_t _e = cudaGetLastError();                                   \
+        if (_e != cudaSuccess) return ::blco::cuda_fail(_e, name, __FILE__, __LINE__); \
+    } while (0)
+
+int fail(int status, const std::string& msg);
+void count_launch();
+
+// ----------------------------------------------------------- device info --
+
+struct DeviceInfo {
+    int device = 0;
+    int sm_count = 148;
+    size_t smem_optin = 227 * 1024;
+};
+int device_info(int device, DeviceInfo* out);
+
+// ------------------------------------------------------------ bit layout --
+
+// Per-tensor layout constants, passed by value to kernels.
+struct Layout {
+    int nmodes;
+    uint64_t dims[BLCO_MAX_MODES];
+    uint64_t mode_masks[BLCO_MAX_MODES];
+    int mode_pos[BLCO_MAX_MODES];
+    uint64_t alto_masks[BLCO_MAX_MODES];
+    int alto_bits;
+};
+
+// Computes masks/positions from dims (include/alto.hpp:597-695,
+// include/blco.hpp:221-233).  Returns BLCO_OK or BLCO_ERR_INVALID.
+int make_layout(int nmodes, const uint64_t* dims, Layout* out);
+
+// ---------------------------------------------------------------- tensor --
+
+// Per-mode heavy-row table: open-addressing hash of the rows that receive
+// the most nonzeros, used by the MTTKRP kernels to keep those rows'
+// partial sums in shared memory.
+struct HotTable {
+    uint32_t* d_keys = nullptr; // hash_size entries: row + 1, 0 = empty
+    uint32_t* d_slot = nullptr; // hash_size entries: slot in the smem table
+    uint32_t* d_rows = nullptr; // nhot entries: slot -> row (slots by descending nnz)
+    int hash_size = 0;          // power of two (0 = no table)
+    int nhot = 0;               // number of rows in the table
+    uint64_t hot_nnz = 0;       // nonzeros that fall on hot rows
+};
+
+struct ModeStats {
+    uint64_t max_row_nnz = 0;
+    uint64_t nonempty_rows = 0;
+    uint64_t log2_hist[40] = {}; // rows with nnz in [2^b, 2^(b+1))
+};
+
+} // namespace blco
+
+struct blco_cpals_plan;
+
+struct blco_tensor {
+    blco::Layout layout;
+    uint64_t nnz = 0;
+    uint64_t max_block_size = 0;
+    uint64_t block_count = 0;
+    int device = 0;
+    bool resident = true;
+    // resident stream (HBM)
+    uint64_t* d_coords = nullptr;
+    double* d_values = nullptr;
+    float* d_values_f32 = nullptr; // mixed form, created on first use
+    // streamed blocks (pinned host)
+    uint64_t* h_coords = nullptr;
+    double* h_values = nullptr;
+    // heavy-row tables, one per mode, built at encode time
+    blco::HotTable hot[BLCO_MAX_MODES];
+    blco::ModeStats stats[BLCO_MAX_MODES];
+    double norm_sq = 0.0; // sum of squared values
+    cudaStream_t own_stream = nullptr;
+};
+
+namespace blco {
+
+cudaStream_t pick_stream(const blco_tensor* t, const blco_opts* opts);
+
+// encode.cu
+int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz,
+                const uint64_t* const* d_cidx, const double* d_vals,
+                uint64_t max_block_size, const blco_opts* opts, blco_tensor** out);
+int build_hot_tables(blco_tensor* t, cudaStream_t s);
+
+// mttkrp.cu
+struct MttkrpArgs {
+    const uint64_t* coords;
+    const double* vals;
+    uint64_t nnz;
+    int mode;
+    int rank;
+    const double* factors[BLCO_MAX_MODES];
+    double* out;
+    int kernel;
+    int thread_cf;
+};
+int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
+int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested);
+
+// cpals.cu
+int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_lambda, const blco_opts* opts,
+                blco_cpals_plan** out);
+int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* iters_done, bool verbose);
+int plan_destroy(blco_cpals_plan* p);
+int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
+int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda, int maxiter,
+               double tol, const blco_opts* opts, double* fit_out, double* fits, int* iters_out);
+
+} // namespace blco

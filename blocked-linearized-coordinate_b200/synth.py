@@ -1,0 +1,108 @@
+"""Seeded synthetic sparse tensors of the benchmark shapes.
+
+The reference is benchmarked on FROSTT tensors (scripts/run_cpd.sh) that are
+not available offline; these generators stand in for them with the shapes
+and value distributions of the named workloads:
+
+  * zipf_tensor_device: per-mode Zipf(s) coordinates over [0, I_n) (rank k
+    has probability ~ (k+1)^-s; rows are not permuted, so heavy rows have
+    small indices), values lognormal(0,1) drawn in FP32 and summed over
+    duplicate coordinates in FP64, exactly `nnz` distinct coordinates.
+    Generated on the GPU with torch (plumbing only; not the engine).
+  * uniform_tensor_host: distinct uniform coordinates, U(0,1) FP64 values,
+    generated with numpy (the small CPU-runnable workload).
+"""
+import numpy as np
+
+
+def _zipf_cdf(torch, d, s, device):
+    k = torch.arange(1, d + 1, dtype=torch.float64, device=device)
+    w = k.pow(-s)
+    c = torch.cumsum(w, 0)
+    return c / c[-1]
+
+
+def zipf_tensor_device(nnz, dims, s, seed=0, device="cuda", value_dist="lognormal"):
+    """Returns dict(dims, cidx=[int64 CUDA tensors], vals=float64 CUDA tensor)."""
+    import torch
+    dims = [int(d) for d in dims]
+    key_space = 1
+    for d in dims:
+        key_space *= d
+    if key_space >= 2 ** 63:
+        raise ValueError("coordinate space too large for 63-bit linear keys")
+    if nnz > key_space:
+        raise ValueError("more nonzeros than cells")
+    g = torch.Generator(device=device).manual_seed(int(seed))
+    cdfs = [_zipf_cdf(torch, d, s, device) if s > 0 else None for d in dims]
+    mult = []
+    m = 1
+    for d in reversed(dims):
+        mult.append(m)
+        m *= d
+    mult = list(reversed(mult))
+
+    keys = torch.empty(0, dtype=torch.int64, device=device)
+    vals = torch.empty(0, dtype=torch.float64, device=device)
+    draw = int(nnz * 1.05) + 1024
+    for _ in range(64):
+        k = torch.zeros(draw, dtype=torch.int64, device=device)
+        for n, d in enumerate(dims):
+            if cdfs[n] is None:
+                c = torch.randint(0, d, (draw,), generator=g, device=device, dtype=torch.int64)
+            else:
+                u = torch.rand(draw, dtype=torch.float64, generator=g, device=device)
+                c = torch.searchsorted(cdfs[n], u).clamp_(max=d - 1)
+            k += c * mult[n]
+            del c
+        if value_dist == "lognormal":
+            v = torch.randn(draw, dtype=torch.float32, generator=g, device=device).exp_().double()
+        else:
+            v = torch.rand(draw, dtype=torch.float32, generator=g, device=device).double()
+        keys = torch.cat([keys, k])
+        vals = torch.cat([vals, v])
+        del k, v
+        uk, inv = torch.unique(keys, sorted=True, return_inverse=True)
+        uv = torch.zeros(uk.numel(), dtype=torch.float64, device=device).index_add_(0, inv, vals)
+        del inv
+        keys, vals = uk, uv
+        have = keys.numel()
+        if have >= nnz:
+            break
+        # draw more, scaled by the observed yield of new distinct keys
+        draw = int((nnz - have) * 2.0) + 1024
+    else:
+        raise RuntimeError("could not reach the requested number of distinct coordinates")
+    if keys.numel() > nnz:
+        pick = torch.randperm(keys.numel(), generator=g, device=device)[:nnz]
+        keys, vals = keys[pick], vals[pick]
+    else:
+        pick = torch.randperm(keys.numel(), generator=g, device=device)
+        keys, vals = keys[pick], vals[pick]
+    cidx = []
+    rem = keys
+    for n, mu in enumerate(mult):
+        cidx.append(torch.div(rem, mu, rounding_mode="floor"))
+        rem = rem - cidx[-1] * mu
+    del keys, rem
+    return dict(dims=dims, cidx=cidx, vals=vals.contiguous())
+
+
+def uniform_tensor_host(nnz, dims, seed=0):
+    """Distinct uniform coordinates and U(0,1) FP64 values (numpy)."""
+    rng = np.random.default_rng(seed)
+    dims = [int(d) for d in dims]
+    mult = np.cumprod([1] + dims[::-1][:-1])[::-1].astype(np.int64)
+    total = int(np.prod(np.array(dims, dtype=np.float64)))
+    lin = rng.choice(total, size=nnz, replace=False) if total < 50 * nnz else np.unique(
+        rng.integers(0, total, size=int(nnz * 1.2) + 16))
+    while len(lin) < nnz:
+        lin = np.unique(np.concatenate([lin, rng.integers(0, total, size=nnz)]))
+    lin = rng.permutation(lin)[:nnz]
+    cidx = np.zeros((len(dims), nnz), dtype=np.uint64)
+    rem = lin.astype(np.int64)
+    for n, mu in enumerate(mult):
+        cidx[n] = (rem // mu).astype(np.uint64)
+        rem = rem % mu
+    vals = rng.random(nnz)
+    return dict(dims=dims, cidx=cidx, vals=vals)

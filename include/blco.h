@@ -1,0 +1,208 @@
+/*
+ * blco.h -- C ABI of the B200 BLCO engine (libblco_b200.so).
+ *
+ * The reference (jeewhanchoi/blocked-linearized-coordinate) has no FFI: its
+ * boundary is the cpd64 CLI plus three in-process C++ entry points.  Each
+ * function below replaces one of them with plain pointers, sizes and status
+ * codes; the citation names the reference interface it stands in for.
+ *
+ * Conventions
+ *   - Every function returns a blco_status (0 = BLCO_OK).  The reference
+ *     exits the process on any CUDA error (src/utils.cu:131-137); here the
+ *     error is returned and blco_last_error() gives the message of the
+ *     calling thread's last failure.
+ *   - Factor matrices are row-major dims[n] x rank FP64, as KruskalModel::U
+ *     (include/kruskal_model.hpp:8-16).
+ *   - BLCO coordinates are uint64 with mode n in bits
+ *     [mode_pos[n], mode_pos[n] + bits_n), in ALTO order, exactly as
+ *     gen_blcotensor_host<uint64> produces them (include/blco.hpp:196-331).
+ *   - "d_" pointers are device (HBM) pointers, others are host pointers.
+ *   - A tensor handle may be used from one host thread at a time.
+ */
+#ifndef BLCO_B200_H_
+#define BLCO_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BLCO_MAX_MODES 5 /* MAX_NUM_MODES, config.mk:19 */
+
+typedef enum blco_status {
+    BLCO_OK = 0,
+    BLCO_ERR_INVALID = 1,     /* bad argument (mode, rank, sizes, pointers) */
+    BLCO_ERR_UNSUPPORTED = 2, /* valid input outside what this build handles */
+    BLCO_ERR_CUDA = 3,        /* a CUDA runtime call or kernel failed */
+    BLCO_ERR_NOMEM = 4,       /* device or pinned allocation failed */
+    BLCO_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    BLCO_ERR_IO = 6,          /* file could not be read or parsed */
+    BLCO_ERR_STATE = 7        /* handle used in a state that does not allow it */
+} blco_status;
+
+/* MTTKRP kernel ids, the values of the reference -k flag
+ * (src/alto_dev.cu:1974-2011).  The reference variants are re-designed for
+ * B200, keeping each id's role:
+ *   1  register/segmented conflict resolution (lvl1)
+ *   2  lvl1 + shared-memory privatisation of heavy output rows (lvl2 role)
+ *   3  shared-memory partial output matrix, for short modes (lvl3 role)
+ *   10 automatic selection (the reference heuristic: 3 if the mode has at
+ *      most 100 rows, else 1; replaced by the selector when one is loaded)
+ *   11, 12 one launch over all blocks (always the case here; mapped to 1)
+ *   13 one atomic per (nonzero, column)                                  */
+enum {
+    BLCO_KERNEL_AUTO = 10,
+    BLCO_KERNEL_LVL1 = 1,
+    BLCO_KERNEL_LVL2 = 2,
+    BLCO_KERNEL_LVL3 = 3,
+    BLCO_KERNEL_BATCHED = 11,
+    BLCO_KERNEL_BATCHED_V2 = 12,
+    BLCO_KERNEL_ATOMIC = 13
+};
+
+/* Numeric form. */
+enum {
+    BLCO_PRECISION_FP64 = 0, /* plain form: all values and factors FP64 */
+    BLCO_PRECISION_MIXED = 1 /* FP32 values/accumulation, BF16 factor gathers */
+};
+
+/* Options shared by the MTTKRP and CP-ALS entry points; the fields mirror
+ * the reference flags (src/main.cpp:70-96).  Fill with blco_opts_init. */
+typedef struct blco_opts {
+    int kernel;            /* -k, default 10 */
+    int nprtn;             /* -n: partial matrices for kernel 3; 0 = auto */
+    int thread_cf;         /* --thread-cf: tiles per warp step, default 2 */
+    int stream_data;       /* --stream-data: blocks stay in pinned host memory */
+    int precision;         /* BLCO_PRECISION_* */
+    int verbose;           /* print the reference's progress lines */
+    int device;            /* --device */
+    uint64_t residency_bytes; /* device budget for streamed blocks; 0 = 8 GiB */
+    void* stream;          /* cudaStream_t to run on; NULL = library stream */
+} blco_opts;
+
+typedef struct blco_tensor blco_tensor; /* opaque */
+
+typedef struct blco_tensor_info {
+    int nmodes;
+    uint64_t dims[BLCO_MAX_MODES];
+    uint64_t nnz;
+    uint64_t block_count;
+    uint64_t max_block_size;
+    uint64_t mode_masks[BLCO_MAX_MODES]; /* (1 << bits_n) - 1 */
+    int mode_pos[BLCO_MAX_MODES];        /* field offsets */
+    uint64_t alto_masks[BLCO_MAX_MODES]; /* interleaved ALTO masks */
+    int alto_bits;                       /* sum of bits_n */
+    int device;
+    int resident; /* 1: stream in HBM; 0: pinned host blocks (streamed) */
+} blco_tensor_info;
+
+/* ---- library ------------------------------------------------------------ */
+
+void blco_opts_init(blco_opts* opts);
+const char* blco_status_string(int status);
+/* Message of the calling thread's last failed call ("" if none). */
+const char* blco_last_error(void);
+/* Library version string. */
+const char* blco_version(void);
+
+/* ---- encoder ------------------------------------------------------------ */
+
+/* Encode a COO tensor into 64-bit BLCO on the GPU.
+ * Replaces gen_blcotensor_host<uint64> (include/blco.hpp:196) followed by
+ * gen_blcotensor_device + send_blcotensor_over (src/blco.cu:12, 120): the
+ * linearization, ALTO sort, re-linearization and block split all run as
+ * sm_100a kernels and the result matches the reference bit for bit.
+ *   cidx[n] (host): nnz 0-based coordinates of mode n; vals (host): nnz values.
+ *   max_block_size: the --max-block-size of the reference (0 = nnz).
+ *   opts->stream_data: keep the encoded blocks in pinned host memory instead
+ *   of HBM, for the streamed out-of-memory path.
+ * Ties between equal coordinates keep input order. */
+int blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
+                const uint64_t* const* cidx, const double* vals,
+                uint64_t max_block_size, const blco_opts* opts,
+                blco_tensor** out);
+
+/* Same, with the COO arrays already in device memory (d_cidx[n], d_vals). */
+int blco_encode_device(int nmodes, const uint64_t* dims, uint64_t nnz,
+                       const uint64_t* const* d_cidx, const double* d_vals,
+                       uint64_t max_block_size, const blco_opts* opts,
+                       blco_tensor** out);
+
+/* Free a tensor.  Replaces delete_blcotensor_host/_device
+ * (src/blco.cu:61-91). */
+int blco_tensor_free(blco_tensor* t);
+
+int blco_tensor_get_info(const blco_tensor* t, blco_tensor_info* info);
+
+/* Copy the encoded arrays to host memory: coords/values (nnz entries, the
+ * reference's blcotensor::coords / ::values), block_offsets (block_count + 1
+ * entries: start of every block, then nnz) and block_coords
+ * (block_count * nmodes, blco_block::block_coords).  Any pointer may be
+ * NULL to skip that array. */
+int blco_tensor_copy_out(const blco_tensor* t, uint64_t* coords, double* values,
+                         uint64_t* block_offsets, uint64_t* block_coords);
+
+/* Device pointers of the resident stream (BLCO_ERR_STATE if streamed). */
+int blco_tensor_device_arrays(const blco_tensor* t, const uint64_t** d_coords,
+                              const double** d_values);
+
+/* ---- MTTKRP ------------------------------------------------------------- */
+
+/* d_out += MTTKRP of mode `mode` (row-major dims[mode] x rank) using device
+ * factor matrices d_factors[n] (row-major dims[n] x rank; d_factors[mode]
+ * is not read).  Replaces mttkrp_alto_dev_onemode<IType>
+ * (src/alto_dev.cu:1955-2032), which also accumulates into its output.
+ * Runs on opts->stream; returns after enqueueing (streamed tensors: after
+ * the last block is enqueued). */
+int blco_mttkrp(blco_tensor* t, int mode, int rank, const double* const* d_factors,
+                double* d_out, const blco_opts* opts);
+
+/* Host-pointer form: out (host) += MTTKRP, factors are host arrays.  The
+ * role of the reference -p benchmark driver mttkrp_alto_dev
+ * (src/alto_dev.cu:1857-1952) for one call; synchronous. */
+int blco_mttkrp_host(blco_tensor* t, int mode, int rank, const double* const* factors,
+                     double* out, const blco_opts* opts);
+
+/* ---- CP-ALS ------------------------------------------------------------- */
+
+/* CP-ALS with host factors.  Replaces cpals_blco_dev (src/cpd_gpu.cu:21-242)
+ * and keeps its arithmetic: modes in descending length order, pseudoinverse
+ * of the Hadamard product of Grams with the n*ulp(s_max) cut-off, column
+ * L2 scaling with lambda_c <- sqrt(lambda_c + ||u_c||^2) (lambda is not
+ * reset, as in the reference), fit as kruskal_fit_gpu, stop when
+ * |fit - fit_old| < tol or the fit is NaN.  factors (host, dims[n] x rank)
+ * and lambda (host, rank) are read and updated in place.
+ *   fit_out: last fit; fits (may be NULL): one entry per executed
+ *   iteration (maxiter entries must fit); iters_out: iterations executed. */
+int blco_cpals(blco_tensor* t, int rank, double* const* factors, double* lambda,
+               int maxiter, double tol, const blco_opts* opts, double* fit_out,
+               double* fits, int* iters_out);
+
+/* Re-usable CP-ALS state over device factors: set-up (||X||, Grams and
+ * workspace) once, then run iterations.  d_factors and d_lambda stay owned
+ * by the caller and must outlive the plan. */
+typedef struct blco_cpals_plan blco_cpals_plan;
+
+int blco_cpals_plan_create(blco_tensor* t, int rank, double* const* d_factors,
+                           double* d_lambda, const blco_opts* opts,
+                           blco_cpals_plan** out);
+/* Run up to `iters` iterations (the convergence test uses tol and the fit
+ * of the previous call).  fits: host array of `iters` entries or NULL. */
+int blco_cpals_plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits,
+                            int* iters_done);
+/* Milliseconds of device time spent in MTTKRP per mode over all iterations
+ * run so far (CUDA events on the plan's stream); ms has nmodes entries. */
+int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
+int blco_cpals_plan_destroy(blco_cpals_plan* p);
+
+/* Number of this library's kernels launched by the calling thread since the
+ * last reset (for reporting launch counts). */
+uint64_t blco_launch_count(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BLCO_B200_H_ */

@@ -1,0 +1,193 @@
+"""ctypes bindings for the CPU oracle (test infrastructure only).
+
+Loads oracle/liboracle.so (the C restatement in blco_oracle.c) and, when it
+was built, oracle/_ref/libblco_ref.so (the reference's own CPU code compiled
+from its sources by `make -C oracle ref`).  Only tests/, the smoke check in
+__graft_entry__.py and bench.py's CPU-baseline leg use this module; the
+product path never does.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _ptr_array(arrs):
+    return (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (run make -C oracle)")
+        L = ctypes.CDLL(path)
+        L.orc_pdep.restype = ctypes.c_uint64
+        L.orc_pdep.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        L.orc_pext.restype = ctypes.c_uint64
+        L.orc_pext.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
+        L.orc_alto_masks.restype = ctypes.c_int
+        L.orc_blco_encode.restype = ctypes.c_int
+        L.orc_pinv_sym.restype = ctypes.c_int
+        L.orc_cpals.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's own CPU code, or None when oracle/_ref was not built."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libblco_ref.so")
+        if not os.path.exists(path):
+            return None
+        R = ctypes.CDLL(path)
+        R.ref_blco_encode.restype = ctypes.c_int
+        R.ref_alto_create.restype = ctypes.c_void_p
+        R.ref_alto_create.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int]
+        R.ref_alto_mttkrp.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        R.ref_alto_destroy.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        _ref = R
+    return _ref
+
+
+def alto_masks(dims):
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    out = np.zeros(len(dims), dtype=np.uint64)
+    bits = lib().orc_alto_masks(ctypes.c_int(len(dims)), _p(dims, _u64p), _p(out, _u64p))
+    if bits < 0:
+        raise ValueError("ALTO key wider than 64 bits")
+    return out, bits
+
+
+def _encode_with(fn, dims, cidx, vals, max_block_size, with_alto):
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    nmodes, nnz = cidx.shape
+    coords = np.zeros(nnz, dtype=np.uint64)
+    ovals = np.zeros(nnz, dtype=np.float64)
+    masks = np.zeros(nmodes, dtype=np.uint64)
+    pos = np.zeros(nmodes, dtype=np.int32)
+    nb = np.zeros(1, dtype=np.uint64)
+    B = max_block_size if max_block_size else max(nnz, 1)
+    offs = np.zeros(nnz // B + 2, dtype=np.uint64)
+    if with_alto:
+        amasks = np.zeros(nmodes, dtype=np.uint64)
+        rc = fn(ctypes.c_int(nmodes), _p(dims, _u64p), ctypes.c_uint64(nnz), _p(cidx, _u64p),
+                _p(vals, _f64p), ctypes.c_uint64(max_block_size), _p(coords, _u64p),
+                _p(ovals, _f64p), _p(masks, _u64p), _p(pos, _i32p), _p(amasks, _u64p),
+                _p(nb, _u64p), _p(offs, _u64p))
+        extra = amasks
+    else:
+        bcoords = np.zeros((nnz // B + 2) * nmodes, dtype=np.uint64)
+        rc = fn(ctypes.c_int(nmodes), _p(dims, _u64p), ctypes.c_uint64(nnz), _p(cidx, _u64p),
+                _p(vals, _f64p), ctypes.c_uint64(max_block_size), _p(coords, _u64p),
+                _p(ovals, _f64p), _p(masks, _u64p), _p(pos, _i32p), _p(nb, _u64p),
+                _p(offs, _u64p), _p(bcoords, _u64p))
+        extra = bcoords[: int(nb[0]) * nmodes].reshape(-1, nmodes)
+    if rc != 0:
+        raise ValueError("encode rejected the input")
+    n_blocks = int(nb[0])
+    return dict(coords=coords, vals=ovals, mode_masks=masks, mode_pos=pos,
+                nblocks=n_blocks, block_offsets=offs[: n_blocks + 1].copy(), extra=extra)
+
+
+def blco_encode(dims, cidx, vals, max_block_size=0):
+    """Oracle encoder; returns dict with coords, vals, mode_masks, mode_pos,
+    nblocks, block_offsets and alto_masks."""
+    r = _encode_with(lib().orc_blco_encode, dims, cidx, vals, max_block_size, True)
+    r["alto_masks"] = r.pop("extra")
+    return r
+
+
+def ref_blco_encode(dims, cidx, vals, max_block_size=0):
+    """The reference encoder (oracle/_ref); same fields plus block_coords."""
+    R = ref_lib()
+    if R is None:
+        raise FileNotFoundError("oracle/_ref not built")
+    r = _encode_with(R.ref_blco_encode, dims, cidx, vals, max_block_size, False)
+    r["block_coords"] = r.pop("extra")
+    return r
+
+
+def mttkrp_coo(cidx, vals, factors, mode, out=None):
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    factors = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    nmodes, nnz = cidx.shape
+    rank = factors[0].shape[1]
+    if out is None:
+        out = np.zeros((factors[mode].shape[0], rank), dtype=np.float64)
+    lib().orc_mttkrp_coo(ctypes.c_int(nmodes), ctypes.c_uint64(nnz), _p(cidx, _u64p),
+                         _p(vals, _f64p), ctypes.c_int(rank), _ptr_array(factors),
+                         ctypes.c_int(mode), _p(out, _f64p))
+    return out
+
+
+def mttkrp_blco(enc, factors, mode, out=None):
+    factors = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    rank = factors[0].shape[1]
+    nmodes = len(factors)
+    if out is None:
+        out = np.zeros((factors[mode].shape[0], rank), dtype=np.float64)
+    masks = np.ascontiguousarray(enc["mode_masks"], dtype=np.uint64)
+    pos = np.ascontiguousarray(enc["mode_pos"], dtype=np.int32)
+    coords = np.ascontiguousarray(enc["coords"], dtype=np.uint64)
+    vals = np.ascontiguousarray(enc["vals"], dtype=np.float64)
+    lib().orc_mttkrp_blco(ctypes.c_int(nmodes), _p(masks, _u64p), _p(pos, _i32p),
+                          ctypes.c_uint64(len(coords)), _p(coords, _u64p), _p(vals, _f64p),
+                          ctypes.c_int(rank), _ptr_array(factors), ctypes.c_int(mode),
+                          _p(out, _f64p))
+    return out
+
+
+def pinv_sym(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    p = np.zeros_like(a)
+    lib().orc_pinv_sym(ctypes.c_int(a.shape[0]), _p(a, _f64p), _p(p, _f64p))
+    return p
+
+
+def cpals(dims, enc, factors, lam, maxiter, tol):
+    """Oracle CP-ALS (GPU semantics).  factors/lam are updated in place;
+    returns the list of per-iteration fits."""
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    masks = np.ascontiguousarray(enc["mode_masks"], dtype=np.uint64)
+    pos = np.ascontiguousarray(enc["mode_pos"], dtype=np.int32)
+    coords = np.ascontiguousarray(enc["coords"], dtype=np.uint64)
+    vals = np.ascontiguousarray(enc["vals"], dtype=np.float64)
+    for f in factors:
+        assert f.flags.c_contiguous and f.dtype == np.float64
+    rank = factors[0].shape[1]
+    fits = np.zeros(max(maxiter, 1), dtype=np.float64)
+    it = lib().orc_cpals(ctypes.c_int(len(dims)), _p(dims, _u64p), _p(masks, _u64p),
+                         _p(pos, _i32p), ctypes.c_uint64(len(coords)), _p(coords, _u64p),
+                         _p(vals, _f64p), ctypes.c_int(rank), _ptr_array(factors),
+                         _p(lam, _f64p), ctypes.c_int(maxiter), ctypes.c_double(tol),
+                         _p(fits, _f64p))
+    return list(fits[:it])
+
+
+def kruskal_random_init(dims, rank, seed, nthreads):
+    factors = [np.zeros((int(d), rank), dtype=np.float64) for d in dims]
+    lam = np.zeros(rank, dtype=np.float64)
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    lib().orc_kruskal_random_init(ctypes.c_int(len(dims)), _p(dims, _u64p), ctypes.c_int(rank),
+                                  ctypes.c_uint(seed), ctypes.c_int(nthreads),
+                                  _ptr_array(factors), _p(lam, _f64p))
+    return factors, lam

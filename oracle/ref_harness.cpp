@@ -1,0 +1,189 @@
+// ref_harness.cpp -- builds the reference's own CPU code into oracle/_ref.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is compiled together with the
+// reference's headers and src/{sptensor,kruskal_model,common}.cpp, read in
+// place from the reference checkout (oracle/Makefile, target `ref`).  It
+// exposes a small extern "C" surface so tests and bench.py's CPU-baseline
+// leg can run:
+//   * the reference BLCO encoder gen_blcotensor_host<uint64>
+//     (include/blco.hpp:196-331),
+//   * the reference sequential COO MTTKRP, the -c check oracle
+//     (include/cpd.hpp:510-544),
+//   * the reference OpenMP ALTO CPU MTTKRP mttkrp_alto_par
+//     (include/alto.hpp:544-550) on a create_alto tensor,
+//   * the reference KruskalModelRandomInit (src/kruskal_model.cpp:93-110).
+// The reference's BLAS/LAPACK CP-ALS (include/cpd.hpp) needs an external
+// BLAS and is not built: its BLAS symbols are stubs that abort.
+//
+// Stand-ins needed to run the reference host code without a GPU driver:
+//   * cudaHostAlloc/cudaMallocHost/cudaFreeHost map to malloc/free;
+//   * AlignedMalloc zero-fills, because gen_alto leaves prtn_ptr,
+//     prtn_intervals and cr_masks uninitialised and destroy_alto frees them
+//     (include/alto.hpp:118, 248-250).
+#include <stdlib.h>
+#include <string.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+
+static int refh_zero_memalign(void** p, size_t a, size_t n)
+{
+    int r = posix_memalign(p, a, n ? n : 1);
+    if (r == 0) memset(*p, 0, n);
+    return r;
+}
+#define posix_memalign refh_zero_memalign
+#include "common.hpp"
+#undef posix_memalign
+
+#include "sptensor.hpp"
+#include "kruskal_model.hpp"
+#include "alto.hpp"
+#include "blco.hpp"
+#include "cpd.hpp"
+
+extern "C" cudaError_t cudaHostAlloc(void** p, size_t n, unsigned int)
+{
+    *p = malloc(n ? n : 1);
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+extern "C" cudaError_t cudaMallocHost(void** p, size_t n) { return cudaHostAlloc(p, n, 0); }
+extern "C" cudaError_t cudaFreeHost(void* p) { free(p); return cudaSuccess; }
+extern "C" const char* cudaGetErrorString(cudaError_t) { return "host stand-in error"; }
+
+void check_cuda(cudaError_t status, std::string message)
+{
+    if (status != cudaSuccess) {
+        fprintf(stderr, "ref_harness: %s failed\n", message.c_str());
+        abort();
+    }
+}
+
+extern "C" void cblas_dsyrk(CBLAS_ORDER, CBLAS_UPLO, CBLAS_TRANSPOSE, long, long, double,
+                            const double*, long, double, double*, long) { abort(); }
+extern "C" void dpotrf_(char*, lapack_int*, double*, lapack_int*, lapack_int*) { abort(); }
+extern "C" void dpotrs_(char*, lapack_int*, lapack_int*, double*, lapack_int*, double*,
+                        lapack_int*, lapack_int*) { abort(); }
+extern "C" void dgelsy_(lapack_int*, lapack_int*, lapack_int*, double*, lapack_int*, double*,
+                        lapack_int*, lapack_int*, double*, lapack_int*, double*, lapack_int*,
+                        lapack_int*) { abort(); }
+
+static SparseTensor* refh_make_tensor(int nmodes, const uint64_t* dims, uint64_t nnz,
+                                      const uint64_t* cidx, const double* vals)
+{
+    SparseTensor* X = (SparseTensor*)AlignedMalloc(sizeof(SparseTensor));
+    X->nmodes = nmodes;
+    X->nnz = nnz;
+    X->dims = (IType*)AlignedMalloc(sizeof(IType) * nmodes);
+    X->cidx = (IType**)AlignedMalloc(sizeof(IType*) * nmodes);
+    for (int n = 0; n < nmodes; n++) {
+        X->dims[n] = dims[n];
+        X->cidx[n] = (IType*)AlignedMalloc(sizeof(IType) * (nnz ? nnz : 1));
+        memcpy(X->cidx[n], cidx + (size_t)n * nnz, sizeof(IType) * nnz);
+    }
+    X->vals = (FType*)AlignedMalloc(sizeof(FType) * (nnz ? nnz : 1));
+    memcpy(X->vals, vals, sizeof(FType) * nnz);
+    return X;
+}
+
+extern "C" int ref_blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
+                               const uint64_t* cidx, const double* vals,
+                               uint64_t max_block_size, uint64_t* coords_out,
+                               double* vals_out, uint64_t* mode_masks_out,
+                               int* mode_pos_out, uint64_t* nblocks_out,
+                               uint64_t* block_offsets_out, uint64_t* block_coords_out)
+{
+    SparseTensor* X = refh_make_tensor(nmodes, dims, nnz, cidx, vals);
+    blcotensor* T = gen_blcotensor_host<unsigned long long>(X, max_block_size);
+    memcpy(coords_out, T->coords, sizeof(uint64_t) * nnz);
+    memcpy(vals_out, T->values, sizeof(double) * nnz);
+    for (int n = 0; n < nmodes; n++) {
+        mode_masks_out[n] = T->mode_masks[n];
+        mode_pos_out[n] = T->mode_pos[n];
+    }
+    *nblocks_out = T->block_count;
+    for (IType b = 0; b < T->block_count; b++) {
+        block_offsets_out[b] = (uint64_t)(T->blocks[b]->idx - T->coords);
+        for (int n = 0; n < nmodes; n++)
+            block_coords_out[b * nmodes + n] = T->blocks[b]->block_coords[n];
+        free(T->blocks[b]->block_coords);
+        delete T->blocks[b];
+    }
+    block_offsets_out[T->block_count] = nnz;
+    delete[] T->blocks;
+    free(T->coords);
+    free(T->values);
+    delete[] T->modes;
+    delete[] T->mode_pos;
+    delete[] T->mode_masks;
+    delete T;
+    DestroySparseTensor(X);
+    return 0;
+}
+
+extern "C" void ref_mttkrp_coo(int nmodes, const uint64_t* dims, uint64_t nnz,
+                               const uint64_t* cidx, const double* vals, int rank,
+                               double* const* factors, int mode)
+{
+    // The reference accumulates into U[mode] in place.
+    SparseTensor* X = refh_make_tensor(nmodes, dims, nnz, cidx, vals);
+    KruskalModel M;
+    M.mode = nmodes;
+    M.dims = X->dims;
+    M.rank = rank;
+    M.U = (FType**)factors;
+    M.lambda = nullptr;
+    M.U_dev = nullptr;
+    mttkrp(X, &M, (IType)mode);
+    DestroySparseTensor(X);
+}
+
+extern "C" void ref_kruskal_random_init(int nmodes, const uint64_t* dims, int rank,
+                                        unsigned int seed, double* const* factors,
+                                        double* lambda)
+{
+    KruskalModel* M;
+    CreateKruskalModel(nmodes, (IType*)dims, rank, &M);
+    KruskalModelRandomInit(M, seed);
+    for (int n = 0; n < nmodes; n++)
+        memcpy(factors[n], M->U[n], sizeof(double) * dims[n] * rank);
+    memcpy(lambda, M->lambda, sizeof(double) * rank);
+    DestroyKruskalModel(M);
+}
+
+struct refh_alto {
+    AltoTensor<unsigned long long>* at;
+    FType** ofibs;
+    int target;
+};
+
+extern "C" void* ref_alto_create(int nmodes, const uint64_t* dims, uint64_t nnz,
+                                 const uint64_t* cidx, const double* vals, int nprtn)
+{
+    SparseTensor* X = refh_make_tensor(nmodes, dims, nnz, cidx, vals);
+    refh_alto* h = new refh_alto;
+    create_alto(X, &h->at, nprtn);
+    h->ofibs = nullptr;
+    h->target = -2;
+    DestroySparseTensor(X);
+    return h;
+}
+
+// out-of-place wrapper of mttkrp_alto_par: factors[mode] receives += MTTKRP.
+extern "C" void ref_alto_mttkrp(void* hv, int mode, int rank, double* const* factors)
+{
+    refh_alto* h = (refh_alto*)hv;
+    if (h->ofibs == nullptr) {
+        create_da_mem(-1, rank, h->at, &h->ofibs);
+        h->target = -1;
+    }
+    mttkrp_alto_par(mode, (FType**)factors, (IType)rank, h->at, nullptr, h->ofibs);
+}
+
+extern "C" void ref_alto_destroy(void* hv, int rank)
+{
+    refh_alto* h = (refh_alto*)hv;
+    if (h->ofibs) destroy_da_mem(h->at, h->ofibs, rank, -1);
+    destroy_alto(h->at);
+    delete h;
+}

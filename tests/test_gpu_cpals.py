@@ -1,0 +1,119 @@
+"""GPU parity of CP-ALS (through the C ABI) against the oracle's
+restatement of cpals_blco_dev (src/cpd_gpu.cu:21-242).
+
+Tolerances: per-iteration fits within 1e-10 absolute and factors within
+1e-9 relative (Frobenius).  The GPU MTTKRP sums with FP64 atomics in a
+different order from the oracle, and the GPU solves the normal equations by
+Cholesky where the oracle uses a Jacobi eigen pseudoinverse, so the two
+differ by rounding amplified by the conditioning of the ALS steps; the
+reference itself is not bitwise reproducible across runs for the same
+reason.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import unique_coords
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_both(blco, dims, cidx, vals, R, iters, tol, seed, kernel=10):
+    rng = np.random.default_rng(seed)
+    fs0 = [rng.random((d, R)) for d in dims]
+    enc = po.blco_encode(dims, cidx, vals)
+    fo = [f.copy() for f in fs0]
+    lo = np.ones(R)
+    fits_o = po.cpals(dims, enc, fo, lo, iters, tol)
+    t = blco.Tensor.encode(dims, cidx, vals)
+    fg = [f.copy() for f in fs0]
+    lg = np.ones(R)
+    fit_g, fits_g = blco.cpals(t, fg, lg, iters, tol, blco.make_opts(kernel=kernel))
+    return fits_o, fo, lo, fits_g, fg, lg, fit_g
+
+
+@pytest.mark.parametrize("kernel", [1, 2, 10])
+def test_cpals_matches_oracle_small_uniform(blco, kernel):
+    """The CPU-runnable workload's shape (1000 x 800 x 600, unique uniform
+    coordinates, U(0,1) values, rank 16, 20 iterations, tol 0) at 20k
+    nonzeros so the oracle finishes in seconds."""
+    from blco_b200 import synth
+    X = synth.uniform_tensor_host(20_000, [1000, 800, 600], seed=0)
+    fits_o, fo, lo, fits_g, fg, lg, fit_g = _run_both(blco, X["dims"], X["cidx"], X["vals"], 16, 20, 0.0, 1, kernel)
+    assert len(fits_g) == len(fits_o) == 20
+    assert np.allclose(fits_g, fits_o, rtol=0, atol=1e-10), np.max(np.abs(np.array(fits_g) - fits_o))
+    assert fit_g == fits_g[-1]
+    for a, b in zip(fg, fo):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+    assert np.allclose(lg, lo, rtol=1e-9)
+
+
+def test_cpals_matches_oracle_skewed_4mode(blco):
+    rng = np.random.default_rng(3)
+    dims = [3000, 800, 200, 50]
+    cidx = unique_coords(rng, dims, 40_000, zipf=0.9)
+    vals = rng.random(40_000)
+    fits_o, fo, lo, fits_g, fg, lg, _ = _run_both(blco, dims, cidx, vals, 8, 10, 0.0, 2)
+    assert np.allclose(fits_g, fits_o, rtol=0, atol=1e-10)
+    for a, b in zip(fg, fo):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+
+
+def test_cpals_convergence_stop_matches(blco):
+    rng = np.random.default_rng(4)
+    dims = [200, 150, 100]
+    cidx = unique_coords(rng, dims, 10_000)
+    vals = rng.random(10_000)
+    fits_o, _, _, fits_g, _, _, _ = _run_both(blco, dims, cidx, vals, 4, 100, 1e-4, 5)
+    assert len(fits_o) < 100
+    assert len(fits_g) == len(fits_o)
+    assert np.allclose(fits_g, fits_o, atol=1e-10)
+
+
+def test_cpals_rank_deficient_uses_pseudoinverse(blco):
+    """Two equal columns in every initial factor make every Gram, and so the
+    Hadamard product V, singular: the update must fall back to the
+    eigen-based pseudoinverse with the reference cut-off, like the oracle."""
+    rng = np.random.default_rng(6)
+    dims = [60, 50, 40]
+    cidx = unique_coords(rng, dims, 3000)
+    vals = rng.random(3000)
+    R = 4
+    fs0 = []
+    for d in dims:
+        f = rng.random((d, R))
+        f[:, 3] = f[:, 2]
+        fs0.append(f)
+    enc = po.blco_encode(dims, cidx, vals)
+    fo = [f.copy() for f in fs0]
+    lo = np.ones(R)
+    fits_o = po.cpals(dims, enc, fo, lo, 3, 0.0)
+    t = blco.Tensor.encode(dims, cidx, vals)
+    fg = [f.copy() for f in fs0]
+    lg = np.ones(R)
+    _, fits_g = blco.cpals(t, fg, lg, 3, 0.0)
+    assert np.allclose(fits_g, fits_o, atol=1e-8), (fits_g, fits_o)
+    for a, b in zip(fg, fo):
+        assert np.linalg.norm(a - b) <= 1e-7 * np.linalg.norm(b)
+
+
+def test_cpals_plan_device_factors(blco):
+    import torch
+    from blco_b200 import synth
+    X = synth.uniform_tensor_host(30_000, [500, 400, 300], seed=3)
+    R = 16
+    rng = np.random.default_rng(8)
+    fs0 = [rng.random((d, R)) for d in X["dims"]]
+    t = blco.Tensor.encode(X["dims"], X["cidx"], X["vals"])
+    dfs = [torch.from_numpy(f.copy()).cuda() for f in fs0]
+    dl = torch.ones(R, dtype=torch.float64, device="cuda")
+    plan = blco.CpalsPlan(t, dfs, dl)
+    fits_a = plan.iterate(3)
+    fits_b = plan.iterate(2)
+    ms, calls = plan.mttkrp_ms()
+    assert calls == 5 and np.all(ms > 0)
+    plan.destroy()
+    enc = po.blco_encode(X["dims"], X["cidx"], X["vals"])
+    fo = [f.copy() for f in fs0]
+    fits_o = po.cpals(X["dims"], enc, fo, np.ones(R), 5, -1.0)
+    assert np.allclose(fits_a + fits_b, fits_o, atol=1e-10)
