@@ -55,19 +55,11 @@ int device_info(int device, DeviceInfo* out)
     return BLCO_OK;
 }
 
-cudaStream_t pick_stream(const blco_tensor* t, const blco_opts* opts)
+cudaStream_t pick_stream(const blco_tensor*, const blco_opts* opts)
 {
-    if (opts && opts->stream) return (cudaStream_t)opts->stream;
-    if (t && t->own_stream) return t->own_stream;
-    if (t) {
-        blco_tensor* tm = const_cast<blco_tensor*>(t);
-        if (cudaStreamCreateWithFlags(&tm->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
-            set_error("cudaStreamCreate failed");
-            return nullptr;
-        }
-        return tm->own_stream;
-    }
-    return nullptr;
+    // NULL selects the default stream, so work is ordered with the caller's
+    // other default-stream work.
+    return opts ? (cudaStream_t)opts->stream : (cudaStream_t)0;
 }
 
 // Streamed MTTKRP: the blocks stay in pinned host memory; they are copied
@@ -235,7 +227,7 @@ int blco_tensor_free(blco_tensor* t)
 {
     if (!t) return BLCO_OK;
     cudaSetDevice(t->device);
-    if (t->own_stream) cudaStreamSynchronize(t->own_stream);
+    cudaDeviceSynchronize();
     cudaFree(t->d_coords);
     cudaFree(t->d_values);
     cudaFree(t->d_values_f32);
@@ -246,7 +238,6 @@ int blco_tensor_free(blco_tensor* t)
         cudaFree(t->hot[n].d_slot);
         cudaFree(t->hot[n].d_rows);
     }
-    if (t->own_stream) cudaStreamDestroy(t->own_stream);
     delete t;
     return BLCO_OK;
 }
@@ -315,7 +306,6 @@ int blco_mttkrp(blco_tensor* t, int mode, int rank, const double* const* d_facto
         if (m != mode && !d_factors[m]) return fail(BLCO_ERR_INVALID, "null factor matrix");
     BLCO_CUDA(cudaSetDevice(t->device));
     cudaStream_t s = pick_stream(t, opts);
-    if (!s) return BLCO_ERR_CUDA;
     MttkrpArgs a;
     memset(&a, 0, sizeof(a));
     a.nnz = t->nnz;
@@ -339,7 +329,6 @@ int blco_mttkrp_host(blco_tensor* t, int mode, int rank, const double* const* fa
     if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
     BLCO_CUDA(cudaSetDevice(t->device));
     cudaStream_t s = pick_stream(t, opts);
-    if (!s) return BLCO_ERR_CUDA;
     const int N = t->layout.nmodes;
     double* df[BLCO_MAX_MODES] = {};
     int st = BLCO_OK;

@@ -318,6 +318,7 @@ __global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, i
                 __syncthreads();
             }
         }
+        __syncthreads(); // every thread has read off_s before thread 0 rewrites it
     }
     __shared__ double smax;
     if (tid == 0) {

@@ -606,7 +606,6 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
     cudaError_t e = cudaSetDevice(t->device);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(e, "cudaSetDevice", __FILE__, __LINE__));
     cudaStream_t s = pick_stream(t, opts);
-    if (!s) return cleanup_fail(last_error()[0] ? BLCO_ERR_CUDA : BLCO_ERR_CUDA);
 
     uint64_t n_alloc = nnz ? nnz : 1;
     uint64_t *k0 = nullptr, *k1 = nullptr;

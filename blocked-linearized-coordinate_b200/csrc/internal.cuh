@@ -108,7 +108,6 @@ struct blco_tensor {
     blco::HotTable hot[BLCO_MAX_MODES];
     blco::ModeStats stats[BLCO_MAX_MODES];
     double norm_sq = 0.0; // sum of squared values
-    cudaStream_t own_stream = nullptr;
 };
 
 namespace blco {

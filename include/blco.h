@@ -79,7 +79,7 @@ typedef struct blco_opts {
     int verbose;           /* print the reference's progress lines */
     int device;            /* --device */
     uint64_t residency_bytes; /* device budget for streamed blocks; 0 = 8 GiB */
-    void* stream;          /* cudaStream_t to run on; NULL = library stream */
+    void* stream;          /* cudaStream_t to run on; NULL = the default stream */
 } blco_opts;
 
 typedef struct blco_tensor blco_tensor; /* opaque */
