@@ -41,12 +41,17 @@ KERNEL_ATOMIC = 13
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_MIXED_BF16 = 2
+
+DTYPE_F64 = 0
+DTYPE_F32 = 1
+DTYPE_BF16 = 2
 
 # Every symbol include/blco.h declares.
 EXPORTS = (
     "blco_opts_init", "blco_status_string", "blco_last_error", "blco_version",
     "blco_encode", "blco_encode_device", "blco_tensor_free", "blco_tensor_get_info",
-    "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_host",
+    "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_ex", "blco_mttkrp_host",
     "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
     "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_launch_count",
 )
@@ -113,6 +118,7 @@ def lib():
         L.blco_tensor_device_arrays.argtypes = [vp, vp, vp]
         L.blco_mttkrp.argtypes = [vp, i32, i32, vp, vp, vp]
         L.blco_mttkrp_host.argtypes = [vp, i32, i32, vp, vp, vp]
+        L.blco_mttkrp_ex.argtypes = [vp, i32, i32, i32, vp, vp, vp]
         L.blco_cpals.argtypes = [vp, i32, vp, vp, i32, f64, vp, vp, vp, vp]
         L.blco_cpals_plan_create.argtypes = [vp, i32, vp, vp, vp, vp]
         L.blco_cpals_plan_iterate.argtypes = [vp, i32, f64, vp, vp]
@@ -238,6 +244,15 @@ def mttkrp(t, mode, factors, out, opts=None):
     ptrs = _ptrs([int(f.data_ptr()) if f is not None else 0 for f in factors])
     o = opts if opts is not None else make_opts()
     _check(lib().blco_mttkrp(t.handle, mode, rank, ptrs, int(out.data_ptr()), ctypes.byref(o)))
+
+
+def mttkrp_ex(t, mode, factors, out, factor_dtype, opts=None):
+    """Mixed-precision MTTKRP: out (torch CUDA float32) += MTTKRP with
+    torch CUDA float32 or bfloat16 factors."""
+    rank = int(out.shape[1])
+    ptrs = _ptrs([int(f.data_ptr()) if f is not None else 0 for f in factors])
+    o = opts if opts is not None else make_opts()
+    _check(lib().blco_mttkrp_ex(t.handle, mode, rank, factor_dtype, ptrs, int(out.data_ptr()), ctypes.byref(o)))
 
 
 def mttkrp_host(t, mode, factors, out=None, opts=None):

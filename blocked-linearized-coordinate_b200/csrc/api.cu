@@ -313,11 +313,45 @@ int blco_mttkrp(blco_tensor* t, int mode, int rank, const double* const* d_facto
     a.rank = rank;
     for (int m = 0; m < t->layout.nmodes; m++) a.factors[m] = d_factors[m];
     a.out = d_out;
+    a.factor_dtype = BLCO_DTYPE_F64;
     a.kernel = opts ? opts->kernel : BLCO_KERNEL_AUTO;
     a.thread_cf = opts ? opts->thread_cf : 2;
     if (!t->resident) return mttkrp_streamed(t, a, opts, s);
     a.coords = t->d_coords;
     a.vals = t->d_values;
+    return mttkrp_launch(t, a, s);
+}
+
+int blco_mttkrp_ex(blco_tensor* t, int mode, int rank, int factor_dtype, const void* const* d_factors,
+                   void* d_out, const blco_opts* opts)
+{
+    if (factor_dtype == BLCO_DTYPE_F64)
+        return blco_mttkrp(t, mode, rank, reinterpret_cast<const double* const*>(d_factors),
+                           reinterpret_cast<double*>(d_out), opts);
+    if (!t || !d_factors || !d_out) return fail(BLCO_ERR_INVALID, "null argument");
+    if (factor_dtype != BLCO_DTYPE_F32 && factor_dtype != BLCO_DTYPE_BF16)
+        return fail(BLCO_ERR_INVALID, "factor_dtype must be BLCO_DTYPE_F32 or BLCO_DTYPE_BF16");
+    if (mode < 0 || mode >= t->layout.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
+    if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
+    if (!t->resident) return fail(BLCO_ERR_UNSUPPORTED, "mixed-precision MTTKRP needs a resident tensor");
+    for (int m = 0; m < t->layout.nmodes; m++)
+        if (m != mode && !d_factors[m]) return fail(BLCO_ERR_INVALID, "null factor matrix");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    cudaStream_t s = pick_stream(t, opts);
+    const float* v32 = nullptr;
+    BLCO_TRY(values_f32(t, s, &v32));
+    MttkrpArgs a;
+    memset(&a, 0, sizeof(a));
+    a.coords = t->d_coords;
+    a.vals = v32;
+    a.nnz = t->nnz;
+    a.mode = mode;
+    a.rank = rank;
+    for (int m = 0; m < t->layout.nmodes; m++) a.factors[m] = d_factors[m];
+    a.out = d_out;
+    a.factor_dtype = factor_dtype;
+    a.kernel = opts ? opts->kernel : BLCO_KERNEL_AUTO;
+    a.thread_cf = opts ? opts->thread_cf : 2;
     return mttkrp_launch(t, a, s);
 }
 

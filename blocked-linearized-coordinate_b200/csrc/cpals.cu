@@ -36,13 +36,13 @@ constexpr int MAX_SOLVE_R = 96; // k_solve keeps two R x R FP64 buffers in share
 // 8 up to R = 128, so that 256 threads cover the result).
 constexpr int GR_CH = 32; // rows staged per step
 
-template <bool SCALE, int TS>
-__global__ __launch_bounds__(DN_THREADS) void k_gram(double* __restrict__ U, uint64_t I, int R,
+template <typename T, bool SCALE, int TS>
+__global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t I, int R,
                                                      const double* __restrict__ inv, double* __restrict__ partials)
 {
     extern __shared__ __align__(16) double gs[];
-    double* tile = gs;                 // GR_CH x R
-    double* red = gs + GR_CH * R;      // R x R reduction buffer
+    double* red = gs;                                 // R x R reduction buffer
+    T* tile = reinterpret_cast<T*>(gs + R * R);       // GR_CH x R
     const int tpr = (R + TS - 1) / TS; // tiles per row of the result
     const int ntile = tpr * tpr;
     const int groups = max(1, DN_THREADS / ntile);
@@ -62,9 +62,9 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(double* __restrict__ U, uin
         const int nr = (int)min((uint64_t)GR_CH, end - r0);
         __syncthreads();
         for (int k = tid; k < nr * R; k += DN_THREADS) {
-            double v = U[r0 * R + k];
+            T v = U[r0 * R + k];
             if (SCALE) {
-                v *= inv[k % R];
+                v = (T)((double)v * inv[k % R]);
                 U[r0 * R + k] = v;
             }
             tile[k] = v;
@@ -74,12 +74,12 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(double* __restrict__ U, uin
             // Tiles that reach past R read columns clamped to R-1 and are
             // discarded at the end.
             for (int r = g; r < nr; r += groups) {
-                const double* row = tile + r * R;
+                const T* row = tile + r * R;
                 double va[TS], vb[TS];
 #pragma unroll
                 for (int x = 0; x < TS; x++) {
-                    va[x] = row[min(a0 + x, R - 1)];
-                    vb[x] = row[min(b0 + x, R - 1)];
+                    va[x] = (double)row[min(a0 + x, R - 1)];
+                    vb[x] = (double)row[min(b0 + x, R - 1)];
                 }
 #pragma unroll
                 for (int x = 0; x < TS; x++)
@@ -120,17 +120,18 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int nblocks,
 // squares of U.  A warp computes a row; lane c owns columns c, c+32, ...
 constexpr int UP_MAXC = 4; // R <= 128
 
-__global__ __launch_bounds__(DN_THREADS) void k_update(const double* __restrict__ M, const double* __restrict__ P,
-                                                       double* __restrict__ U, uint64_t I, int R,
+template <typename T>
+__global__ __launch_bounds__(DN_THREADS) void k_update(const T* __restrict__ M, const double* __restrict__ P,
+                                                       T* __restrict__ U, uint64_t I, int R,
                                                        double* __restrict__ colsq_partials)
 {
     extern __shared__ __align__(16) double us[];
-    double* PT = us;              // PT[k][c] = P[c][k]
-    double* csq = us + R * R;     // [warps][R]
+    double* csq = us;                                   // [warps][R]
+    T* PT = reinterpret_cast<T*>(us + (DN_THREADS / 32) * R); // PT[k][c] = P[c][k]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = DN_THREADS / 32;
     for (int k = tid; k < R * R; k += DN_THREADS) {
         int c = k / R, kk = k % R;
-        PT[kk * R + c] = P[k];
+        PT[kk * R + c] = (T)P[k];
     }
     __syncthreads();
     double sq[UP_MAXC];
@@ -139,20 +140,20 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const double* __restrict_
     const uint64_t per = (I + gridDim.x - 1) / gridDim.x;
     const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
     for (uint64_t i = beg + warp; i < end; i += nw) {
-        const double* mrow = M + i * R;
-        double mreg[UP_MAXC];
+        const T* mrow = M + i * R;
+        T mreg[UP_MAXC];
 #pragma unroll
-        for (int j = 0; j < UP_MAXC; j++) mreg[j] = (lane + 32 * j < R) ? mrow[lane + 32 * j] : 0.0;
-        double acc[UP_MAXC];
+        for (int j = 0; j < UP_MAXC; j++) mreg[j] = (lane + 32 * j < R) ? mrow[lane + 32 * j] : T(0);
+        T acc[UP_MAXC];
 #pragma unroll
-        for (int j = 0; j < UP_MAXC; j++) acc[j] = 0.0;
+        for (int j = 0; j < UP_MAXC; j++) acc[j] = T(0);
 #pragma unroll
         for (int kb = 0; kb < UP_MAXC; kb++) {
             if (32 * kb >= R) break;
             const int kn = min(32, R - 32 * kb);
             for (int kk = 0; kk < kn; kk++) {
                 const int k = 32 * kb + kk;
-                double mk = __shfl_sync(0xffffffffu, mreg[kb], kk);
+                T mk = __shfl_sync(0xffffffffu, mreg[kb], kk);
 #pragma unroll
                 for (int j = 0; j < UP_MAXC; j++) {
                     int c = lane + 32 * j;
@@ -165,7 +166,7 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const double* __restrict_
             int c = lane + 32 * j;
             if (c < R) {
                 U[i * R + c] = acc[j];
-                sq[j] += acc[j] * acc[j];
+                sq[j] += (double)acc[j] * (double)acc[j];
             }
         }
     }
@@ -345,7 +346,8 @@ __global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, i
 // ----------------------------------------------------------------- fit --
 // Per-block column sums of U[i][c] * M[i][c] (columnwise_inner_product,
 // src/cpd_gpu.cu:307-330).
-__global__ __launch_bounds__(DN_THREADS) void k_iprod(const double* __restrict__ U, const double* __restrict__ M,
+template <typename T>
+__global__ __launch_bounds__(DN_THREADS) void k_iprod(const T* __restrict__ U, const T* __restrict__ M,
                                                       uint64_t I, int R, double* __restrict__ partials)
 {
     extern __shared__ __align__(16) double ip[];
@@ -359,7 +361,7 @@ __global__ __launch_bounds__(DN_THREADS) void k_iprod(const double* __restrict__
 #pragma unroll
         for (int j = 0; j < UP_MAXC; j++) {
             int c = lane + 32 * j;
-            if (c < R) s[j] += U[i * R + c] * M[i * R + c];
+            if (c < R) s[j] += (double)U[i * R + c] * (double)M[i * R + c];
         }
     }
 #pragma unroll
@@ -431,9 +433,16 @@ int grid_rows(uint64_t I, int sm)
 struct blco_cpals_plan {
     blco_tensor* t = nullptr;
     int R = 0, N = 0;
-    double* U[BLCO_MAX_MODES] = {};
-    double* lambda = nullptr;
-    double* M = nullptr;
+    double* U[BLCO_MAX_MODES] = {};   // caller's FP64 factors
+    double* lambda = nullptr;         // caller's FP64 lambda
+    double* M = nullptr;              // MTTKRP result (FP64, plain form)
+    // mixed form working set
+    bool mixed = false;
+    int gather_dtype = BLCO_DTYPE_F64;
+    float* Uf[BLCO_MAX_MODES] = {};   // FP32 working factors
+    void* Ub[BLCO_MAX_MODES] = {};    // BF16 gather copies (BF16 gathers only)
+    float* Mf = nullptr;              // MTTKRP result (FP32)
+    const float* vals32 = nullptr;
     double* grams[BLCO_MAX_MODES] = {};
     double* P = nullptr;
     double* partials = nullptr; // max(grid) * R * R
@@ -450,18 +459,44 @@ struct blco_cpals_plan {
     cudaEvent_t ev[2 * BLCO_MAX_MODES] = {};
     double mttkrp_ms[BLCO_MAX_MODES] = {};
     int mttkrp_calls = 0;
-    bool mixed = false;
 };
 
 namespace blco {
 namespace {
+
+__global__ void k_f64_to_f32(const double* __restrict__ in, float* __restrict__ out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+__global__ void k_f32_to_f64(const float* __restrict__ in, double* __restrict__ out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+// Round-to-nearest-even FP32 -> BF16 (the BF16 bits are the high half).
+__global__ void k_f32_to_bf16(const float* __restrict__ in, uint16_t* __restrict__ out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t x = __float_as_uint(in[i]);
+        uint32_t r = x + 0x7fffu + ((x >> 16) & 1u);
+        out[i] = (uint16_t)(r >> 16);
+    }
+}
 
 int plan_free(blco_cpals_plan* p)
 {
     if (!p) return BLCO_OK;
     if (p->s) cudaStreamSynchronize(p->s);
     cudaFree(p->M);
-    for (int n = 0; n < BLCO_MAX_MODES; n++) cudaFree(p->grams[n]);
+    cudaFree(p->Mf);
+    for (int n = 0; n < BLCO_MAX_MODES; n++) {
+        cudaFree(p->grams[n]);
+        cudaFree(p->Uf[n]);
+        cudaFree(p->Ub[n]);
+    }
     cudaFree(p->P);
     cudaFree(p->partials);
     cudaFree(p->inv);
@@ -473,14 +508,15 @@ int plan_free(blco_cpals_plan* p)
     return BLCO_OK;
 }
 
-int gram_launch(blco_cpals_plan* p, double* U, uint64_t I, const double* inv, double* G)
+template <typename T>
+int gram_launch(blco_cpals_plan* p, T* U, uint64_t I, const double* inv, double* G)
 {
     const int R = p->R;
     int grid = grid_rows(I, p->sm);
-    size_t smem = (size_t)(GR_CH * R + R * R) * sizeof(double);
-    void (*fn)(double*, uint64_t, int, const double*, double*);
-    if (R <= 64) fn = inv ? k_gram<true, 4> : k_gram<false, 4>;
-    else fn = inv ? k_gram<true, 8> : k_gram<false, 8>;
+    size_t smem = (size_t)R * R * sizeof(double) + (size_t)GR_CH * R * sizeof(T);
+    void (*fn)(T*, uint64_t, int, const double*, double*);
+    if (R <= 64) fn = inv ? k_gram<T, true, 4> : k_gram<T, false, 4>;
+    else fn = inv ? k_gram<T, true, 8> : k_gram<T, false, 8>;
     BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     fn<<<grid, DN_THREADS, smem, p->s>>>(U, I, R, inv, p->partials);
     BLCO_CHECK_LAUNCH("k_gram");
@@ -489,23 +525,35 @@ int gram_launch(blco_cpals_plan* p, double* U, uint64_t I, const double* inv, do
     return BLCO_OK;
 }
 
+int conv_grid(uint64_t n, int sm) { return (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm * 8)); }
+
 int mode_update(blco_cpals_plan* p, int n)
 {
     blco_tensor* t = p->t;
     const int R = p->R, N = p->N;
     const uint64_t I = t->layout.dims[n];
-    BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
     MttkrpArgs a;
     memset(&a, 0, sizeof(a));
     a.coords = t->d_coords;
-    a.vals = t->d_values;
     a.nnz = t->nnz;
     a.mode = n;
     a.rank = R;
-    for (int m = 0; m < N; m++) a.factors[m] = p->U[m];
-    a.out = p->M;
     a.kernel = p->opts.kernel;
     a.thread_cf = p->opts.thread_cf;
+    if (p->mixed) {
+        BLCO_CUDA(cudaMemsetAsync(p->Mf, 0, I * R * sizeof(float), p->s));
+        a.vals = p->vals32;
+        for (int m = 0; m < N; m++)
+            a.factors[m] = p->gather_dtype == BLCO_DTYPE_BF16 ? (const void*)p->Ub[m] : (const void*)p->Uf[m];
+        a.out = p->Mf;
+        a.factor_dtype = p->gather_dtype;
+    } else {
+        BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
+        a.vals = t->d_values;
+        for (int m = 0; m < N; m++) a.factors[m] = p->U[m];
+        a.out = p->M;
+        a.factor_dtype = BLCO_DTYPE_F64;
+    }
     BLCO_CUDA(cudaEventRecord(p->ev[2 * n], p->s));
     BLCO_TRY(mttkrp_launch(t, a, p->s));
     BLCO_CUDA(cudaEventRecord(p->ev[2 * n + 1], p->s));
@@ -520,12 +568,25 @@ int mode_update(blco_cpals_plan* p, int n)
 
     int grid = grid_rows(I, p->sm);
     size_t usmem = (size_t)(R * R + (DN_THREADS / 32) * R) * sizeof(double);
-    BLCO_CUDA(cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
-    k_update<<<grid, DN_THREADS, usmem, p->s>>>(p->M, p->P, p->U[n], I, R, p->partials);
+    if (p->mixed) {
+        BLCO_CUDA(cudaFuncSetAttribute(k_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
+        k_update<float><<<grid, DN_THREADS, usmem, p->s>>>(p->Mf, p->P, p->Uf[n], I, R, p->partials);
+    } else {
+        BLCO_CUDA(cudaFuncSetAttribute(k_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
+        k_update<double><<<grid, DN_THREADS, usmem, p->s>>>(p->M, p->P, p->U[n], I, R, p->partials);
+    }
     BLCO_CHECK_LAUNCH("k_update");
     k_lambda<<<1, 128, 0, p->s>>>(p->partials, grid, R, p->lambda, p->inv);
     BLCO_CHECK_LAUNCH("k_lambda");
-    BLCO_TRY(gram_launch(p, p->U[n], I, p->inv, p->grams[n]));
+    if (p->mixed) {
+        BLCO_TRY(gram_launch<float>(p, p->Uf[n], I, p->inv, p->grams[n]));
+        if (p->gather_dtype == BLCO_DTYPE_BF16) {
+            k_f32_to_bf16<<<conv_grid(I * R, p->sm), 256, 0, p->s>>>(p->Uf[n], (uint16_t*)p->Ub[n], I * R);
+            BLCO_CHECK_LAUNCH("k_f32_to_bf16");
+        }
+    } else {
+        BLCO_TRY(gram_launch<double>(p, p->U[n], I, p->inv, p->grams[n]));
+    }
     return BLCO_OK;
 }
 
@@ -536,13 +597,26 @@ int fit_launch(blco_cpals_plan* p)
     const uint64_t I = p->t->layout.dims[lm];
     int grid = grid_rows(I, p->sm);
     size_t smem = (size_t)(DN_THREADS / 32) * R * sizeof(double);
-    k_iprod<<<grid, DN_THREADS, smem, p->s>>>(p->U[lm], p->M, I, R, p->partials);
+    if (p->mixed) k_iprod<float><<<grid, DN_THREADS, smem, p->s>>>(p->Uf[lm], p->Mf, I, R, p->partials);
+    else k_iprod<double><<<grid, DN_THREADS, smem, p->s>>>(p->U[lm], p->M, I, R, p->partials);
     BLCO_CHECK_LAUNCH("k_iprod");
     GramPtrs gp;
     memset(&gp, 0, sizeof(gp));
     for (int m = 0; m < N; m++) gp.g[m] = p->grams[m];
     k_fit<<<1, DN_THREADS, 0, p->s>>>(p->partials, grid, gp, N, R, p->lambda, p->xnorm, p->fit);
     BLCO_CHECK_LAUNCH("k_fit");
+    return BLCO_OK;
+}
+
+// Mixed form: FP32 working factors back into the caller's FP64 arrays.
+int export_factors(blco_cpals_plan* p)
+{
+    if (!p->mixed) return BLCO_OK;
+    for (int n = 0; n < p->N; n++) {
+        const uint64_t len = p->t->layout.dims[n] * (uint64_t)p->R;
+        k_f32_to_f64<<<conv_grid(len, p->sm), 256, 0, p->s>>>(p->Uf[n], p->U[n], len);
+        BLCO_CHECK_LAUNCH("k_f32_to_f64");
+    }
     return BLCO_OK;
 }
 
@@ -583,7 +657,20 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
             return _s;                                                         \
         }                                                                      \
     } while (0)
-    PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
+    p->mixed = p->opts.precision != BLCO_PRECISION_FP64;
+    p->gather_dtype = p->opts.precision == BLCO_PRECISION_MIXED_BF16 ? BLCO_DTYPE_BF16
+                      : p->mixed                                     ? BLCO_DTYPE_F32
+                                                                     : BLCO_DTYPE_F64;
+    if (p->mixed) {
+        PC(cudaMalloc(&p->Mf, std::max<uint64_t>(maxdim, 1) * R * sizeof(float)));
+        for (int n = 0; n < p->N; n++) {
+            const uint64_t len = t->layout.dims[n] * (uint64_t)R;
+            PC(cudaMalloc(&p->Uf[n], len * sizeof(float)));
+            if (p->gather_dtype == BLCO_DTYPE_BF16) PC(cudaMalloc(&p->Ub[n], len * 2));
+        }
+    } else {
+        PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
+    }
     for (int n = 0; n < p->N; n++) PC(cudaMalloc(&p->grams[n], (size_t)R * R * sizeof(double)));
     PC(cudaMalloc(&p->P, (size_t)R * R * sizeof(double)));
     PC(cudaMalloc(&p->partials, (size_t)gmax * R * R * sizeof(double)));
@@ -593,8 +680,23 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     for (auto& e : p->ev) PC(cudaEventCreate(&e));
 #undef PC
     p->xnorm = std::sqrt(t->norm_sq);
+    if (p->mixed) {
+        st = values_f32(t, p->s, &p->vals32);
+        if (st != BLCO_OK) { plan_free(p); return st; }
+    }
     for (int n = 0; n < p->N; n++) {
-        st = gram_launch(p, p->U[n], t->layout.dims[n], nullptr, p->grams[n]);
+        const uint64_t len = t->layout.dims[n] * (uint64_t)R;
+        if (p->mixed) {
+            k_f64_to_f32<<<conv_grid(len, p->sm), 256, 0, p->s>>>(p->U[n], p->Uf[n], len);
+            count_launch();
+            if (p->gather_dtype == BLCO_DTYPE_BF16) {
+                k_f32_to_bf16<<<conv_grid(len, p->sm), 256, 0, p->s>>>(p->Uf[n], (uint16_t*)p->Ub[n], len);
+                count_launch();
+            }
+            st = gram_launch<float>(p, p->Uf[n], t->layout.dims[n], nullptr, p->grams[n]);
+        } else {
+            st = gram_launch<double>(p, p->U[n], t->layout.dims[n], nullptr, p->grams[n]);
+        }
         if (st != BLCO_OK) { plan_free(p); return st; }
     }
     // Descending mode length, ties in natural order (src/cpd_gpu.cu:137-139).
@@ -649,6 +751,7 @@ int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* i
     }
     cudaEventDestroy(it0);
     cudaEventDestroy(it1);
+    if (st == BLCO_OK) st = export_factors(p);
     if (iters_done) *iters_done = done;
     return st;
 }

@@ -121,19 +121,25 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz,
 int build_hot_tables(blco_tensor* t, cudaStream_t s);
 
 // mttkrp.cu
+// factor_dtype selects the precision policy: BLCO_DTYPE_F64 (FP64 values,
+// factors and output) or BLCO_DTYPE_F32 / BLCO_DTYPE_BF16 (FP32 values and
+// output, FP32 or BF16 factors).
 struct MttkrpArgs {
     const uint64_t* coords;
-    const double* vals;
+    const void* vals;
     uint64_t nnz;
     int mode;
     int rank;
-    const double* factors[BLCO_MAX_MODES];
-    double* out;
+    const void* factors[BLCO_MAX_MODES];
+    void* out;
+    int factor_dtype;
     int kernel;
     int thread_cf;
 };
 int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
-int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested);
+int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested, int factor_dtype);
+// FP32 copy of the resident values (created on first use).
+int values_f32(blco_tensor* t, cudaStream_t s, const float** out);
 
 // cpals.cu
 int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_lambda, const blco_opts* opts,

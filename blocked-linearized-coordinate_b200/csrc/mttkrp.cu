@@ -1,4 +1,4 @@
-// mttkrp.cu -- sparse MTTKRP over the 64-bit BLCO stream (plain FP64 form).
+// mttkrp.cu -- sparse MTTKRP over the 64-bit BLCO stream.
 //
 //   out[r_t(i), :] += val_i * prod_{m != t} U_m[r_m(i), :]
 //
@@ -8,16 +8,26 @@
 //   * persistent CTAs, one per SM (grid = SM count), each owning one
 //     contiguous slice of the ALTO-ordered stream, 24 warps per CTA;
 //   * a warp takes 32 nonzeros, decodes rows with shifts and masks
-//     (alt_pext, src/alto_dev.cu:13-16), groups equal output rows with
-//     __match_any_sync and orders the tile by group (counting sort in
-//     registers + a per-warp shared staging area);
-//   * factor rows are gathered with 128-bit loads: R/2 lanes per nonzero,
-//     two FP64 columns per lane, several nonzeros in flight per warp;
+//     (alt_pext, src/alto_dev.cu:13-16), looks each output row up in the
+//     mode's heavy-row table once, groups equal output rows with
+//     __match_any_sync and writes the tile in row order into a per-warp
+//     shared staging area as packed 32-byte records (two 16-byte loads per
+//     record; the slot ranges are offset by 16 bytes so concurrent slots hit
+//     different banks);
+//   * factor rows are gathered with 128-bit loads: R/VEC lanes per nonzero
+//     (VEC = 2 FP64, 4 FP32 or 8 BF16 columns per load), several nonzeros in
+//     flight per warp;
 //   * runs of equal output rows are summed in registers and flushed once:
-//     into a shared-memory accumulator when the row is one of the mode's
-//     heaviest rows (a per-CTA privatised copy, written back once per CTA),
-//     or into the whole output when the mode is short enough to fit
-//     (the lvl3 role), otherwise with FP64 global atomics (red.global).
+//     into a per-CTA shared-memory accumulator when the row is one of the
+//     mode's heaviest rows (written back once per CTA), or into the whole
+//     output when the mode is short enough to fit (the lvl3 role), otherwise
+//     with global atomics (FP64 red, or 4-wide FP32 vector red).
+// Precision policies:
+//   PolicyF64   plain form: FP64 values, factors, accumulation and output;
+//   PolicyF32   mixed form: FP32 values, FP32 factor gathers, FP32 output;
+//   PolicyBF16  mixed form: FP32 values, BF16 factor gathers, FP32 output.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cstring>
 
@@ -28,14 +38,44 @@ namespace {
 
 constexpr int MT_THREADS = 768; // 24 warps, one CTA per SM
 constexpr int MT_WARPS = MT_THREADS / 32;
-constexpr int MT_UNROLL = 4;
+constexpr int REC_BYTES = 32;
+
+__global__ void k_to_f32(const double* __restrict__ in, float* __restrict__ out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+// VEC: columns per 16-byte gather; UNROLL: nonzeros whose gathers are in
+// flight per slot (bounded by the registers the gathered values take).
+struct PolicyF64 {
+    typedef double TV;
+    typedef double TF;
+    typedef double TA;
+    static constexpr int VEC = 2;
+    static constexpr int UNROLL = 4;
+};
+struct PolicyF32 {
+    typedef float TV;
+    typedef float TF;
+    typedef float TA;
+    static constexpr int VEC = 4;
+    static constexpr int UNROLL = 4;
+};
+struct PolicyBF16 {
+    typedef float TV;
+    typedef __nv_bfloat16 TF;
+    typedef float TA;
+    static constexpr int VEC = 8;
+    static constexpr int UNROLL = 2;
+};
 
 struct MtParams {
     const uint64_t* coords;
-    const double* vals;
+    const void* vals;
     uint64_t nnz;
-    const double* f[BLCO_MAX_MODES];
-    double* out;
+    const void* f[BLCO_MAX_MODES];
+    void* out;
     uint64_t mask[BLCO_MAX_MODES];
     int pos[BLCO_MAX_MODES];
     int mode;
@@ -73,15 +113,6 @@ __device__ __forceinline__ int hot_lookup(const MtParams& p, const uint32_t* ske
     return -1;
 }
 
-// Shared memory: [hash keys | hash slots] [accumulator nhot x R doubles]
-// [per-warp staging].
-template <int NM>
-struct Stage {
-    uint32_t row[32];
-    uint32_t oth[NM > 1 ? NM - 1 : 1][32];
-    double val[32];
-};
-
 // Per-thread copy of the target/other mode fields, resolved once with
 // compile-time indices so the hot loop keeps them in registers.
 template <int NM>
@@ -91,7 +122,7 @@ struct ModeSel {
     uint64_t tmask;
     int opos[NO];
     uint64_t omask[NO];
-    const double* of[NO];
+    const void* of[NO];
 
     __device__ __forceinline__ explicit ModeSel(const MtParams& p)
     {
@@ -103,6 +134,12 @@ struct ModeSel {
                 tpos = p.pos[m];
                 tmask = p.mask[m];
             }
+#pragma unroll
+        for (int k = 0; k < NO; k++) {
+            opos[k] = 0;
+            omask[k] = 0;
+            of[k] = nullptr;
+        }
 #pragma unroll
         for (int k = 0; k < NM - 1; k++) {
             // k-th mode other than the target: k if k < mode, else k + 1
@@ -118,21 +155,68 @@ struct ModeSel {
     }
 };
 
+// Packed staging record (32 bytes):
+//   a = {row_t, slot, oth0, oth1}, b = {oth2, oth3, value (FP64 bits, or FP32 in .z)}
+struct Rec {
+    uint4 a;
+    uint4 b;
+};
+
+template <int PER>
+__device__ __forceinline__ int rec_offset(int p)
+{
+    return p * REC_BYTES + (p / PER) * 16;
+}
+
+template <typename TV>
+__device__ __forceinline__ TV rec_val(const uint4& b);
+template <>
+__device__ __forceinline__ double rec_val<double>(const uint4& b)
+{
+    return __hiloint2double((int)b.w, (int)b.z);
+}
+template <>
+__device__ __forceinline__ float rec_val<float>(const uint4& b)
+{
+    return __uint_as_float(b.z);
+}
+
+template <typename TV>
+__device__ __forceinline__ void rec_set_val(uint4& b, TV v);
+template <>
+__device__ __forceinline__ void rec_set_val<double>(uint4& b, double v)
+{
+    b.z = (uint32_t)__double2loint(v);
+    b.w = (uint32_t)__double2hiint(v);
+}
+template <>
+__device__ __forceinline__ void rec_set_val<float>(uint4& b, float v)
+{
+    b.z = __float_as_uint(v);
+    b.w = 0;
+}
+
+__device__ __forceinline__ uint32_t rec_oth(const Rec& r, int k)
+{
+    return k == 0 ? r.a.z : k == 1 ? r.a.w : k == 2 ? r.b.x : r.b.y;
+}
+
 // Sorts the warp's tile by output row into the staging area.  Returns the
 // number of valid entries and the bitmask of positions that end a run.
-template <int NM>
-__device__ __forceinline__ int stage_tile(const MtParams& p, const ModeSel<NM>& ms, uint64_t i0, Stage<NM>* st,
-                                          uint32_t& ends)
+template <int NM, int PER, typename TV>
+__device__ __forceinline__ int stage_tile(const MtParams& p, const ModeSel<NM>& ms, const uint32_t* skeys,
+                                          const uint32_t* sslot, uint64_t i0, unsigned char* st, uint32_t& ends)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t i = i0 + lane;
     const bool valid = i < p.nnz;
     uint64_t c = valid ? __ldcs(p.coords + i) : 0;
-    double v = valid ? __ldcs(p.vals + i) : 0.0;
+    TV v = valid ? __ldcs(reinterpret_cast<const TV*>(p.vals) + i) : TV(0);
     uint32_t rt = (uint32_t)((c >> ms.tpos) & ms.tmask);
-    uint32_t ro[ModeSel<NM>::NO];
+    uint32_t ro[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int k = 0; k < NM - 1; k++) ro[k] = (uint32_t)((c >> ms.opos[k]) & ms.omask[k]);
+    int slot = valid ? hot_lookup(p, skeys, sslot, rt) : -1;
     uint32_t key = valid ? rt : 0xffffffffu;
     uint32_t peers = __match_any_sync(0xffffffffu, key);
     const uint32_t lt = (1u << lane) - 1;
@@ -148,97 +232,151 @@ __device__ __forceinline__ int stage_tile(const MtParams& p, const ModeSel<NM>& 
     int sp = (int)start + __popc(peers & lt);
     bool last = (peers >> lane) == 1u;
     ends = __reduce_or_sync(0xffffffffu, last ? (1u << sp) : 0u);
-    st->row[sp] = rt;
-#pragma unroll
-    for (int k = 0; k < NM - 1; k++) st->oth[k][sp] = ro[k];
-    st->val[sp] = v;
+    Rec r;
+    r.a = make_uint4(rt, (uint32_t)slot, ro[0], ro[1]);
+    r.b = make_uint4(ro[2], ro[3], 0u, 0u);
+    rec_set_val<TV>(r.b, v);
+    uint4* dst = reinterpret_cast<uint4*>(st + rec_offset<PER>(sp));
+    dst[0] = r.a;
+    dst[1] = r.b;
     __syncwarp();
     uint64_t rem = p.nnz - i0;
     return rem >= 32 ? 32 : (int)rem;
 }
 
-template <int R>
-__device__ __forceinline__ void flush2(const MtParams& p, double* sacc, const uint32_t* skeys,
-                                       const uint32_t* sslot, uint32_t row, int q, double2 a)
+// 16-byte gather of VEC factor entries, widened to the accumulator type.
+template <class P>
+struct Gather;
+template <>
+struct Gather<PolicyF64> {
+    static __device__ __forceinline__ void load(const void* base, uint32_t row, int R, int q, double (&g)[2])
+    {
+        double2 v = __ldg(reinterpret_cast<const double2*>(base) + ((size_t)row * R) / 2 + q);
+        g[0] = v.x;
+        g[1] = v.y;
+    }
+};
+template <>
+struct Gather<PolicyF32> {
+    static __device__ __forceinline__ void load(const void* base, uint32_t row, int R, int q, float (&g)[4])
+    {
+        float4 v = __ldg(reinterpret_cast<const float4*>(base) + ((size_t)row * R) / 4 + q);
+        g[0] = v.x;
+        g[1] = v.y;
+        g[2] = v.z;
+        g[3] = v.w;
+    }
+};
+template <>
+struct Gather<PolicyBF16> {
+    static __device__ __forceinline__ void load(const void* base, uint32_t row, int R, int q, float (&g)[8])
+    {
+        uint4 v = __ldg(reinterpret_cast<const uint4*>(base) + ((size_t)row * R) / 8 + q);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            // bf16 -> fp32 is exact: the bf16 bits are the high half of the fp32.
+            g[2 * j] = __uint_as_float(w[j] << 16);
+            g[2 * j + 1] = __uint_as_float(w[j] & 0xffff0000u);
+        }
+    }
+};
+
+template <class P>
+__device__ __forceinline__ void flush_global(void* out, uint32_t row, int R, int q,
+                                             const typename P::TA (&a)[P::VEC])
 {
-    int s = hot_lookup(p, skeys, sslot, row);
-    if (s >= 0) {
-        atomicAdd(sacc + (size_t)s * R + 2 * q, a.x);
-        atomicAdd(sacc + (size_t)s * R + 2 * q + 1, a.y);
+    constexpr int VEC = P::VEC;
+    typename P::TA* o = reinterpret_cast<typename P::TA*>(out) + (size_t)row * R + VEC * q;
+    if constexpr (sizeof(typename P::TA) == 8) {
+#pragma unroll
+        for (int j = 0; j < VEC; j++) atomicAdd(o + j, a[j]);
     } else {
-        double* o = p.out + (size_t)row * R + 2 * q;
-        atomicAdd(o, a.x);
-        atomicAdd(o + 1, a.y);
+#pragma unroll
+        for (int j = 0; j < VEC; j += 4)
+            atomicAdd(reinterpret_cast<float4*>(o + j), make_float4(a[j], a[j + 1], a[j + 2], a[j + 3]));
     }
 }
 
-// Vectorised kernel: R in {2,4,...,64}; LPN = R/2 lanes per nonzero, each
-// lane two columns.
-template <int NM, int R>
+template <int NM, int R, class P>
 __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
 {
-    constexpr int LPN = R / 2;
+    typedef typename P::TV TV;
+    typedef typename P::TA TA;
+    constexpr int VEC = P::VEC;
+    constexpr int LPN = R / VEC;
     constexpr int SLOTS = 32 / LPN;
     constexpr int PER = 32 / SLOTS;
+    constexpr int STAGE = 32 * REC_BYTES + SLOTS * 16;
+    constexpr int MT_UNROLL = P::UNROLL;
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t* skeys = reinterpret_cast<uint32_t*>(smem);
     uint32_t* sslot = skeys + p.hash_size;
-    double* sacc = reinterpret_cast<double*>(sslot + p.hash_size + ((2 * p.hash_size) & 1));
+    TA* sacc = reinterpret_cast<TA*>(smem + 8 * (size_t)p.hash_size);
     const int nacc = p.nacc;
-    Stage<NM>* stages = reinterpret_cast<Stage<NM>*>(sacc + (size_t)nacc * R);
+    unsigned char* stages = reinterpret_cast<unsigned char*>(sacc + (size_t)nacc * R);
+    stages = reinterpret_cast<unsigned char*>(((uintptr_t)stages + 15) & ~(uintptr_t)15);
 
     for (int i = threadIdx.x; i < p.hash_size; i += blockDim.x) {
         skeys[i] = p.hot_keys[i];
         sslot[i] = p.hot_slot[i];
     }
-    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = 0.0;
+    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = TA(0);
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int slot = lane / LPN, q = lane % LPN;
-    Stage<NM>* st = stages + warp;
+    unsigned char* st = stages + (size_t)warp * STAGE;
     const uint64_t ntiles = (p.nnz + 31) / 32;
     const uint64_t t_beg = (uint64_t)blockIdx.x * p.tiles_per_cta;
     const uint64_t t_end = min(ntiles, t_beg + p.tiles_per_cta);
     const ModeSel<NM> ms(p);
-    const double2* fv[ModeSel<NM>::NO];
-#pragma unroll
-    for (int k = 0; k < NM - 1; k++) fv[k] = reinterpret_cast<const double2*>(ms.of[k]);
 
     for (uint64_t tile = t_beg + warp; tile < t_end; tile += MT_WARPS) {
         uint32_t ends;
-        const int count = stage_tile<NM>(p, ms, tile * 32, st, ends);
+        const int count = stage_tile<NM, PER, TV>(p, ms, skeys, sslot, tile * 32, st, ends);
         if (!p.merge) ends = 0xffffffffu;
         const int pb = slot * PER, pe = min(pb + PER, count);
-        double2 acc = make_double2(0.0, 0.0);
+        TA acc[VEC];
+#pragma unroll
+        for (int j = 0; j < VEC; j++) acc[j] = TA(0);
         for (int p0 = pb; p0 < pe; p0 += MT_UNROLL) {
-            double2 g[MT_UNROLL][ModeSel<NM>::NO];
-            double vv[MT_UNROLL];
+            TA g[MT_UNROLL][NM > 1 ? NM - 1 : 1][VEC];
+            Rec rec[MT_UNROLL];
 #pragma unroll
             for (int u = 0; u < MT_UNROLL; u++) {
                 int pp = p0 + u;
                 if (pp < pe) {
-                    vv[u] = st->val[pp];
+                    const uint4* src = reinterpret_cast<const uint4*>(st + rec_offset<PER>(pp));
+                    rec[u].a = src[0];
+                    rec[u].b = src[1];
 #pragma unroll
-                    for (int k = 0; k < NM - 1; k++)
-                        g[u][k] = __ldg(fv[k] + (size_t)st->oth[k][pp] * LPN + q);
+                    for (int k = 0; k < NM - 1; k++) Gather<P>::load(ms.of[k], rec_oth(rec[u], k), R, q, g[u][k]);
                 }
             }
 #pragma unroll
             for (int u = 0; u < MT_UNROLL; u++) {
                 int pp = p0 + u;
                 if (pp < pe) {
-                    double2 prod = make_double2(vv[u], vv[u]);
+                    const TA v = (TA)rec_val<TV>(rec[u].b);
 #pragma unroll
-                    for (int k = 0; k < NM - 1; k++) {
-                        prod.x *= g[u][k].x;
-                        prod.y *= g[u][k].y;
+                    for (int j = 0; j < VEC; j++) {
+                        TA prod = v;
+#pragma unroll
+                        for (int k = 0; k < NM - 1; k++) prod *= g[u][k][j];
+                        acc[j] += prod;
                     }
-                    acc.x += prod.x;
-                    acc.y += prod.y;
                     if (((ends >> pp) & 1u) || pp == pe - 1) {
-                        flush2<R>(p, sacc, skeys, sslot, st->row[pp], q, acc);
-                        acc = make_double2(0.0, 0.0);
+                        const int s = (int)rec[u].a.y;
+                        if (s >= 0) {
+                            TA* d = sacc + (size_t)s * R + VEC * q;
+#pragma unroll
+                            for (int j = 0; j < VEC; j++) atomicAdd(d + j, acc[j]);
+                        } else {
+                            flush_global<P>(p.out, rec[u].a.x, R, q, acc);
+                        }
+#pragma unroll
+                        for (int j = 0; j < VEC; j++) acc[j] = TA(0);
                     }
                 }
             }
@@ -247,38 +385,46 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
     }
     __syncthreads();
     // Write the privatised rows back once.
+    TA* out = reinterpret_cast<TA*>(p.out);
     for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) {
-        double v = sacc[i];
-        if (v != 0.0) {
+        TA v = sacc[i];
+        if (v != TA(0)) {
             size_t s = i / R;
             uint32_t row = p.direct ? (uint32_t)s : p.hot_rows[s];
-            atomicAdd(p.out + (size_t)row * R + (i % R), v);
+            atomicAdd(out + (size_t)row * R + (i % R), v);
         }
     }
 }
 
 // Generic kernel: any R up to 256, a whole warp per nonzero, columns
-// lane, lane+32, ...
+// lane, lane+32, ...  Used for ranks the vectorised kernels do not cover and
+// for factor pointers that are not 16-byte aligned.
 constexpr int GEN_MAXC = 8;
 
-template <int NM>
+template <int NM, class P>
 __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_gen(MtParams p)
 {
+    typedef typename P::TV TV;
+    typedef typename P::TF TF;
+    typedef typename P::TA TA;
+    constexpr int PER = 32;
+    constexpr int STAGE = 32 * REC_BYTES + 16;
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t* skeys = reinterpret_cast<uint32_t*>(smem);
     uint32_t* sslot = skeys + p.hash_size;
-    double* sacc = reinterpret_cast<double*>(sslot + p.hash_size + ((2 * p.hash_size) & 1));
+    TA* sacc = reinterpret_cast<TA*>(smem + 8 * (size_t)p.hash_size);
     const int R = p.rank;
     const int nacc = p.nacc;
-    Stage<NM>* stages = reinterpret_cast<Stage<NM>*>(sacc + (size_t)nacc * R);
+    unsigned char* stages = reinterpret_cast<unsigned char*>(sacc + (size_t)nacc * R);
+    stages = reinterpret_cast<unsigned char*>(((uintptr_t)stages + 15) & ~(uintptr_t)15);
     for (int i = threadIdx.x; i < p.hash_size; i += blockDim.x) {
         skeys[i] = p.hot_keys[i];
         sslot[i] = p.hot_slot[i];
     }
-    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = 0.0;
+    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = TA(0);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    Stage<NM>* st = stages + warp;
+    unsigned char* st = stages + (size_t)warp * STAGE;
     const uint64_t ntiles = (p.nnz + 31) / 32;
     const uint64_t t_beg = (uint64_t)blockIdx.x * p.tiles_per_cta;
     const uint64_t t_end = min(ntiles, t_beg + p.tiles_per_cta);
@@ -286,112 +432,123 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_gen(MtParams p)
     const int ncol = (R + 31) / 32;
     for (uint64_t tile = t_beg + warp; tile < t_end; tile += MT_WARPS) {
         uint32_t ends;
-        const int count = stage_tile<NM>(p, ms, tile * 32, st, ends);
+        const int count = stage_tile<NM, PER, TV>(p, ms, skeys, sslot, tile * 32, st, ends);
         if (!p.merge) ends = 0xffffffffu;
-        double acc[GEN_MAXC];
+        TA acc[GEN_MAXC];
 #pragma unroll
-        for (int j = 0; j < GEN_MAXC; j++) acc[j] = 0.0;
+        for (int j = 0; j < GEN_MAXC; j++) acc[j] = TA(0);
         for (int pp = 0; pp < count; pp++) {
-            const double v = st->val[pp];
+            const uint4* src = reinterpret_cast<const uint4*>(st + rec_offset<PER>(pp));
+            Rec rec;
+            rec.a = src[0];
+            rec.b = src[1];
+            const TA v = (TA)rec_val<TV>(rec.b);
 #pragma unroll
             for (int j = 0; j < GEN_MAXC; j++) {
                 int c = lane + 32 * j;
                 if (j < ncol && c < R) {
-                    double prod = v;
+                    TA prod = v;
 #pragma unroll
-                    for (int k = 0; k < NM - 1; k++) prod *= __ldg(ms.of[k] + (size_t)st->oth[k][pp] * R + c);
+                    for (int k = 0; k < NM - 1; k++)
+                        prod *= (TA)reinterpret_cast<const TF*>(ms.of[k])[(size_t)rec_oth(rec, k) * R + c];
                     acc[j] += prod;
                 }
             }
             if (((ends >> pp) & 1u) || pp == count - 1) {
-                const uint32_t row = st->row[pp];
-                int s = hot_lookup(p, skeys, sslot, row);
+                const uint32_t row = rec.a.x;
+                const int s = (int)rec.a.y;
 #pragma unroll
                 for (int j = 0; j < GEN_MAXC; j++) {
                     int c = lane + 32 * j;
                     if (j < ncol && c < R) {
                         if (s >= 0) atomicAdd(sacc + (size_t)s * R + c, acc[j]);
-                        else atomicAdd(p.out + (size_t)row * R + c, acc[j]);
+                        else atomicAdd(reinterpret_cast<TA*>(p.out) + (size_t)row * R + c, acc[j]);
                     }
-                    acc[j] = 0.0;
+                    acc[j] = TA(0);
                 }
             }
         }
         __syncwarp();
     }
     __syncthreads();
+    TA* out = reinterpret_cast<TA*>(p.out);
     for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) {
-        double v = sacc[i];
-        if (v != 0.0) {
+        TA v = sacc[i];
+        if (v != TA(0)) {
             size_t s = i / R;
             uint32_t row = p.direct ? (uint32_t)s : p.hot_rows[s];
-            atomicAdd(p.out + (size_t)row * R + (i % R), v);
+            atomicAdd(out + (size_t)row * R + (i % R), v);
         }
-    }
-}
-
-template <int NM>
-size_t stage_bytes() { return sizeof(Stage<NM>) * MT_WARPS; }
-
-size_t stage_bytes_rt(int nm)
-{
-    switch (nm) {
-    case 1: return stage_bytes<1>();
-    case 2: return stage_bytes<2>();
-    case 3: return stage_bytes<3>();
-    case 4: return stage_bytes<4>();
-    default: return stage_bytes<5>();
     }
 }
 
 typedef void (*KernelFn)(MtParams);
 
-template <int NM>
+template <int NM, class P>
 KernelFn pick_vec(int R)
 {
+    constexpr int V = P::VEC;
     switch (R) {
-    case 2: return k_mttkrp_vec<NM, 2>;
-    case 4: return k_mttkrp_vec<NM, 4>;
-    case 8: return k_mttkrp_vec<NM, 8>;
-    case 16: return k_mttkrp_vec<NM, 16>;
-    case 32: return k_mttkrp_vec<NM, 32>;
-    case 64: return k_mttkrp_vec<NM, 64>;
+    case 2: if constexpr (V <= 2) return k_mttkrp_vec<NM, 2, P>; else return nullptr;
+    case 4: if constexpr (V <= 4) return k_mttkrp_vec<NM, 4, P>; else return nullptr;
+    case 8: return k_mttkrp_vec<NM, 8, P>;
+    case 16: return k_mttkrp_vec<NM, 16, P>;
+    case 32: return k_mttkrp_vec<NM, 32, P>;
+    case 64: return k_mttkrp_vec<NM, 64, P>;
+    case 128: if constexpr (V >= 4) return k_mttkrp_vec<NM, 128, P>; else return nullptr;
     default: return nullptr;
     }
 }
 
+template <class P>
 KernelFn pick_generic(int nm)
 {
     switch (nm) {
-    case 1: return k_mttkrp_gen<1>;
-    case 2: return k_mttkrp_gen<2>;
-    case 3: return k_mttkrp_gen<3>;
-    case 4: return k_mttkrp_gen<4>;
-    default: return k_mttkrp_gen<5>;
+    case 1: return k_mttkrp_gen<1, P>;
+    case 2: return k_mttkrp_gen<2, P>;
+    case 3: return k_mttkrp_gen<3, P>;
+    case 4: return k_mttkrp_gen<4, P>;
+    default: return k_mttkrp_gen<5, P>;
     }
 }
 
-KernelFn pick_kernel(int nm, int R)
+template <class P>
+KernelFn pick_kernel(int nm, int R, bool aligned16)
 {
     KernelFn f = nullptr;
-    switch (nm) {
-    case 1: f = pick_vec<1>(R); break;
-    case 2: f = pick_vec<2>(R); break;
-    case 3: f = pick_vec<3>(R); break;
-    case 4: f = pick_vec<4>(R); break;
-    case 5: f = pick_vec<5>(R); break;
+    if (aligned16) {
+        switch (nm) {
+        case 1: f = pick_vec<1, P>(R); break;
+        case 2: f = pick_vec<2, P>(R); break;
+        case 3: f = pick_vec<3, P>(R); break;
+        case 4: f = pick_vec<4, P>(R); break;
+        case 5: f = pick_vec<5, P>(R); break;
+        }
     }
-    return f ? f : pick_generic(nm);
+    return f ? f : pick_generic<P>(nm);
 }
+
+// Per-CTA staging bytes: 32 records per warp plus one 16-byte pad per slot
+// range (slots = 32 lanes / lanes per nonzero).
+size_t stage_bytes(int rank, int vec)
+{
+    int lpn = rank / vec;
+    int slots = (lpn >= 1 && lpn <= 32 && rank % vec == 0) ? 32 / lpn : 1;
+    return (size_t)MT_WARPS * (32 * REC_BYTES + slots * 16) + 16;
+}
+
+int policy_vec(int dtype) { return dtype == BLCO_DTYPE_F64 ? 2 : dtype == BLCO_DTYPE_F32 ? 4 : 8; }
+
+size_t acc_elem_bytes(int dtype) { return dtype == BLCO_DTYPE_F64 ? 8 : 4; }
 
 } // namespace
 
-int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested)
+int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested, int factor_dtype)
 {
     DeviceInfo di;
     if (device_info(t->device, &di) != BLCO_OK) return BLCO_KERNEL_LVL1;
-    size_t budget = di.smem_optin - stage_bytes_rt(t->layout.nmodes) - 2 * sizeof(uint32_t) * 4096 - 1024;
-    bool fits_direct = t->layout.dims[mode] * (uint64_t)rank * sizeof(double) <= budget;
+    size_t budget = di.smem_optin - stage_bytes(rank, policy_vec(factor_dtype)) - 2 * sizeof(uint32_t) * 4096 - 1024;
+    bool fits_direct = t->layout.dims[mode] * (uint64_t)rank * acc_elem_bytes(factor_dtype) <= budget;
     switch (requested) {
     case BLCO_KERNEL_LVL1:
     case BLCO_KERNEL_BATCHED:
@@ -405,11 +562,25 @@ int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested
     }
 }
 
+int values_f32(blco_tensor* t, cudaStream_t s, const float** out)
+{
+    if (!t->d_values_f32 && t->nnz) {
+        if (!t->resident) return fail(BLCO_ERR_STATE, "FP32 values of a streamed tensor are made per block");
+        BLCO_CUDA(cudaMalloc(&t->d_values_f32, t->nnz * sizeof(float)));
+        k_to_f32<<<1024, 256, 0, s>>>(t->d_values, t->d_values_f32, t->nnz);
+        BLCO_CHECK_LAUNCH("k_to_f32");
+    }
+    *out = t->d_values_f32;
+    return BLCO_OK;
+}
+
 int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
 {
     const Layout& L = t->layout;
     if (a.nnz == 0) return BLCO_OK;
     if (a.rank < 1 || a.rank > 256) return fail(BLCO_ERR_UNSUPPORTED, "rank must be 1..256");
+    if (a.factor_dtype != BLCO_DTYPE_F64 && a.factor_dtype != BLCO_DTYPE_F32 && a.factor_dtype != BLCO_DTYPE_BF16)
+        return fail(BLCO_ERR_INVALID, "unknown factor dtype");
     DeviceInfo di;
     BLCO_TRY(device_info(t->device, &di));
     MtParams p;
@@ -426,8 +597,9 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     p.mode = a.mode;
     p.rank = a.rank;
     p.merge = 1;
-    const int kern = mttkrp_select_kernel(t, a.mode, a.rank, a.kernel);
-    const size_t stage = stage_bytes_rt(L.nmodes);
+    const size_t accb = acc_elem_bytes(a.factor_dtype);
+    const int kern = mttkrp_select_kernel(t, a.mode, a.rank, a.kernel, a.factor_dtype);
+    const size_t stage = stage_bytes(a.rank, policy_vec(a.factor_dtype));
     const HotTable& ht = t->hot[a.mode];
     size_t hash_bytes = 0;
     if (kern == BLCO_KERNEL_LVL3) {
@@ -437,9 +609,9 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
         p.hot_slot = ht.d_slot;
         p.hot_rows = ht.d_rows;
         p.hash_size = ht.hash_size;
-        hash_bytes = 2 * sizeof(uint32_t) * ht.hash_size + 8;
+        hash_bytes = 2 * sizeof(uint32_t) * ht.hash_size;
         size_t avail = di.smem_optin - stage - hash_bytes - 1024;
-        size_t fit = avail / (sizeof(double) * a.rank);
+        size_t fit = avail / (accb * a.rank);
         p.nhot = (int)std::min<size_t>(fit, (size_t)ht.nhot);
         if (p.nhot == 0) p.hash_size = 0, hash_bytes = 0;
     } else if (kern == BLCO_KERNEL_ATOMIC) {
@@ -447,14 +619,20 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     }
     const size_t nacc = p.direct ? (size_t)L.dims[a.mode] : (size_t)p.nhot;
     p.nacc = (int)nacc;
-    const size_t smem = hash_bytes + nacc * a.rank * sizeof(double) + stage + 16;
+    const size_t smem = hash_bytes + nacc * a.rank * accb + stage + 16;
     if (smem > di.smem_optin) return fail(BLCO_ERR_UNSUPPORTED, "MTTKRP shared memory plan exceeds the device limit");
-    // The vectorised kernels load two FP64 columns at a time: every factor
-    // must start on a 16-byte boundary, otherwise take the scalar kernel.
-    bool aligned16 = true;
+    // The vectorised kernels load 16 bytes at a time: every factor must start
+    // on a 16-byte boundary (and the FP32 output on 16 bytes for the vector
+    // atomics), otherwise take the scalar kernel.
+    bool aligned16 = ((uintptr_t)a.out & 15u) == 0;
     for (int m = 0; m < L.nmodes; m++)
         if (m != a.mode && ((uintptr_t)a.factors[m] & 15u) != 0) aligned16 = false;
-    KernelFn fn = aligned16 ? pick_kernel(L.nmodes, a.rank) : pick_generic(L.nmodes);
+    KernelFn fn;
+    switch (a.factor_dtype) {
+    case BLCO_DTYPE_F64: fn = pick_kernel<PolicyF64>(L.nmodes, a.rank, aligned16); break;
+    case BLCO_DTYPE_F32: fn = pick_kernel<PolicyF32>(L.nmodes, a.rank, aligned16); break;
+    default: fn = pick_kernel<PolicyBF16>(L.nmodes, a.rank, aligned16); break;
+    }
     BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint64_t ntiles = (a.nnz + 31) / 32;
     uint64_t grid = std::min<uint64_t>((uint64_t)di.sm_count, (ntiles + MT_WARPS - 1) / MT_WARPS);

@@ -64,8 +64,17 @@ enum {
 
 /* Numeric form. */
 enum {
-    BLCO_PRECISION_FP64 = 0, /* plain form: all values and factors FP64 */
-    BLCO_PRECISION_MIXED = 1 /* FP32 values/accumulation, BF16 factor gathers */
+    BLCO_PRECISION_FP64 = 0,      /* plain form: all values and factors FP64 */
+    BLCO_PRECISION_MIXED = 1,     /* chosen form: FP32 values, factors and
+                                     accumulation; FP64 Grams, solve, lambda, fit */
+    BLCO_PRECISION_MIXED_BF16 = 2 /* as MIXED, with BF16 factor-row gathers */
+};
+
+/* Element types of factor/output arrays for blco_mttkrp_ex. */
+enum {
+    BLCO_DTYPE_F64 = 0,
+    BLCO_DTYPE_F32 = 1,
+    BLCO_DTYPE_BF16 = 2
 };
 
 /* Options shared by the MTTKRP and CP-ALS entry points; the fields mirror
@@ -158,6 +167,15 @@ int blco_tensor_device_arrays(const blco_tensor* t, const uint64_t** d_coords,
  * the last block is enqueued). */
 int blco_mttkrp(blco_tensor* t, int mode, int rank, const double* const* d_factors,
                 double* d_out, const blco_opts* opts);
+
+/* Mixed-precision MTTKRP (the chosen form's kernel): d_out (FP32,
+ * dims[mode] x rank) += MTTKRP computed from the tensor's values rounded to
+ * FP32, factor rows of type factor_dtype (BLCO_DTYPE_F32 or
+ * BLCO_DTYPE_BF16, row-major dims[n] x rank) and FP32 accumulation.
+ * BLCO_DTYPE_F64 factors with an FP64 output is the same as blco_mttkrp.
+ * No reference counterpart (the reference is FP64 only). */
+int blco_mttkrp_ex(blco_tensor* t, int mode, int rank, int factor_dtype,
+                   const void* const* d_factors, void* d_out, const blco_opts* opts);
 
 /* Host-pointer form: out (host) += MTTKRP, factors are host arrays.  The
  * role of the reference -p benchmark driver mttkrp_alto_dev
