@@ -36,9 +36,21 @@ constexpr int MAX_SOLVE_R = 96; // k_solve keeps two R x R FP64 buffers in share
 // 8 up to R = 128, so that 256 threads cover the result).
 constexpr int GR_CH = 32; // rows staged per step
 
-template <typename T, bool SCALE, int TS>
+__device__ __forceinline__ float round_bf16(float x, uint16_t* bits)
+{
+    uint32_t u = __float_as_uint(x);
+    uint32_t r = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+    *bits = (uint16_t)(r >> 16);
+    return __uint_as_float(r);
+}
+
+// With BF16OUT the (scaled) factor is rounded to BF16 precision, the rounded
+// value is kept in U and its BF16 bits are written to bf16_out, so the Gram,
+// the fit and the MTTKRP gathers all see the same factor.
+template <typename T, bool SCALE, int TS, bool BF16OUT = false>
 __global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t I, int R,
-                                                     const double* __restrict__ inv, double* __restrict__ partials)
+                                                     const double* __restrict__ inv, double* __restrict__ partials,
+                                                     uint16_t* __restrict__ bf16_out = nullptr)
 {
     extern __shared__ __align__(16) double gs[];
     double* red = gs;                                 // R x R reduction buffer
@@ -63,10 +75,13 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t
         __syncthreads();
         for (int k = tid; k < nr * R; k += DN_THREADS) {
             T v = U[r0 * R + k];
-            if (SCALE) {
-                v = (T)((double)v * inv[k % R]);
-                U[r0 * R + k] = v;
+            if (SCALE) v = (T)((double)v * inv[k % R]);
+            if constexpr (BF16OUT) {
+                uint16_t b;
+                v = (T)round_bf16((float)v, &b);
+                bf16_out[r0 * R + k] = b;
             }
+            if (SCALE || BF16OUT) U[r0 * R + k] = v;
             tile[k] = v;
         }
         __syncthreads();
@@ -476,16 +491,6 @@ __global__ void k_f32_to_f64(const float* __restrict__ in, double* __restrict__ 
         out[i] = (double)in[i];
 }
 
-// Round-to-nearest-even FP32 -> BF16 (the BF16 bits are the high half).
-__global__ void k_f32_to_bf16(const float* __restrict__ in, uint16_t* __restrict__ out, uint64_t n)
-{
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t x = __float_as_uint(in[i]);
-        uint32_t r = x + 0x7fffu + ((x >> 16) & 1u);
-        out[i] = (uint16_t)(r >> 16);
-    }
-}
-
 int plan_free(blco_cpals_plan* p)
 {
     if (!p) return BLCO_OK;
@@ -509,16 +514,21 @@ int plan_free(blco_cpals_plan* p)
 }
 
 template <typename T>
-int gram_launch(blco_cpals_plan* p, T* U, uint64_t I, const double* inv, double* G)
+int gram_launch(blco_cpals_plan* p, T* U, uint64_t I, const double* inv, double* G, uint16_t* bf16_out = nullptr)
 {
     const int R = p->R;
     int grid = grid_rows(I, p->sm);
     size_t smem = (size_t)R * R * sizeof(double) + (size_t)GR_CH * R * sizeof(T);
-    void (*fn)(T*, uint64_t, int, const double*, double*);
-    if (R <= 64) fn = inv ? k_gram<T, true, 4> : k_gram<T, false, 4>;
-    else fn = inv ? k_gram<T, true, 8> : k_gram<T, false, 8>;
+    void (*fn)(T*, uint64_t, int, const double*, double*, uint16_t*);
+    if (bf16_out) {
+        if (R <= 64) fn = inv ? k_gram<T, true, 4, true> : k_gram<T, false, 4, true>;
+        else fn = inv ? k_gram<T, true, 8, true> : k_gram<T, false, 8, true>;
+    } else {
+        if (R <= 64) fn = inv ? k_gram<T, true, 4> : k_gram<T, false, 4>;
+        else fn = inv ? k_gram<T, true, 8> : k_gram<T, false, 8>;
+    }
     BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    fn<<<grid, DN_THREADS, smem, p->s>>>(U, I, R, inv, p->partials);
+    fn<<<grid, DN_THREADS, smem, p->s>>>(U, I, R, inv, p->partials, bf16_out);
     BLCO_CHECK_LAUNCH("k_gram");
     k_sum_partials<<<(R * R + 255) / 256, 256, 0, p->s>>>(p->partials, grid, R * R, G);
     BLCO_CHECK_LAUNCH("k_sum_partials");
@@ -579,11 +589,8 @@ int mode_update(blco_cpals_plan* p, int n)
     k_lambda<<<1, 128, 0, p->s>>>(p->partials, grid, R, p->lambda, p->inv);
     BLCO_CHECK_LAUNCH("k_lambda");
     if (p->mixed) {
-        BLCO_TRY(gram_launch<float>(p, p->Uf[n], I, p->inv, p->grams[n]));
-        if (p->gather_dtype == BLCO_DTYPE_BF16) {
-            k_f32_to_bf16<<<conv_grid(I * R, p->sm), 256, 0, p->s>>>(p->Uf[n], (uint16_t*)p->Ub[n], I * R);
-            BLCO_CHECK_LAUNCH("k_f32_to_bf16");
-        }
+        uint16_t* b = p->gather_dtype == BLCO_DTYPE_BF16 ? (uint16_t*)p->Ub[n] : nullptr;
+        BLCO_TRY(gram_launch<float>(p, p->Uf[n], I, p->inv, p->grams[n], b));
     } else {
         BLCO_TRY(gram_launch<double>(p, p->U[n], I, p->inv, p->grams[n]));
     }
@@ -689,11 +696,8 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
         if (p->mixed) {
             k_f64_to_f32<<<conv_grid(len, p->sm), 256, 0, p->s>>>(p->U[n], p->Uf[n], len);
             count_launch();
-            if (p->gather_dtype == BLCO_DTYPE_BF16) {
-                k_f32_to_bf16<<<conv_grid(len, p->sm), 256, 0, p->s>>>(p->Uf[n], (uint16_t*)p->Ub[n], len);
-                count_launch();
-            }
-            st = gram_launch<float>(p, p->Uf[n], t->layout.dims[n], nullptr, p->grams[n]);
+            uint16_t* b = p->gather_dtype == BLCO_DTYPE_BF16 ? (uint16_t*)p->Ub[n] : nullptr;
+            st = gram_launch<float>(p, p->Uf[n], t->layout.dims[n], nullptr, p->grams[n], b);
         } else {
             st = gram_launch<double>(p, p->U[n], t->layout.dims[n], nullptr, p->grams[n]);
         }

@@ -18,8 +18,8 @@
 //     (VEC = 2 FP64, 4 FP32 or 8 BF16 columns per load), several nonzeros in
 //     flight per warp;
 //   * runs of equal output rows are summed in registers and flushed once:
-//     into a per-CTA shared-memory accumulator when the row is one of the
-//     mode's heaviest rows (written back once per CTA), or into the whole
+//     into a per-CTA FP64 shared-memory accumulator when the row is one of
+//     the mode's heaviest rows (written back once per CTA), or into the whole
 //     output when the mode is short enough to fit (the lvl3 role), otherwise
 //     with global atomics (FP64 red, or 4-wide FP32 vector red).
 // Precision policies:
@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
 {
     typedef typename P::TV TV;
     typedef typename P::TA TA;
+    typedef double TS; // shared accumulators are FP64 in every form
     constexpr int VEC = P::VEC;
     constexpr int LPN = R / VEC;
     constexpr int SLOTS = 32 / LPN;
@@ -312,7 +313,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t* skeys = reinterpret_cast<uint32_t*>(smem);
     uint32_t* sslot = skeys + p.hash_size;
-    TA* sacc = reinterpret_cast<TA*>(smem + 8 * (size_t)p.hash_size);
+    TS* sacc = reinterpret_cast<TS*>(smem + 8 * (size_t)p.hash_size);
     const int nacc = p.nacc;
     unsigned char* stages = reinterpret_cast<unsigned char*>(sacc + (size_t)nacc * R);
     stages = reinterpret_cast<unsigned char*>(((uintptr_t)stages + 15) & ~(uintptr_t)15);
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
         skeys[i] = p.hot_keys[i];
         sslot[i] = p.hot_slot[i];
     }
-    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = TA(0);
+    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = TS(0);
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -369,9 +370,9 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
                     if (((ends >> pp) & 1u) || pp == pe - 1) {
                         const int s = (int)rec[u].a.y;
                         if (s >= 0) {
-                            TA* d = sacc + (size_t)s * R + VEC * q;
+                            TS* d = sacc + (size_t)s * R + VEC * q;
 #pragma unroll
-                            for (int j = 0; j < VEC; j++) atomicAdd(d + j, acc[j]);
+                            for (int j = 0; j < VEC; j++) atomicAdd(d + j, (TS)acc[j]);
                         } else {
                             flush_global<P>(p.out, rec[u].a.x, R, q, acc);
                         }
@@ -387,11 +388,11 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
     // Write the privatised rows back once.
     TA* out = reinterpret_cast<TA*>(p.out);
     for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) {
-        TA v = sacc[i];
-        if (v != TA(0)) {
+        TS v = sacc[i];
+        if (v != TS(0)) {
             size_t s = i / R;
             uint32_t row = p.direct ? (uint32_t)s : p.hot_rows[s];
-            atomicAdd(out + (size_t)row * R + (i % R), v);
+            atomicAdd(out + (size_t)row * R + (i % R), (TA)v);
         }
     }
 }
@@ -407,12 +408,13 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_gen(MtParams p)
     typedef typename P::TV TV;
     typedef typename P::TF TF;
     typedef typename P::TA TA;
+    typedef double TS;
     constexpr int PER = 32;
     constexpr int STAGE = 32 * REC_BYTES + 16;
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t* skeys = reinterpret_cast<uint32_t*>(smem);
     uint32_t* sslot = skeys + p.hash_size;
-    TA* sacc = reinterpret_cast<TA*>(smem + 8 * (size_t)p.hash_size);
+    TS* sacc = reinterpret_cast<TS*>(smem + 8 * (size_t)p.hash_size);
     const int R = p.rank;
     const int nacc = p.nacc;
     unsigned char* stages = reinterpret_cast<unsigned char*>(sacc + (size_t)nacc * R);
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_gen(MtParams p)
         skeys[i] = p.hot_keys[i];
         sslot[i] = p.hot_slot[i];
     }
-    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = TA(0);
+    for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) sacc[i] = TS(0);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* st = stages + (size_t)warp * STAGE;
@@ -461,7 +463,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_gen(MtParams p)
                 for (int j = 0; j < GEN_MAXC; j++) {
                     int c = lane + 32 * j;
                     if (j < ncol && c < R) {
-                        if (s >= 0) atomicAdd(sacc + (size_t)s * R + c, acc[j]);
+                        if (s >= 0) atomicAdd(sacc + (size_t)s * R + c, (TS)acc[j]);
                         else atomicAdd(reinterpret_cast<TA*>(p.out) + (size_t)row * R + c, acc[j]);
                     }
                     acc[j] = TA(0);
@@ -473,11 +475,11 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_gen(MtParams p)
     __syncthreads();
     TA* out = reinterpret_cast<TA*>(p.out);
     for (size_t i = threadIdx.x; i < (size_t)nacc * R; i += blockDim.x) {
-        TA v = sacc[i];
-        if (v != TA(0)) {
+        TS v = sacc[i];
+        if (v != TS(0)) {
             size_t s = i / R;
             uint32_t row = p.direct ? (uint32_t)s : p.hot_rows[s];
-            atomicAdd(out + (size_t)row * R + (i % R), v);
+            atomicAdd(out + (size_t)row * R + (i % R), (TA)v);
         }
     }
 }
@@ -539,7 +541,9 @@ size_t stage_bytes(int rank, int vec)
 
 int policy_vec(int dtype) { return dtype == BLCO_DTYPE_F64 ? 2 : dtype == BLCO_DTYPE_F32 ? 4 : 8; }
 
-size_t acc_elem_bytes(int dtype) { return dtype == BLCO_DTYPE_F64 ? 8 : 4; }
+// Shared-memory accumulators are FP64 in every form: a heavy row collects
+// up to millions of contributions per CTA, too many to sum in FP32.
+size_t acc_elem_bytes(int) { return 8; }
 
 } // namespace
 

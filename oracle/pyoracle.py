@@ -191,3 +191,54 @@ def kruskal_random_init(dims, rank, seed, nthreads):
                                   ctypes.c_uint(seed), ctypes.c_int(nthreads),
                                   _ptr_array(factors), _p(lam, _f64p))
     return factors, lam
+
+
+_refgpu = None
+
+
+def refgpu_lib():
+    """The reference's own GPU CP-ALS/MTTKRP (oracle/_ref/libblco_refgpu.so,
+    built by `make -C oracle ref-gpu`), or None.  Needs a B200 to run."""
+    global _refgpu
+    if _refgpu is None:
+        path = os.path.join(HERE, "_ref", "libblco_refgpu.so")
+        if not os.path.exists(path):
+            return None
+        G = ctypes.CDLL(path)
+        G.refgpu_cpals.restype = ctypes.c_double
+        G.refgpu_cpals.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int,
+                                   ctypes.c_void_p, _f64p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int]
+        G.refgpu_mttkrp.restype = None
+        G.refgpu_mttkrp.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int,
+                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int]
+        _refgpu = G
+    return _refgpu
+
+
+def refgpu_cpals(dims, cidx, vals, factors, lam, maxiter, tol, kernel=10, nprtn=8, thread_cf=2):
+    """Runs the reference cpals_blco_dev; factors/lam updated in place."""
+    G = refgpu_lib()
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    for f in factors:
+        assert f.flags.c_contiguous and f.dtype == np.float64
+    return G.refgpu_cpals(len(dims), _p(dims, _u64p), cidx.shape[1], _p(cidx, _u64p), _p(vals, _f64p),
+                          factors[0].shape[1], _ptr_array(factors), _p(lam, _f64p), maxiter, tol, kernel,
+                          nprtn, thread_cf)
+
+
+def refgpu_mttkrp(dims, cidx, vals, factors, mode, kernel=1, nprtn=8, thread_cf=2):
+    """Runs the reference mttkrp_alto_dev once into a zeroed target factor;
+    returns the MTTKRP."""
+    G = refgpu_lib()
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    fs = [np.ascontiguousarray(f, dtype=np.float64).copy() for f in factors]
+    fs[mode][:] = 0.0
+    G.refgpu_mttkrp(len(dims), _p(dims, _u64p), cidx.shape[1], _p(cidx, _u64p), _p(vals, _f64p),
+                    fs[0].shape[1], _ptr_array(fs), mode, kernel, 1, nprtn, thread_cf)
+    return fs[mode]

@@ -1,0 +1,84 @@
+"""GPU parity against the reference's own GPU code, rebuilt unchanged for
+sm_100a into oracle/_ref/libblco_refgpu.so (make -C oracle ref-gpu):
+cpals_blco_dev (src/cpd_gpu.cu:21-242) and mttkrp_alto_dev
+(src/alto_dev.cu:1857-1952) on the same inputs and initial factors.
+
+Tolerances: MTTKRP normwise relative 1e-12; CP-ALS fit 1e-10 absolute and
+factors 1e-9 relative (Frobenius) after each tested iteration count.  Both
+sides sum with FP64 atomics in run-dependent order, and the reference solves
+with a Jacobi SVD (cuSOLVER gesvdj) where this engine uses Cholesky.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import unique_coords
+
+pytestmark = pytest.mark.gpu
+
+if po.refgpu_lib() is None:
+    pytest.skip("oracle/_ref/libblco_refgpu.so not built", allow_module_level=True)
+
+
+@pytest.mark.parametrize("ref_kernel", [1, 2, 3, 10, 13])
+def test_mttkrp_matches_reference_gpu(blco, ref_kernel):
+    import torch
+    rng = np.random.default_rng(ref_kernel)
+    dims = [3000, 2000, 90] if ref_kernel in (3, 10) else [3000, 2000, 400]
+    nnz = 60_000
+    cidx = unique_coords(rng, dims, nnz, zipf=0.9)
+    vals = rng.random(nnz)
+    R = 16
+    fs = [rng.random((d, R)) for d in dims]
+    t = blco.Tensor.encode(dims, cidx, vals)
+    dev = [torch.from_numpy(f).cuda() for f in fs]
+    for m in range(3):
+        ref = po.refgpu_mttkrp(dims, cidx, vals, fs, m, kernel=ref_kernel)
+        out = torch.zeros(dims[m], R, dtype=torch.float64, device="cuda")
+        blco.mttkrp(t, m, dev, out, blco.make_opts(kernel=ref_kernel))
+        torch.cuda.synchronize()
+        o = out.cpu().numpy()
+        err = np.linalg.norm(o - ref) / np.linalg.norm(ref)
+        assert err <= 1e-12, (m, err)
+
+
+@pytest.mark.parametrize("iters", [1, 5, 20])
+def test_cpals_matches_reference_gpu(blco, iters):
+    """The CPU-runnable workload's shape (1000 x 800 x 600, unique uniform
+    coordinates, U(0,1) values, rank 16, tolerance 0) at 100k nonzeros."""
+    from blco_b200 import synth
+    X = synth.uniform_tensor_host(100_000, [1000, 800, 600], seed=0)
+    R = 16
+    fs0, lam0 = po.kruskal_random_init(X["dims"], R, 1, 1)
+    fr = [f.copy() for f in fs0]
+    lr = lam0.copy()
+    fit_r = po.refgpu_cpals(X["dims"], X["cidx"], X["vals"], fr, lr, iters, 0.0, kernel=10)
+    t = blco.Tensor.encode(X["dims"], X["cidx"], X["vals"])
+    fg = [f.copy() for f in fs0]
+    lg = lam0.copy()
+    fit_g, fits_g = blco.cpals(t, fg, lg, iters, 0.0)
+    assert len(fits_g) == iters
+    assert abs(fit_g - fit_r) <= 1e-10, (fit_g, fit_r)
+    for a, b in zip(fg, fr):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+    assert np.allclose(lg, lr, rtol=1e-9)
+
+
+def test_cpals_skewed_matches_reference_gpu(blco):
+    rng = np.random.default_rng(17)
+    dims = [20_000, 15_000, 500]
+    nnz = 150_000
+    cidx = unique_coords(rng, dims, nnz, zipf=1.1)
+    vals = rng.lognormal(0.0, 1.0, nnz)
+    R = 32
+    fs0 = [rng.random((d, R)) for d in dims]
+    fr = [f.copy() for f in fs0]
+    lr = np.ones(R)
+    fit_r = po.refgpu_cpals(dims, cidx, vals, fr, lr, 8, 0.0, kernel=1)
+    t = blco.Tensor.encode(dims, cidx, vals)
+    fg = [f.copy() for f in fs0]
+    lg = np.ones(R)
+    fit_g, _ = blco.cpals(t, fg, lg, 8, 0.0)
+    assert abs(fit_g - fit_r) <= 1e-10, (fit_g, fit_r)
+    for a, b in zip(fg, fr):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
