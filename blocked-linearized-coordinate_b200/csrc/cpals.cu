@@ -141,12 +141,12 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const T* __restrict__ M, 
                                                        double* __restrict__ colsq_partials)
 {
     extern __shared__ __align__(16) double us[];
-    double* csq = us;                                   // [warps][R]
-    T* PT = reinterpret_cast<T*>(us + (DN_THREADS / 32) * R); // PT[k][c] = P[c][k]
+    double* csq = us;                   // [warps][R]
+    double* PT = us + (DN_THREADS / 32) * R; // PT[k][c] = P[c][k]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = DN_THREADS / 32;
     for (int k = tid; k < R * R; k += DN_THREADS) {
         int c = k / R, kk = k % R;
-        PT[kk * R + c] = (T)P[k];
+        PT[kk * R + c] = P[k];
     }
     __syncthreads();
     double sq[UP_MAXC];
@@ -156,19 +156,19 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const T* __restrict__ M, 
     const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
     for (uint64_t i = beg + warp; i < end; i += nw) {
         const T* mrow = M + i * R;
-        T mreg[UP_MAXC];
+        double mreg[UP_MAXC];
 #pragma unroll
-        for (int j = 0; j < UP_MAXC; j++) mreg[j] = (lane + 32 * j < R) ? mrow[lane + 32 * j] : T(0);
-        T acc[UP_MAXC];
+        for (int j = 0; j < UP_MAXC; j++) mreg[j] = (lane + 32 * j < R) ? (double)mrow[lane + 32 * j] : 0.0;
+        double acc[UP_MAXC];
 #pragma unroll
-        for (int j = 0; j < UP_MAXC; j++) acc[j] = T(0);
+        for (int j = 0; j < UP_MAXC; j++) acc[j] = 0.0;
 #pragma unroll
         for (int kb = 0; kb < UP_MAXC; kb++) {
             if (32 * kb >= R) break;
             const int kn = min(32, R - 32 * kb);
             for (int kk = 0; kk < kn; kk++) {
                 const int k = 32 * kb + kk;
-                T mk = __shfl_sync(0xffffffffu, mreg[kb], kk);
+                double mk = __shfl_sync(0xffffffffu, mreg[kb], kk);
 #pragma unroll
                 for (int j = 0; j < UP_MAXC; j++) {
                     int c = lane + 32 * j;
@@ -180,8 +180,9 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const T* __restrict__ M, 
         for (int j = 0; j < UP_MAXC; j++) {
             int c = lane + 32 * j;
             if (c < R) {
-                U[i * R + c] = acc[j];
-                sq[j] += (double)acc[j] * (double)acc[j];
+                const T u = (T)acc[j];
+                U[i * R + c] = u;
+                sq[j] += (double)u * (double)u;
             }
         }
     }
@@ -195,6 +196,81 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const T* __restrict__ M, 
         double s = 0.0;
         for (int w = 0; w < nw; w++) s += csq[w * R + c];
         colsq_partials[(size_t)blockIdx.x * R + c] = s;
+    }
+}
+
+// Register-tiled form of k_update for R in {16, 32, 64}: a block stages 64
+// rows of M in shared memory; thread (rg, cg) of 16 x 16 computes rows
+// 4*rg..4*rg+3 and columns cg*CPT..cg*CPT+CPT-1 (CPT = R / 16), so each
+// inner step reuses 4 M values and CPT P values for 4*CPT FMAs.
+constexpr int UT_ROWS = 64;
+
+// The product is formed in FP64 whatever the storage type T: the
+// pseudoinverse of an ill-conditioned Hadamard product of Grams turns FP32
+// rounding in this step into fit errors well above 1e-5.
+template <typename T, int R>
+__global__ __launch_bounds__(DN_THREADS) void k_update_tiled(const T* __restrict__ M, const double* __restrict__ P,
+                                                             T* __restrict__ U, uint64_t I,
+                                                             double* __restrict__ colsq_partials)
+{
+    constexpr int CPT = R / 16;
+    extern __shared__ __align__(16) double us[];
+    double* csq = us;                                        // [16 row groups][R]
+    double* PT = us + 16 * R;                                // [R][R], PT[k][c] = P[c][k]
+    double* Ms = PT + R * R;                                 // [UT_ROWS][R + 1]
+    const int tid = threadIdx.x, rg = tid / 16, cg = tid % 16;
+    for (int k = tid; k < R * R; k += DN_THREADS) {
+        int c = k / R, kk = k % R;
+        PT[kk * R + c] = P[k];
+    }
+    double sq[CPT];
+#pragma unroll
+    for (int j = 0; j < CPT; j++) sq[j] = 0.0;
+    const uint64_t per = (I + gridDim.x - 1) / gridDim.x;
+    const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
+    for (uint64_t r0 = beg; r0 < end; r0 += UT_ROWS) {
+        const int nr = (int)min((uint64_t)UT_ROWS, end - r0);
+        __syncthreads();
+        for (int k = tid; k < nr * R; k += DN_THREADS) Ms[(k / R) * (R + 1) + (k % R)] = (double)M[r0 * R + k];
+        __syncthreads();
+        double acc[4][CPT];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < CPT; j++) acc[i][j] = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < R; k++) {
+            double m[4], pv[CPT];
+#pragma unroll
+            for (int i = 0; i < 4; i++) m[i] = Ms[(4 * rg + i) * (R + 1) + k];
+#pragma unroll
+            for (int j = 0; j < CPT; j++) pv[j] = PT[k * R + cg * CPT + j];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < CPT; j++) acc[i][j] += m[i] * pv[j];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int r = 4 * rg + i;
+            if (r < nr) {
+#pragma unroll
+                for (int j = 0; j < CPT; j++) {
+                    const T u = (T)acc[i][j];
+                    U[(r0 + r) * R + cg * CPT + j] = u;
+                    sq[j] += (double)u * (double)u;
+                }
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < CPT; j++) csq[rg * R + cg * CPT + j] = sq[j];
+    __syncthreads();
+    for (int c = tid; c < R; c += DN_THREADS) {
+        double t = 0.0;
+        for (int g = 0; g < 16; g++) t += csq[g * R + c];
+        colsq_partials[(size_t)blockIdx.x * R + c] = t;
     }
 }
 
@@ -535,6 +611,25 @@ int gram_launch(blco_cpals_plan* p, T* U, uint64_t I, const double* inv, double*
     return BLCO_OK;
 }
 
+template <typename T>
+int update_launch(blco_cpals_plan* p, const T* M, T* U, uint64_t I, int grid)
+{
+    const int R = p->R;
+    if (R == 16 || R == 32 || R == 64) {
+        size_t smem = ((size_t)16 * R + (size_t)R * R + (size_t)UT_ROWS * (R + 1)) * sizeof(double);
+        void (*fn)(const T*, const double*, T*, uint64_t, double*) =
+            R == 16 ? k_update_tiled<T, 16> : R == 32 ? k_update_tiled<T, 32> : k_update_tiled<T, 64>;
+        BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        fn<<<grid, DN_THREADS, smem, p->s>>>(M, p->P, U, I, p->partials);
+    } else {
+        size_t smem = (size_t)(R * R + (DN_THREADS / 32) * R) * sizeof(double);
+        BLCO_CUDA(cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_update<T><<<grid, DN_THREADS, smem, p->s>>>(M, p->P, U, I, R, p->partials);
+    }
+    BLCO_CHECK_LAUNCH("k_update");
+    return BLCO_OK;
+}
+
 int conv_grid(uint64_t n, int sm) { return (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm * 8)); }
 
 int mode_update(blco_cpals_plan* p, int n)
@@ -577,15 +672,8 @@ int mode_update(blco_cpals_plan* p, int n)
     BLCO_CHECK_LAUNCH("k_solve");
 
     int grid = grid_rows(I, p->sm);
-    size_t usmem = (size_t)(R * R + (DN_THREADS / 32) * R) * sizeof(double);
-    if (p->mixed) {
-        BLCO_CUDA(cudaFuncSetAttribute(k_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
-        k_update<float><<<grid, DN_THREADS, usmem, p->s>>>(p->Mf, p->P, p->Uf[n], I, R, p->partials);
-    } else {
-        BLCO_CUDA(cudaFuncSetAttribute(k_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usmem));
-        k_update<double><<<grid, DN_THREADS, usmem, p->s>>>(p->M, p->P, p->U[n], I, R, p->partials);
-    }
-    BLCO_CHECK_LAUNCH("k_update");
+    if (p->mixed) BLCO_TRY(update_launch<float>(p, p->Mf, p->Uf[n], I, grid));
+    else BLCO_TRY(update_launch<double>(p, p->M, p->U[n], I, grid));
     k_lambda<<<1, 128, 0, p->s>>>(p->partials, grid, R, p->lambda, p->inv);
     BLCO_CHECK_LAUNCH("k_lambda");
     if (p->mixed) {

@@ -193,52 +193,58 @@ def kruskal_random_init(dims, rank, seed, nthreads):
     return factors, lam
 
 
-_refgpu = None
+def refgpu_available():
+    """True when the reference's GPU build (oracle/_ref/libblco_refgpu.so,
+    `make -C oracle ref-gpu`) is present.  It needs a B200 to run."""
+    return os.path.exists(os.path.join(HERE, "_ref", "libblco_refgpu.so"))
 
 
-def refgpu_lib():
-    """The reference's own GPU CP-ALS/MTTKRP (oracle/_ref/libblco_refgpu.so,
-    built by `make -C oracle ref-gpu`), or None.  Needs a B200 to run."""
-    global _refgpu
-    if _refgpu is None:
-        path = os.path.join(HERE, "_ref", "libblco_refgpu.so")
-        if not os.path.exists(path):
-            return None
-        G = ctypes.CDLL(path)
-        G.refgpu_cpals.restype = ctypes.c_double
-        G.refgpu_cpals.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int,
-                                   ctypes.c_void_p, _f64p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                   ctypes.c_int, ctypes.c_int]
-        G.refgpu_mttkrp.restype = None
-        G.refgpu_mttkrp.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int,
-                                    ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                    ctypes.c_int]
-        _refgpu = G
-    return _refgpu
+def _refgpu_call(req, log_path=None):
+    """Runs one reference call in a child interpreter (the reference exits
+    the process on CUDA errors); returns the result arrays."""
+    import subprocess
+    import sys
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        qp, rp = os.path.join(d, "req.npz"), os.path.join(d, "res.npz")
+        np.savez(qp, **req)
+        p = subprocess.run([sys.executable, os.path.join(HERE, "refgpu_run.py"), qp, rp],
+                           capture_output=True, text=True, timeout=600)
+        if log_path:
+            with open(log_path, "a") as f:
+                f.write(p.stdout + p.stderr)
+        if p.returncode != 0 or not os.path.exists(rp):
+            tail = (p.stdout + p.stderr)[-2000:]
+            raise RuntimeError(f"reference GPU call failed (exit {p.returncode}):\n{tail}")
+        return dict(np.load(rp))
 
 
-def refgpu_cpals(dims, cidx, vals, factors, lam, maxiter, tol, kernel=10, nprtn=8, thread_cf=2):
-    """Runs the reference cpals_blco_dev; factors/lam updated in place."""
-    G = refgpu_lib()
-    dims = np.ascontiguousarray(dims, dtype=np.uint64)
-    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
-    vals = np.ascontiguousarray(vals, dtype=np.float64)
-    for f in factors:
-        assert f.flags.c_contiguous and f.dtype == np.float64
-    return G.refgpu_cpals(len(dims), _p(dims, _u64p), cidx.shape[1], _p(cidx, _u64p), _p(vals, _f64p),
-                          factors[0].shape[1], _ptr_array(factors), _p(lam, _f64p), maxiter, tol, kernel,
-                          nprtn, thread_cf)
+def _req(dims, cidx, vals, factors, **kw):
+    r = dict(dims=np.asarray(dims, dtype=np.uint64), cidx=np.asarray(cidx, dtype=np.uint64),
+             vals=np.asarray(vals, dtype=np.float64), rank=np.int64(factors[0].shape[1]))
+    for m, f in enumerate(factors):
+        r[f"f{m}"] = np.asarray(f, dtype=np.float64)
+    for k, v in kw.items():
+        r[k] = np.asarray(v)
+    return r
 
 
-def refgpu_mttkrp(dims, cidx, vals, factors, mode, kernel=1, nprtn=8, thread_cf=2):
+def refgpu_cpals(dims, cidx, vals, factors, lam, maxiter, tol, kernel=10, nprtn=8, thread_cf=2, log_path=None):
+    """Runs the reference cpals_blco_dev; factors/lam updated in place;
+    returns the final fit."""
+    res = _refgpu_call(_req(dims, cidx, vals, factors, op="cpals", lam=lam, maxiter=maxiter, tol=tol,
+                            kernel=kernel, nprtn=nprtn, thread_cf=thread_cf), log_path)
+    for m, f in enumerate(factors):
+        f[:] = res[f"f{m}"]
+    lam[:] = res["lam"]
+    return float(res["fit"])
+
+
+def refgpu_mttkrp(dims, cidx, vals, factors, mode, kernel=1, nprtn=8, thread_cf=2, log_path=None):
     """Runs the reference mttkrp_alto_dev once into a zeroed target factor;
     returns the MTTKRP."""
-    G = refgpu_lib()
-    dims = np.ascontiguousarray(dims, dtype=np.uint64)
-    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
-    vals = np.ascontiguousarray(vals, dtype=np.float64)
-    fs = [np.ascontiguousarray(f, dtype=np.float64).copy() for f in factors]
+    fs = [np.array(f, dtype=np.float64) for f in factors]
     fs[mode][:] = 0.0
-    G.refgpu_mttkrp(len(dims), _p(dims, _u64p), cidx.shape[1], _p(cidx, _u64p), _p(vals, _f64p),
-                    fs[0].shape[1], _ptr_array(fs), mode, kernel, 1, nprtn, thread_cf)
-    return fs[mode]
+    res = _refgpu_call(_req(dims, cidx, vals, fs, op="mttkrp", mode=mode, kernel=kernel, nprtn=nprtn,
+                            thread_cf=thread_cf), log_path)
+    return res[f"f{mode}"]

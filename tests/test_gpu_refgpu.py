@@ -16,7 +16,7 @@ from conftest import unique_coords
 
 pytestmark = pytest.mark.gpu
 
-if po.refgpu_lib() is None:
+if not po.refgpu_available():
     pytest.skip("oracle/_ref/libblco_refgpu.so not built", allow_module_level=True)
 
 
