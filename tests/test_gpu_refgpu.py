@@ -20,7 +20,12 @@ if not po.refgpu_available():
     pytest.skip("oracle/_ref/libblco_refgpu.so not built", allow_module_level=True)
 
 
-@pytest.mark.parametrize("ref_kernel", [1, 2, 3, 10, 13])
+# The reference's kernel 13 (mttkrp_atomic, src/alto_dev.cu:1831-1847) reads
+# blk->mode_pos / blk->mode_masks, which are null on the device blocks built
+# by gen_block_device (src/blco.cu:93-103): it raised an illegal memory
+# access on the B200 and is not run again.  This engine's kernel 13 is
+# covered against the oracle in test_gpu_mttkrp.py.
+@pytest.mark.parametrize("ref_kernel", [1, 2, 3, 10])
 def test_mttkrp_matches_reference_gpu(blco, ref_kernel):
     import torch
     rng = np.random.default_rng(ref_kernel)
