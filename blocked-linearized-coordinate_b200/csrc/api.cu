@@ -237,6 +237,8 @@ int blco_tensor_free(blco_tensor* t)
         cudaFree(t->hot[n].d_keys);
         cudaFree(t->hot[n].d_slot);
         cudaFree(t->hot[n].d_rows);
+        cudaFree(t->hot[n].d_idx);
+        cudaFree(t->hot[n].d_ptr);
     }
     delete t;
     return BLCO_OK;

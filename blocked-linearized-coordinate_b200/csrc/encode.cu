@@ -320,13 +320,14 @@ int scan_u32(uint32_t* a, uint64_t n, uint32_t* sums, cudaStream_t s)
     return BLCO_OK;
 }
 
-// Sorts (k0, v0) by the low `bits` key bits; ping-pongs with (k1, v1).
-// *in_alt is set when the result ends up in (k1, v1).
-int radix_sort_pairs(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint64_t n, int bits,
+// Sorts (k0, v0) stably by key bits [begin_bit, end_bit); ping-pongs with
+// (k1, v1).  *in_alt is set when the result ends up in (k1, v1).
+int radix_sort_pairs(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint64_t n, int begin_bit, int end_bit,
                      cudaStream_t s, bool* in_alt)
 {
     *in_alt = false;
-    if (n <= 1 || bits <= 0) return BLCO_OK;
+    const int bits = end_bit;
+    if (n <= 1 || end_bit <= begin_bit) return BLCO_OK;
     uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
     uint64_t L = (uint64_t)RS_RADIX * ntiles;
     uint32_t nsums = (uint32_t)((L + SC_CHUNK - 1) / SC_CHUNK);
@@ -337,7 +338,7 @@ int radix_sort_pairs(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint64_
     uint64_t *ki = k0, *ko = k1;
     double *vi = v0, *vo = v1;
     int st = BLCO_OK;
-    for (int shift = 0; shift < bits; shift += 8) {
+    for (int shift = begin_bit; shift < bits; shift += 8) {
         k_rs_hist<<<ntiles, RS_THREADS, 0, s>>>(ki, n, shift, counts, ntiles);
         count_launch();
         if ((st = scan_u32(counts, L, sums, s)) != BLCO_OK) break;
@@ -440,8 +441,8 @@ __global__ void k_row_stats(const uint32_t* __restrict__ counts, uint64_t rows, 
 }
 
 constexpr int HOT_CAND_MAX = 8192;
-constexpr int HOT_MAX = 2048;     // rows kept per mode
-constexpr int HOT_HASH = 4096;    // hash size (power of two, 2x HOT_MAX)
+constexpr int HOT_MAX = 4096;     // rows kept per mode
+constexpr int HOT_HASH = 8192;    // hash size (power of two, 2x HOT_MAX)
 constexpr uint32_t HOT_MIN_COUNT = 256;
 
 __global__ void k_collect_hot(const uint32_t* __restrict__ counts, uint64_t rows, uint32_t thresh,
@@ -458,6 +459,33 @@ __global__ void k_collect_hot(const uint32_t* __restrict__ counts, uint64_t rows
             }
         }
     }
+}
+
+// key_i = (slot of the mode-n row of nonzero i, or 0xffff) << 32 | i.
+__global__ void k_hot_keys(const uint64_t* __restrict__ coords, uint64_t nnz, int pos, uint64_t mask,
+                           const uint32_t* __restrict__ hkeys, const uint32_t* __restrict__ hslot, int hsize,
+                           uint64_t* __restrict__ keys)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t row = (uint32_t)((coords[i] >> pos) & mask);
+        uint32_t h = hash_row(row) & (hsize - 1), slot = 0xffffu;
+        for (int probe = 0; probe < hsize; probe++) {
+            uint32_t k = hkeys[h];
+            if (k == row + 1) {
+                slot = hslot[h];
+                break;
+            }
+            if (k == 0) break;
+            h = (h + 1) & (hsize - 1);
+        }
+        keys[i] = ((uint64_t)slot << 32) | i;
+    }
+}
+
+__global__ void k_low32(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (uint32_t)keys[i];
 }
 
 __global__ void k_sumsq(const double* __restrict__ v, uint64_t n, double* __restrict__ partial)
@@ -479,6 +507,56 @@ __global__ void k_sumsq(const double* __restrict__ v, uint64_t n, double* __rest
 } // namespace
 
 uint32_t host_hash_row(uint32_t r) { return (r * 2654435761u) >> 7; }
+
+// Positions of the hot-row nonzeros of every mode, grouped by slot: a stable
+// radix sort of (slot << 32 | position) on the slot bits keeps the ALTO
+// order inside each row.
+int build_hot_csr(blco_tensor* t, cudaStream_t s)
+{
+    const Layout& L = t->layout;
+    if (t->nnz == 0) return BLCO_OK;
+    bool any = false;
+    for (int n = 0; n < L.nmodes; n++) any |= t->hot[n].nhot > 0;
+    if (!any) return BLCO_OK;
+    DeviceInfo di;
+    BLCO_TRY(device_info(t->device, &di));
+    uint64_t *k0 = nullptr, *k1 = nullptr;
+    double *v0 = nullptr, *v1 = nullptr;
+    int st = BLCO_OK;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(s);
+        cudaFree(k0);
+        cudaFree(k1);
+        cudaFree(v0);
+        cudaFree(v1);
+    };
+    cudaError_t e = cudaMalloc(&k0, t->nnz * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&k1, t->nnz * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&v0, t->nnz * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&v1, t->nnz * 8);
+    if (e != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "hot-row index scratch", __FILE__, __LINE__);
+    }
+    const int grid = (int)std::min<uint64_t>((t->nnz + 255) / 256, (uint64_t)di.sm_count * 16);
+    for (int n = 0; n < L.nmodes && st == BLCO_OK; n++) {
+        HotTable& ht = t->hot[n];
+        if (ht.nhot == 0 || ht.hot_nnz == 0) continue;
+        k_hot_keys<<<grid, 256, 0, s>>>(t->d_coords, t->nnz, L.mode_pos[n], L.mode_masks[n], ht.d_keys, ht.d_slot,
+                                        ht.hash_size, k0);
+        count_launch();
+        if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "k_hot_keys", __FILE__, __LINE__); break; }
+        bool alt = false;
+        if ((st = radix_sort_pairs(k0, v0, k1, v1, t->nnz, 32, 48, s, &alt)) != BLCO_OK) break;
+        e = cudaMalloc(&ht.d_idx, ht.hot_nnz * sizeof(uint32_t));
+        if (e != cudaSuccess) { st = cuda_fail(e, "hot-row index", __FILE__, __LINE__); break; }
+        k_low32<<<grid, 256, 0, s>>>(alt ? k1 : k0, ht.hot_nnz, ht.d_idx);
+        count_launch();
+        if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "k_low32", __FILE__, __LINE__); break; }
+    }
+    cleanup();
+    return st;
+}
 
 int build_hot_tables(blco_tensor* t, cudaStream_t s)
 {
@@ -579,8 +657,13 @@ int build_hot_tables(blco_tensor* t, cudaStream_t s)
         BLCO_CUDA(cudaMemcpyAsync(ht.d_keys, keys.data(), HOT_HASH * 4, cudaMemcpyHostToDevice, s));
         BLCO_CUDA(cudaMemcpyAsync(ht.d_slot, slots.data(), HOT_HASH * 4, cudaMemcpyHostToDevice, s));
         BLCO_CUDA(cudaMemcpyAsync(ht.d_rows, rowlist.data(), ht.nhot * 4, cudaMemcpyHostToDevice, s));
+        std::vector<uint32_t> ptr(ht.nhot + 1, 0);
+        for (int k = 0; k < ht.nhot; k++) ptr[k + 1] = ptr[k] + rows[k].first;
+        BLCO_CUDA(cudaMalloc(&ht.d_ptr, (ht.nhot + 1) * sizeof(uint32_t)));
+        BLCO_CUDA(cudaMemcpyAsync(ht.d_ptr, ptr.data(), (ht.nhot + 1) * 4, cudaMemcpyHostToDevice, s));
     }
     BLCO_CUDA(cudaStreamSynchronize(s));
+    BLCO_TRY(build_hot_csr(t, s));
     return BLCO_OK;
 }
 
@@ -663,7 +746,7 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
             cudaFree(v0);
             return cleanup_fail(fail(BLCO_ERR_INVALID, "a coordinate is not below its mode length"));
         }
-        st = radix_sort_pairs(k0, v0, k1, v1, nnz, t->layout.alto_bits, s, &in_alt);
+        st = radix_sort_pairs(k0, v0, k1, v1, nnz, 0, t->layout.alto_bits, s, &in_alt);
         if (st != BLCO_OK) {
             free_tmp();
             cudaFree(k0);

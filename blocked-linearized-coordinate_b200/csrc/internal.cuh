@@ -78,6 +78,10 @@ struct HotTable {
     int hash_size = 0;          // power of two (0 = no table)
     int nhot = 0;               // number of rows in the table
     uint64_t hot_nnz = 0;       // nonzeros that fall on hot rows
+    // CSR view of the hot rows: positions (into the BLCO stream) of the
+    // nonzeros of hot row slot s are d_idx[d_ptr[s] .. d_ptr[s+1]), ascending.
+    uint32_t* d_idx = nullptr;
+    uint32_t* d_ptr = nullptr;  // nhot + 1 entries
 };
 
 struct ModeStats {

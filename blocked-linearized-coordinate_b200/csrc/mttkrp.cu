@@ -89,7 +89,18 @@ struct MtParams {
     int direct;                // 1: every row of the target mode is a slot (slot = row)
     int nacc;                  // rows held in the shared accumulator
     int merge;                 // 0: flush every nonzero on its own (kernel 13)
+    int skip_hot;              // 1: nonzeros of table rows are left to k_mttkrp_hot
     uint64_t tiles_per_cta;
+};
+
+// The CSR view of a mode's hot rows (HotTable::d_idx / d_ptr).
+struct HotParams {
+    const uint32_t* idx;  // stream positions, grouped by slot, ascending inside a slot
+    const uint32_t* ptr;  // nhot + 1 offsets into idx
+    const uint32_t* rows; // slot -> row
+    int nhot;
+    uint32_t total;       // ptr[nhot]
+    uint32_t chunk;       // positions per warp task (multiple of 32)
 };
 
 __device__ __forceinline__ uint32_t hot_hash(uint32_t r) { return (r * 2654435761u) >> 7; }
@@ -217,11 +228,15 @@ __device__ __forceinline__ int stage_tile(const MtParams& p, const ModeSel<NM>& 
 #pragma unroll
     for (int k = 0; k < NM - 1; k++) ro[k] = (uint32_t)((c >> ms.opos[k]) & ms.omask[k]);
     int slot = valid ? hot_lookup(p, skeys, sslot, rt) : -1;
-    uint32_t key = valid ? rt : 0xffffffffu;
+    // Entries that take no part (past the end, or hot rows handled by the
+    // CSR kernel) are ordered after the working ones.
+    const bool work = valid && !(p.skip_hot && slot >= 0);
+    const uint32_t wmask = __ballot_sync(0xffffffffu, work);
+    uint32_t key = work ? rt : 0xffffffffu;
     uint32_t peers = __match_any_sync(0xffffffffu, key);
     const uint32_t lt = (1u << lane) - 1;
     int leader = __ffs(peers) - 1;
-    uint32_t x = lane == leader ? (uint32_t)__popc(peers) : 0u;
+    uint32_t x = (lane == leader && work) ? (uint32_t)__popc(peers) : 0u;
     uint32_t inc = x;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -229,8 +244,9 @@ __device__ __forceinline__ int stage_tile(const MtParams& p, const ModeSel<NM>& 
         if (lane >= o) inc += y;
     }
     uint32_t start = __shfl_sync(0xffffffffu, inc - x, leader);
-    int sp = (int)start + __popc(peers & lt);
-    bool last = (peers >> lane) == 1u;
+    const int count = __popc(wmask);
+    int sp = work ? (int)start + __popc(peers & lt) : count + __popc(~wmask & lt);
+    bool last = work && (peers >> lane) == 1u;
     ends = __reduce_or_sync(0xffffffffu, last ? (1u << sp) : 0u);
     Rec r;
     r.a = make_uint4(rt, (uint32_t)slot, ro[0], ro[1]);
@@ -240,8 +256,7 @@ __device__ __forceinline__ int stage_tile(const MtParams& p, const ModeSel<NM>& 
     dst[0] = r.a;
     dst[1] = r.b;
     __syncwarp();
-    uint64_t rem = p.nnz - i0;
-    return rem >= 32 ? 32 : (int)rem;
+    return count;
 }
 
 // 16-byte gather of VEC factor entries, widened to the accumulator type.
@@ -397,6 +412,120 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
     }
 }
 
+// Hot-row kernel: walks the CSR view of the mode's heaviest rows.  Warp
+// tasks are chunks of `chunk` consecutive positions; inside a chunk the
+// nonzeros come grouped by row, so each lane group keeps its partial sum in
+// registers across the whole chunk and flushes it (global atomics) only when
+// its row changes and at the chunk end.  No shared-memory accumulators and
+// no sorting are needed.
+template <int NM, int R, class P>
+__global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_hot(MtParams p, HotParams h)
+{
+    typedef typename P::TV TV;
+    typedef typename P::TA TA;
+    constexpr int VEC = P::VEC;
+    constexpr int LPN = R / VEC;
+    constexpr int GROUPS = 32 / LPN;
+    constexpr int PER = 32 / GROUPS;
+    constexpr int STAGE = 32 * REC_BYTES + GROUPS * 16;
+    constexpr int MT_UNROLL = P::UNROLL;
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t* sptr = reinterpret_cast<uint32_t*>(smem);   // nhot + 1
+    uint32_t* srows = sptr + h.nhot + 1;                    // nhot
+    unsigned char* stages =
+        reinterpret_cast<unsigned char*>(((uintptr_t)(srows + h.nhot) + 15) & ~(uintptr_t)15);
+    for (int i = threadIdx.x; i <= h.nhot; i += blockDim.x) sptr[i] = h.ptr[i];
+    for (int i = threadIdx.x; i < h.nhot; i += blockDim.x) srows[i] = h.rows[i];
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = lane / LPN, q = lane % LPN;
+    unsigned char* st = stages + (size_t)warp * STAGE;
+    const ModeSel<NM> ms(p);
+    const uint32_t nchunks = (h.total + h.chunk - 1) / h.chunk;
+    const uint32_t nw = gridDim.x * MT_WARPS;
+    TA acc[VEC];
+    int acc_slot = -1;
+    for (uint32_t c = blockIdx.x * MT_WARPS + warp; c < nchunks; c += nw) {
+        const uint32_t j0 = c * h.chunk, j1 = min(h.total, j0 + h.chunk);
+        // slot holding position j0: the last s with sptr[s] <= j0
+        int lo = 0, hi = h.nhot - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (sptr[mid] <= j0) lo = mid;
+            else hi = mid - 1;
+        }
+        int cur = lo;
+#pragma unroll
+        for (int j = 0; j < VEC; j++) acc[j] = TA(0);
+        acc_slot = -1;
+        for (uint32_t sub = j0; sub < j1; sub += 32) {
+            while (cur < h.nhot - 1 && sptr[cur + 1] <= sub) cur++;
+            const uint32_t jj = sub + lane;
+            const bool valid = jj < j1;
+            int ls = cur;
+            if (valid)
+                while (ls < h.nhot - 1 && sptr[ls + 1] <= jj) ls++;
+            const uint32_t i = valid ? __ldg(h.idx + jj) : 0u;
+            const uint64_t cc = valid ? p.coords[i] : 0ull;
+            const TV v = valid ? reinterpret_cast<const TV*>(p.vals)[i] : TV(0);
+            uint32_t ro[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < NM - 1; k++) ro[k] = (uint32_t)((cc >> ms.opos[k]) & ms.omask[k]);
+            Rec r;
+            r.a = make_uint4(0u, (uint32_t)ls, ro[0], ro[1]);
+            r.b = make_uint4(ro[2], ro[3], 0u, 0u);
+            rec_set_val<TV>(r.b, v);
+            uint4* dst = reinterpret_cast<uint4*>(st + rec_offset<PER>(lane));
+            dst[0] = r.a;
+            dst[1] = r.b;
+            __syncwarp();
+            const int count = (int)min(32u, j1 - sub);
+            const int pb = grp * PER, pe = min(pb + PER, count);
+            for (int p0 = pb; p0 < pe; p0 += MT_UNROLL) {
+                TA g[MT_UNROLL][NM > 1 ? NM - 1 : 1][VEC];
+                Rec rec[MT_UNROLL];
+#pragma unroll
+                for (int u = 0; u < MT_UNROLL; u++) {
+                    int pp = p0 + u;
+                    if (pp < pe) {
+                        const uint4* src = reinterpret_cast<const uint4*>(st + rec_offset<PER>(pp));
+                        rec[u].a = src[0];
+                        rec[u].b = src[1];
+#pragma unroll
+                        for (int k = 0; k < NM - 1; k++)
+                            Gather<P>::load(ms.of[k], rec_oth(rec[u], k), R, q, g[u][k]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < MT_UNROLL; u++) {
+                    int pp = p0 + u;
+                    if (pp < pe) {
+                        const int s = (int)rec[u].a.y;
+                        if (s != acc_slot) {
+                            if (acc_slot >= 0) flush_global<P>(p.out, srows[acc_slot], R, q, acc);
+#pragma unroll
+                            for (int j = 0; j < VEC; j++) acc[j] = TA(0);
+                            acc_slot = s;
+                        }
+                        const TA vv = (TA)rec_val<TV>(rec[u].b);
+#pragma unroll
+                        for (int j = 0; j < VEC; j++) {
+                            TA prod = vv;
+#pragma unroll
+                            for (int k = 0; k < NM - 1; k++) prod *= g[u][k][j];
+                            acc[j] += prod;
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        if (acc_slot >= 0) flush_global<P>(p.out, srows[acc_slot], R, q, acc);
+        acc_slot = -1;
+    }
+}
+
 // Generic kernel: any R up to 256, a whole warp per nonzero, columns
 // lane, lane+32, ...  Used for ranks the vectorised kernels do not cover and
 // for factor pointers that are not 16-byte aligned.
@@ -498,6 +627,34 @@ KernelFn pick_vec(int R)
     case 32: return k_mttkrp_vec<NM, 32, P>;
     case 64: return k_mttkrp_vec<NM, 64, P>;
     case 128: if constexpr (V >= 4) return k_mttkrp_vec<NM, 128, P>; else return nullptr;
+    default: return nullptr;
+    }
+}
+
+typedef void (*HotFn)(MtParams, HotParams);
+
+template <int NM, class P>
+HotFn pick_hot_nm(int R)
+{
+    constexpr int V = P::VEC;
+    switch (R) {
+    case 8: return k_mttkrp_hot<NM, 8, P>;
+    case 16: return k_mttkrp_hot<NM, 16, P>;
+    case 32: return k_mttkrp_hot<NM, 32, P>;
+    case 64: return k_mttkrp_hot<NM, 64, P>;
+    case 128: if constexpr (V >= 4) return k_mttkrp_hot<NM, 128, P>; else return nullptr;
+    default: return nullptr;
+    }
+}
+
+template <class P>
+HotFn pick_hot(int nm, int R)
+{
+    switch (nm) {
+    case 2: return pick_hot_nm<2, P>(R);
+    case 3: return pick_hot_nm<3, P>(R);
+    case 4: return pick_hot_nm<4, P>(R);
+    case 5: return pick_hot_nm<5, P>(R);
     default: return nullptr;
     }
 }
@@ -605,9 +762,32 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     const int kern = mttkrp_select_kernel(t, a.mode, a.rank, a.kernel, a.factor_dtype);
     const size_t stage = stage_bytes(a.rank, policy_vec(a.factor_dtype));
     const HotTable& ht = t->hot[a.mode];
+    // The vectorised kernels load 16 bytes at a time: every factor must start
+    // on a 16-byte boundary (and the FP32 output on 16 bytes for the vector
+    // atomics), otherwise take the scalar kernel.
+    bool aligned16 = ((uintptr_t)a.out & 15u) == 0;
+    for (int m = 0; m < L.nmodes; m++)
+        if (m != a.mode && ((uintptr_t)a.factors[m] & 15u) != 0) aligned16 = false;
     size_t hash_bytes = 0;
+    HotFn hot_fn = nullptr;
+    if (kern == BLCO_KERNEL_LVL2 && ht.nhot > 0 && ht.d_idx && aligned16 && a.coords == t->d_coords) {
+        switch (a.factor_dtype) {
+        case BLCO_DTYPE_F64: hot_fn = pick_hot<PolicyF64>(L.nmodes, a.rank); break;
+        case BLCO_DTYPE_F32: hot_fn = pick_hot<PolicyF32>(L.nmodes, a.rank); break;
+        default: hot_fn = pick_hot<PolicyBF16>(L.nmodes, a.rank); break;
+        }
+    }
     if (kern == BLCO_KERNEL_LVL3) {
         p.direct = 1;
+    } else if (hot_fn) {
+        // Hot rows go to the CSR kernel; the tile kernel skips them.
+        p.hot_keys = ht.d_keys;
+        p.hot_slot = ht.d_slot;
+        p.hot_rows = ht.d_rows;
+        p.hash_size = ht.hash_size;
+        p.nhot = ht.nhot;
+        p.skip_hot = 1;
+        hash_bytes = 2 * sizeof(uint32_t) * ht.hash_size;
     } else if (kern == BLCO_KERNEL_LVL2 && ht.nhot > 0) {
         p.hot_keys = ht.d_keys;
         p.hot_slot = ht.d_slot;
@@ -621,16 +801,25 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     } else if (kern == BLCO_KERNEL_ATOMIC) {
         p.merge = 0;
     }
-    const size_t nacc = p.direct ? (size_t)L.dims[a.mode] : (size_t)p.nhot;
+    const size_t nacc = p.direct ? (size_t)L.dims[a.mode] : p.skip_hot ? 0 : (size_t)p.nhot;
     p.nacc = (int)nacc;
     const size_t smem = hash_bytes + nacc * a.rank * accb + stage + 16;
     if (smem > di.smem_optin) return fail(BLCO_ERR_UNSUPPORTED, "MTTKRP shared memory plan exceeds the device limit");
-    // The vectorised kernels load 16 bytes at a time: every factor must start
-    // on a 16-byte boundary (and the FP32 output on 16 bytes for the vector
-    // atomics), otherwise take the scalar kernel.
-    bool aligned16 = ((uintptr_t)a.out & 15u) == 0;
-    for (int m = 0; m < L.nmodes; m++)
-        if (m != a.mode && ((uintptr_t)a.factors[m] & 15u) != 0) aligned16 = false;
+    if (hot_fn) {
+        HotParams h;
+        h.idx = ht.d_idx;
+        h.ptr = ht.d_ptr;
+        h.rows = ht.d_rows;
+        h.nhot = ht.nhot;
+        h.total = (uint32_t)ht.hot_nnz;
+        h.chunk = 8192;
+        const size_t hsmem = (size_t)(2 * ht.nhot + 1) * sizeof(uint32_t) + 16 + stage;
+        BLCO_CUDA(cudaFuncSetAttribute((const void*)hot_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+        const uint32_t nchunks = (h.total + h.chunk - 1) / h.chunk;
+        const uint32_t hgrid = std::max<uint32_t>(1, std::min<uint32_t>(di.sm_count, (nchunks + MT_WARPS - 1) / MT_WARPS));
+        hot_fn<<<hgrid, MT_THREADS, hsmem, s>>>(p, h);
+        BLCO_CHECK_LAUNCH("k_mttkrp_hot");
+    }
     KernelFn fn;
     switch (a.factor_dtype) {
     case BLCO_DTYPE_F64: fn = pick_kernel<PolicyF64>(L.nmodes, a.rank, aligned16); break;
