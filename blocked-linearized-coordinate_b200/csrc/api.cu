@@ -237,8 +237,11 @@ int blco_tensor_free(blco_tensor* t)
         cudaFree(t->hot[n].d_keys);
         cudaFree(t->hot[n].d_slot);
         cudaFree(t->hot[n].d_rows);
-        cudaFree(t->hot[n].d_idx);
         cudaFree(t->hot[n].d_ptr);
+        cudaFree(t->hot[n].d_hcoords);
+        cudaFree(t->hot[n].d_hvals);
+        cudaFree(t->hot[n].d_hvals32);
+        cudaFree(t->hot[n].d_acc);
     }
     delete t;
     return BLCO_OK;

@@ -6,8 +6,8 @@
 //   1. linearize: key_i = OR_n pdep(c_n,i, alto_mask_n)      (k_alto_keys)
 //   2. sort (key, value) pairs by key: stable LSD radix sort, 8-bit digits,
 //      one pass per 8 significant key bits                   (k_rs_*)
-//   3. re-linearize in place: coord_i = OR_n pext(key_i, alto_mask_n)
-//      << mode_pos_n                                         (k_relinearize)
+//   3. re-linearize: coord_i = OR_n pext(key_i, alto_mask_n) << mode_pos_n,
+//      fused into the last sort pass                         (k_rs_scatter)
 //   4. block split: consecutive max_block_size slices (host arithmetic; the
 //      upper key half is always zero for 64-bit keys, so every nonzero is in
 //      histogram bucket 0, include/blco.hpp:249-321)
@@ -58,33 +58,76 @@ struct CooPtrs {
     const uint64_t* c[BLCO_MAX_MODES];
 };
 
-// Software bit deposit/extract over the set bits of a mask, LSB first
-// (the ALT_PEXT semantics of include/bitops.hpp:18-41).
-__device__ __forceinline__ uint64_t dev_pdep(uint64_t x, uint64_t m)
+// Byte tables for the bit permutations of the encoder:
+//   dep[n][b][v] = pdep(v << 8b, alto_mask_n)            (coordinate -> key)
+//   rel[b][v]    = relinearized field bits of (v << 8b)   (key -> BLCO coord)
+// so a key is the OR of one lookup per coordinate byte and a BLCO coordinate
+// the OR of one lookup per key byte.
+struct EncTables {
+    uint64_t dep[BLCO_MAX_MODES][4][256];
+    uint64_t rel[8][256];
+};
+
+EncTables make_tables(const Layout& L)
 {
-    uint64_t r = 0;
-    for (int j = 0; m; j++) {
-        int p = __ffsll((long long)m) - 1;
-        r |= ((x >> j) & 1ull) << p;
-        m &= m - 1;
+    EncTables T;
+    memset(&T, 0, sizeof(T));
+    int mode_of[64], bit_of[64];
+    for (int p = 0; p < 64; p++) mode_of[p] = -1;
+    for (int n = 0; n < L.nmodes; n++) {
+        int j = 0;
+        for (int p = 0; p < 64; p++)
+            if (L.alto_masks[n] >> p & 1) {
+                mode_of[p] = n;
+                bit_of[p] = j++;
+            }
     }
-    return r;
+    for (int n = 0; n < L.nmodes; n++)
+        for (int b = 0; b < 4; b++)
+            for (int v = 0; v < 256; v++) {
+                uint64_t key = 0;
+                for (int p = 0; p < 64; p++)
+                    if (mode_of[p] == n && bit_of[p] >= 8 * b && bit_of[p] < 8 * b + 8 && (v >> (bit_of[p] - 8 * b) & 1))
+                        key |= 1ull << p;
+                T.dep[n][b][v] = key;
+            }
+    for (int b = 0; b < 8; b++)
+        for (int v = 0; v < 256; v++) {
+            uint64_t c = 0;
+            for (int j = 0; j < 8; j++) {
+                int p = 8 * b + j;
+                if ((v >> j & 1) && mode_of[p] >= 0) c |= 1ull << (L.mode_pos[mode_of[p]] + bit_of[p]);
+            }
+            T.rel[b][v] = c;
+        }
+    return T;
 }
 
-__device__ __forceinline__ uint64_t dev_pext(uint64_t x, uint64_t m)
+__device__ __forceinline__ uint64_t relin(const uint64_t (*rel)[256], uint64_t key, int nbytes)
 {
-    uint64_t r = 0;
-    for (int j = 0; m; j++) {
-        int p = __ffsll((long long)m) - 1;
-        r |= ((x >> p) & 1ull) << j;
-        m &= m - 1;
-    }
-    return r;
+    uint64_t c = 0;
+#pragma unroll
+    for (int b = 0; b < 8; b++)
+        if (b < nbytes) c |= rel[b][(key >> (8 * b)) & 255];
+    return c;
+}
+
+// Re-linearization on its own, for streams the sort leaves untouched (a
+// single nonzero).
+__global__ void k_relin(uint64_t* __restrict__ keys, uint64_t n, const EncTables* __restrict__ tabs, int nbytes)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        keys[i] = relin(tabs->rel, keys[i], nbytes);
 }
 
 __global__ void k_alto_keys(CooPtrs coo, const double* __restrict__ vals, uint64_t nnz, Layout L,
-                            uint64_t* __restrict__ keys, double* __restrict__ vout, int* __restrict__ bad)
+                            const EncTables* __restrict__ tabs, uint64_t* __restrict__ keys,
+                            double* __restrict__ vout, int* __restrict__ bad)
 {
+    __shared__ uint64_t dep[BLCO_MAX_MODES][4][256];
+    for (int i = threadIdx.x; i < BLCO_MAX_MODES * 4 * 256; i += blockDim.x)
+        (&dep[0][0][0])[i] = (&tabs->dep[0][0][0])[i];
+    __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
          i += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t key = 0;
@@ -94,7 +137,8 @@ __global__ void k_alto_keys(CooPtrs coo, const double* __restrict__ vals, uint64
             if (n < L.nmodes) {
                 uint64_t c = coo.c[n][i];
                 ok &= c < L.dims[n];
-                key |= dev_pdep(c, L.alto_masks[n]);
+#pragma unroll
+                for (int b = 0; b < 4; b++) key |= dep[n][b][(c >> (8 * b)) & 255];
             }
         }
         if (!ok) atomicExch(bad, 1);
@@ -103,26 +147,14 @@ __global__ void k_alto_keys(CooPtrs coo, const double* __restrict__ vals, uint64
     }
 }
 
-__global__ void k_relinearize(uint64_t* __restrict__ keys, uint64_t nnz, Layout L)
-{
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t key = keys[i], c = 0;
-#pragma unroll
-        for (int n = 0; n < BLCO_MAX_MODES; n++)
-            if (n < L.nmodes) c |= (dev_pext(key, L.alto_masks[n]) & L.mode_masks[n]) << L.mode_pos[n];
-        keys[i] = c;
-    }
-}
-
 // ----------------------------------------------------------- radix sort --
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ITEMS = 16;
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS; // 4096 keys per tile
+constexpr int RS_ITEMS = 8;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS; // 2048 keys per tile
 constexpr int RS_RADIX = 256;
-constexpr size_t RS_SMEM = RS_TILE * 16 + (RS_WARPS + 2) * RS_RADIX * 4;
+constexpr size_t RS_SMEM = RS_TILE * 16 + (RS_WARPS + 2) * RS_RADIX * 4 + 8 * 256 * 8;
 
 // Per-tile digit counts, digit-major: counts[d * ntiles + tile].
 __global__ __launch_bounds__(RS_THREADS) void k_rs_hist(const uint64_t* __restrict__ keys, uint64_t n, int shift,
@@ -229,19 +261,25 @@ __global__ __launch_bounds__(SC_THREADS) void k_scan_apply(uint32_t* __restrict_
 // warps) + (earlier rounds and lower lanes of its own warp), which keeps the
 // input order of equal digits.  The tile is reordered in shared memory and
 // written out with per-digit global offsets.
+// With rel != nullptr (last pass of the encoder sort) the keys are written
+// out re-linearized into BLCO coordinates.
 __global__ __launch_bounds__(RS_THREADS) void k_rs_scatter(const uint64_t* __restrict__ kin,
                                                            const double* __restrict__ vin,
                                                            uint64_t* __restrict__ kout, double* __restrict__ vout,
                                                            uint64_t n, int shift, const uint32_t* __restrict__ offsets,
-                                                           uint32_t ntiles)
+                                                           uint32_t ntiles, const EncTables* __restrict__ rel_tabs,
+                                                           int rel_bytes)
 {
     extern __shared__ __align__(16) unsigned char rs_smem[];
     uint64_t* skeys = reinterpret_cast<uint64_t*>(rs_smem);
     double* svals = reinterpret_cast<double*>(skeys + RS_TILE);
-    uint32_t* whist = reinterpret_cast<uint32_t*>(svals + RS_TILE);
+    uint64_t(*rel)[256] = reinterpret_cast<uint64_t(*)[256]>(svals + RS_TILE);
+    uint32_t* whist = reinterpret_cast<uint32_t*>(svals + RS_TILE + 8 * 256);
     uint32_t* tstart = whist + RS_WARPS * RS_RADIX;
     uint32_t* gbase = tstart + RS_RADIX;
     __shared__ uint32_t wsum[SC_THREADS / 32];
+    if (rel_tabs)
+        for (int i = threadIdx.x; i < 8 * 256; i += RS_THREADS) (&rel[0][0])[i] = (&rel_tabs->rel[0][0])[i];
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1;
@@ -303,7 +341,7 @@ __global__ __launch_bounds__(RS_THREADS) void k_rs_scatter(const uint64_t* __res
         uint64_t kk = skeys[i];
         uint32_t d = (uint32_t)((kk >> shift) & 255);
         uint64_t o = (uint64_t)gbase[d] + (i - tstart[d]);
-        kout[o] = kk;
+        kout[o] = rel_tabs ? relin(rel, kk, rel_bytes) : kk;
         vout[o] = svals[i];
     }
 }
@@ -323,7 +361,7 @@ int scan_u32(uint32_t* a, uint64_t n, uint32_t* sums, cudaStream_t s)
 // Sorts (k0, v0) stably by key bits [begin_bit, end_bit); ping-pongs with
 // (k1, v1).  *in_alt is set when the result ends up in (k1, v1).
 int radix_sort_pairs(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint64_t n, int begin_bit, int end_bit,
-                     cudaStream_t s, bool* in_alt)
+                     cudaStream_t s, bool* in_alt, const EncTables* rel_tabs = nullptr)
 {
     *in_alt = false;
     const int bits = end_bit;
@@ -342,7 +380,9 @@ int radix_sort_pairs(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint64_
         k_rs_hist<<<ntiles, RS_THREADS, 0, s>>>(ki, n, shift, counts, ntiles);
         count_launch();
         if ((st = scan_u32(counts, L, sums, s)) != BLCO_OK) break;
-        k_rs_scatter<<<ntiles, RS_THREADS, RS_SMEM, s>>>(ki, vi, ko, vo, n, shift, counts, ntiles);
+        const bool last = shift + 8 >= bits;
+        k_rs_scatter<<<ntiles, RS_THREADS, RS_SMEM, s>>>(ki, vi, ko, vo, n, shift, counts, ntiles,
+                                                         last ? rel_tabs : nullptr, (bits + 7) / 8);
         count_launch();
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { st = cuda_fail(e, "k_rs_scatter", __FILE__, __LINE__); break; }
@@ -482,10 +522,16 @@ __global__ void k_hot_keys(const uint64_t* __restrict__ coords, uint64_t nnz, in
     }
 }
 
-__global__ void k_low32(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ out)
+// hc[j] = coords[pos_j], hv[j] = vals[pos_j] with pos_j the low 32 bits of
+// the sorted key j.
+__global__ void k_gather_hot(const uint64_t* __restrict__ keys, uint64_t n, const uint64_t* __restrict__ coords,
+                             const double* __restrict__ vals, uint64_t* __restrict__ hc, double* __restrict__ hv)
 {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        out[i] = (uint32_t)keys[i];
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = (uint32_t)keys[j];
+        hc[j] = coords[i];
+        hv[j] = vals[i];
+    }
 }
 
 __global__ void k_sumsq(const double* __restrict__ v, uint64_t n, double* __restrict__ partial)
@@ -508,9 +554,10 @@ __global__ void k_sumsq(const double* __restrict__ v, uint64_t n, double* __rest
 
 uint32_t host_hash_row(uint32_t r) { return (r * 2654435761u) >> 7; }
 
-// Positions of the hot-row nonzeros of every mode, grouped by slot: a stable
-// radix sort of (slot << 32 | position) on the slot bits keeps the ALTO
-// order inside each row.
+// Row-grouped copies of the hot-row nonzeros of every mode: a stable radix
+// sort of (slot << 32 | position) on the slot bits gives the positions grouped
+// by slot with the ALTO order kept inside each row; the coordinates and
+// values are then gathered into a contiguous per-mode stream.
 int build_hot_csr(blco_tensor* t, cudaStream_t s)
 {
     const Layout& L = t->layout;
@@ -548,11 +595,13 @@ int build_hot_csr(blco_tensor* t, cudaStream_t s)
         if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "k_hot_keys", __FILE__, __LINE__); break; }
         bool alt = false;
         if ((st = radix_sort_pairs(k0, v0, k1, v1, t->nnz, 32, 48, s, &alt)) != BLCO_OK) break;
-        e = cudaMalloc(&ht.d_idx, ht.hot_nnz * sizeof(uint32_t));
-        if (e != cudaSuccess) { st = cuda_fail(e, "hot-row index", __FILE__, __LINE__); break; }
-        k_low32<<<grid, 256, 0, s>>>(alt ? k1 : k0, ht.hot_nnz, ht.d_idx);
+        e = cudaMalloc(&ht.d_hcoords, ht.hot_nnz * sizeof(uint64_t));
+        if (e == cudaSuccess) e = cudaMalloc(&ht.d_hvals, ht.hot_nnz * sizeof(double));
+        if (e != cudaSuccess) { st = cuda_fail(e, "hot-row stream copy", __FILE__, __LINE__); break; }
+        k_gather_hot<<<grid, 256, 0, s>>>(alt ? k1 : k0, ht.hot_nnz, t->d_coords, t->d_values, ht.d_hcoords,
+                                          ht.d_hvals);
         count_launch();
-        if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "k_low32", __FILE__, __LINE__); break; }
+        if ((e = cudaGetLastError()) != cudaSuccess) { st = cuda_fail(e, "k_gather_hot", __FILE__, __LINE__); break; }
     }
     cleanup();
     return st;
@@ -694,14 +743,17 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
     uint64_t *k0 = nullptr, *k1 = nullptr;
     double *v0 = nullptr, *v1 = nullptr;
     int* d_bad = nullptr;
+    EncTables* d_tabs = nullptr;
     auto free_tmp = [&]() {
         cudaStreamSynchronize(s);
         cudaFree(k1);
         cudaFree(v1);
         cudaFree(d_bad);
+        cudaFree(d_tabs);
         k1 = nullptr;
         v1 = nullptr;
         d_bad = nullptr;
+        d_tabs = nullptr;
     };
 #define ENC_CUDA(call)                                                          \
     do {                                                                        \
@@ -734,7 +786,10 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
         memset(&coo, 0, sizeof(coo));
         for (int n = 0; n < nmodes; n++) coo.c[n] = d_cidx[n];
         int grid = (int)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)di.sm_count * 16);
-        k_alto_keys<<<grid, 256, 0, s>>>(coo, d_vals, nnz, t->layout, k0, v0, d_bad);
+        EncTables htabs = make_tables(t->layout);
+        ENC_CUDA(cudaMalloc(&d_tabs, sizeof(EncTables)));
+        ENC_CUDA(cudaMemcpyAsync(d_tabs, &htabs, sizeof(EncTables), cudaMemcpyHostToDevice, s));
+        k_alto_keys<<<grid, 256, 0, s>>>(coo, d_vals, nnz, t->layout, d_tabs, k0, v0, d_bad);
         count_launch();
         ENC_CUDA(cudaGetLastError());
         int bad = 0;
@@ -746,7 +801,15 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
             cudaFree(v0);
             return cleanup_fail(fail(BLCO_ERR_INVALID, "a coordinate is not below its mode length"));
         }
-        st = radix_sort_pairs(k0, v0, k1, v1, nnz, 0, t->layout.alto_bits, s, &in_alt);
+        // The last pass writes BLCO coordinates (re-linearized keys).  With
+        // a key of 0 bits (every mode of length 1) no pass runs and the keys
+        // are all 0, which is also the coordinate.
+        st = radix_sort_pairs(k0, v0, k1, v1, nnz, 0, t->layout.alto_bits, s, &in_alt, d_tabs);
+        if (st == BLCO_OK && nnz <= 1 && t->layout.alto_bits > 0) {
+            k_relin<<<1, 32, 0, s>>>(k0, nnz, d_tabs, (t->layout.alto_bits + 7) / 8);
+            count_launch();
+            if (cudaGetLastError() != cudaSuccess) st = fail(BLCO_ERR_CUDA, "k_relin launch failed");
+        }
         if (st != BLCO_OK) {
             free_tmp();
             cudaFree(k0);
@@ -757,9 +820,6 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
             std::swap(k0, k1);
             std::swap(v0, v1);
         }
-        k_relinearize<<<grid, 256, 0, s>>>(k0, nnz, t->layout);
-        count_launch();
-        ENC_CUDA(cudaGetLastError());
         double* partial = reinterpret_cast<double*>(k1); // k1 is free now
         int g2 = std::min(grid, 1024);
         k_sumsq<<<g2, 256, 0, s>>>(v0, nnz, partial);

@@ -78,10 +78,15 @@ struct HotTable {
     int hash_size = 0;          // power of two (0 = no table)
     int nhot = 0;               // number of rows in the table
     uint64_t hot_nnz = 0;       // nonzeros that fall on hot rows
-    // CSR view of the hot rows: positions (into the BLCO stream) of the
-    // nonzeros of hot row slot s are d_idx[d_ptr[s] .. d_ptr[s+1]), ascending.
-    uint32_t* d_idx = nullptr;
+    // CSR copy of the hot rows' nonzeros: entries d_ptr[s] .. d_ptr[s+1] of
+    // d_hcoords / d_hvals are the nonzeros of hot row slot s, in ALTO order
+    // (a row-grouped copy of part of the stream, read contiguously).
     uint32_t* d_ptr = nullptr;  // nhot + 1 entries
+    uint64_t* d_hcoords = nullptr;
+    double* d_hvals = nullptr;
+    float* d_hvals32 = nullptr; // mixed form, made on first use
+    double* d_acc = nullptr;    // mixed form: FP64 sums of the hot rows (nhot x acc_rank)
+    int acc_rank = 0;
 };
 
 struct ModeStats {

@@ -93,14 +93,16 @@ struct MtParams {
     uint64_t tiles_per_cta;
 };
 
-// The CSR view of a mode's hot rows (HotTable::d_idx / d_ptr).
+// The row-grouped copy of a mode's hot rows (HotTable::d_hcoords / d_hvals).
 struct HotParams {
-    const uint32_t* idx;  // stream positions, grouped by slot, ascending inside a slot
-    const uint32_t* ptr;  // nhot + 1 offsets into idx
-    const uint32_t* rows; // slot -> row
+    const uint64_t* coords; // grouped by slot, ALTO order inside a slot
+    const void* vals;       // same order, TV of the policy
+    const uint32_t* ptr;    // nhot + 1 offsets
+    const uint32_t* rows;   // slot -> row
+    double* acc;            // non-null: FP64 per-slot sums (nhot x R) instead of the output
     int nhot;
-    uint32_t total;       // ptr[nhot]
-    uint32_t chunk;       // positions per warp task (multiple of 32)
+    uint32_t total;         // ptr[nhot]
+    uint32_t chunk;         // positions per warp task (multiple of 32)
 };
 
 __device__ __forceinline__ uint32_t hot_hash(uint32_t r) { return (r * 2654435761u) >> 7; }
@@ -444,8 +446,21 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_hot(MtParams p, HotPar
     const ModeSel<NM> ms(p);
     const uint32_t nchunks = (h.total + h.chunk - 1) / h.chunk;
     const uint32_t nw = gridDim.x * MT_WARPS;
-    TA acc[VEC];
+    // Partial sums run over up to `chunk` nonzeros: kept in FP64 in every form.
+    double acc[VEC];
     int acc_slot = -1;
+    auto flush = [&](int slot_id) {
+        if (h.acc) {
+            double* d = h.acc + (size_t)slot_id * R + VEC * q;
+#pragma unroll
+            for (int j = 0; j < VEC; j++) atomicAdd(d + j, acc[j]);
+        } else {
+            TA a[VEC];
+#pragma unroll
+            for (int j = 0; j < VEC; j++) a[j] = (TA)acc[j];
+            flush_global<P>(p.out, srows[slot_id], R, q, a);
+        }
+    };
     for (uint32_t c = blockIdx.x * MT_WARPS + warp; c < nchunks; c += nw) {
         const uint32_t j0 = c * h.chunk, j1 = min(h.total, j0 + h.chunk);
         // slot holding position j0: the last s with sptr[s] <= j0
@@ -457,7 +472,7 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_hot(MtParams p, HotPar
         }
         int cur = lo;
 #pragma unroll
-        for (int j = 0; j < VEC; j++) acc[j] = TA(0);
+        for (int j = 0; j < VEC; j++) acc[j] = 0.0;
         acc_slot = -1;
         for (uint32_t sub = j0; sub < j1; sub += 32) {
             while (cur < h.nhot - 1 && sptr[cur + 1] <= sub) cur++;
@@ -466,9 +481,8 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_hot(MtParams p, HotPar
             int ls = cur;
             if (valid)
                 while (ls < h.nhot - 1 && sptr[ls + 1] <= jj) ls++;
-            const uint32_t i = valid ? __ldg(h.idx + jj) : 0u;
-            const uint64_t cc = valid ? p.coords[i] : 0ull;
-            const TV v = valid ? reinterpret_cast<const TV*>(p.vals)[i] : TV(0);
+            const uint64_t cc = valid ? __ldcs(h.coords + jj) : 0ull;
+            const TV v = valid ? __ldcs(reinterpret_cast<const TV*>(h.vals) + jj) : TV(0);
             uint32_t ro[4] = {0, 0, 0, 0};
 #pragma unroll
             for (int k = 0; k < NM - 1; k++) ro[k] = (uint32_t)((cc >> ms.opos[k]) & ms.omask[k]);
@@ -503,9 +517,9 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_hot(MtParams p, HotPar
                     if (pp < pe) {
                         const int s = (int)rec[u].a.y;
                         if (s != acc_slot) {
-                            if (acc_slot >= 0) flush_global<P>(p.out, srows[acc_slot], R, q, acc);
+                            if (acc_slot >= 0) flush(acc_slot);
 #pragma unroll
-                            for (int j = 0; j < VEC; j++) acc[j] = TA(0);
+                            for (int j = 0; j < VEC; j++) acc[j] = 0.0;
                             acc_slot = s;
                         }
                         const TA vv = (TA)rec_val<TV>(rec[u].b);
@@ -514,15 +528,26 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_hot(MtParams p, HotPar
                             TA prod = vv;
 #pragma unroll
                             for (int k = 0; k < NM - 1; k++) prod *= g[u][k][j];
-                            acc[j] += prod;
+                            acc[j] += (double)prod;
                         }
                     }
                 }
             }
             __syncwarp();
         }
-        if (acc_slot >= 0) flush_global<P>(p.out, srows[acc_slot], R, q, acc);
+        if (acc_slot >= 0) flush(acc_slot);
         acc_slot = -1;
+    }
+}
+
+// out[rows[s]] += (float)acc[s] for the mixed form's hot rows (one rounding).
+__global__ void k_merge_hot(const double* __restrict__ acc, const uint32_t* __restrict__ rows, int nhot, int R,
+                            float* __restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nhot * R; i += gridDim.x * blockDim.x) {
+        const int s = i / R, c = i % R;
+        float* o = out + (size_t)rows[s] * R + c;
+        *o = (float)((double)*o + acc[i]);
     }
 }
 
@@ -770,7 +795,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
         if (m != a.mode && ((uintptr_t)a.factors[m] & 15u) != 0) aligned16 = false;
     size_t hash_bytes = 0;
     HotFn hot_fn = nullptr;
-    if (kern == BLCO_KERNEL_LVL2 && ht.nhot > 0 && ht.d_idx && aligned16 && a.coords == t->d_coords) {
+    if (kern == BLCO_KERNEL_LVL2 && ht.nhot > 0 && ht.d_hcoords && aligned16 && a.coords == t->d_coords) {
         switch (a.factor_dtype) {
         case BLCO_DTYPE_F64: hot_fn = pick_hot<PolicyF64>(L.nmodes, a.rank); break;
         case BLCO_DTYPE_F32: hot_fn = pick_hot<PolicyF32>(L.nmodes, a.rank); break;
@@ -806,19 +831,45 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     const size_t smem = hash_bytes + nacc * a.rank * accb + stage + 16;
     if (smem > di.smem_optin) return fail(BLCO_ERR_UNSUPPORTED, "MTTKRP shared memory plan exceeds the device limit");
     if (hot_fn) {
+        HotTable& hm = const_cast<HotTable&>(ht);
         HotParams h;
-        h.idx = ht.d_idx;
+        h.coords = ht.d_hcoords;
         h.ptr = ht.d_ptr;
         h.rows = ht.d_rows;
         h.nhot = ht.nhot;
         h.total = (uint32_t)ht.hot_nnz;
         h.chunk = 8192;
+        h.acc = nullptr;
+        if (a.factor_dtype == BLCO_DTYPE_F64) {
+            h.vals = ht.d_hvals;
+        } else {
+            // Mixed form: FP32 copy of the hot values, FP64 per-slot sums.
+            if (!hm.d_hvals32) {
+                BLCO_CUDA(cudaMalloc(&hm.d_hvals32, ht.hot_nnz * sizeof(float)));
+                k_to_f32<<<1024, 256, 0, s>>>(ht.d_hvals, hm.d_hvals32, ht.hot_nnz);
+                BLCO_CHECK_LAUNCH("k_to_f32");
+            }
+            if (hm.acc_rank < a.rank) {
+                cudaFree(hm.d_acc);
+                hm.d_acc = nullptr;
+                BLCO_CUDA(cudaMalloc(&hm.d_acc, (size_t)ht.nhot * a.rank * sizeof(double)));
+                hm.acc_rank = a.rank;
+            }
+            BLCO_CUDA(cudaMemsetAsync(hm.d_acc, 0, (size_t)ht.nhot * a.rank * sizeof(double), s));
+            h.vals = hm.d_hvals32;
+            h.acc = hm.d_acc;
+        }
         const size_t hsmem = (size_t)(2 * ht.nhot + 1) * sizeof(uint32_t) + 16 + stage;
         BLCO_CUDA(cudaFuncSetAttribute((const void*)hot_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
         const uint32_t nchunks = (h.total + h.chunk - 1) / h.chunk;
         const uint32_t hgrid = std::max<uint32_t>(1, std::min<uint32_t>(di.sm_count, (nchunks + MT_WARPS - 1) / MT_WARPS));
         hot_fn<<<hgrid, MT_THREADS, hsmem, s>>>(p, h);
         BLCO_CHECK_LAUNCH("k_mttkrp_hot");
+        if (h.acc) {
+            k_merge_hot<<<std::max(1, std::min(1024, (ht.nhot * a.rank + 255) / 256)), 256, 0, s>>>(
+                h.acc, ht.d_rows, ht.nhot, a.rank, reinterpret_cast<float*>(a.out));
+            BLCO_CHECK_LAUNCH("k_merge_hot");
+        }
     }
     KernelFn fn;
     switch (a.factor_dtype) {
