@@ -242,6 +242,9 @@ int blco_tensor_free(blco_tensor* t)
         cudaFree(t->hot[n].d_hvals);
         cudaFree(t->hot[n].d_hvals32);
         cudaFree(t->hot[n].d_acc);
+        cudaFree(t->hot[n].d_ccoords);
+        cudaFree(t->hot[n].d_cvals);
+        cudaFree(t->hot[n].d_cvals32);
     }
     delete t;
     return BLCO_OK;

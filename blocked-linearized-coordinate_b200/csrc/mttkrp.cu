@@ -805,14 +805,21 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     if (kern == BLCO_KERNEL_LVL3) {
         p.direct = 1;
     } else if (hot_fn) {
-        // Hot rows go to the CSR kernel; the tile kernel skips them.
-        p.hot_keys = ht.d_keys;
-        p.hot_slot = ht.d_slot;
-        p.hot_rows = ht.d_rows;
-        p.hash_size = ht.hash_size;
-        p.nhot = ht.nhot;
-        p.skip_hot = 1;
-        hash_bytes = 2 * sizeof(uint32_t) * ht.hash_size;
+        // Hot rows go to the CSR kernel; the tile kernel runs on the mode's
+        // cold stream copy with global atomics only.
+        HotTable& hm = const_cast<HotTable&>(ht);
+        p.coords = ht.d_ccoords;
+        p.nnz = ht.cold_nnz;
+        if (a.factor_dtype == BLCO_DTYPE_F64) {
+            p.vals = ht.d_cvals;
+        } else {
+            if (!hm.d_cvals32 && ht.cold_nnz) {
+                BLCO_CUDA(cudaMalloc(&hm.d_cvals32, ht.cold_nnz * sizeof(float)));
+                k_to_f32<<<1024, 256, 0, s>>>(ht.d_cvals, hm.d_cvals32, ht.cold_nnz);
+                BLCO_CHECK_LAUNCH("k_to_f32");
+            }
+            p.vals = hm.d_cvals32;
+        }
     } else if (kern == BLCO_KERNEL_LVL2 && ht.nhot > 0) {
         p.hot_keys = ht.d_keys;
         p.hot_slot = ht.d_slot;
@@ -838,7 +845,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
         h.rows = ht.d_rows;
         h.nhot = ht.nhot;
         h.total = (uint32_t)ht.hot_nnz;
-        h.chunk = 8192;
+        h.chunk = 2048;
         h.acc = nullptr;
         if (a.factor_dtype == BLCO_DTYPE_F64) {
             h.vals = ht.d_hvals;
@@ -862,7 +869,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
         const size_t hsmem = (size_t)(2 * ht.nhot + 1) * sizeof(uint32_t) + 16 + stage;
         BLCO_CUDA(cudaFuncSetAttribute((const void*)hot_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
         const uint32_t nchunks = (h.total + h.chunk - 1) / h.chunk;
-        const uint32_t hgrid = std::max<uint32_t>(1, std::min<uint32_t>(di.sm_count, (nchunks + MT_WARPS - 1) / MT_WARPS));
+        const uint32_t hgrid = std::max<uint32_t>(1, std::min<uint32_t>(di.sm_count, nchunks));
         hot_fn<<<hgrid, MT_THREADS, hsmem, s>>>(p, h);
         BLCO_CHECK_LAUNCH("k_mttkrp_hot");
         if (h.acc) {
@@ -871,6 +878,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
             BLCO_CHECK_LAUNCH("k_merge_hot");
         }
     }
+    if (p.nnz == 0) return BLCO_OK;
     KernelFn fn;
     switch (a.factor_dtype) {
     case BLCO_DTYPE_F64: fn = pick_kernel<PolicyF64>(L.nmodes, a.rank, aligned16); break;
@@ -878,7 +886,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     default: fn = pick_kernel<PolicyBF16>(L.nmodes, a.rank, aligned16); break;
     }
     BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint64_t ntiles = (a.nnz + 31) / 32;
+    const uint64_t ntiles = (p.nnz + 31) / 32;
     uint64_t grid = std::min<uint64_t>((uint64_t)di.sm_count, (ntiles + MT_WARPS - 1) / MT_WARPS);
     if (grid < 1) grid = 1;
     p.tiles_per_cta = (ntiles + grid - 1) / grid;
