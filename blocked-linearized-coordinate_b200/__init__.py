@@ -50,7 +50,7 @@ DTYPE_BF16 = 2
 # Every symbol include/blco.h declares.
 EXPORTS = (
     "blco_opts_init", "blco_status_string", "blco_last_error", "blco_version",
-    "blco_encode", "blco_encode_device", "blco_tensor_free", "blco_tensor_get_info",
+    "blco_encode", "blco_encode_device", "blco_encode_device_noalloc", "blco_tensor_free", "blco_tensor_get_info",
     "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_ex", "blco_mttkrp_host",
     "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
     "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_launch_count",
@@ -112,6 +112,7 @@ def lib():
         L.blco_opts_init.argtypes = [vp]
         L.blco_encode.argtypes = [i32, vp, u64, vp, vp, u64, vp, vp]
         L.blco_encode_device.argtypes = [i32, vp, u64, vp, vp, u64, vp, vp]
+        L.blco_encode_device_noalloc.argtypes = [i32, vp, u64, vp, vp, vp, vp, vp]
         L.blco_tensor_free.argtypes = [vp]
         L.blco_tensor_get_info.argtypes = [vp, vp]
         L.blco_tensor_copy_out.argtypes = [vp, vp, vp, vp, vp]
@@ -235,6 +236,24 @@ class Tensor:
             self.free()
         except Exception:
             pass
+
+
+NOALLOC_MAX_NNZ = 1_900_000  # BLCO_NOALLOC_MAX_NNZ in include/blco.h
+
+
+def encode_device_noalloc(dims, d_cidx, d_vals, d_coords_out, d_vals_out, stream=None):
+    """Allocation-free encode (blco_encode_device_noalloc): COO torch CUDA
+    arrays in, BLCO coordinates/values written to the caller's torch CUDA
+    arrays (uint64/int64 and float64, nnz entries).  Uses the library's
+    fixed device scratch array; no device memory is allocated."""
+    dims = _u64arr(dims)
+    nnz = int(d_vals.numel())
+    ptrs = _ptrs([int(c.data_ptr()) for c in d_cidx])
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream().cuda_stream
+    _check(lib().blco_encode_device_noalloc(len(d_cidx), dims.ctypes.data, nnz, ptrs, int(d_vals.data_ptr()),
+                                            int(d_coords_out.data_ptr()), int(d_vals_out.data_ptr()), stream))
 
 
 def mttkrp(t, mode, factors, out, opts=None):

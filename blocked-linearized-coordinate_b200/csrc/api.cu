@@ -223,6 +223,12 @@ int blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
     return st;
 }
 
+int blco_encode_device_noalloc(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* d_cidx,
+                               const double* d_vals, uint64_t* d_coords_out, double* d_vals_out, void* stream)
+{
+    return encode_noalloc_impl(nmodes, dims, nnz, d_cidx, d_vals, d_coords_out, d_vals_out, (cudaStream_t)stream);
+}
+
 int blco_tensor_free(blco_tensor* t)
 {
     if (!t) return BLCO_OK;

@@ -14,6 +14,7 @@
 // Then per-mode row statistics and heavy-row tables for the MTTKRP kernels.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "internal.cuh"
 
@@ -870,6 +871,145 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
         t->d_values = nullptr;
     }
     *out = t;
+    return BLCO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free encoder.
+//
+// Some callers of this library cannot allocate device memory when they
+// encode: a process whose device memory is owned by another allocator (a
+// framework's pool, a budgeted service), or code that must not call
+// cudaMalloc, which synchronises the device and can fail at a bad time.
+// blco_encode_device_noalloc serves them: the caller passes the COO input and
+// the two output arrays, and the sort's scratch lives in the file-scope array
+// below, which every GPU that loads this library holds until exit.
+//
+// Limits and sharing: at most BLCO_NOALLOC_MAX_NNZ nonzeros; one array per
+// device shared by every call, so calls that overlap on the GPU (other
+// streams, other host threads) race and must be serialised by the caller.
+// The first call on a device looks up the array's device address with
+// cudaGetSymbolAddress; make that first call before any stream capture.
+
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = 32ull << 20; // 32 MiB per device
+constexpr uint64_t NOALLOC_TILES = (BLCO_NOALLOC_MAX_NNZ + RS_TILE - 1) / RS_TILE;
+constexpr uint64_t NOALLOC_COUNTS = (uint64_t)RS_RADIX * NOALLOC_TILES;
+constexpr uint64_t NOALLOC_SUMS = (NOALLOC_COUNTS + SC_CHUNK - 1) / SC_CHUNK + 1;
+constexpr size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+// Scratch layout: alternate keys | alternate values | digit counts | scan
+// sums | encoder tables | invalid-coordinate flag.
+constexpr size_t NA_K1 = 0;
+constexpr size_t NA_V1 = NA_K1 + na_align(BLCO_NOALLOC_MAX_NNZ * 8);
+constexpr size_t NA_COUNTS = NA_V1 + na_align(BLCO_NOALLOC_MAX_NNZ * 8);
+constexpr size_t NA_SUMS = NA_COUNTS + na_align(NOALLOC_COUNTS * 4);
+constexpr size_t NA_TABS = NA_SUMS + na_align(NOALLOC_SUMS * 4);
+constexpr size_t NA_BAD = NA_TABS + na_align(sizeof(EncTables));
+constexpr size_t NA_END = NA_BAD + 256;
+static_assert(NA_END <= NOALLOC_SCRATCH_BYTES, "allocation-free encoder scratch layout exceeds the array");
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// The same passes as radix_sort_pairs, with the digit counts and scan sums
+// in caller-provided memory.
+int radix_sort_pairs_in(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint64_t n, int end_bit,
+                        cudaStream_t s, bool* in_alt, const EncTables* rel_tabs, uint32_t* counts, uint32_t* sums)
+{
+    *in_alt = false;
+    if (n <= 1 || end_bit <= 0) return BLCO_OK;
+    const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    const uint64_t L = (uint64_t)RS_RADIX * ntiles;
+    BLCO_CUDA(cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMEM));
+    uint64_t *ki = k0, *ko = k1;
+    double *vi = v0, *vo = v1;
+    for (int shift = 0; shift < end_bit; shift += 8) {
+        k_rs_hist<<<ntiles, RS_THREADS, 0, s>>>(ki, n, shift, counts, ntiles);
+        BLCO_CHECK_LAUNCH("k_rs_hist");
+        BLCO_TRY(scan_u32(counts, L, sums, s));
+        const bool last = shift + 8 >= end_bit;
+        k_rs_scatter<<<ntiles, RS_THREADS, RS_SMEM, s>>>(ki, vi, ko, vo, n, shift, counts, ntiles,
+                                                         last ? rel_tabs : nullptr, (end_bit + 7) / 8);
+        BLCO_CHECK_LAUNCH("k_rs_scatter");
+        std::swap(ki, ko);
+        std::swap(vi, vo);
+        *in_alt = !*in_alt;
+    }
+    return BLCO_OK;
+}
+
+} // namespace
+
+// Device address of g_noalloc_scratch for the current device.
+static int noalloc_scratch(int device, unsigned char** out)
+{
+    static std::mutex mu;
+    static unsigned char* ptr[64] = {};
+    if (device < 0 || device >= 64) return fail(BLCO_ERR_INVALID, "bad device ordinal");
+    std::lock_guard<std::mutex> g(mu);
+    if (!ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+        ptr[device] = static_cast<unsigned char*>(p);
+    }
+    *out = ptr[device];
+    return BLCO_OK;
+}
+
+int encode_noalloc_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* d_cidx,
+                        const double* d_vals, uint64_t* d_coords_out, double* d_vals_out, cudaStream_t s)
+{
+    if (!dims || (nnz && (!d_cidx || !d_vals || !d_coords_out || !d_vals_out)))
+        return fail(BLCO_ERR_INVALID, "null argument");
+    if (nnz > BLCO_NOALLOC_MAX_NNZ)
+        return fail(BLCO_ERR_UNSUPPORTED, "nnz above BLCO_NOALLOC_MAX_NNZ, the limit of the allocation-free encoder");
+    Layout L;
+    BLCO_TRY(make_layout(nmodes, dims, &L));
+    for (int n = 0; n < nmodes; n++)
+        if (nnz && !d_cidx[n]) return fail(BLCO_ERR_INVALID, "null coordinate array");
+    if (nnz == 0) return BLCO_OK;
+    int device = 0;
+    BLCO_CUDA(cudaGetDevice(&device));
+    DeviceInfo di;
+    BLCO_TRY(device_info(device, &di));
+    unsigned char* base = nullptr;
+    BLCO_TRY(noalloc_scratch(device, &base));
+    uint64_t* k1 = reinterpret_cast<uint64_t*>(base + NA_K1);
+    double* v1 = reinterpret_cast<double*>(base + NA_V1);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(base + NA_COUNTS);
+    uint32_t* sums = reinterpret_cast<uint32_t*>(base + NA_SUMS);
+    EncTables* tabs = reinterpret_cast<EncTables*>(base + NA_TABS);
+    int* bad = reinterpret_cast<int*>(base + NA_BAD);
+
+    // The flag keeps the previous call's value: clear it.
+    BLCO_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    {
+        EncTables htabs = make_tables(L);
+        BLCO_CUDA(cudaMemcpyAsync(tabs, &htabs, sizeof(EncTables), cudaMemcpyHostToDevice, s));
+        // htabs is pageable host memory: make sure the copy has read it.
+        BLCO_CUDA(cudaStreamSynchronize(s));
+    }
+    CooPtrs coo;
+    memset(&coo, 0, sizeof(coo));
+    for (int n = 0; n < nmodes; n++) coo.c[n] = d_cidx[n];
+    const int grid = (int)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)di.sm_count * 16);
+    k_alto_keys<<<grid, 256, 0, s>>>(coo, d_vals, nnz, L, tabs, d_coords_out, d_vals_out, bad);
+    BLCO_CHECK_LAUNCH("k_alto_keys");
+    bool in_alt = false;
+    BLCO_TRY(radix_sort_pairs_in(d_coords_out, d_vals_out, k1, v1, nnz, L.alto_bits, s, &in_alt, tabs, counts, sums));
+    if (nnz <= 1 && L.alto_bits > 0) {
+        k_relin<<<1, 32, 0, s>>>(d_coords_out, nnz, tabs, (L.alto_bits + 7) / 8);
+        BLCO_CHECK_LAUNCH("k_relin");
+    }
+    if (in_alt) {
+        BLCO_CUDA(cudaMemcpyAsync(d_coords_out, k1, nnz * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        BLCO_CUDA(cudaMemcpyAsync(d_vals_out, v1, nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    int bad_h = 0;
+    BLCO_CUDA(cudaMemcpyAsync(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BLCO_CUDA(cudaStreamSynchronize(s));
+    if (bad_h) return fail(BLCO_ERR_INVALID, "a coordinate is not below its mode length");
     return BLCO_OK;
 }
 

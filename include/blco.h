@@ -139,6 +139,29 @@ int blco_encode_device(int nmodes, const uint64_t* dims, uint64_t nnz,
                        uint64_t max_block_size, const blco_opts* opts,
                        blco_tensor** out);
 
+/* Allocation-free encoder.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory while they encode, for example
+ * code whose device memory is owned by another allocator (a framework's
+ * memory pool, a service with a fixed budget) or that must not call
+ * cudaMalloc, which can synchronise the device and fail.
+ * Encodes nnz nonzeros (COO in device memory: d_cidx[n], d_vals) into the
+ * caller's device arrays d_coords_out / d_vals_out (nnz entries each), with
+ * the same bits as blco_encode; no tensor handle, no heavy-row tables.
+ * Scratch: a fixed 32 MiB device array inside the library, held by every GPU
+ * that loads it until the process exits; this function calls no cudaMalloc,
+ * cudaFree or allocating library routine.
+ *   - nnz above BLCO_NOALLOC_MAX_NNZ is rejected with BLCO_ERR_UNSUPPORTED;
+ *   - every call on a device shares that one array: calls that overlap on
+ *     the GPU (other streams or host threads) race, so serialise them;
+ *   - the first call on a device looks up the array's address with
+ *     cudaGetSymbolAddress; make that first call before any stream capture.
+ * Runs on `stream` (NULL = default stream) and returns after the stream has
+ * finished the encode (it reads back the coordinate-range check). */
+#define BLCO_NOALLOC_MAX_NNZ 1900000ull
+int blco_encode_device_noalloc(int nmodes, const uint64_t* dims, uint64_t nnz,
+                               const uint64_t* const* d_cidx, const double* d_vals,
+                               uint64_t* d_coords_out, double* d_vals_out, void* stream);
+
 /* Free a tensor.  Replaces delete_blcotensor_host/_device
  * (src/blco.cu:61-91). */
 int blco_tensor_free(blco_tensor* t);
