@@ -53,7 +53,8 @@ EXPORTS = (
     "blco_encode", "blco_encode_device", "blco_encode_device_noalloc", "blco_tensor_free", "blco_tensor_get_info",
     "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_ex", "blco_mttkrp_host",
     "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
-    "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_launch_count",
+    "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_batch_create", "blco_batch_iterate",
+    "blco_batch_destroy", "blco_launch_count",
 )
 
 
@@ -125,6 +126,9 @@ def lib():
         L.blco_cpals_plan_iterate.argtypes = [vp, i32, f64, vp, vp]
         L.blco_cpals_plan_mttkrp_ms.argtypes = [vp, vp, vp]
         L.blco_cpals_plan_destroy.argtypes = [vp]
+        L.blco_batch_create.argtypes = [i32, vp, vp, vp, vp, f64, vp, vp]
+        L.blco_batch_iterate.argtypes = [vp, i32, vp, vp]
+        L.blco_batch_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -333,6 +337,47 @@ class CpalsPlan:
     def destroy(self):
         if self._h and self._h.value:
             _check(lib().blco_cpals_plan_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Batched CP-ALS over many resident tensors (blco_batch_*).
+
+    tensors: list of Tensor; factors[t]: list of torch CUDA float64
+    (dims[n], rank_t) tensors; lams[t]: torch CUDA float64 (rank_t,).
+    Factors and lambdas are updated in place."""
+
+    def __init__(self, tensors, factors, lams, tol=1e-5, opts=None):
+        T = len(tensors)
+        self.count = T
+        self._keep = (tensors, factors, lams)
+        ranks = (ctypes.c_int * T)(*[int(f[0].shape[1]) for f in factors])
+        rows = [_ptrs([int(m.data_ptr()) for m in f]) for f in factors]
+        self._rows = rows
+        fptrs = (ctypes.c_void_p * T)(*[ctypes.cast(r, ctypes.c_void_p).value for r in rows])
+        lptrs = _ptrs([int(l.data_ptr()) for l in lams])
+        hs = _ptrs([int(t.handle.value) for t in tensors])
+        o = opts if opts is not None else make_opts()
+        h = ctypes.c_void_p()
+        _check(lib().blco_batch_create(T, hs, ranks, fptrs, lptrs, float(tol), ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    def iterate(self, iters):
+        """Run `iters` sweeps; returns (fits (iters, count), iterations per tensor)."""
+        fits = np.zeros((max(iters, 1), self.count), dtype=np.float64)
+        done = np.zeros(self.count, dtype=np.int32)
+        _check(lib().blco_batch_iterate(self._h, iters, fits.ctypes.data, done.ctypes.data))
+        return fits[:iters], done
+
+    def destroy(self):
+        if self._h and self._h.value:
+            _check(lib().blco_batch_destroy(self._h))
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -15,6 +15,8 @@ static thread_local uint64_t g_launches = 0;
 void set_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
 void count_launch() { g_launches++; }
+void add_launches(long long n) { g_launches += (uint64_t)n; }
+unsigned long long launches_so_far() { return g_launches; }
 
 int fail(int status, const std::string& msg)
 {
@@ -426,5 +428,20 @@ int blco_cpals_plan_iterate(blco_cpals_plan* p, int iters, double tol, double* f
 int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls) { return plan_mttkrp_ms(p, ms, calls); }
 
 int blco_cpals_plan_destroy(blco_cpals_plan* p) { return plan_destroy(p); }
+
+int blco_batch_create(int count, blco_tensor* const* tensors, const int* ranks, double* const* const* d_factors,
+                      double* const* d_lambdas, double tol, const blco_opts* opts, blco_batch** out)
+{
+    if (!out) return fail(BLCO_ERR_INVALID, "null output handle");
+    return batch_create(count, tensors, ranks, d_factors, d_lambdas, tol, opts, out);
+}
+
+int blco_batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done)
+{
+    if (!b) return fail(BLCO_ERR_INVALID, "null batch");
+    return batch_iterate(b, iters, fits, iters_done);
+}
+
+int blco_batch_destroy(blco_batch* b) { return batch_destroy(b); }
 
 } // extern "C"

@@ -297,8 +297,8 @@ struct GramPtrs {
 // positive, the pseudoinverse is taken from a cyclic Jacobi
 // eigen-decomposition V = Q diag(w) Q^T instead, dropping |w| <= R*ulp(max|w|)
 // as the reference does for its SVD.
-__global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, int skip, int R,
-                                                      double* __restrict__ Pout, int* __restrict__ used_eigen)
+__device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __restrict__ Pout,
+                           int* __restrict__ used_eigen)
 {
     extern __shared__ __align__(16) double ss[];
     double* A = ss;          // R x R
@@ -434,6 +434,12 @@ __global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, i
     if (tid == 0) *used_eigen = 1;
 }
 
+__global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, int skip, int R,
+                                                      double* __restrict__ Pout, int* __restrict__ used_eigen)
+{
+    solve_body(gp, nmodes, skip, R, Pout, used_eigen);
+}
+
 // ----------------------------------------------------------------- fit --
 // Per-block column sums of U[i][c] * M[i][c] (columnwise_inner_product,
 // src/cpd_gpu.cu:307-330).
@@ -469,6 +475,41 @@ __global__ __launch_bounds__(DN_THREADS) void k_iprod(const T* __restrict__ U, c
 }
 
 // fit = 1 - sqrt(| ||A||^2 - 2 <X,A> + ||X||^2 |) / ||X|| (src/cpd_gpu.cu:331-384)
+// Block-wide sum of one value per thread (blockDim.x == DN_THREADS).
+__device__ double block_sum(double v, double* red)
+{
+    const int tid = threadIdx.x;
+    red[tid] = v;
+    __syncthreads();
+    for (int o = DN_THREADS / 2; o; o >>= 1) {
+        if (tid < o) red[tid] += red[tid + o];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// fit from <X, A> (iprod), the Grams and lambda; every thread returns it.
+__device__ double fit_body(double iprod, GramPtrs gp, int nmodes, int R, const double* __restrict__ lambda,
+                           double xnorm, double* red)
+{
+    double na = 0.0;
+    for (int e = threadIdx.x; e < R * R; e += DN_THREADS) {
+        double v = lambda[e / R] * lambda[e % R];
+        for (int m = 0; m < nmodes; m++) v *= gp.g[m][e];
+        na += v;
+    }
+    na = block_sum(na, red);
+    double norm_a = sqrt(fabs(na));
+    double fit = norm_a * norm_a - 2.0 * iprod;
+    if (xnorm != 0.0) {
+        fit = sqrt(fabs(fit + xnorm * xnorm));
+        fit = 1.0 - fit / xnorm;
+    }
+    return fit;
+}
+
 __global__ void k_fit(const double* __restrict__ ipart, int nblocks, GramPtrs gp, int nmodes, int R,
                       const double* __restrict__ lambda, double xnorm, double* __restrict__ fit_out)
 {
@@ -481,35 +522,9 @@ __global__ void k_fit(const double* __restrict__ ipart, int nblocks, GramPtrs gp
         for (int b = 0; b < nblocks; b++) s += ipart[(size_t)b * R + c];
         ip += s * lambda[c];
     }
-    red[tid] = ip;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o; o >>= 1) {
-        if (tid < o) red[tid] += red[tid + o];
-        __syncthreads();
-    }
-    const double iprod = red[0];
-    __syncthreads();
-    double na = 0.0;
-    for (int e = tid; e < R * R; e += blockDim.x) {
-        double v = lambda[e / R] * lambda[e % R];
-        for (int m = 0; m < nmodes; m++) v *= gp.g[m][e];
-        na += v;
-    }
-    red[tid] = na;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o; o >>= 1) {
-        if (tid < o) red[tid] += red[tid + o];
-        __syncthreads();
-    }
-    if (tid == 0) {
-        double norm_a = sqrt(fabs(red[0]));
-        double fit = norm_a * norm_a - 2.0 * iprod;
-        if (xnorm != 0.0) {
-            fit = sqrt(fabs(fit + xnorm * xnorm));
-            fit = 1.0 - fit / xnorm;
-        }
-        fit_out[0] = fit;
-    }
+    const double iprod = block_sum(ip, red);
+    const double fit = fit_body(iprod, gp, nmodes, R, lambda, xnorm, red);
+    if (tid == 0) fit_out[0] = fit;
 }
 
 int grid_rows(uint64_t I, int sm)
@@ -908,5 +923,613 @@ int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls)
     if (calls) *calls = p->mttkrp_calls;
     return BLCO_OK;
 }
+
+} // namespace blco
+
+// ==================================================================== batch
+// Batched CP-ALS: many independent tensors of uneven nnz, order (1..5 modes)
+// and rank (1..64), decomposed together.  Every step of a sweep is one launch
+// over all tensors: the MTTKRP is one persistent launch over the tiles of all
+// streams (a tile table maps a global tile to its tensor), and the dense steps
+// use one CTA per tensor (solve, lambda, Gram reduction, fit) or per row
+// chunk (update, Gram).  Tensor t takes its k-th mode (by descending length)
+// in mode slot k.  Convergence is decided on the device per tensor (a tensor
+// whose |fit - fit_old| < tol stops taking part), so the whole sweep is
+// captured once as a CUDA graph and replayed once per iteration.
+
+namespace blco {
+namespace {
+
+constexpr int BATCH_MAX_R = 64;
+constexpr int BATCH_MAX_T = 4096;
+constexpr int BATCH_CHUNK = 2048;      // rows per update / Gram CTA
+constexpr int BATCH_FIT_RING = 4096;   // iterations of fits kept on the device
+
+struct BDesc {
+    const uint64_t* coords;
+    const double* vals;
+    uint64_t nnz;
+    uint64_t tile_off;                 // first global tile of this tensor
+    int nmodes, rank;
+    int order[BLCO_MAX_MODES];         // modes by descending length
+    uint64_t dims[BLCO_MAX_MODES];
+    uint64_t mask[BLCO_MAX_MODES];
+    int pos[BLCO_MAX_MODES];
+    double* U[BLCO_MAX_MODES];
+    double* lambda;
+    double* M;                         // MTTKRP result, max dim x rank
+    double* G[BLCO_MAX_MODES];         // Grams, rank x rank
+    double* P;                         // pseudoinverse, rank x rank
+    double* inv;                       // 1 / lambda
+    double xnorm;
+    double fit_old;
+    int active;
+    int iters;
+};
+
+__global__ void k_b_zero(BDesc* __restrict__ d, int T, int slot)
+{
+    const int t = blockIdx.x / 8, part = blockIdx.x % 8;
+    if (t >= T) return;
+    const BDesc& b = d[t];
+    if (!b.active || slot >= b.nmodes) return;
+    const uint64_t len = b.dims[b.order[slot]] * (uint64_t)b.rank;
+    for (uint64_t i = (uint64_t)part * blockDim.x + threadIdx.x; i < len; i += 8ull * blockDim.x) b.M[i] = 0.0;
+}
+
+// One persistent launch over the tiles of all tensors.  Per tile: the 32
+// nonzeros are ordered by output row (match_any), then lane groups of
+// min(R, 32) lanes take one nonzero each, a lane owning columns q, q+32;
+// equal-row runs are summed in registers and flushed with FP64 atomics.
+__global__ void __launch_bounds__(768, 1) k_b_mttkrp(BDesc* __restrict__ d, int T, uint64_t total_tiles, int slot,
+                                                    uint64_t tiles_per_cta)
+{
+    __shared__ uint32_t toff[BATCH_MAX_T + 1];
+    __shared__ __align__(16) uint32_t srow[24][32];
+    __shared__ __align__(16) uint32_t soth[24][4][32];
+    __shared__ __align__(16) double sval[24][32];
+    for (int i = threadIdx.x; i < T; i += blockDim.x) toff[i] = (uint32_t)d[i].tile_off;
+    if (threadIdx.x == 0) toff[T] = (uint32_t)total_tiles;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t t_beg = (uint64_t)blockIdx.x * tiles_per_cta;
+    const uint64_t t_end = min(total_tiles, t_beg + tiles_per_cta);
+    for (uint64_t g = t_beg + warp; g < t_end; g += 24) {
+        int lo = 0, hi = T - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (toff[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const BDesc& b = d[lo];
+        if (!b.active || slot >= b.nmodes) continue; // warp-uniform
+        const int n = b.order[slot], R = b.rank, nm = b.nmodes;
+        const uint64_t i0 = (g - toff[lo]) * 32;
+        const uint64_t i = i0 + lane;
+        const bool valid = i < b.nnz;
+        const uint64_t c = valid ? b.coords[i] : 0;
+        const double v = valid ? b.vals[i] : 0.0;
+        uint32_t rt = 0, r0 = 0, r1 = 0, r2 = 0, r3 = 0;
+        const double *f0 = nullptr, *f1 = nullptr, *f2 = nullptr, *f3 = nullptr;
+        int k = 0;
+#pragma unroll
+        for (int m = 0; m < BLCO_MAX_MODES; m++) {
+            if (m < nm) {
+                const uint32_t r = (uint32_t)((c >> b.pos[m]) & b.mask[m]);
+                if (m == n) {
+                    rt = r;
+                } else {
+                    if (k == 0) { r0 = r; f0 = b.U[m]; }
+                    else if (k == 1) { r1 = r; f1 = b.U[m]; }
+                    else if (k == 2) { r2 = r; f2 = b.U[m]; }
+                    else { r3 = r; f3 = b.U[m]; }
+                    k++;
+                }
+            }
+        }
+        const uint32_t key = valid ? rt : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key);
+        const uint32_t lt = (1u << lane) - 1;
+        const int leader = __ffs(peers) - 1;
+        const uint32_t x = lane == leader ? (uint32_t)__popc(peers) : 0u;
+        uint32_t inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const int sp = (int)__shfl_sync(0xffffffffu, inc - x, leader) + __popc(peers & lt);
+        const uint32_t ends = __reduce_or_sync(0xffffffffu, ((peers >> lane) == 1u) ? (1u << sp) : 0u);
+        srow[warp][sp] = rt;
+        soth[warp][0][sp] = r0;
+        soth[warp][1][sp] = r1;
+        soth[warp][2][sp] = r2;
+        soth[warp][3][sp] = r3;
+        sval[warp][sp] = v;
+        __syncwarp();
+        const int count = (int)min((uint64_t)32, b.nnz - i0);
+        const int lpn = R < 32 ? R : 32;
+        const int groups = 32 / lpn;
+        const int per = (32 + groups - 1) / groups;
+        const int grp = lane / lpn, q = lane % lpn;
+        if (grp < groups) {
+            const int pb = grp * per, pe = min(pb + per, count);
+            double acc0 = 0.0, acc1 = 0.0;
+            const int c0 = q, c1 = q + 32;
+            for (int pp = pb; pp < pe; pp++) {
+                const double val = sval[warp][pp];
+                double p0 = val, p1 = val;
+                const uint32_t o0 = soth[warp][0][pp], o1 = soth[warp][1][pp], o2 = soth[warp][2][pp],
+                               o3 = soth[warp][3][pp];
+                if (nm > 1) { p0 *= f0[(size_t)o0 * R + c0]; if (c1 < R) p1 *= f0[(size_t)o0 * R + c1]; }
+                if (nm > 2) { p0 *= f1[(size_t)o1 * R + c0]; if (c1 < R) p1 *= f1[(size_t)o1 * R + c1]; }
+                if (nm > 3) { p0 *= f2[(size_t)o2 * R + c0]; if (c1 < R) p1 *= f2[(size_t)o2 * R + c1]; }
+                if (nm > 4) { p0 *= f3[(size_t)o3 * R + c0]; if (c1 < R) p1 *= f3[(size_t)o3 * R + c1]; }
+                acc0 += p0;
+                acc1 += p1;
+                if (((ends >> pp) & 1u) || pp == pe - 1) {
+                    double* o = b.M + (size_t)srow[warp][pp] * R;
+                    atomicAdd(o + c0, acc0);
+                    if (c1 < R) atomicAdd(o + c1, acc1);
+                    acc0 = acc1 = 0.0;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+__global__ __launch_bounds__(DN_THREADS) void k_b_solve(BDesc* __restrict__ d, int slot, int* __restrict__ dummy)
+{
+    const BDesc& b = d[blockIdx.x];
+    if (!b.active || slot >= b.nmodes) return; // block-uniform
+    GramPtrs gp;
+    for (int m = 0; m < BLCO_MAX_MODES; m++) gp.g[m] = b.G[m];
+    solve_body(gp, b.nmodes, b.order[slot], b.rank, b.P, dummy);
+}
+
+// One CTA per row chunk: U = M P^T in FP64 (a warp per row, lane per
+// column pair) and the chunk's column sums of squares.
+__global__ __launch_bounds__(DN_THREADS) void k_b_update(BDesc* __restrict__ d, const uint32_t* __restrict__ ct,
+                                                         const uint32_t* __restrict__ cr0,
+                                                         const uint32_t* __restrict__ cr1, int slot,
+                                                         double* __restrict__ colsq)
+{
+    __shared__ double PT[BATCH_MAX_R * BATCH_MAX_R];
+    __shared__ double csq[DN_THREADS / 32][BATCH_MAX_R];
+    const int chunk = blockIdx.x, t = ct[chunk];
+    const BDesc& b = d[t];
+    if (!b.active || slot >= b.nmodes) return;
+    const int R = b.rank, n = b.order[slot];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k = tid; k < R * R; k += DN_THREADS) PT[(k % R) * R + k / R] = b.P[k];
+    for (int k = tid; k < (DN_THREADS / 32) * BATCH_MAX_R; k += DN_THREADS) (&csq[0][0])[k] = 0.0;
+    __syncthreads();
+    double sq0 = 0.0, sq1 = 0.0;
+    const int c0 = lane, c1 = lane + 32;
+    for (uint32_t r = cr0[chunk] + warp; r < cr1[chunk]; r += DN_THREADS / 32) {
+        const double* mrow = b.M + (size_t)r * R;
+        const double m0 = c0 < R ? mrow[c0] : 0.0, m1 = c1 < R ? mrow[c1] : 0.0;
+        double a0 = 0.0, a1 = 0.0;
+        for (int kk = 0; kk < R; kk++) {
+            const double mk = __shfl_sync(0xffffffffu, kk < 32 ? m0 : m1, kk & 31);
+            if (c0 < R) a0 += mk * PT[kk * R + c0];
+            if (c1 < R) a1 += mk * PT[kk * R + c1];
+        }
+        double* urow = b.U[n] + (size_t)r * R;
+        if (c0 < R) { urow[c0] = a0; sq0 += a0 * a0; }
+        if (c1 < R) { urow[c1] = a1; sq1 += a1 * a1; }
+    }
+    if (c0 < R) csq[warp][c0] = sq0;
+    if (c1 < R) csq[warp][c1] = sq1;
+    __syncthreads();
+    for (int c = tid; c < R; c += DN_THREADS) {
+        double s = 0.0;
+        for (int w = 0; w < DN_THREADS / 32; w++) s += csq[w][c];
+        colsq[(size_t)chunk * BATCH_MAX_R + c] = s;
+    }
+}
+
+__global__ void k_b_lambda(BDesc* __restrict__ d, const uint32_t* __restrict__ cbeg, const uint32_t* __restrict__ cend,
+                           int slot, const double* __restrict__ colsq)
+{
+    BDesc& b = d[blockIdx.x];
+    if (!b.active || slot >= b.nmodes) return;
+    for (int c = threadIdx.x; c < b.rank; c += blockDim.x) {
+        double s = 0.0;
+        for (uint32_t k = cbeg[blockIdx.x]; k < cend[blockIdx.x]; k++) s += colsq[(size_t)k * BATCH_MAX_R + c];
+        const double l = sqrt(b.lambda[c] + s);
+        b.lambda[c] = l;
+        b.inv[c] = l == 0.0 ? 0.0 : 1.0 / l;
+    }
+}
+
+// One CTA per row chunk: optionally scale the rows by inv, then the chunk's
+// Gram (R x R) partial; thread (a, b) pairs strided over R*R.
+__global__ __launch_bounds__(DN_THREADS) void k_b_gram(BDesc* __restrict__ d, const uint32_t* __restrict__ ct,
+                                                       const uint32_t* __restrict__ cr0,
+                                                       const uint32_t* __restrict__ cr1, int slot, int scale,
+                                                       double* __restrict__ gpart)
+{
+    __shared__ double tile[32][BATCH_MAX_R + 1];
+    const int chunk = blockIdx.x, t = ct[chunk];
+    const BDesc& b = d[t];
+    if ((scale && !b.active) || slot >= b.nmodes) return;
+    const int R = b.rank, n = b.order[slot], tid = threadIdx.x;
+    double acc[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) acc[j] = 0.0;
+    const uint32_t r_beg = cr0[chunk], r_end = cr1[chunk];
+    for (uint32_t r0 = r_beg; r0 < r_end; r0 += 32) {
+        const int nr = (int)min(32u, r_end - r0);
+        __syncthreads();
+        for (int k = tid; k < nr * R; k += DN_THREADS) {
+            double v = b.U[n][(size_t)r0 * R + k];
+            if (scale) {
+                v *= b.inv[k % R];
+                b.U[n][(size_t)r0 * R + k] = v;
+            }
+            tile[k / R][k % R] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int e = tid + j * DN_THREADS;
+            if (e < R * R) {
+                const int a = e / R, c = e % R;
+                double s = 0.0;
+                for (int r = 0; r < nr; r++) s += tile[r][a] * tile[r][c];
+                acc[j] += s;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        const int e = tid + j * DN_THREADS;
+        if (e < R * R) gpart[(size_t)chunk * BATCH_MAX_R * BATCH_MAX_R + e] = acc[j];
+    }
+}
+
+__global__ void k_b_gram_reduce(BDesc* __restrict__ d, const uint32_t* __restrict__ cbeg,
+                                const uint32_t* __restrict__ cend, int slot, int need_active,
+                                const double* __restrict__ gpart)
+{
+    BDesc& b = d[blockIdx.x];
+    if ((need_active && !b.active) || slot >= b.nmodes) return;
+    const int R = b.rank, n = b.order[slot];
+    for (int e = threadIdx.x; e < R * R; e += blockDim.x) {
+        double s = 0.0;
+        for (uint32_t k = cbeg[blockIdx.x]; k < cend[blockIdx.x]; k++)
+            s += gpart[(size_t)k * BATCH_MAX_R * BATCH_MAX_R + e];
+        b.G[n][e] = s;
+    }
+}
+
+// Per tensor: <X, A> from the last mode's factor and MTTKRP, the fit
+// (kruskal_fit_gpu, src/cpd_gpu.cu:331-384) and the convergence test.
+__global__ __launch_bounds__(DN_THREADS) void k_b_fit(BDesc* __restrict__ d, int T, const int* __restrict__ iter,
+                                                      double tol, double* __restrict__ fits)
+{
+    __shared__ double red[DN_THREADS];
+    BDesc& b = d[blockIdx.x];
+    if (!b.active) {
+        if (threadIdx.x == 0) fits[(size_t)(*iter % BATCH_FIT_RING) * T + blockIdx.x] = b.fit_old;
+        return;
+    }
+    const int R = b.rank, lm = b.order[b.nmodes - 1];
+    const uint64_t len = b.dims[lm] * (uint64_t)R;
+    double ip = 0.0;
+    for (uint64_t i = threadIdx.x; i < len; i += DN_THREADS) ip += b.U[lm][i] * b.M[i] * b.lambda[i % R];
+    const double iprod = block_sum(ip, red);
+    GramPtrs gp;
+    for (int m = 0; m < BLCO_MAX_MODES; m++) gp.g[m] = b.G[m];
+    const double fit = fit_body(iprod, gp, b.nmodes, R, b.lambda, b.xnorm, red);
+    if (threadIdx.x == 0) {
+        fits[(size_t)(*iter % BATCH_FIT_RING) * T + blockIdx.x] = fit;
+        b.iters++;
+        if (fabs(fit - b.fit_old) < tol || isnan(fit)) b.active = 0;
+        b.fit_old = fit;
+    }
+}
+
+__global__ void k_b_next(int* iter) { *iter += 1; }
+
+} // namespace
+} // namespace blco
+
+struct blco_batch {
+    int T = 0, maxN = 0, maxR = 0;
+    blco::BDesc* d_desc = nullptr;
+    std::vector<blco::BDesc> h_desc;
+    uint64_t total_tiles = 0;
+    // per mode slot: chunk -> tensor, row range; per tensor chunk range
+    uint32_t* d_ct[BLCO_MAX_MODES] = {};
+    uint32_t* d_cr0[BLCO_MAX_MODES] = {};
+    uint32_t* d_cr1[BLCO_MAX_MODES] = {};
+    uint32_t* d_cbeg[BLCO_MAX_MODES] = {};
+    uint32_t* d_cend[BLCO_MAX_MODES] = {};
+    int nchunks[BLCO_MAX_MODES] = {};
+    double* d_colsq = nullptr;
+    double* d_gpart = nullptr;
+    double* d_fits = nullptr;
+    int* d_iter = nullptr;
+    int* d_dummy = nullptr;
+    void* pool = nullptr;
+    int sm = 148;
+    cudaStream_t s = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long graph_kernels = 0;
+    double tol = 0.0;
+    int iters_run = 0;
+};
+
+namespace blco {
+namespace {
+
+int batch_free(blco_batch* b)
+{
+    if (!b) return BLCO_OK;
+    if (b->s) cudaStreamSynchronize(b->s);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (int k = 0; k < BLCO_MAX_MODES; k++) {
+        cudaFree(b->d_ct[k]);
+        cudaFree(b->d_cr0[k]);
+        cudaFree(b->d_cr1[k]);
+        cudaFree(b->d_cbeg[k]);
+        cudaFree(b->d_cend[k]);
+    }
+    cudaFree(b->d_desc);
+    cudaFree(b->d_colsq);
+    cudaFree(b->d_gpart);
+    cudaFree(b->d_fits);
+    cudaFree(b->d_iter);
+    cudaFree(b->d_dummy);
+    cudaFree(b->pool);
+    if (b->s) cudaStreamDestroy(b->s);
+    delete b;
+    return BLCO_OK;
+}
+
+// One sweep over all mode slots plus the fit, enqueued on b->s.
+int batch_enqueue_sweep(blco_batch* b)
+{
+    const size_t ssmem = 2 * (size_t)b->maxR * b->maxR * sizeof(double);
+    const uint64_t grid = std::min<uint64_t>((uint64_t)b->sm, (b->total_tiles + 23) / 24);
+    const uint64_t tpc = (b->total_tiles + std::max<uint64_t>(grid, 1) - 1) / std::max<uint64_t>(grid, 1);
+    for (int k = 0; k < b->maxN; k++) {
+        k_b_zero<<<b->T * 8, 256, 0, b->s>>>(b->d_desc, b->T, k);
+        BLCO_CHECK_LAUNCH("k_b_zero");
+        if (grid) {
+            k_b_mttkrp<<<(unsigned)grid, 768, 0, b->s>>>(b->d_desc, b->T, b->total_tiles, k, tpc);
+            BLCO_CHECK_LAUNCH("k_b_mttkrp");
+        }
+        k_b_solve<<<b->T, DN_THREADS, ssmem, b->s>>>(b->d_desc, k, b->d_dummy);
+        BLCO_CHECK_LAUNCH("k_b_solve");
+        if (b->nchunks[k]) {
+            k_b_update<<<b->nchunks[k], DN_THREADS, 0, b->s>>>(b->d_desc, b->d_ct[k], b->d_cr0[k], b->d_cr1[k], k,
+                                                                b->d_colsq);
+            BLCO_CHECK_LAUNCH("k_b_update");
+        }
+        k_b_lambda<<<b->T, 64, 0, b->s>>>(b->d_desc, b->d_cbeg[k], b->d_cend[k], k, b->d_colsq);
+        BLCO_CHECK_LAUNCH("k_b_lambda");
+        if (b->nchunks[k]) {
+            k_b_gram<<<b->nchunks[k], DN_THREADS, 0, b->s>>>(b->d_desc, b->d_ct[k], b->d_cr0[k], b->d_cr1[k], k, 1,
+                                                              b->d_gpart);
+            BLCO_CHECK_LAUNCH("k_b_gram");
+        }
+        k_b_gram_reduce<<<b->T, 256, 0, b->s>>>(b->d_desc, b->d_cbeg[k], b->d_cend[k], k, 1, b->d_gpart);
+        BLCO_CHECK_LAUNCH("k_b_gram_reduce");
+    }
+    k_b_fit<<<b->T, DN_THREADS, 0, b->s>>>(b->d_desc, b->T, b->d_iter, b->tol, b->d_fits);
+    BLCO_CHECK_LAUNCH("k_b_fit");
+    k_b_next<<<1, 1, 0, b->s>>>(b->d_iter);
+    BLCO_CHECK_LAUNCH("k_b_next");
+    return BLCO_OK;
+}
+
+} // namespace
+
+int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* const* const* d_factors,
+                 double* const* d_lambdas, double tol, const blco_opts* opts, blco_batch** out)
+{
+    *out = nullptr;
+    if (T < 1 || T > BATCH_MAX_T) return fail(BLCO_ERR_INVALID, "batch size must be 1..4096");
+    if (!tensors || !ranks || !d_factors || !d_lambdas) return fail(BLCO_ERR_INVALID, "null argument");
+    const int device = tensors[0] ? tensors[0]->device : 0;
+    for (int t = 0; t < T; t++) {
+        if (!tensors[t] || !d_factors[t] || !d_lambdas[t]) return fail(BLCO_ERR_INVALID, "null tensor or factors");
+        if (!tensors[t]->resident) return fail(BLCO_ERR_UNSUPPORTED, "batched CP-ALS needs resident tensors");
+        if (tensors[t]->device != device) return fail(BLCO_ERR_INVALID, "all tensors must be on one device");
+        if (ranks[t] < 1 || ranks[t] > BATCH_MAX_R) return fail(BLCO_ERR_UNSUPPORTED, "batched rank must be 1..64");
+        for (int n = 0; n < tensors[t]->layout.nmodes; n++)
+            if (!d_factors[t][n]) return fail(BLCO_ERR_INVALID, "null factor matrix");
+    }
+    BLCO_CUDA(cudaSetDevice(device));
+    DeviceInfo di;
+    BLCO_TRY(device_info(device, &di));
+    blco_batch* b = new blco_batch();
+    b->T = T;
+    b->sm = di.sm_count;
+    b->tol = tol;
+    b->h_desc.resize(T);
+    // workspace sizes
+    size_t pool_doubles = 0;
+    for (int t = 0; t < T; t++) {
+        const Layout& L = tensors[t]->layout;
+        uint64_t maxdim = 0;
+        for (int n = 0; n < L.nmodes; n++) maxdim = std::max(maxdim, L.dims[n]);
+        const size_t R = ranks[t];
+        pool_doubles += maxdim * R + (size_t)L.nmodes * R * R + R * R + R;
+        b->maxN = std::max(b->maxN, L.nmodes);
+        b->maxR = std::max(b->maxR, ranks[t]);
+    }
+    auto bail = [&](int st) {
+        batch_free(b);
+        return st;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&b->pool, pool_doubles * sizeof(double));
+    if (e != cudaSuccess) return bail(cuda_fail(e, "batch workspace", __FILE__, __LINE__));
+    double* cur = static_cast<double*>(b->pool);
+    uint64_t tiles = 0;
+    for (int t = 0; t < T; t++) {
+        blco_tensor* x = tensors[t];
+        const Layout& L = x->layout;
+        BDesc& d = b->h_desc[t];
+        memset(&d, 0, sizeof(d));
+        d.coords = x->d_coords;
+        d.vals = x->d_values;
+        d.nnz = x->nnz;
+        d.tile_off = tiles;
+        tiles += (x->nnz + 31) / 32;
+        d.nmodes = L.nmodes;
+        d.rank = ranks[t];
+        for (int n = 0; n < L.nmodes; n++) {
+            d.dims[n] = L.dims[n];
+            d.mask[n] = L.mode_masks[n];
+            d.pos[n] = L.mode_pos[n];
+            d.U[n] = d_factors[t][n];
+            d.order[n] = n;
+        }
+        std::stable_sort(d.order, d.order + L.nmodes, [&](int a2, int b2) { return L.dims[a2] > L.dims[b2]; });
+        d.lambda = d_lambdas[t];
+        uint64_t maxdim = 0;
+        for (int n = 0; n < L.nmodes; n++) maxdim = std::max(maxdim, L.dims[n]);
+        const size_t R = ranks[t];
+        d.M = cur;
+        cur += maxdim * R;
+        for (int n = 0; n < L.nmodes; n++) {
+            d.G[n] = cur;
+            cur += R * R;
+        }
+        d.P = cur;
+        cur += R * R;
+        d.inv = cur;
+        cur += R;
+        d.xnorm = std::sqrt(x->norm_sq);
+        d.fit_old = 0.0;
+        d.active = 1;
+    }
+    b->total_tiles = tiles;
+    if (tiles >= (1ull << 32)) return bail(fail(BLCO_ERR_UNSUPPORTED, "batch holds too many nonzeros (2^37 at most)"));
+    // chunk tables per slot
+    int maxchunks = 0;
+    for (int k = 0; k < b->maxN; k++) {
+        std::vector<uint32_t> ct, cr0, cr1, cbeg(T, 0), cend(T, 0);
+        for (int t = 0; t < T; t++) {
+            const BDesc& d = b->h_desc[t];
+            cbeg[t] = (uint32_t)ct.size();
+            if (k < d.nmodes) {
+                const uint64_t I = d.dims[d.order[k]];
+                for (uint64_t r = 0; r < I; r += BATCH_CHUNK) {
+                    ct.push_back((uint32_t)t);
+                    cr0.push_back((uint32_t)r);
+                    cr1.push_back((uint32_t)std::min<uint64_t>(I, r + BATCH_CHUNK));
+                }
+            }
+            cend[t] = (uint32_t)ct.size();
+        }
+        b->nchunks[k] = (int)ct.size();
+        maxchunks = std::max(maxchunks, b->nchunks[k]);
+        const size_t nc = std::max<size_t>(1, ct.size());
+        e = cudaMalloc(&b->d_ct[k], nc * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_cr0[k], nc * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_cr1[k], nc * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_cbeg[k], T * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_cend[k], T * 4);
+        if (e == cudaSuccess && !ct.empty()) {
+            e = cudaMemcpyAsync(b->d_ct[k], ct.data(), ct.size() * 4, cudaMemcpyHostToDevice, b->s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cr0[k], cr0.data(), ct.size() * 4, cudaMemcpyHostToDevice, b->s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cr1[k], cr1.data(), ct.size() * 4, cudaMemcpyHostToDevice, b->s);
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cbeg[k], cbeg.data(), T * 4, cudaMemcpyHostToDevice, b->s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_cend[k], cend.data(), T * 4, cudaMemcpyHostToDevice, b->s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->s);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "batch chunk tables", __FILE__, __LINE__));
+    }
+    const size_t mc = std::max(1, maxchunks);
+    e = cudaMalloc(&b->d_colsq, mc * BATCH_MAX_R * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_gpart, mc * BATCH_MAX_R * BATCH_MAX_R * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_fits, (size_t)BATCH_FIT_RING * T * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_iter, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_dummy, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_desc, T * sizeof(BDesc));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_iter, 0, sizeof(int), b->s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_desc, b->h_desc.data(), T * sizeof(BDesc), cudaMemcpyHostToDevice, b->s);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "batch buffers", __FILE__, __LINE__));
+    e = cudaFuncSetAttribute(k_b_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * (size_t)b->maxR * b->maxR * sizeof(double)));
+    if (e != cudaSuccess) return bail(cuda_fail(e, "k_b_solve shared memory", __FILE__, __LINE__));
+    // initial Grams of every mode (unscaled)
+    for (int k = 0; k < b->maxN; k++) {
+        if (b->nchunks[k]) {
+            k_b_gram<<<b->nchunks[k], DN_THREADS, 0, b->s>>>(b->d_desc, b->d_ct[k], b->d_cr0[k], b->d_cr1[k], k, 0,
+                                                              b->d_gpart);
+            count_launch();
+        }
+        k_b_gram_reduce<<<T, 256, 0, b->s>>>(b->d_desc, b->d_cbeg[k], b->d_cend[k], k, 0, b->d_gpart);
+        count_launch();
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->s);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "batch initial Grams", __FILE__, __LINE__));
+    // capture one sweep as a graph
+    const bool use_graph = !(opts && opts->verbose < 0);
+    if (use_graph) {
+        e = cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaStreamBeginCapture", __FILE__, __LINE__));
+        const unsigned long long before = launches_so_far();
+        int st = batch_enqueue_sweep(b);
+        // captured launches run only when the graph is replayed
+        b->graph_kernels = (long long)(launches_so_far() - before);
+        add_launches(-b->graph_kernels);
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(b->s, &g);
+        if (st != BLCO_OK) {
+            if (g) cudaGraphDestroy(g);
+            return bail(st);
+        }
+        if (e2 != cudaSuccess) return bail(cuda_fail(e2, "cudaStreamEndCapture", __FILE__, __LINE__));
+        b->graph = g;
+        e = cudaGraphInstantiate(&b->exec, g, 0);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__));
+    }
+    *out = b;
+    return BLCO_OK;
+}
+
+int batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done)
+{
+    if (iters < 0 || iters > BATCH_FIT_RING) return fail(BLCO_ERR_INVALID, "iterations per call must be 0..4096");
+    for (int i = 0; i < iters; i++) {
+        if (b->exec) {
+            BLCO_CUDA(cudaGraphLaunch(b->exec, b->s));
+            add_launches(b->graph_kernels);
+        } else {
+            BLCO_TRY(batch_enqueue_sweep(b));
+        }
+    }
+    BLCO_CUDA(cudaStreamSynchronize(b->s));
+    const int first = b->iters_run;
+    b->iters_run += iters;
+    BLCO_CUDA(cudaMemcpy(b->h_desc.data(), b->d_desc, b->T * sizeof(BDesc), cudaMemcpyDeviceToHost));
+    if (fits && iters) {
+        // ring rows first..first+iters-1 (mod the ring), in at most two pieces
+        const int r0 = first % BATCH_FIT_RING;
+        const int n1 = std::min(iters, BATCH_FIT_RING - r0);
+        const size_t row = (size_t)b->T * sizeof(double);
+        BLCO_CUDA(cudaMemcpy(fits, b->d_fits + (size_t)r0 * b->T, n1 * row, cudaMemcpyDeviceToHost));
+        if (iters > n1)
+            BLCO_CUDA(cudaMemcpy(fits + (size_t)n1 * b->T, b->d_fits, (iters - n1) * row, cudaMemcpyDeviceToHost));
+    }
+    if (iters_done)
+        for (int t = 0; t < b->T; t++) iters_done[t] = b->h_desc[t].iters;
+    return BLCO_OK;
+}
+
+int batch_destroy(blco_batch* b) { return batch_free(b); }
 
 } // namespace blco

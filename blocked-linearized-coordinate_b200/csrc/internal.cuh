@@ -40,6 +40,9 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 
 int fail(int status, const std::string& msg);
 void count_launch();
+// Adds n (may be negative) to the calling thread's launch counter.
+void add_launches(long long n);
+unsigned long long launches_so_far();
 
 // ----------------------------------------------------------- device info --
 
@@ -103,6 +106,7 @@ struct ModeStats {
 } // namespace blco
 
 struct blco_cpals_plan;
+struct blco_batch;
 
 struct blco_tensor {
     blco::Layout layout;
@@ -163,6 +167,11 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
 int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* iters_done, bool verbose);
 int plan_destroy(blco_cpals_plan* p);
 int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
+
+int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* const* const* d_factors,
+                 double* const* d_lambdas, double tol, const blco_opts* opts, blco_batch** out);
+int batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done);
+int batch_destroy(blco_batch* b);
 int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda, int maxiter,
                double tol, const blco_opts* opts, double* fit_out, double* fits, int* iters_out);
 

@@ -106,3 +106,23 @@ def uniform_tensor_host(nnz, dims, seed=0):
         rem = rem % mu
     vals = rng.random(nnz)
     return dict(dims=dims, cidx=cidx, vals=vals)
+
+
+def batch_tensors_device(count=512, seed=0, device="cuda", median_nnz=200_000, nnz_range=(10_000, 2_000_000),
+                         dim_range=(100, 50_000), ranks=(8, 16, 32), nmodes=3):
+    """Many small 3-mode tensors of uneven size (the batched CP-ALS
+    workload): nnz lognormal(log median, 1) clipped to nnz_range and to half
+    the tensor's cells, each mode length uniform in dim_range, uniform
+    coordinates, FP32 U(0,1) values, rank drawn from `ranks`.  Returns a list
+    of dict(dims, cidx, vals, rank)."""
+    rng = np.random.default_rng(int(seed))
+    out = []
+    for i in range(count):
+        dims = [int(x) for x in rng.integers(dim_range[0], dim_range[1] + 1, size=nmodes)]
+        cells = int(np.prod(np.array(dims, dtype=np.float64)))
+        nnz = int(np.exp(rng.normal(np.log(median_nnz), 1.0)))
+        nnz = int(min(max(nnz, nnz_range[0]), nnz_range[1], cells // 2))
+        X = zipf_tensor_device(nnz, dims, 0.0, seed=int(seed) * 100_003 + i, device=device, value_dist="uniform")
+        X["rank"] = int(rng.choice(ranks))
+        out.append(X)
+    return out

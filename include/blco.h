@@ -238,6 +238,32 @@ int blco_cpals_plan_iterate(blco_cpals_plan* p, int iters, double tol, double* f
 int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
 int blco_cpals_plan_destroy(blco_cpals_plan* p);
 
+/* Batched CP-ALS of many independent resident tensors (no counterpart in the
+ * reference, which decomposes one tensor per run).  Tensors may differ in
+ * nnz, order (1..5) and rank (ranks[t] in 1..64); up to 4096 tensors, all on
+ * one device.  Each iteration is one sweep over every unconverged tensor:
+ * the MTTKRP of mode slot k (a tensor's k-th longest mode) of all tensors
+ * is one persistent launch, the dense steps are one launch per step over
+ * all tensors, and the fit and the convergence test (|fit - fit_old| < tol,
+ * or NaN, per tensor) run on the device.  The sweep is captured once as a
+ * CUDA graph and replayed per iteration.  The arithmetic is FP64 and the
+ * algorithm is that of blco_cpals, tensor by tensor.
+ *   d_factors[t][n]: device FP64 dims[n] x ranks[t] row-major, updated in
+ *   place; d_lambdas[t]: device FP64 ranks[t], updated in place.  Both stay
+ *   owned by the caller and must outlive the batch.  opts->verbose < 0
+ *   disables the graph (each sweep is enqueued launch by launch). */
+typedef struct blco_batch blco_batch;
+
+int blco_batch_create(int count, blco_tensor* const* tensors, const int* ranks,
+                      double* const* const* d_factors, double* const* d_lambdas,
+                      double tol, const blco_opts* opts, blco_batch** out);
+/* Run `iters` sweeps (0..4096).  fits (may be NULL): host array of
+ * iters x count, entry [i * count + t] the fit of tensor t after sweep i of
+ * this call (a converged tensor keeps its last value there).  iters_done
+ * (may be NULL): per tensor, iterations executed since creation. */
+int blco_batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done);
+int blco_batch_destroy(blco_batch* b);
+
 /* Number of this library's kernels launched by the calling thread since the
  * last reset (for reporting launch counts). */
 uint64_t blco_launch_count(int reset);
