@@ -949,8 +949,10 @@ struct BDesc {
     const uint64_t* coords;
     const double* vals;
     uint64_t nnz;
-    uint64_t tile_off;                 // first global tile of this tensor
+    const uint64_t* sc[BLCO_MAX_MODES]; // stream copy sorted by the row of mode n
+    const double* sv[BLCO_MAX_MODES];
     int nmodes, rank;
+    int vec2;                          // rank even and 16-byte aligned rows: 2-double gathers
     int order[BLCO_MAX_MODES];         // modes by descending length
     uint64_t dims[BLCO_MAX_MODES];
     uint64_t mask[BLCO_MAX_MODES];
@@ -977,105 +979,164 @@ __global__ void k_b_zero(BDesc* __restrict__ d, int T, int slot)
     for (uint64_t i = (uint64_t)part * blockDim.x + threadIdx.x; i < len; i += 8ull * blockDim.x) b.M[i] = 0.0;
 }
 
-// One persistent launch over the tiles of all tensors.  Per tile: the 32
-// nonzeros are ordered by output row (match_any), then lane groups of
-// min(R, 32) lanes take one nonzero each, a lane owning columns q, q+32;
-// equal-row runs are summed in registers and flushed with FP64 atomics.
-__global__ void __launch_bounds__(768, 1) k_b_mttkrp(BDesc* __restrict__ d, int T, uint64_t total_tiles, int slot,
-                                                    uint64_t tiles_per_cta)
+// One persistent launch over the chunks of all tensors.  For mode slot k,
+// tensor t contributes ceil(nnz / BM_CHUNK) chunks of its stream copy sorted
+// by the row of its k-th mode; a warp takes a chunk and splits it into one
+// contiguous segment per lane group (LPN lanes, each owning VEC adjacent
+// columns, W column blocks).  Each step the group loads LPN nonzeros (one per
+// lane, coalesced), then walks them in order with the row, value and other
+// indices broadcast by shuffles; the factor rows of U positions are gathered
+// before they are multiplied.  Because the segment is row-sorted, the FP64
+// partial sum stays in registers until the row changes and is then added to
+// M with one atomic per column, so atomics scale with rows, not nonzeros.
+// Chunks are dealt round-robin to the warps of the whole grid, which keeps
+// the warps on neighbouring chunks (a few tensors at a time) and their
+// factor rows in L2.
+constexpr int BM_CHUNK = 1024;
+constexpr int BM_THREADS = 512;
+constexpr int BM_WARPS = BM_THREADS / 32;
+
+// VEC: 2 gathers two adjacent FP64 columns per lane (even rank, 16-byte
+// aligned rows), 1 one column in each of two 32-column blocks.  NMO: the
+// number of other modes (2 for third-order tensors, specialised) or -1 for
+// any count up to 4 (runtime, fewer positions in flight).  lpn: lanes per
+// nonzero (a power of two, 4..32).
+template <int VEC, int NMO>
+__device__ __forceinline__ void b_chunk(const BDesc& b, int n, uint64_t j0, uint64_t j1, int lane, int lpn)
+{
+    constexpr int KMAX = NMO > 0 ? NMO : 4;
+    constexpr int U = NMO == 2 ? 4 : 2;
+    constexpr int W = VEC == 2 ? 1 : 2;
+    constexpr int NC = W * VEC;
+    const int nmo = NMO >= 0 ? NMO : b.nmodes - 1;
+    const int groups = 32 / lpn;
+    const int grp = lane / lpn, q = lane % lpn;
+    const int R = b.rank;
+    const uint64_t* __restrict__ sc = b.sc[n];
+    const double* __restrict__ sv = b.sv[n];
+    const int rpos = b.pos[n];
+    const uint64_t rmask = b.mask[n];
+    const double* f[KMAX];
+    int opos[KMAX];
+    uint64_t omask[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; k++) {
+        const int m = k + (k >= n ? 1 : 0); // the k-th mode other than n
+        f[k] = k < nmo ? b.U[m] : nullptr;
+        opos[k] = k < nmo ? b.pos[m] : 0;
+        omask[k] = k < nmo ? b.mask[m] : 0;
+    }
+    const uint64_t len = j1 - j0;
+    const uint64_t seg = ((len + groups - 1) / groups + lpn - 1) / lpn * lpn;
+    const uint64_t gb = j0 + grp * seg, ge = min(j1, gb + seg);
+    const int nsteps = (int)(seg / lpn);
+    double acc[NC];
+#pragma unroll
+    for (int j = 0; j < NC; j++) acc[j] = 0.0;
+    uint32_t acc_row = 0xffffffffu;
+    auto col = [&](int w) { return VEC == 2 ? q * 2 : w * 32 + q; };
+    auto flush = [&]() {
+        double* o = b.M + (size_t)acc_row * R;
+#pragma unroll
+        for (int w = 0; w < W; w++) {
+            const int c = col(w);
+#pragma unroll
+            for (int j = 0; j < VEC; j++)
+                if (c + j < R) atomicAdd(o + c + j, acc[w * VEC + j]);
+        }
+    };
+    for (int st = 0; st < nsteps; st++) {
+        const uint64_t jj = gb + (uint64_t)st * lpn + q;
+        const bool valid = jj < ge;
+        const uint64_t c = valid ? __ldcs(sc + jj) : 0ull;
+        const double v = valid ? __ldcs(sv + jj) : 0.0;
+        const uint32_t row = valid ? (uint32_t)((c >> rpos) & rmask) : 0xffffffffu;
+        uint32_t oth[KMAX];
+#pragma unroll
+        for (int k = 0; k < KMAX; k++) oth[k] = (uint32_t)((c >> opos[k]) & omask[k]);
+        for (int p0 = 0; p0 < lpn; p0 += U) {
+            uint32_t rp[U];
+            double vp[U];
+            double g[U][KMAX][NC];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                rp[u] = __shfl_sync(0xffffffffu, row, p0 + u, lpn);
+                vp[u] = __shfl_sync(0xffffffffu, v, p0 + u, lpn);
+#pragma unroll
+                for (int k = 0; k < KMAX; k++) {
+                    const uint32_t o = __shfl_sync(0xffffffffu, oth[k], p0 + u, lpn);
+#pragma unroll
+                    for (int w = 0; w < W; w++) {
+                        const int cc = col(w);
+                        if (k < nmo && rp[u] != 0xffffffffu && cc < R) {
+                            const double* a = f[k] + (size_t)o * R + cc;
+                            if constexpr (VEC == 2) {
+                                const double2 x = __ldg(reinterpret_cast<const double2*>(a));
+                                g[u][k][w * 2] = x.x;
+                                g[u][k][w * 2 + 1] = x.y;
+                            } else {
+                                g[u][k][w] = __ldg(a);
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < VEC; j++) g[u][k][w * VEC + j] = 1.0;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (rp[u] != 0xffffffffu) {
+                    if (rp[u] != acc_row) {
+                        if (acc_row != 0xffffffffu) flush();
+                        acc_row = rp[u];
+#pragma unroll
+                        for (int j = 0; j < NC; j++) acc[j] = 0.0;
+                    }
+#pragma unroll
+                    for (int j = 0; j < NC; j++) {
+                        double x = vp[u];
+#pragma unroll
+                        for (int k = 0; k < KMAX; k++)
+                            if (NMO > 0 || k < nmo) x *= g[u][k][j];
+                        acc[j] += x;
+                    }
+                }
+            }
+        }
+    }
+    if (acc_row != 0xffffffffu) flush();
+}
+
+__global__ void __launch_bounds__(BM_THREADS, 1) k_b_mttkrp(const BDesc* __restrict__ d, int T,
+                                                           const uint32_t* __restrict__ choff, int slot)
 {
     __shared__ uint32_t toff[BATCH_MAX_T + 1];
-    __shared__ __align__(16) uint32_t srow[24][32];
-    __shared__ __align__(16) uint32_t soth[24][4][32];
-    __shared__ __align__(16) double sval[24][32];
-    for (int i = threadIdx.x; i < T; i += blockDim.x) toff[i] = (uint32_t)d[i].tile_off;
-    if (threadIdx.x == 0) toff[T] = (uint32_t)total_tiles;
+    for (int i = threadIdx.x; i <= T; i += blockDim.x) toff[i] = choff[i];
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint64_t t_beg = (uint64_t)blockIdx.x * tiles_per_cta;
-    const uint64_t t_end = min(total_tiles, t_beg + tiles_per_cta);
-    for (uint64_t g = t_beg + warp; g < t_end; g += 24) {
+    const uint32_t nchunks = toff[T];
+    for (uint32_t c = blockIdx.x * BM_WARPS + warp; c < nchunks; c += gridDim.x * BM_WARPS) {
         int lo = 0, hi = T - 1;
         while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (toff[mid] <= g) lo = mid;
+            const int mid = (lo + hi + 1) >> 1;
+            if (toff[mid] <= c) lo = mid;
             else hi = mid - 1;
         }
         const BDesc& b = d[lo];
-        if (!b.active || slot >= b.nmodes) continue; // warp-uniform
-        const int n = b.order[slot], R = b.rank, nm = b.nmodes;
-        const uint64_t i0 = (g - toff[lo]) * 32;
-        const uint64_t i = i0 + lane;
-        const bool valid = i < b.nnz;
-        const uint64_t c = valid ? b.coords[i] : 0;
-        const double v = valid ? b.vals[i] : 0.0;
-        uint32_t rt = 0, r0 = 0, r1 = 0, r2 = 0, r3 = 0;
-        const double *f0 = nullptr, *f1 = nullptr, *f2 = nullptr, *f3 = nullptr;
-        int k = 0;
-#pragma unroll
-        for (int m = 0; m < BLCO_MAX_MODES; m++) {
-            if (m < nm) {
-                const uint32_t r = (uint32_t)((c >> b.pos[m]) & b.mask[m]);
-                if (m == n) {
-                    rt = r;
-                } else {
-                    if (k == 0) { r0 = r; f0 = b.U[m]; }
-                    else if (k == 1) { r1 = r; f1 = b.U[m]; }
-                    else if (k == 2) { r2 = r; f2 = b.U[m]; }
-                    else { r3 = r; f3 = b.U[m]; }
-                    k++;
-                }
-            }
+        if (!b.active) continue; // warp-uniform
+        const int n = b.order[slot];
+        const uint64_t j0 = (uint64_t)(c - toff[lo]) * BM_CHUNK;
+        const uint64_t j1 = min(b.nnz, j0 + BM_CHUNK);
+        const int R = b.rank;
+        if (b.vec2) {
+            const int lpn = R <= 8 ? 4 : R <= 16 ? 8 : R <= 32 ? 16 : 32;
+            if (b.nmodes == 3) b_chunk<2, 2>(b, n, j0, j1, lane, lpn);
+            else b_chunk<2, -1>(b, n, j0, j1, lane, lpn);
+        } else {
+            if (b.nmodes == 3) b_chunk<1, 2>(b, n, j0, j1, lane, 32);
+            else b_chunk<1, -1>(b, n, j0, j1, lane, 32);
         }
-        const uint32_t key = valid ? rt : 0xffffffffu;
-        const uint32_t peers = __match_any_sync(0xffffffffu, key);
-        const uint32_t lt = (1u << lane) - 1;
-        const int leader = __ffs(peers) - 1;
-        const uint32_t x = lane == leader ? (uint32_t)__popc(peers) : 0u;
-        uint32_t inc = x;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        const int sp = (int)__shfl_sync(0xffffffffu, inc - x, leader) + __popc(peers & lt);
-        const uint32_t ends = __reduce_or_sync(0xffffffffu, ((peers >> lane) == 1u) ? (1u << sp) : 0u);
-        srow[warp][sp] = rt;
-        soth[warp][0][sp] = r0;
-        soth[warp][1][sp] = r1;
-        soth[warp][2][sp] = r2;
-        soth[warp][3][sp] = r3;
-        sval[warp][sp] = v;
-        __syncwarp();
-        const int count = (int)min((uint64_t)32, b.nnz - i0);
-        const int lpn = R < 32 ? R : 32;
-        const int groups = 32 / lpn;
-        const int per = (32 + groups - 1) / groups;
-        const int grp = lane / lpn, q = lane % lpn;
-        if (grp < groups) {
-            const int pb = grp * per, pe = min(pb + per, count);
-            double acc0 = 0.0, acc1 = 0.0;
-            const int c0 = q, c1 = q + 32;
-            for (int pp = pb; pp < pe; pp++) {
-                const double val = sval[warp][pp];
-                double p0 = val, p1 = val;
-                const uint32_t o0 = soth[warp][0][pp], o1 = soth[warp][1][pp], o2 = soth[warp][2][pp],
-                               o3 = soth[warp][3][pp];
-                if (nm > 1) { p0 *= f0[(size_t)o0 * R + c0]; if (c1 < R) p1 *= f0[(size_t)o0 * R + c1]; }
-                if (nm > 2) { p0 *= f1[(size_t)o1 * R + c0]; if (c1 < R) p1 *= f1[(size_t)o1 * R + c1]; }
-                if (nm > 3) { p0 *= f2[(size_t)o2 * R + c0]; if (c1 < R) p1 *= f2[(size_t)o2 * R + c1]; }
-                if (nm > 4) { p0 *= f3[(size_t)o3 * R + c0]; if (c1 < R) p1 *= f3[(size_t)o3 * R + c1]; }
-                acc0 += p0;
-                acc1 += p1;
-                if (((ends >> pp) & 1u) || pp == pe - 1) {
-                    double* o = b.M + (size_t)srow[warp][pp] * R;
-                    atomicAdd(o + c0, acc0);
-                    if (c1 < R) atomicAdd(o + c1, acc1);
-                    acc0 = acc1 = 0.0;
-                }
-            }
-        }
-        __syncwarp();
     }
 }
 
@@ -1241,7 +1302,9 @@ struct blco_batch {
     int T = 0, maxN = 0, maxR = 0;
     blco::BDesc* d_desc = nullptr;
     std::vector<blco::BDesc> h_desc;
-    uint64_t total_tiles = 0;
+    uint32_t* d_choff = nullptr;       // per mode slot: T + 1 MTTKRP chunk offsets
+    uint32_t mt_chunks[BLCO_MAX_MODES] = {};
+    void* streams = nullptr;           // row-sorted stream copies of every mode
     // per mode slot: chunk -> tensor, row range; per tensor chunk range
     uint32_t* d_ct[BLCO_MAX_MODES] = {};
     uint32_t* d_cr0[BLCO_MAX_MODES] = {};
@@ -1281,6 +1344,8 @@ int batch_free(blco_batch* b)
         cudaFree(b->d_cend[k]);
     }
     cudaFree(b->d_desc);
+    cudaFree(b->d_choff);
+    cudaFree(b->streams);
     cudaFree(b->d_colsq);
     cudaFree(b->d_gpart);
     cudaFree(b->d_fits);
@@ -1296,13 +1361,12 @@ int batch_free(blco_batch* b)
 int batch_enqueue_sweep(blco_batch* b)
 {
     const size_t ssmem = 2 * (size_t)b->maxR * b->maxR * sizeof(double);
-    const uint64_t grid = std::min<uint64_t>((uint64_t)b->sm, (b->total_tiles + 23) / 24);
-    const uint64_t tpc = (b->total_tiles + std::max<uint64_t>(grid, 1) - 1) / std::max<uint64_t>(grid, 1);
     for (int k = 0; k < b->maxN; k++) {
         k_b_zero<<<b->T * 8, 256, 0, b->s>>>(b->d_desc, b->T, k);
         BLCO_CHECK_LAUNCH("k_b_zero");
-        if (grid) {
-            k_b_mttkrp<<<(unsigned)grid, 768, 0, b->s>>>(b->d_desc, b->T, b->total_tiles, k, tpc);
+        if (b->mt_chunks[k]) {
+            const unsigned grid = (unsigned)std::min<uint64_t>(b->sm, (b->mt_chunks[k] + BM_WARPS - 1) / BM_WARPS);
+            k_b_mttkrp<<<grid, BM_THREADS, 0, b->s>>>(b->d_desc, b->T, b->d_choff + (size_t)k * (b->T + 1), k);
             BLCO_CHECK_LAUNCH("k_b_mttkrp");
         }
         k_b_solve<<<b->T, DN_THREADS, ssmem, b->s>>>(b->d_desc, k, b->d_dummy);
@@ -1361,7 +1425,8 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
         uint64_t maxdim = 0;
         for (int n = 0; n < L.nmodes; n++) maxdim = std::max(maxdim, L.dims[n]);
         const size_t R = ranks[t];
-        pool_doubles += maxdim * R + (size_t)L.nmodes * R * R + R * R + R;
+        auto al = [](size_t x) { return (x + 3) & ~(size_t)3; };
+        pool_doubles += al(maxdim * R) + (size_t)L.nmodes * al(R * R) + al(R * R) + al(R);
         b->maxN = std::max(b->maxN, L.nmodes);
         b->maxR = std::max(b->maxR, ranks[t]);
     }
@@ -1373,7 +1438,11 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
     if (e == cudaSuccess) e = cudaMalloc(&b->pool, pool_doubles * sizeof(double));
     if (e != cudaSuccess) return bail(cuda_fail(e, "batch workspace", __FILE__, __LINE__));
     double* cur = static_cast<double*>(b->pool);
-    uint64_t tiles = 0;
+    auto take = [&](size_t nd) {
+        double* r = cur;
+        cur += (nd + 3) & ~(size_t)3; // 32-byte aligned pieces
+        return r;
+    };
     for (int t = 0; t < T; t++) {
         blco_tensor* x = tensors[t];
         const Layout& L = x->layout;
@@ -1382,10 +1451,10 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
         d.coords = x->d_coords;
         d.vals = x->d_values;
         d.nnz = x->nnz;
-        d.tile_off = tiles;
-        tiles += (x->nnz + 31) / 32;
         d.nmodes = L.nmodes;
         d.rank = ranks[t];
+        d.vec2 = ranks[t] % 2 == 0;
+        for (int n = 0; n < L.nmodes; n++) d.vec2 &= ((uintptr_t)d_factors[t][n] & 15) == 0;
         for (int n = 0; n < L.nmodes; n++) {
             d.dims[n] = L.dims[n];
             d.mask[n] = L.mode_masks[n];
@@ -1398,22 +1467,65 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
         uint64_t maxdim = 0;
         for (int n = 0; n < L.nmodes; n++) maxdim = std::max(maxdim, L.dims[n]);
         const size_t R = ranks[t];
-        d.M = cur;
-        cur += maxdim * R;
-        for (int n = 0; n < L.nmodes; n++) {
-            d.G[n] = cur;
-            cur += R * R;
-        }
-        d.P = cur;
-        cur += R * R;
-        d.inv = cur;
-        cur += R;
+        d.M = take(maxdim * R);
+        for (int n = 0; n < L.nmodes; n++) d.G[n] = take(R * R);
+        d.P = take(R * R);
+        d.inv = take(R);
         d.xnorm = std::sqrt(x->norm_sq);
         d.fit_old = 0.0;
         d.active = 1;
     }
-    b->total_tiles = tiles;
-    if (tiles >= (1ull << 32)) return bail(fail(BLCO_ERR_UNSUPPORTED, "batch holds too many nonzeros (2^37 at most)"));
+    // Row-sorted stream copies of every mode of every tensor (16 bytes per
+    // nonzero per mode) and the MTTKRP chunk offsets of every mode slot.
+    {
+        uint64_t total = 0, maxnnz = 0;
+        for (int t = 0; t < T; t++) {
+            total += tensors[t]->nnz * (uint64_t)tensors[t]->layout.nmodes;
+            maxnnz = std::max(maxnnz, tensors[t]->nnz);
+        }
+        uint64_t *tk = nullptr;
+        double* tv = nullptr;
+        e = cudaMalloc(&b->streams, std::max<uint64_t>(1, total) * 16);
+        if (e == cudaSuccess) e = cudaMalloc(&tk, std::max<uint64_t>(1, maxnnz) * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&tv, std::max<uint64_t>(1, maxnnz) * 8);
+        if (e != cudaSuccess) {
+            cudaFree(tk);
+            cudaFree(tv);
+            return bail(cuda_fail(e, "batch stream copies", __FILE__, __LINE__));
+        }
+        uint64_t* sc = static_cast<uint64_t*>(b->streams);
+        double* sv = reinterpret_cast<double*>(sc + total);
+        int st = BLCO_OK;
+        for (int t = 0; t < T && st == BLCO_OK; t++) {
+            BDesc& d = b->h_desc[t];
+            for (int n = 0; n < d.nmodes && st == BLCO_OK; n++) {
+                st = sort_stream_by_mode(tensors[t], n, sc, sv, tk, tv, b->s);
+                d.sc[n] = sc;
+                d.sv[n] = sv;
+                sc += d.nnz;
+                sv += d.nnz;
+            }
+        }
+        cudaStreamSynchronize(b->s);
+        cudaFree(tk);
+        cudaFree(tv);
+        if (st != BLCO_OK) return bail(st);
+        std::vector<uint32_t> choff((size_t)b->maxN * (T + 1));
+        for (int k = 0; k < b->maxN; k++) {
+            uint64_t c = 0;
+            for (int t = 0; t < T; t++) {
+                choff[(size_t)k * (T + 1) + t] = (uint32_t)c;
+                if (k < b->h_desc[t].nmodes) c += (b->h_desc[t].nnz + BM_CHUNK - 1) / BM_CHUNK;
+            }
+            if (c >= (1ull << 32)) return bail(fail(BLCO_ERR_UNSUPPORTED, "batch holds too many nonzeros"));
+            choff[(size_t)k * (T + 1) + T] = (uint32_t)c;
+            b->mt_chunks[k] = (uint32_t)c;
+        }
+        e = cudaMalloc(&b->d_choff, choff.size() * 4);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->d_choff, choff.data(), choff.size() * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "batch chunk offsets", __FILE__, __LINE__));
+    }
     // chunk tables per slot
     int maxchunks = 0;
     for (int k = 0; k < b->maxN; k++) {

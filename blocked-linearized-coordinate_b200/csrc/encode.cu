@@ -622,6 +622,28 @@ int build_hot_csr(blco_tensor* t, cudaStream_t s)
     return st;
 }
 
+// A copy of the tensor's stream sorted stably by the row index of `mode`
+// (ALTO order inside each row), written to d_coords / d_vals (nnz entries
+// each); tmp_k / tmp_v are nnz-entry scratch arrays.
+int sort_stream_by_mode(const blco_tensor* t, int mode, uint64_t* d_coords, double* d_vals, uint64_t* tmp_k,
+                        double* tmp_v, cudaStream_t s)
+{
+    const Layout& L = t->layout;
+    if (t->nnz == 0) return BLCO_OK;
+    BLCO_CUDA(cudaMemcpyAsync(d_coords, t->d_coords, t->nnz * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+    BLCO_CUDA(cudaMemcpyAsync(d_vals, t->d_values, t->nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    const int bits = __builtin_popcountll(L.mode_masks[mode]);
+    if (bits == 0) return BLCO_OK;
+    bool alt = false;
+    BLCO_TRY(radix_sort_pairs(d_coords, d_vals, tmp_k, tmp_v, t->nnz, L.mode_pos[mode], L.mode_pos[mode] + bits, s,
+                              &alt));
+    if (alt) {
+        BLCO_CUDA(cudaMemcpyAsync(d_coords, tmp_k, t->nnz * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        BLCO_CUDA(cudaMemcpyAsync(d_vals, tmp_v, t->nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    return BLCO_OK;
+}
+
 int build_hot_tables(blco_tensor* t, cudaStream_t s)
 {
     const Layout& L = t->layout;
