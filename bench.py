@@ -258,6 +258,58 @@ def time_form(pkg, torch, t, dims, rk, fs0, form, args, stream, dist):
                 fits=fits, launches=int(launches), clocks=ck)
 
 
+BATCH = dict(
+    workload=("512 independent 3-mode tensors: nnz lognormal(median 2e5, sigma 1) clipped to [1e4, 2e6] and to half "
+              "the cells, mode lengths U[100, 50000], uniform coordinates, FP32 U(0,1) values, rank in {8,16,32}"),
+    count=512, seed=4)
+
+
+def batched_leg(pkg, torch, args):
+    """Batched CP-ALS of the many-small-tensors workload: device ms per
+    sweep of the captured graph, next to per-tensor plans run one after
+    another (timed on the first 32 tensors, scaled by nnz)."""
+    from blco_b200 import synth
+    Xs = synth.batch_tensors_device(BATCH["count"], seed=BATCH["seed"])
+    nnzs = [int(x["vals"].numel()) for x in Xs]
+    ts = [pkg.Tensor.encode_device(x["dims"], x["cidx"], x["vals"]) for x in Xs]
+    ranks = [x["rank"] for x in Xs]
+    dims = [x["dims"] for x in Xs]
+    del Xs
+    torch.cuda.empty_cache()
+    g = torch.Generator(device="cuda").manual_seed(99)
+    fs = [[torch.rand(d, r, dtype=torch.float64, device="cuda", generator=g) for d in dd] for dd, r in zip(dims, ranks)]
+    f0 = [[m.clone() for m in f] for f in fs]
+    ls = [torch.ones(r, dtype=torch.float64, device="cuda") for r in ranks]
+    b = pkg.Batch(ts, fs, ls, tol=0.0)
+    b.iterate(args.warmup)
+    pkg.launch_count(reset=True)
+    b.iterate(args.steps)
+    launches = pkg.launch_count(reset=True)
+    ms = b.last_ms() / max(1, args.steps)
+    b.destroy()
+    # per-tensor plans, one after another, on a prefix of the batch
+    k = min(32, len(ts))
+    seq = 0.0
+    for i in range(k):
+        lam = torch.ones(ranks[i], dtype=torch.float64, device="cuda")
+        p = pkg.CpalsPlan(ts[i], f0[i], lam)
+        p.iterate(2, tol=-1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p.iterate(3, tol=-1.0)
+        torch.cuda.synchronize()
+        seq += (time.perf_counter() - t0) / 3
+        p.destroy()
+    seq_est = seq * 1e3 * sum(nnzs) / sum(nnzs[:k])
+    for t in ts:
+        t.free()
+    return dict(workload=BATCH["workload"], tensors=len(ts), nnz=sum(nnzs), ms_per_sweep=ms, sweeps=args.steps,
+                gpu_launches=int(launches), dtype="f64", graph="one CUDA graph per sweep",
+                sequential_plans_ms_per_iter_est=seq_est, speedup_vs_sequential=seq_est / ms,
+                note="device time (CUDA events on the batch stream); sequential estimate from the first "
+                     f"{k} tensors' plans (wall time), scaled by nnz")
+
+
 def run_ours(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
@@ -338,6 +390,11 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_quick(args, dims, rk)
     t.free()
+    del fs0
+    torch.cuda.empty_cache()
+    batched = None
+    if not args.no_batched:
+        batched = batched_leg(pkg, torch, args)
     if rank == 0:
         forms_out = {}
         for f, r in res.items():
@@ -368,6 +425,7 @@ def run_ours(args, world, rank, local):
                               "factors; job time / iterations; bytes are per iteration")),
             "gpu_launches": C["launches"],
             "clocks": C["clocks"],
+            "batched": batched,
         }
         print(json.dumps(line))
     if dist:
@@ -386,6 +444,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--ref-sample", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched many-small-tensors leg")
     ap.add_argument("--forms", default="fp64,mixed_f32,mixed_bf16")
     args = ap.parse_args()
     world, rank, local = dist_setup()

@@ -43,6 +43,10 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRECISION_MIXED_BF16 = 2
 
+KERNEL_TUNED = 20
+KERNEL_LEARNED = 21
+TUNE_CONFIGS = 12
+MLP_FEATURES = 25
 DTYPE_F64 = 0
 DTYPE_F32 = 1
 DTYPE_BF16 = 2
@@ -54,7 +58,9 @@ EXPORTS = (
     "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_ex", "blco_mttkrp_host",
     "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
     "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_batch_create", "blco_batch_iterate",
-    "blco_batch_destroy", "blco_launch_count",
+    "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
+    "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
+    "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_launch_count",
 )
 
 
@@ -129,6 +135,20 @@ def lib():
         L.blco_batch_create.argtypes = [i32, vp, vp, vp, vp, f64, vp, vp]
         L.blco_batch_iterate.argtypes = [vp, i32, vp, vp]
         L.blco_batch_destroy.argtypes = [vp]
+        L.blco_batch_last_ms.argtypes = [vp, vp]
+        L.blco_tune_space.argtypes = [vp]
+        L.blco_autotune.argtypes = [vp, i32, i32, i32, i32, vp, vp, vp]
+        L.blco_tune_features.argtypes = [vp, i32, i32, i32, vp]
+        L.blco_mlp_create.argtypes = [i32, u64, i32, vp]
+        L.blco_mlp_num_params.argtypes = [vp, vp]
+        L.blco_mlp_set_params.argtypes = [vp, vp, i32]
+        L.blco_mlp_get_params.argtypes = [vp, vp, i32]
+        L.blco_mlp_predict.argtypes = [vp, vp, i32, vp]
+        L.blco_mlp_grad.argtypes = [vp, vp, vp, vp, i32, vp, vp]
+        L.blco_mlp_train.argtypes = [vp, vp, vp, vp, i32, i32, i32, ctypes.c_float, u64, vp]
+        L.blco_mlp_destroy.argtypes = [vp]
+        L.blco_selector_set.argtypes = [vp, ctypes.c_float]
+        L.blco_select.argtypes = [vp, i32, i32, i32, vp, ctypes.c_float, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -375,6 +395,12 @@ class Batch:
         _check(lib().blco_batch_iterate(self._h, iters, fits.ctypes.data, done.ctypes.data))
         return fits[:iters], done
 
+    def last_ms(self):
+        """Device milliseconds of the sweeps of the last iterate call."""
+        ms = ctypes.c_double()
+        _check(lib().blco_batch_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
     def destroy(self):
         if self._h and self._h.value:
             _check(lib().blco_batch_destroy(self._h))
@@ -385,3 +411,103 @@ class Batch:
             self.destroy()
         except Exception:
             pass
+
+
+class TuneConfig(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int), ("hot_chunk", ctypes.c_int), ("interleave", ctypes.c_int)]
+
+
+def tune_space():
+    """The autotuner's schedules: list of dict(kernel, hot_chunk, interleave)."""
+    arr = (TuneConfig * TUNE_CONFIGS)()
+    _check(lib().blco_tune_space(arr))
+    return [dict(kernel=c.kernel, hot_chunk=c.hot_chunk, interleave=c.interleave) for c in arr]
+
+
+def autotune(t, mode, rank, factor_dtype=DTYPE_F64, reps=3, opts=None):
+    """Exhaustive sweep: (ms per schedule as numpy float32, -1 = not valid; best index)."""
+    ms = np.zeros(TUNE_CONFIGS, dtype=np.float32)
+    best = ctypes.c_int()
+    o = opts if opts is not None else make_opts()
+    _check(lib().blco_autotune(t.handle, mode, rank, factor_dtype, reps, ctypes.byref(o), ms.ctypes.data,
+                               ctypes.byref(best)))
+    return ms, best.value
+
+
+def tune_features(t, mode, rank, factor_dtype=DTYPE_F64):
+    f = np.zeros(MLP_FEATURES, dtype=np.float32)
+    _check(lib().blco_tune_features(t.handle, mode, rank, factor_dtype, f.ctypes.data))
+    return f
+
+
+class Mlp:
+    """The schedule selector network (blco_mlp_*), trained on the GPU by the
+    library's kernels."""
+
+    def __init__(self, hidden=64, seed=0, device=0):
+        h = ctypes.c_void_p()
+        _check(lib().blco_mlp_create(hidden, seed, device, ctypes.byref(h)))
+        self._h = h
+        n = ctypes.c_int()
+        _check(lib().blco_mlp_num_params(h, ctypes.byref(n)))
+        self.nparams = n.value
+        self.hidden = hidden
+
+    @property
+    def handle(self):
+        return self._h
+
+    def params(self):
+        p = np.zeros(self.nparams, dtype=np.float32)
+        _check(lib().blco_mlp_get_params(self._h, p.ctypes.data, self.nparams))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(lib().blco_mlp_set_params(self._h, p.ctypes.data, int(p.size)))
+
+    def predict(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        out = np.zeros((X.shape[0], TUNE_CONFIGS), dtype=np.float32)
+        _check(lib().blco_mlp_predict(self._h, X.ctypes.data, X.shape[0], out.ctypes.data))
+        return out
+
+    def grad(self, X, Y, M):
+        X, Y, M = (np.ascontiguousarray(a, dtype=np.float32) for a in (X, Y, M))
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().blco_mlp_grad(self._h, X.ctypes.data, Y.ctypes.data, M.ctypes.data, X.shape[0], g.ctypes.data,
+                                   ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, X, Y, M, epochs=200, batch=64, lr=1e-3, seed=0):
+        X, Y, M = (np.ascontiguousarray(a, dtype=np.float32) for a in (X, Y, M))
+        loss = ctypes.c_float()
+        _check(lib().blco_mlp_train(self._h, X.ctypes.data, Y.ctypes.data, M.ctypes.data, X.shape[0], epochs, batch,
+                                    ctypes.c_float(lr), seed, ctypes.byref(loss)))
+        return loss.value
+
+    def destroy(self):
+        if self._h and self._h.value:
+            _check(lib().blco_mlp_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def selector_set(net, margin=0.1):
+    _check(lib().blco_selector_set(net.handle if net is not None else None, ctypes.c_float(margin)))
+
+
+def select(t, mode, rank, factor_dtype=DTYPE_F64, net=None, margin=0.1, opts=None):
+    """(schedule index, used_sweep) as kernel id 21 would choose."""
+    cfg = ctypes.c_int()
+    sw = ctypes.c_int()
+    o = opts if opts is not None else make_opts()
+    _check(lib().blco_select(t.handle, mode, rank, factor_dtype, net.handle if net is not None else None,
+                             ctypes.c_float(margin), ctypes.byref(o), ctypes.byref(cfg), ctypes.byref(sw)))
+    return cfg.value, bool(sw.value)

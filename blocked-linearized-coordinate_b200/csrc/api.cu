@@ -330,8 +330,8 @@ int blco_mttkrp(blco_tensor* t, int mode, int rank, const double* const* d_facto
     for (int m = 0; m < t->layout.nmodes; m++) a.factors[m] = d_factors[m];
     a.out = d_out;
     a.factor_dtype = BLCO_DTYPE_F64;
-    a.kernel = opts ? opts->kernel : BLCO_KERNEL_AUTO;
     a.thread_cf = opts ? opts->thread_cf : 2;
+    BLCO_TRY(resolve_schedule(t, mode, rank, BLCO_DTYPE_F64, opts ? opts->kernel : BLCO_KERNEL_AUTO, s, &a));
     if (!t->resident) return mttkrp_streamed(t, a, opts, s);
     a.coords = t->d_coords;
     a.vals = t->d_values;
@@ -366,8 +366,8 @@ int blco_mttkrp_ex(blco_tensor* t, int mode, int rank, int factor_dtype, const v
     for (int m = 0; m < t->layout.nmodes; m++) a.factors[m] = d_factors[m];
     a.out = d_out;
     a.factor_dtype = factor_dtype;
-    a.kernel = opts ? opts->kernel : BLCO_KERNEL_AUTO;
     a.thread_cf = opts ? opts->thread_cf : 2;
+    BLCO_TRY(resolve_schedule(t, mode, rank, factor_dtype, opts ? opts->kernel : BLCO_KERNEL_AUTO, s, &a));
     return mttkrp_launch(t, a, s);
 }
 
@@ -443,5 +443,103 @@ int blco_batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done)
 }
 
 int blco_batch_destroy(blco_batch* b) { return batch_destroy(b); }
+
+int blco_tune_space(blco_tune_config* configs)
+{
+    if (!configs) return fail(BLCO_ERR_INVALID, "null argument");
+    for (int k = 0; k < BLCO_TUNE_CONFIGS; k++) {
+        configs[k].kernel = TUNE_SPACE[k].kernel;
+        configs[k].hot_chunk = TUNE_SPACE[k].hot_chunk;
+        configs[k].interleave = TUNE_SPACE[k].interleave;
+    }
+    return BLCO_OK;
+}
+
+int blco_autotune(blco_tensor* t, int mode, int rank, int factor_dtype, int reps, const blco_opts* opts, float* ms,
+                  int* best)
+{
+    if (!t) return fail(BLCO_ERR_INVALID, "null tensor");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    float local[BLCO_TUNE_CONFIGS];
+    BLCO_TRY(tune_sweep(t, mode, rank, factor_dtype, reps, pick_stream(t, opts), local));
+    if (ms) memcpy(ms, local, sizeof(local));
+    if (best) *best = tune_best(local);
+    return BLCO_OK;
+}
+
+int blco_tune_features(const blco_tensor* t, int mode, int rank, int factor_dtype, float* features)
+{
+    if (!t || !features) return fail(BLCO_ERR_INVALID, "null argument");
+    if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
+    return tune_features(t, mode, rank, factor_dtype, features);
+}
+
+int blco_mlp_create(int hidden, uint64_t seed, int device, blco_mlp** out)
+{
+    if (!out) return fail(BLCO_ERR_INVALID, "null output handle");
+    return mlp_create(hidden, seed, device, out);
+}
+
+int blco_mlp_num_params(const blco_mlp* net, int* n)
+{
+    if (!net || !n) return fail(BLCO_ERR_INVALID, "null argument");
+    *n = mlp_num_params(net);
+    return BLCO_OK;
+}
+
+int blco_mlp_set_params(blco_mlp* net, const float* params, int n)
+{
+    if (!net || !params) return fail(BLCO_ERR_INVALID, "null argument");
+    return mlp_set_params(net, params, n);
+}
+
+int blco_mlp_get_params(const blco_mlp* net, float* params, int n)
+{
+    if (!net || !params) return fail(BLCO_ERR_INVALID, "null argument");
+    return mlp_get_params(net, params, n);
+}
+
+int blco_mlp_predict(blco_mlp* net, const float* X, int n, float* out)
+{
+    if (!net || (n > 0 && (!X || !out))) return fail(BLCO_ERR_INVALID, "null argument");
+    return mlp_predict(net, X, n, out);
+}
+
+int blco_mlp_grad(blco_mlp* net, const float* X, const float* Y, const float* mask, int n, float* grad, float* loss)
+{
+    if (!net || !X || !Y || !mask) return fail(BLCO_ERR_INVALID, "null argument");
+    return mlp_grad(net, X, Y, mask, n, grad, loss);
+}
+
+int blco_mlp_train(blco_mlp* net, const float* X, const float* Y, const float* mask, int n, int epochs, int batch,
+                   float lr, uint64_t seed, float* loss)
+{
+    if (!net || !X || !Y || !mask) return fail(BLCO_ERR_INVALID, "null argument");
+    return mlp_train(net, X, Y, mask, n, epochs, batch, lr, seed, loss);
+}
+
+int blco_mlp_destroy(blco_mlp* net) { return mlp_destroy(net); }
+
+int blco_selector_set(blco_mlp* net, float margin) { return selector_set(net, margin); }
+
+int blco_select(blco_tensor* t, int mode, int rank, int factor_dtype, blco_mlp* net, float margin,
+                const blco_opts* opts, int* config, int* used_sweep)
+{
+    if (!t || !config) return fail(BLCO_ERR_INVALID, "null argument");
+    if (!t->resident) return fail(BLCO_ERR_UNSUPPORTED, "schedule selection needs a resident tensor");
+    if (mode < 0 || mode >= t->layout.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
+    BLCO_CUDA(cudaSetDevice(t->device));
+    int swept = 0;
+    BLCO_TRY(select_config(t, mode, rank, factor_dtype, net, margin, pick_stream(t, opts), config, &swept));
+    if (used_sweep) *used_sweep = swept;
+    return BLCO_OK;
+}
+
+int blco_batch_last_ms(const blco_batch* b, double* ms)
+{
+    if (!b || !ms) return fail(BLCO_ERR_INVALID, "null argument");
+    *ms = batch_last_ms(b);
+    return BLCO_OK;
+}
 
 } // extern "C"

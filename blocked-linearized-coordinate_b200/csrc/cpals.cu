@@ -549,6 +549,7 @@ struct blco_cpals_plan {
     void* Ub[BLCO_MAX_MODES] = {};    // BF16 gather copies (BF16 gathers only)
     float* Mf = nullptr;              // MTTKRP result (FP32)
     const float* vals32 = nullptr;
+    blco::MttkrpArgs sched[BLCO_MAX_MODES] = {}; // per-mode schedule (kernel, hot_chunk, interleave)
     double* grams[BLCO_MAX_MODES] = {};
     double* P = nullptr;
     double* partials = nullptr; // max(grid) * R * R
@@ -658,7 +659,9 @@ int mode_update(blco_cpals_plan* p, int n)
     a.nnz = t->nnz;
     a.mode = n;
     a.rank = R;
-    a.kernel = p->opts.kernel;
+    a.kernel = p->sched[n].kernel;
+    a.hot_chunk = p->sched[n].hot_chunk;
+    a.interleave = p->sched[n].interleave;
     a.thread_cf = p->opts.thread_cf;
     if (p->mixed) {
         BLCO_CUDA(cudaMemsetAsync(p->Mf, 0, I * R * sizeof(float), p->s));
@@ -806,6 +809,11 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
         }
         if (st != BLCO_OK) { plan_free(p); return st; }
     }
+    // Per-mode MTTKRP schedules, resolved once (kernels 20 and 21 may time
+    // the autotuner's sweep here).
+    for (int n = 0; n < p->N && st == BLCO_OK; n++)
+        st = resolve_schedule(t, n, R, p->gather_dtype, p->opts.kernel, p->s, &p->sched[n]);
+    if (st != BLCO_OK) { plan_free(p); return st; }
     // Descending mode length, ties in natural order (src/cpd_gpu.cu:137-139).
     for (int n = 0; n < p->N; n++) p->order[n] = n;
     std::stable_sort(p->order, p->order + p->N,
@@ -992,9 +1000,10 @@ __global__ void k_b_zero(BDesc* __restrict__ d, int T, int slot)
 // Chunks are dealt round-robin to the warps of the whole grid, which keeps
 // the warps on neighbouring chunks (a few tensors at a time) and their
 // factor rows in L2.
-constexpr int BM_CHUNK = 1024;
+constexpr int BM_CHUNK = 256;
 constexpr int BM_THREADS = 512;
 constexpr int BM_WARPS = BM_THREADS / 32;
+constexpr int BM_MINB = 1; // resident CTAs per SM
 
 // VEC: 2 gathers two adjacent FP64 columns per lane (even rank, 16-byte
 // aligned rows), 1 one column in each of two 32-column blocks.  NMO: the
@@ -1005,7 +1014,7 @@ template <int VEC, int NMO>
 __device__ __forceinline__ void b_chunk(const BDesc& b, int n, uint64_t j0, uint64_t j1, int lane, int lpn)
 {
     constexpr int KMAX = NMO > 0 ? NMO : 4;
-    constexpr int U = NMO == 2 ? 4 : 2;
+    constexpr int U = NMO == 2 ? 4 : 2; // positions per gather batch; must not exceed the smallest lpn (4)
     constexpr int W = VEC == 2 ? 1 : 2;
     constexpr int NC = W * VEC;
     const int nmo = NMO >= 0 ? NMO : b.nmodes - 1;
@@ -1045,11 +1054,24 @@ __device__ __forceinline__ void b_chunk(const BDesc& b, int n, uint64_t j0, uint
                 if (c + j < R) atomicAdd(o + c + j, acc[w * VEC + j]);
         }
     };
+    // the next step's coordinate and value are loaded one step ahead
+    uint64_t c_next = 0;
+    double v_next = 0.0;
+    if (gb + q < ge) {
+        c_next = __ldcs(sc + gb + q);
+        v_next = __ldcs(sv + gb + q);
+    }
     for (int st = 0; st < nsteps; st++) {
         const uint64_t jj = gb + (uint64_t)st * lpn + q;
         const bool valid = jj < ge;
-        const uint64_t c = valid ? __ldcs(sc + jj) : 0ull;
-        const double v = valid ? __ldcs(sv + jj) : 0.0;
+        const uint64_t c = c_next;
+        const double v = v_next;
+        c_next = 0;
+        v_next = 0.0;
+        if (st + 1 < nsteps && jj + lpn < ge) {
+            c_next = __ldcs(sc + jj + lpn);
+            v_next = __ldcs(sv + jj + lpn);
+        }
         const uint32_t row = valid ? (uint32_t)((c >> rpos) & rmask) : 0xffffffffu;
         uint32_t oth[KMAX];
 #pragma unroll
@@ -1108,7 +1130,7 @@ __device__ __forceinline__ void b_chunk(const BDesc& b, int n, uint64_t j0, uint
     if (acc_row != 0xffffffffu) flush();
 }
 
-__global__ void __launch_bounds__(BM_THREADS, 1) k_b_mttkrp(const BDesc* __restrict__ d, int T,
+__global__ void __launch_bounds__(BM_THREADS, BM_MINB) k_b_mttkrp(const BDesc* __restrict__ d, int T,
                                                            const uint32_t* __restrict__ choff, int slot)
 {
     __shared__ uint32_t toff[BATCH_MAX_T + 1];
@@ -1149,45 +1171,96 @@ __global__ __launch_bounds__(DN_THREADS) void k_b_solve(BDesc* __restrict__ d, i
     solve_body(gp, b.nmodes, b.order[slot], b.rank, b.P, dummy);
 }
 
-// One CTA per row chunk: U = M P^T in FP64 (a warp per row, lane per
-// column pair) and the chunk's column sums of squares.
+// Register tiling shared by the batched update and Gram kernels: columns
+// go in groups of 4 (cg = ceil(R / 4) groups, at most 16), and the 256
+// threads of a CTA form (256 / cg) x cg; a block of rows staged in shared
+// memory holds BT_ELEMS doubles.
+constexpr int BT_ELEMS = 4096;
+constexpr size_t BU_SMEM = (BATCH_MAX_R * BATCH_MAX_R + BT_ELEMS) * sizeof(double);
+
+// One CTA per row chunk: U = M P^T in FP64, thread (rg, cg) computing rows
+// 4*rg .. 4*rg+3 of each staged block and columns 4*cg .. 4*cg+3 (the sum
+// over k runs in order, as in the single-tensor update).  Also the chunk's
+// column sums of U^2 (for lambda) and of U .* M (for <X, model> when this is
+// the tensor's last mode).
 __global__ __launch_bounds__(DN_THREADS) void k_b_update(BDesc* __restrict__ d, const uint32_t* __restrict__ ct,
                                                          const uint32_t* __restrict__ cr0,
                                                          const uint32_t* __restrict__ cr1, int slot,
-                                                         double* __restrict__ colsq)
+                                                         double* __restrict__ colsq, double* __restrict__ ippart)
 {
-    __shared__ double PT[BATCH_MAX_R * BATCH_MAX_R];
-    __shared__ double csq[DN_THREADS / 32][BATCH_MAX_R];
+    extern __shared__ __align__(16) double bus[];
+    double* PT = bus;                          // R x R, transposed
+    double* Ms = bus + BATCH_MAX_R * BATCH_MAX_R; // staged rows of M
+    double* red = Ms;                          // [2][threads * 4], after the row loop
     const int chunk = blockIdx.x, t = ct[chunk];
     const BDesc& b = d[t];
-    if (!b.active || slot >= b.nmodes) return;
-    const int R = b.rank, n = b.order[slot];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (!b.active || slot >= b.nmodes) return; // block-uniform
+    const int R = b.rank, n = b.order[slot], tid = threadIdx.x;
+    const int cgs = (R + 3) / 4, rgs = DN_THREADS / cgs;
+    const int cg = tid % cgs, rg = tid / cgs;
+    const int c0 = cg * 4;
+    const int rows_blk = (BT_ELEMS / R) / 4 * 4 < rgs * 4 ? (BT_ELEMS / R) / 4 * 4 : rgs * 4;
     for (int k = tid; k < R * R; k += DN_THREADS) PT[(k % R) * R + k / R] = b.P[k];
-    for (int k = tid; k < (DN_THREADS / 32) * BATCH_MAX_R; k += DN_THREADS) (&csq[0][0])[k] = 0.0;
-    __syncthreads();
-    double sq0 = 0.0, sq1 = 0.0;
-    const int c0 = lane, c1 = lane + 32;
-    for (uint32_t r = cr0[chunk] + warp; r < cr1[chunk]; r += DN_THREADS / 32) {
-        const double* mrow = b.M + (size_t)r * R;
-        const double m0 = c0 < R ? mrow[c0] : 0.0, m1 = c1 < R ? mrow[c1] : 0.0;
-        double a0 = 0.0, a1 = 0.0;
-        for (int kk = 0; kk < R; kk++) {
-            const double mk = __shfl_sync(0xffffffffu, kk < 32 ? m0 : m1, kk & 31);
-            if (c0 < R) a0 += mk * PT[kk * R + c0];
-            if (c1 < R) a1 += mk * PT[kk * R + c1];
+    double sq[4] = {0.0, 0.0, 0.0, 0.0}, ip[4] = {0.0, 0.0, 0.0, 0.0};
+    const double* __restrict__ M = b.M;
+    double* __restrict__ Un = b.U[n];
+    for (uint32_t r0 = cr0[chunk]; r0 < cr1[chunk]; r0 += rows_blk) {
+        const int nr = (int)min((uint32_t)rows_blk, cr1[chunk] - r0);
+        __syncthreads();
+        for (int k = tid; k < nr * R; k += DN_THREADS) Ms[k] = M[(size_t)r0 * R + k];
+        __syncthreads();
+        if (rg < rows_blk / 4 && cg < cgs) {
+#pragma unroll 1
+            for (int rr = 4 * rg; rr < nr; rr += 4 * rgs) {
+                double acc[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+                for (int k = 0; k < R; k++) {
+                    double m[4], p[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) m[i] = rr + i < nr ? Ms[(rr + i) * R + k] : 0.0;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) p[j] = c0 + j < R ? PT[k * R + c0 + j] : 0.0;
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) acc[i][j] += m[i] * p[j];
+                }
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (rr + i >= nr) break;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const int c = c0 + j;
+                        if (c < R) {
+                            const double u = acc[i][j];
+                            Un[(size_t)(r0 + rr + i) * R + c] = u;
+                            sq[j] += u * u;
+                            ip[j] += u * Ms[(rr + i) * R + c];
+                        }
+                    }
+                }
+            }
         }
-        double* urow = b.U[n] + (size_t)r * R;
-        if (c0 < R) { urow[c0] = a0; sq0 += a0 * a0; }
-        if (c1 < R) { urow[c1] = a1; sq1 += a1 * a1; }
     }
-    if (c0 < R) csq[warp][c0] = sq0;
-    if (c1 < R) csq[warp][c1] = sq1;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        red[tid * 4 + j] = sq[j];
+        red[DN_THREADS * 4 + tid * 4 + j] = ip[j];
+    }
     __syncthreads();
     for (int c = tid; c < R; c += DN_THREADS) {
-        double s = 0.0;
-        for (int w = 0; w < DN_THREADS / 32; w++) s += csq[w][c];
-        colsq[(size_t)chunk * BATCH_MAX_R + c] = s;
+        double s0 = 0.0, s1 = 0.0;
+        const int g = c / 4, j = c % 4;
+        for (int r = 0; r < rgs; r++) {
+            s0 += red[(r * cgs + g) * 4 + j];
+            s1 += red[DN_THREADS * 4 + (r * cgs + g) * 4 + j];
+        }
+        colsq[(size_t)chunk * BATCH_MAX_R + c] = s0;
+        ippart[(size_t)chunk * BATCH_MAX_R + c] = s1;
     }
 }
 
@@ -1205,49 +1278,69 @@ __global__ void k_b_lambda(BDesc* __restrict__ d, const uint32_t* __restrict__ c
     }
 }
 
-// One CTA per row chunk: optionally scale the rows by inv, then the chunk's
-// Gram (R x R) partial; thread (a, b) pairs strided over R*R.
+// One CTA per row chunk: optionally scale the rows by inv (written back),
+// then the chunk's Gram partial.  Thread (ag, cg) of the 4 x 4 blocks of
+// the R x R Gram takes every `splits`-th row of each staged block; the
+// splits are summed in shared memory at the end.
 __global__ __launch_bounds__(DN_THREADS) void k_b_gram(BDesc* __restrict__ d, const uint32_t* __restrict__ ct,
                                                        const uint32_t* __restrict__ cr0,
                                                        const uint32_t* __restrict__ cr1, int slot, int scale,
                                                        double* __restrict__ gpart)
 {
-    __shared__ double tile[32][BATCH_MAX_R + 1];
+    __shared__ double tile[BT_ELEMS];
+    double* red = tile; // [threads * 16], after the row loop
     const int chunk = blockIdx.x, t = ct[chunk];
     const BDesc& b = d[t];
-    if ((scale && !b.active) || slot >= b.nmodes) return;
+    if ((scale && !b.active) || slot >= b.nmodes) return; // block-uniform
     const int R = b.rank, n = b.order[slot], tid = threadIdx.x;
-    double acc[16];
+    const int cgs = (R + 3) / 4, nblk = cgs * cgs, splits = DN_THREADS / nblk;
+    const int blk = tid % nblk, sp = tid / nblk;
+    const int a0 = (blk / cgs) * 4, c0 = (blk % cgs) * 4;
+    const int rows_blk = BT_ELEMS / R;
+    double acc[4][4];
 #pragma unroll
-    for (int j = 0; j < 16; j++) acc[j] = 0.0;
-    const uint32_t r_beg = cr0[chunk], r_end = cr1[chunk];
-    for (uint32_t r0 = r_beg; r0 < r_end; r0 += 32) {
-        const int nr = (int)min(32u, r_end - r0);
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+    double* __restrict__ Un = b.U[n];
+    for (uint32_t r0 = cr0[chunk]; r0 < cr1[chunk]; r0 += rows_blk) {
+        const int nr = (int)min((uint32_t)rows_blk, cr1[chunk] - r0);
         __syncthreads();
         for (int k = tid; k < nr * R; k += DN_THREADS) {
-            double v = b.U[n][(size_t)r0 * R + k];
+            double v = Un[(size_t)r0 * R + k];
             if (scale) {
                 v *= b.inv[k % R];
-                b.U[n][(size_t)r0 * R + k] = v;
+                Un[(size_t)r0 * R + k] = v;
             }
-            tile[k / R][k % R] = v;
+            tile[k] = v;
         }
         __syncthreads();
+        if (sp < splits) {
+            for (int r = sp; r < nr; r += splits) {
+                double x[4], y[4];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-            const int e = tid + j * DN_THREADS;
-            if (e < R * R) {
-                const int a = e / R, c = e % R;
-                double s = 0.0;
-                for (int r = 0; r < nr; r++) s += tile[r][a] * tile[r][c];
-                acc[j] += s;
+                for (int i = 0; i < 4; i++) x[i] = a0 + i < R ? tile[r * R + a0 + i] : 0.0;
+#pragma unroll
+                for (int j = 0; j < 4; j++) y[j] = c0 + j < R ? tile[r * R + c0 + j] : 0.0;
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) acc[i][j] += x[i] * y[j];
             }
         }
     }
+    __syncthreads();
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-        const int e = tid + j * DN_THREADS;
-        if (e < R * R) gpart[(size_t)chunk * BATCH_MAX_R * BATCH_MAX_R + e] = acc[j];
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) red[tid * 16 + i * 4 + j] = acc[i][j];
+    __syncthreads();
+    for (int e = tid; e < R * R; e += DN_THREADS) {
+        const int a = e / R, c = e % R;
+        const int bk = (a / 4) * cgs + c / 4, ij = (a % 4) * 4 + c % 4;
+        double s = 0.0;
+        for (int q = 0; q < splits; q++) s += red[(q * nblk + bk) * 16 + ij];
+        gpart[(size_t)chunk * BATCH_MAX_R * BATCH_MAX_R + e] = s;
     }
 }
 
@@ -1266,10 +1359,18 @@ __global__ void k_b_gram_reduce(BDesc* __restrict__ d, const uint32_t* __restric
     }
 }
 
-// Per tensor: <X, A> from the last mode's factor and MTTKRP, the fit
-// (kruskal_fit_gpu, src/cpd_gpu.cu:331-384) and the convergence test.
+struct SlotChunks {
+    const uint32_t* beg[BLCO_MAX_MODES];
+    const uint32_t* end[BLCO_MAX_MODES];
+    const double* ip[BLCO_MAX_MODES];
+};
+
+// Per tensor: <X, model> from the last mode's chunk sums of U .* M (taken
+// before U was scaled, so each column sum is multiplied by inv * lambda),
+// the fit (kruskal_fit_gpu, src/cpd_gpu.cu:331-384) and the convergence
+// test.
 __global__ __launch_bounds__(DN_THREADS) void k_b_fit(BDesc* __restrict__ d, int T, const int* __restrict__ iter,
-                                                      double tol, double* __restrict__ fits)
+                                                      double tol, SlotChunks sc, double* __restrict__ fits)
 {
     __shared__ double red[DN_THREADS];
     BDesc& b = d[blockIdx.x];
@@ -1277,10 +1378,14 @@ __global__ __launch_bounds__(DN_THREADS) void k_b_fit(BDesc* __restrict__ d, int
         if (threadIdx.x == 0) fits[(size_t)(*iter % BATCH_FIT_RING) * T + blockIdx.x] = b.fit_old;
         return;
     }
-    const int R = b.rank, lm = b.order[b.nmodes - 1];
-    const uint64_t len = b.dims[lm] * (uint64_t)R;
+    const int R = b.rank, last = b.nmodes - 1;
     double ip = 0.0;
-    for (uint64_t i = threadIdx.x; i < len; i += DN_THREADS) ip += b.U[lm][i] * b.M[i] * b.lambda[i % R];
+    for (int c = threadIdx.x; c < R; c += DN_THREADS) {
+        double s = 0.0;
+        for (uint32_t k = sc.beg[last][blockIdx.x]; k < sc.end[last][blockIdx.x]; k++)
+            s += sc.ip[last][(size_t)k * BATCH_MAX_R + c];
+        ip += s * (b.inv[c] * b.lambda[c]);
+    }
     const double iprod = block_sum(ip, red);
     GramPtrs gp;
     for (int m = 0; m < BLCO_MAX_MODES; m++) gp.g[m] = b.G[m];
@@ -1313,6 +1418,8 @@ struct blco_batch {
     uint32_t* d_cend[BLCO_MAX_MODES] = {};
     int nchunks[BLCO_MAX_MODES] = {};
     double* d_colsq = nullptr;
+    double* d_ippart = nullptr;        // per mode slot: maxchunks x 64
+    size_t maxchunks = 1;
     double* d_gpart = nullptr;
     double* d_fits = nullptr;
     int* d_iter = nullptr;
@@ -1323,6 +1430,8 @@ struct blco_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     long long graph_kernels = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    double last_ms = 0.0;              // device time of the last iterate call
     double tol = 0.0;
     int iters_run = 0;
 };
@@ -1347,11 +1456,14 @@ int batch_free(blco_batch* b)
     cudaFree(b->d_choff);
     cudaFree(b->streams);
     cudaFree(b->d_colsq);
+    cudaFree(b->d_ippart);
     cudaFree(b->d_gpart);
     cudaFree(b->d_fits);
     cudaFree(b->d_iter);
     cudaFree(b->d_dummy);
     cudaFree(b->pool);
+    for (cudaEvent_t e : b->ev)
+        if (e) cudaEventDestroy(e);
     if (b->s) cudaStreamDestroy(b->s);
     delete b;
     return BLCO_OK;
@@ -1365,15 +1477,17 @@ int batch_enqueue_sweep(blco_batch* b)
         k_b_zero<<<b->T * 8, 256, 0, b->s>>>(b->d_desc, b->T, k);
         BLCO_CHECK_LAUNCH("k_b_zero");
         if (b->mt_chunks[k]) {
-            const unsigned grid = (unsigned)std::min<uint64_t>(b->sm, (b->mt_chunks[k] + BM_WARPS - 1) / BM_WARPS);
+            const unsigned grid =
+                (unsigned)std::min<uint64_t>((uint64_t)b->sm * BM_MINB, (b->mt_chunks[k] + BM_WARPS - 1) / BM_WARPS);
             k_b_mttkrp<<<grid, BM_THREADS, 0, b->s>>>(b->d_desc, b->T, b->d_choff + (size_t)k * (b->T + 1), k);
             BLCO_CHECK_LAUNCH("k_b_mttkrp");
         }
         k_b_solve<<<b->T, DN_THREADS, ssmem, b->s>>>(b->d_desc, k, b->d_dummy);
         BLCO_CHECK_LAUNCH("k_b_solve");
         if (b->nchunks[k]) {
-            k_b_update<<<b->nchunks[k], DN_THREADS, 0, b->s>>>(b->d_desc, b->d_ct[k], b->d_cr0[k], b->d_cr1[k], k,
-                                                                b->d_colsq);
+            k_b_update<<<b->nchunks[k], DN_THREADS, BU_SMEM, b->s>>>(b->d_desc, b->d_ct[k], b->d_cr0[k], b->d_cr1[k], k,
+                                                                b->d_colsq,
+                                                                b->d_ippart + (size_t)k * b->maxchunks * BATCH_MAX_R);
             BLCO_CHECK_LAUNCH("k_b_update");
         }
         k_b_lambda<<<b->T, 64, 0, b->s>>>(b->d_desc, b->d_cbeg[k], b->d_cend[k], k, b->d_colsq);
@@ -1386,7 +1500,14 @@ int batch_enqueue_sweep(blco_batch* b)
         k_b_gram_reduce<<<b->T, 256, 0, b->s>>>(b->d_desc, b->d_cbeg[k], b->d_cend[k], k, 1, b->d_gpart);
         BLCO_CHECK_LAUNCH("k_b_gram_reduce");
     }
-    k_b_fit<<<b->T, DN_THREADS, 0, b->s>>>(b->d_desc, b->T, b->d_iter, b->tol, b->d_fits);
+    SlotChunks sc;
+    memset(&sc, 0, sizeof(sc));
+    for (int k = 0; k < b->maxN; k++) {
+        sc.beg[k] = b->d_cbeg[k];
+        sc.end[k] = b->d_cend[k];
+        sc.ip[k] = b->d_ippart + (size_t)k * b->maxchunks * BATCH_MAX_R;
+    }
+    k_b_fit<<<b->T, DN_THREADS, 0, b->s>>>(b->d_desc, b->T, b->d_iter, b->tol, sc, b->d_fits);
     BLCO_CHECK_LAUNCH("k_b_fit");
     k_b_next<<<1, 1, 0, b->s>>>(b->d_iter);
     BLCO_CHECK_LAUNCH("k_b_next");
@@ -1435,6 +1556,8 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
         return st;
     };
     cudaError_t e = cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev[1]);
     if (e == cudaSuccess) e = cudaMalloc(&b->pool, pool_doubles * sizeof(double));
     if (e != cudaSuccess) return bail(cuda_fail(e, "batch workspace", __FILE__, __LINE__));
     double* cur = static_cast<double*>(b->pool);
@@ -1562,7 +1685,9 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
         if (e != cudaSuccess) return bail(cuda_fail(e, "batch chunk tables", __FILE__, __LINE__));
     }
     const size_t mc = std::max(1, maxchunks);
+    b->maxchunks = mc;
     e = cudaMalloc(&b->d_colsq, mc * BATCH_MAX_R * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_ippart, (size_t)b->maxN * mc * BATCH_MAX_R * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_gpart, mc * BATCH_MAX_R * BATCH_MAX_R * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_fits, (size_t)BATCH_FIT_RING * T * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_iter, sizeof(int));
@@ -1574,6 +1699,7 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
     if (e != cudaSuccess) return bail(cuda_fail(e, "batch buffers", __FILE__, __LINE__));
     e = cudaFuncSetAttribute(k_b_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(2 * (size_t)b->maxR * b->maxR * sizeof(double)));
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_b_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BU_SMEM);
     if (e != cudaSuccess) return bail(cuda_fail(e, "k_b_solve shared memory", __FILE__, __LINE__));
     // initial Grams of every mode (unscaled)
     for (int k = 0; k < b->maxN; k++) {
@@ -1616,6 +1742,7 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
 int batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done)
 {
     if (iters < 0 || iters > BATCH_FIT_RING) return fail(BLCO_ERR_INVALID, "iterations per call must be 0..4096");
+    BLCO_CUDA(cudaEventRecord(b->ev[0], b->s));
     for (int i = 0; i < iters; i++) {
         if (b->exec) {
             BLCO_CUDA(cudaGraphLaunch(b->exec, b->s));
@@ -1624,7 +1751,11 @@ int batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done)
             BLCO_TRY(batch_enqueue_sweep(b));
         }
     }
+    BLCO_CUDA(cudaEventRecord(b->ev[1], b->s));
     BLCO_CUDA(cudaStreamSynchronize(b->s));
+    float ms = 0.f;
+    BLCO_CUDA(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+    b->last_ms = ms;
     const int first = b->iters_run;
     b->iters_run += iters;
     BLCO_CUDA(cudaMemcpy(b->h_desc.data(), b->d_desc, b->T * sizeof(BDesc), cudaMemcpyDeviceToHost));
@@ -1643,5 +1774,7 @@ int batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done)
 }
 
 int batch_destroy(blco_batch* b) { return batch_free(b); }
+
+double batch_last_ms(const blco_batch* b) { return b->last_ms; }
 
 } // namespace blco

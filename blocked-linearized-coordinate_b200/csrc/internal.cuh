@@ -50,6 +50,7 @@ struct DeviceInfo {
     int device = 0;
     int sm_count = 148;
     size_t smem_optin = 227 * 1024;
+    size_t l2_bytes = 126ull << 20;
 };
 int device_info(int device, DeviceInfo* out);
 
@@ -97,6 +98,21 @@ struct HotTable {
     float* d_cvals32 = nullptr; // mixed form, made on first use
 };
 
+// One MTTKRP schedule of the autotuner's space.
+struct TuneCfg {
+    int kernel;     // BLCO_KERNEL_LVL1 / LVL2 / LVL3 / ATOMIC
+    int hot_chunk;  // LVL2: positions per warp task of the heavy-row kernel
+    int interleave; // tile kernel: round-robin tile order
+};
+extern const TuneCfg TUNE_SPACE[BLCO_TUNE_CONFIGS];
+
+// Autotuner timings of one (mode, factor dtype) of a tensor.
+struct TuneCache {
+    bool valid = false;
+    int rank = 0;
+    float ms[BLCO_TUNE_CONFIGS] = {}; // -1: schedule not valid here
+};
+
 struct ModeStats {
     uint64_t max_row_nnz = 0;
     uint64_t nonempty_rows = 0;
@@ -107,6 +123,7 @@ struct ModeStats {
 
 struct blco_cpals_plan;
 struct blco_batch;
+struct blco_mlp;
 
 struct blco_tensor {
     blco::Layout layout;
@@ -126,6 +143,7 @@ struct blco_tensor {
     blco::HotTable hot[BLCO_MAX_MODES];
     blco::ModeStats stats[BLCO_MAX_MODES];
     double norm_sq = 0.0; // sum of squared values
+    blco::TuneCache tune[BLCO_MAX_MODES][3];
 };
 
 namespace blco {
@@ -157,9 +175,14 @@ struct MttkrpArgs {
     int factor_dtype;
     int kernel;
     int thread_cf;
+    int hot_chunk;  // positions per warp task of the heavy-row kernel (0: 512)
+    int interleave; // tile kernel: 1 deals tiles round-robin to the grid's warps
 };
 int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested, int factor_dtype);
+// Automatic rule: the heavy-row path needs at least this many heavy nonzeros.
+constexpr uint64_t AUTO_HOT_MIN_NNZ = 1ull << 18;
+uint32_t auto_hot_chunk(uint64_t hot_nnz);
 // FP32 copy of the resident values (created on first use).
 int values_f32(blco_tensor* t, cudaStream_t s, const float** out);
 
@@ -174,7 +197,28 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
                  double* const* d_lambdas, double tol, const blco_opts* opts, blco_batch** out);
 int batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done);
 int batch_destroy(blco_batch* b);
+double batch_last_ms(const blco_batch* b);
 int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda, int maxiter,
                double tol, const blco_opts* opts, double* fit_out, double* fits, int* iters_out);
+
+// tune.cu
+int tune_features(const blco_tensor* t, int mode, int rank, int dtype, float* f);
+int tune_sweep(blco_tensor* t, int mode, int rank, int dtype, int reps, cudaStream_t s, float* ms_out);
+int tune_best(const float* ms);
+int mlp_create(int hidden, uint64_t seed, int device, blco_mlp** out);
+int mlp_set_params(blco_mlp* m, const float* params, int n);
+int mlp_get_params(const blco_mlp* m, float* params, int n);
+int mlp_num_params(const blco_mlp* m);
+int mlp_predict(blco_mlp* m, const float* X, int n, float* out);
+int mlp_grad(blco_mlp* m, const float* X, const float* Y, const float* Mk, int n, float* grad, float* loss);
+int mlp_train(blco_mlp* m, const float* X, const float* Y, const float* Mk, int n, int epochs, int batch, float lr,
+              uint64_t seed, float* loss_out);
+int mlp_destroy(blco_mlp* m);
+int selector_set(blco_mlp* net, float margin);
+int select_config(blco_tensor* t, int mode, int rank, int dtype, blco_mlp* net, float margin, cudaStream_t s,
+                  int* cfg, int* used_sweep);
+// Fills a->kernel / hot_chunk / interleave for the requested kernel id
+// (BLCO_KERNEL_TUNED and BLCO_KERNEL_LEARNED resolve to a schedule).
+int resolve_schedule(blco_tensor* t, int mode, int rank, int dtype, int requested, cudaStream_t s, MttkrpArgs* a);
 
 } // namespace blco

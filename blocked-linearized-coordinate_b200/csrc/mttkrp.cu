@@ -89,7 +89,7 @@ struct MtParams {
     int direct;                // 1: every row of the target mode is a slot (slot = row)
     int nacc;                  // rows held in the shared accumulator
     int merge;                 // 0: flush every nonzero on its own (kernel 13)
-    int skip_hot;              // 1: nonzeros of table rows are left to k_mttkrp_hot
+    int interleave;            // 1: tiles dealt round-robin to the grid's warps; 0: a contiguous range per CTA
     uint64_t tiles_per_cta;
 };
 
@@ -230,9 +230,8 @@ __device__ __forceinline__ int stage_tile(const MtParams& p, const ModeSel<NM>& 
 #pragma unroll
     for (int k = 0; k < NM - 1; k++) ro[k] = (uint32_t)((c >> ms.opos[k]) & ms.omask[k]);
     int slot = valid ? hot_lookup(p, skeys, sslot, rt) : -1;
-    // Entries that take no part (past the end, or hot rows handled by the
-    // CSR kernel) are ordered after the working ones.
-    const bool work = valid && !(p.skip_hot && slot >= 0);
+    // Entries past the end are ordered after the working ones.
+    const bool work = valid;
     const uint32_t wmask = __ballot_sync(0xffffffffu, work);
     uint32_t key = work ? rt : 0xffffffffu;
     uint32_t peers = __match_any_sync(0xffffffffu, key);
@@ -346,11 +345,12 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_vec(MtParams p)
     const int slot = lane / LPN, q = lane % LPN;
     unsigned char* st = stages + (size_t)warp * STAGE;
     const uint64_t ntiles = (p.nnz + 31) / 32;
-    const uint64_t t_beg = (uint64_t)blockIdx.x * p.tiles_per_cta;
-    const uint64_t t_end = min(ntiles, t_beg + p.tiles_per_cta);
+    const uint64_t t_beg = p.interleave ? (uint64_t)blockIdx.x * MT_WARPS : (uint64_t)blockIdx.x * p.tiles_per_cta;
+    const uint64_t t_end = p.interleave ? ntiles : min(ntiles, t_beg + p.tiles_per_cta);
+    const uint64_t t_step = p.interleave ? (uint64_t)gridDim.x * MT_WARPS : (uint64_t)MT_WARPS;
     const ModeSel<NM> ms(p);
 
-    for (uint64_t tile = t_beg + warp; tile < t_end; tile += MT_WARPS) {
+    for (uint64_t tile = t_beg + warp; tile < t_end; tile += t_step) {
         uint32_t ends;
         const int count = stage_tile<NM, PER, TV>(p, ms, skeys, sslot, tile * 32, st, ends);
         if (!p.merge) ends = 0xffffffffu;
@@ -582,11 +582,12 @@ __global__ void __launch_bounds__(MT_THREADS, 1) k_mttkrp_gen(MtParams p)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* st = stages + (size_t)warp * STAGE;
     const uint64_t ntiles = (p.nnz + 31) / 32;
-    const uint64_t t_beg = (uint64_t)blockIdx.x * p.tiles_per_cta;
-    const uint64_t t_end = min(ntiles, t_beg + p.tiles_per_cta);
+    const uint64_t t_beg = p.interleave ? (uint64_t)blockIdx.x * MT_WARPS : (uint64_t)blockIdx.x * p.tiles_per_cta;
+    const uint64_t t_end = p.interleave ? ntiles : min(ntiles, t_beg + p.tiles_per_cta);
+    const uint64_t t_step = p.interleave ? (uint64_t)gridDim.x * MT_WARPS : (uint64_t)MT_WARPS;
     const ModeSel<NM> ms(p);
     const int ncol = (R + 31) / 32;
-    for (uint64_t tile = t_beg + warp; tile < t_end; tile += MT_WARPS) {
+    for (uint64_t tile = t_beg + warp; tile < t_end; tile += t_step) {
         uint32_t ends;
         const int count = stage_tile<NM, PER, TV>(p, ms, skeys, sslot, tile * 32, st, ends);
         if (!p.merge) ends = 0xffffffffu;
@@ -744,9 +745,15 @@ int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested
     case BLCO_KERNEL_ATOMIC: return BLCO_KERNEL_ATOMIC;
     default:
         if (fits_direct) return BLCO_KERNEL_LVL3;
-        return t->hot[mode].nhot > 0 ? BLCO_KERNEL_LVL2 : BLCO_KERNEL_LVL1;
+        return t->hot[mode].nhot > 0 && t->hot[mode].hot_nnz >= AUTO_HOT_MIN_NNZ ? BLCO_KERNEL_LVL2
+                                                                                : BLCO_KERNEL_LVL1;
     }
 }
+
+// Heavy-row chunk of the automatic rule: few heavy nonzeros need small
+// chunks to give every warp of the grid work (128 below 1M, 512 below 8M,
+// else 2048, from autotuner sweeps over skewed tensors of 1e5..2e8 nnz).
+uint32_t auto_hot_chunk(uint64_t hot_nnz) { return hot_nnz < (1u << 20) ? 128u : hot_nnz < (8u << 20) ? 512u : 2048u; }
 
 int values_f32(blco_tensor* t, cudaStream_t s, const float** out)
 {
@@ -783,8 +790,12 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     p.mode = a.mode;
     p.rank = a.rank;
     p.merge = 1;
+    p.interleave = a.interleave;
     const size_t accb = acc_elem_bytes(a.factor_dtype);
     const int kern = mttkrp_select_kernel(t, a.mode, a.rank, a.kernel, a.factor_dtype);
+    // the automatic rule deals the cold tiles round-robin when heavy rows
+    // are split off (a few percent faster in sweeps)
+    if (a.kernel == BLCO_KERNEL_AUTO && kern == BLCO_KERNEL_LVL2) p.interleave = 1;
     const size_t stage = stage_bytes(a.rank, policy_vec(a.factor_dtype));
     const HotTable& ht = t->hot[a.mode];
     // The vectorised kernels load 16 bytes at a time: every factor must start
@@ -833,7 +844,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     } else if (kern == BLCO_KERNEL_ATOMIC) {
         p.merge = 0;
     }
-    const size_t nacc = p.direct ? (size_t)L.dims[a.mode] : p.skip_hot ? 0 : (size_t)p.nhot;
+    const size_t nacc = p.direct ? (size_t)L.dims[a.mode] : (size_t)p.nhot;
     p.nacc = (int)nacc;
     const size_t smem = hash_bytes + nacc * a.rank * accb + stage + 16;
     if (smem > di.smem_optin) return fail(BLCO_ERR_UNSUPPORTED, "MTTKRP shared memory plan exceeds the device limit");
@@ -845,7 +856,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
         h.rows = ht.d_rows;
         h.nhot = ht.nhot;
         h.total = (uint32_t)ht.hot_nnz;
-        h.chunk = 2048;
+        h.chunk = a.hot_chunk > 0 ? (uint32_t)a.hot_chunk : auto_hot_chunk(ht.hot_nnz);
         h.acc = nullptr;
         if (a.factor_dtype == BLCO_DTYPE_F64) {
             h.vals = ht.d_hvals;

@@ -48,10 +48,20 @@ typedef enum blco_status {
  *   1  register/segmented conflict resolution (lvl1)
  *   2  lvl1 + shared-memory privatisation of heavy output rows (lvl2 role)
  *   3  shared-memory partial output matrix, for short modes (lvl3 role)
- *   10 automatic selection (the reference heuristic: 3 if the mode has at
- *      most 100 rows, else 1; replaced by the selector when one is loaded)
+ *   10 automatic selection: 3 when the mode's output fits in shared
+ *      memory, else 2 when the mode has at least 2^18 nonzeros in heavy
+ *      rows (heavy-row chunk 128 / 512 / 2048 below 2^20 / below 2^23 /
+ *      above, cold tiles round-robin), else 1 (the reference's rule,
+ *      src/alto_dev.cu:1975,1996-2001, is 3 for at most 100 rows, else 1)
  *   11, 12 one launch over all blocks (always the case here; mapped to 1)
- *   13 one atomic per (nonzero, column)                                  */
+ *   13 one atomic per (nonzero, column)
+ *   20 tuned: the fastest schedule of the autotuner's sweep on this tensor
+ *      and mode (swept on first use, then cached in the tensor)
+ *   21 learned: the schedule the selector network proposes (set with
+ *      blco_selector_set); the sweep when no network is set or when no
+ *      other schedule group is predicted slower by the margin (schedules
+ *      that differ only in tile order form a group)
+ * 20 and 21 are no reference flags; they apply to resident tensors.      */
 enum {
     BLCO_KERNEL_AUTO = 10,
     BLCO_KERNEL_LVL1 = 1,
@@ -59,8 +69,14 @@ enum {
     BLCO_KERNEL_LVL3 = 3,
     BLCO_KERNEL_BATCHED = 11,
     BLCO_KERNEL_BATCHED_V2 = 12,
-    BLCO_KERNEL_ATOMIC = 13
+    BLCO_KERNEL_ATOMIC = 13,
+    BLCO_KERNEL_TUNED = 20,
+    BLCO_KERNEL_LEARNED = 21
 };
+
+/* Schedules of the autotuner's space, and the selector network's inputs. */
+#define BLCO_TUNE_CONFIGS 12
+#define BLCO_MLP_FEATURES 25
 
 /* Numeric form. */
 enum {
@@ -263,6 +279,78 @@ int blco_batch_create(int count, blco_tensor* const* tensors, const int* ranks,
  * (may be NULL): per tensor, iterations executed since creation. */
 int blco_batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done);
 int blco_batch_destroy(blco_batch* b);
+/* Device time (CUDA events on the batch's stream) of the sweeps run by the
+ * last blco_batch_iterate call, in milliseconds. */
+int blco_batch_last_ms(const blco_batch* b, double* ms);
+
+/* ---- MTTKRP schedule selection (no counterpart in the reference, which
+ * has the fixed -k 10 rule, src/alto_dev.cu:1975,1996-2001). */
+
+/* One schedule: kernel id (1, 2, 3 or 13), heavy-row chunk (kernel 2: the
+ * positions of one warp task of the heavy-row kernel; 0 otherwise) and tile
+ * order (1: tiles dealt round-robin over the grid's warps, 0: a contiguous
+ * range of tiles per CTA). */
+typedef struct blco_tune_config {
+    int kernel;
+    int hot_chunk;
+    int interleave;
+} blco_tune_config;
+
+/* The BLCO_TUNE_CONFIGS schedules of the autotuner's space, in index order. */
+int blco_tune_space(blco_tune_config* configs);
+
+/* The exhaustive sweep: times every schedule (CUDA events, `reps` runs after
+ * one warm-up) for this tensor, mode, rank and factor dtype on synthetic
+ * factors.  ms[k] (BLCO_TUNE_CONFIGS entries, may be NULL): milliseconds
+ * per MTTKRP, -1 for schedules that do not apply (kernel 3 when the mode's
+ * output does not fit in shared memory).  best (may be NULL): index of the
+ * fastest.  The result is cached in the tensor (kernel id 20 uses it). */
+int blco_autotune(blco_tensor* t, int mode, int rank, int factor_dtype, int reps,
+                  const blco_opts* opts, float* ms, int* best);
+
+/* The selector's BLCO_MLP_FEATURES inputs for one mode: sizes (log2 nnz,
+ * order, rank, dtype, mode length, factor and output bytes, factor bytes
+ * over L2), row statistics of the mode (row occupancy, mean and longest
+ * fibre, heavy-row share and count, nonzero share by fibre-length bucket),
+ * whether kernel 3 applies, and the block count. */
+int blco_tune_features(const blco_tensor* t, int mode, int rank, int factor_dtype,
+                       float* features);
+
+/* The selector network: BLCO_MLP_FEATURES -> hidden (ReLU) -> hidden (ReLU)
+ * -> BLCO_TUNE_CONFIGS, FP32, trained and run by this library's kernels.
+ * Output k predicts log2(time of schedule k / time of the best schedule).
+ * Parameters (flat, in this order): W1[hidden][F] b1[hidden]
+ * W2[hidden][hidden] b2[hidden] W3[K][hidden] b3[K], row-major. */
+typedef struct blco_mlp blco_mlp;
+
+int blco_mlp_create(int hidden, uint64_t seed, int device, blco_mlp** out);
+int blco_mlp_num_params(const blco_mlp* net, int* n);
+int blco_mlp_set_params(blco_mlp* net, const float* params, int n);
+int blco_mlp_get_params(const blco_mlp* net, float* params, int n);
+/* X: n x F (host), out: n x K (host). */
+int blco_mlp_predict(blco_mlp* net, const float* X, int n, float* out);
+/* Loss (mean over the entries with mask 1 of (out - Y)^2) and its gradient
+ * with respect to the parameters (host array of num_params), for host
+ * arrays X (n x F), Y and mask (n x K). */
+int blco_mlp_grad(blco_mlp* net, const float* X, const float* Y, const float* mask, int n,
+                  float* grad, float* loss);
+/* Adam (0.9, 0.999, 1e-8) over shuffled mini-batches for `epochs` epochs;
+ * loss (may be NULL): the loss over all n rows afterwards. */
+int blco_mlp_train(blco_mlp* net, const float* X, const float* Y, const float* mask, int n,
+                   int epochs, int batch, float lr, uint64_t seed, float* loss);
+int blco_mlp_destroy(blco_mlp* net);
+
+/* The network kernel id 21 uses (NULL: none, the sweep decides), and the
+ * margin in predicted log2 time: when the best schedule's prediction is not
+ * below every other group's by the margin, the sweep runs instead.  The
+ * network must outlive its use. */
+int blco_selector_set(blco_mlp* net, float margin);
+
+/* The schedule index that kernel id 21 would use with this network and
+ * margin (net NULL: the sweep); used_sweep (may be NULL) is set to 1 when
+ * the sweep decided. */
+int blco_select(blco_tensor* t, int mode, int rank, int factor_dtype, blco_mlp* net,
+                float margin, const blco_opts* opts, int* config, int* used_sweep);
 
 /* Number of this library's kernels launched by the calling thread since the
  * last reset (for reporting launch counts). */
