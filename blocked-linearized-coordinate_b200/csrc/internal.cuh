@@ -91,7 +91,7 @@ struct HotTable {
     float* d_hvals32 = nullptr; // mixed form, made on first use
     double* d_acc = nullptr;    // mixed form: FP64 sums of the hot rows (nhot x acc_rank)
     int acc_rank = 0;
-    // The remaining (cold) nonzeros of this mode, in ALTO order.
+    // The remaining (cold) nonzeros of this mode, by row (ALTO order inside a row).
     uint64_t cold_nnz = 0;
     uint64_t* d_ccoords = nullptr;
     double* d_cvals = nullptr;
