@@ -60,7 +60,8 @@ EXPORTS = (
     "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_batch_create", "blco_batch_iterate",
     "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
     "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
-    "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_launch_count",
+    "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_gram_f32",
+    "blco_launch_count",
 )
 
 
@@ -81,6 +82,7 @@ class Opts(ctypes.Structure):
         ("device", ctypes.c_int),
         ("residency_bytes", ctypes.c_uint64),
         ("stream", ctypes.c_void_p),
+        ("gram_tensor_cores", ctypes.c_int),
     ]
 
 
@@ -149,6 +151,7 @@ def lib():
         L.blco_mlp_destroy.argtypes = [vp]
         L.blco_selector_set.argtypes = [vp, ctypes.c_float]
         L.blco_select.argtypes = [vp, i32, i32, i32, vp, ctypes.c_float, vp, vp, vp]
+        L.blco_gram_f32.argtypes = [vp, u64, i32, vp, i32, i32, vp]
         _lib = L
     return _lib
 
@@ -167,12 +170,13 @@ def launch_count(reset=False):
 
 
 def make_opts(kernel=KERNEL_AUTO, nprtn=0, thread_cf=2, stream_data=False, precision=PRECISION_FP64,
-              verbose=False, device=0, residency_bytes=0, stream=None):
+              verbose=False, device=0, residency_bytes=0, stream=None, gram_tensor_cores=False):
     o = Opts()
     lib().blco_opts_init(ctypes.byref(o))
     o.kernel, o.nprtn, o.thread_cf = kernel, nprtn, thread_cf
     o.stream_data, o.precision, o.verbose = int(stream_data), precision, int(verbose)
     o.device, o.residency_bytes = device, residency_bytes
+    o.gram_tensor_cores = int(gram_tensor_cores)
     if stream is None:
         try:
             import torch
@@ -511,3 +515,15 @@ def select(t, mode, rank, factor_dtype=DTYPE_F64, net=None, margin=0.1, opts=Non
     _check(lib().blco_select(t.handle, mode, rank, factor_dtype, net.handle if net is not None else None,
                              ctypes.c_float(margin), ctypes.byref(o), ctypes.byref(cfg), ctypes.byref(sw)))
     return cfg.value, bool(sw.value)
+
+
+def gram_f32(U, tensor_cores=True):
+    """G = U^T U (torch CUDA float64) for a torch CUDA float32 matrix U (I x R, R <= 64)."""
+    import torch
+    U = U.contiguous()
+    R = int(U.shape[1])
+    G = torch.empty(R, R, dtype=torch.float64, device=U.device)
+    stream = torch.cuda.current_stream(U.device).cuda_stream
+    _check(lib().blco_gram_f32(int(U.data_ptr()), int(U.shape[0]), R, int(G.data_ptr()), int(bool(tensor_cores)),
+                               U.device.index or 0, stream))
+    return G

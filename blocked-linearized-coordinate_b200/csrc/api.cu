@@ -535,6 +535,17 @@ int blco_select(blco_tensor* t, int mode, int rank, int factor_dtype, blco_mlp* 
     return BLCO_OK;
 }
 
+int blco_gram_f32(const float* d_U, uint64_t I, int rank, double* d_G, int tensor_cores, int device, void* stream)
+{
+    if (!d_U || !d_G) return fail(BLCO_ERR_INVALID, "null argument");
+    if (rank < 1 || rank > 64) return fail(BLCO_ERR_UNSUPPORTED, "rank must be 1..64");
+    BLCO_CUDA(cudaSetDevice(device));
+    DeviceInfo di;
+    BLCO_TRY(device_info(device, &di));
+    return gram_f32(const_cast<float*>(d_U), I, rank, d_G, tensor_cores != 0, di.sm_count,
+                    static_cast<cudaStream_t>(stream));
+}
+
 int blco_batch_last_ms(const blco_batch* b, double* ms)
 {
     if (!b || !ms) return fail(BLCO_ERR_INVALID, "null argument");

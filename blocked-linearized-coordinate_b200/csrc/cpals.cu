@@ -122,10 +122,16 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t
 // out[k] = sum_b partials[b][k], b ascending.
 __global__ void k_sum_partials(const double* __restrict__ partials, int nblocks, int len, double* __restrict__ out)
 {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < len; k += gridDim.x * blockDim.x) {
+    // a warp per entry: lane l sums partials l, l + 32, ... in order, then
+    // the lanes combine in a fixed tree (the same bits on every run)
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (int k = w; k < len; k += nw) {
         double s = 0.0;
-        for (int b = 0; b < nblocks; b++) s += partials[(size_t)b * len + k];
-        out[k] = s;
+        for (int b = lane; b < nblocks; b += 32) s += partials[(size_t)b * len + k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) out[k] = s;
     }
 }
 
@@ -550,6 +556,9 @@ struct blco_cpals_plan {
     float* Mf = nullptr;              // MTTKRP result (FP32)
     const float* vals32 = nullptr;
     blco::MttkrpArgs sched[BLCO_MAX_MODES] = {}; // per-mode schedule (kernel, hot_chunk, interleave)
+    bool gram_tc = false;             // mixed form: Grams on the tensor cores
+    double* tc_partials = nullptr;    // gram_tc_max_ctas x R x R
+    int* d_err = nullptr;             // set by a timed-out tensor-core wait
     double* grams[BLCO_MAX_MODES] = {};
     double* P = nullptr;
     double* partials = nullptr; // max(grid) * R * R
@@ -599,6 +608,8 @@ int plan_free(blco_cpals_plan* p)
     cudaFree(p->inv);
     cudaFree(p->fit);
     cudaFree(p->used_eigen);
+    cudaFree(p->tc_partials);
+    cudaFree(p->d_err);
     for (auto& e : p->ev)
         if (e) cudaEventDestroy(e);
     delete p;
@@ -622,7 +633,61 @@ int gram_launch(blco_cpals_plan* p, T* U, uint64_t I, const double* inv, double*
     BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     fn<<<grid, DN_THREADS, smem, p->s>>>(U, I, R, inv, p->partials, bf16_out);
     BLCO_CHECK_LAUNCH("k_gram");
-    k_sum_partials<<<(R * R + 255) / 256, 256, 0, p->s>>>(p->partials, grid, R * R, G);
+    k_sum_partials<<<(R * R * 32 + 255) / 256, 256, 0, p->s>>>(p->partials, grid, R * R, G);
+    BLCO_CHECK_LAUNCH("k_sum_partials");
+    return BLCO_OK;
+}
+
+// Standalone Gram G = U^T U (FP64 result) of a device FP32 matrix.
+int gram_f32_impl(float* U, uint64_t I, int R, double* G, bool tensor_cores, int sm, cudaStream_t s)
+{
+    double* parts = nullptr;
+    int* d_err = nullptr;
+    const int maxp = std::max(gram_tc_max_ctas(sm), grid_rows(I, sm));
+    cudaError_t e = cudaMalloc(&parts, (size_t)maxp * R * R * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
+    int st = e == cudaSuccess ? BLCO_OK : cuda_fail(e, "Gram buffers", __FILE__, __LINE__);
+    int np = 0;
+    if (st == BLCO_OK) {
+        if (tensor_cores) {
+            st = gram_tc_launch(U, I, R, nullptr, nullptr, parts, sm, d_err, s, &np);
+        } else {
+            np = grid_rows(I, sm);
+            const size_t smem = (size_t)R * R * sizeof(double) + (size_t)GR_CH * R * sizeof(float);
+            auto fn = R <= 64 ? k_gram<float, false, 4> : k_gram<float, false, 8>;
+            e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e == cudaSuccess) {
+                fn<<<np, DN_THREADS, smem, s>>>(U, I, R, nullptr, parts, nullptr);
+                count_launch();
+                e = cudaGetLastError();
+            }
+            if (e != cudaSuccess) st = cuda_fail(e, "k_gram", __FILE__, __LINE__);
+        }
+    }
+    if (st == BLCO_OK) {
+        k_sum_partials<<<(R * R * 32 + 255) / 256, 256, 0, s>>>(parts, np, R * R, G);
+        count_launch();
+        int herr = 0;
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "Gram", __FILE__, __LINE__);
+        else if (herr) st = fail(BLCO_ERR_TIMEOUT, "tensor-core Gram: an MMA completion wait timed out");
+    }
+    cudaStreamSynchronize(s);
+    cudaFree(parts);
+    cudaFree(d_err);
+    return st;
+}
+
+// The mixed form's Gram on the tensor cores (gram_tc.cu).
+int gram_launch_tc(blco_cpals_plan* p, float* U, uint64_t I, const double* inv, double* G, uint16_t* bf16_out)
+{
+    const int R = p->R;
+    int np = 0;
+    BLCO_TRY(gram_tc_launch(U, I, R, inv, bf16_out, p->tc_partials, p->sm, p->d_err, p->s, &np));
+    k_sum_partials<<<(R * R * 32 + 255) / 256, 256, 0, p->s>>>(p->tc_partials, np, R * R, G);
     BLCO_CHECK_LAUNCH("k_sum_partials");
     return BLCO_OK;
 }
@@ -696,7 +761,8 @@ int mode_update(blco_cpals_plan* p, int n)
     BLCO_CHECK_LAUNCH("k_lambda");
     if (p->mixed) {
         uint16_t* b = p->gather_dtype == BLCO_DTYPE_BF16 ? (uint16_t*)p->Ub[n] : nullptr;
-        BLCO_TRY(gram_launch<float>(p, p->Uf[n], I, p->inv, p->grams[n], b));
+        if (p->gram_tc) BLCO_TRY(gram_launch_tc(p, p->Uf[n], I, p->inv, p->grams[n], b));
+        else BLCO_TRY(gram_launch<float>(p, p->Uf[n], I, p->inv, p->grams[n], b));
     } else {
         BLCO_TRY(gram_launch<double>(p, p->U[n], I, p->inv, p->grams[n]));
     }
@@ -734,6 +800,11 @@ int export_factors(blco_cpals_plan* p)
 }
 
 } // namespace
+
+int gram_f32(float* U, uint64_t I, int R, double* G, bool tensor_cores, int sm, cudaStream_t s)
+{
+    return gram_f32_impl(U, I, R, G, tensor_cores, sm, s);
+}
 
 int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_lambda, const blco_opts* opts,
                 blco_cpals_plan** out)
@@ -775,6 +846,12 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
                       : p->mixed                                     ? BLCO_DTYPE_F32
                                                                      : BLCO_DTYPE_F64;
     if (p->mixed) {
+        p->gram_tc = R <= 64 && p->opts.gram_tensor_cores;
+        if (p->gram_tc) {
+            PC(cudaMalloc(&p->tc_partials, (size_t)gram_tc_max_ctas(p->sm) * R * R * sizeof(double)));
+            PC(cudaMalloc(&p->d_err, sizeof(int)));
+            PC(cudaMemsetAsync(p->d_err, 0, sizeof(int), p->s));
+        }
         PC(cudaMalloc(&p->Mf, std::max<uint64_t>(maxdim, 1) * R * sizeof(float)));
         for (int n = 0; n < p->N; n++) {
             const uint64_t len = t->layout.dims[n] * (uint64_t)R;
@@ -803,7 +880,8 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
             k_f64_to_f32<<<conv_grid(len, p->sm), 256, 0, p->s>>>(p->U[n], p->Uf[n], len);
             count_launch();
             uint16_t* b = p->gather_dtype == BLCO_DTYPE_BF16 ? (uint16_t*)p->Ub[n] : nullptr;
-            st = gram_launch<float>(p, p->Uf[n], t->layout.dims[n], nullptr, p->grams[n], b);
+            st = p->gram_tc ? gram_launch_tc(p, p->Uf[n], t->layout.dims[n], nullptr, p->grams[n], b)
+                            : gram_launch<float>(p, p->Uf[n], t->layout.dims[n], nullptr, p->grams[n], b);
         } else {
             st = gram_launch<double>(p, p->U[n], t->layout.dims[n], nullptr, p->grams[n]);
         }
@@ -866,6 +944,13 @@ int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* i
     }
     cudaEventDestroy(it0);
     cudaEventDestroy(it1);
+    if (st == BLCO_OK && p->gram_tc) {
+        int herr = 0;
+        cudaError_t e = cudaMemcpyAsync(&herr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, p->s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(p->s);
+        if (e != cudaSuccess) st = cuda_fail(e, "tensor-core Gram status", __FILE__, __LINE__);
+        else if (herr) st = fail(BLCO_ERR_TIMEOUT, "tensor-core Gram: an MMA completion wait timed out");
+    }
     if (st == BLCO_OK) st = export_factors(p);
     if (iters_done) *iters_done = done;
     return st;

@@ -201,6 +201,16 @@ double batch_last_ms(const blco_batch* b);
 int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda, int maxiter,
                double tol, const blco_opts* opts, double* fit_out, double* fits, int* iters_out);
 
+// gram_tc.cu: the mixed form's Gram (and optional scale / BF16 copy) on the
+// tensor cores; writes *nparts FP64 R x R partials (at most
+// gram_tc_max_ctas(sm)), sets *d_err when an MMA completion wait times out.
+int gram_tc_max_ctas(int sm);
+int gram_tc_launch(float* U, uint64_t I, int R, const double* inv, uint16_t* bf16_out, double* partials, int sm,
+                   int* d_err, cudaStream_t s, int* nparts);
+
+// cpals.cu: standalone Gram of a device FP32 matrix (tensor or CUDA cores).
+int gram_f32(float* U, uint64_t I, int R, double* G, bool tensor_cores, int sm, cudaStream_t s);
+
 // tune.cu
 int tune_features(const blco_tensor* t, int mode, int rank, int dtype, float* f);
 int tune_sweep(blco_tensor* t, int mode, int rank, int dtype, int reps, cudaStream_t s, float* ms_out);

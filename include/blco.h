@@ -105,6 +105,12 @@ typedef struct blco_opts {
     int device;            /* --device */
     uint64_t residency_bytes; /* device budget for streamed blocks; 0 = 8 GiB */
     void* stream;          /* cudaStream_t to run on; NULL = the default stream */
+    int gram_tensor_cores; /* mixed forms: 1 = Gram products on the tensor
+                              cores (tcgen05, split-BF16, rank <= 64); 0
+                              (default) = FP64 on the CUDA cores.  The tensor
+                              cores' FP32 accumulation leans low (~1e-7
+                              relative per 64-row tile), which moves the fit
+                              of a 200M-nonzero tensor by ~1e-4 */
 } blco_opts;
 
 typedef struct blco_tensor blco_tensor; /* opaque */
@@ -351,6 +357,15 @@ int blco_selector_set(blco_mlp* net, float margin);
  * the sweep decided. */
 int blco_select(blco_tensor* t, int mode, int rank, int factor_dtype, blco_mlp* net,
                 float margin, const blco_opts* opts, int* config, int* used_sweep);
+
+/* G = U^T U for a device FP32 matrix U (I x rank, row-major, rank 1..64),
+ * G (device, rank x rank FP64).  tensor_cores 1: split-BF16 products on the
+ * tensor cores (each value as bf16 hi + bf16 lo, FP32 accumulation over
+ * 64-row tiles, FP64 beyond); 0: FP64 products on the CUDA cores.  The
+ * Gram of the reference's ata_gpu (src/cpd_gpu.cu:547-568) for the mixed
+ * form's FP32 factors.  Synchronous on `stream` (NULL: default stream). */
+int blco_gram_f32(const float* d_U, uint64_t I, int rank, double* d_G, int tensor_cores, int device,
+                  void* stream);
 
 /* Number of this library's kernels launched by the calling thread since the
  * last reset (for reporting launch counts). */
