@@ -58,14 +58,18 @@ def mttkrp_alg_bytes(dims, nnz, R, mode, s_idx=8, s_val=8, s_fac=8, s_out=8):
     return b
 
 
-def traffic_from_profiles():
-    """DRAM bytes per MTTKRP launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "mttkrp_fp64_zipf_2Mx2Mx25k_r32.md")
+def traffic_from_profiles(form, nnz):
+    """DRAM bytes per MTTKRP (all kernels of one mode, mean over the modes)
+    at the full-size workload, from the committed ncu summary of the chosen
+    form, if there is one."""
+    if nnz != WORKLOAD["nnz"]:
+        return None
+    p = os.path.join(ROOT, "profiles", f"mttkrp_{form}_zipf_2Mx2Mx25k_r32.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         for line in f:
-            if line.startswith("traffic_bytes_per_launch_full_size:"):
+            if line.startswith("traffic_bytes_per_mttkrp_full_size:"):
                 try:
                     return float(line.split(":", 1)[1].strip())
                 except ValueError:
@@ -393,7 +397,7 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = peaks()
     alg = [mttkrp_alg_bytes(dims, nnz, rk, m, 8, sv, sf, so) for m in range(3)]
     achieved = sum(alg) / (sum(C["mttkrp_ms"]) * 1e-3) / 1e9  # GB/s over the three launches
-    traffic = traffic_from_profiles() if chosen == "fp64" else None
+    traffic = traffic_from_profiles(chosen, nnz)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_quick(args, dims, rk)
@@ -424,7 +428,9 @@ def run_ours(args, world, rank, local):
             "encode_ms": encode_ms,
             "roofline": dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                              traffic=traffic, peak_kind=peak_kind + " (hbm_gbs burst copy)",
-                             kernel=f"k_mttkrp_vec<3,32,{chosen}> (mean over the 3 modes)",
+                             kernel=(f"MTTKRP of one mode, {chosen}: k_mttkrp_hot + k_mttkrp_vec (+ k_merge_hot); "
+                                     "mean over the 3 modes; traffic = DRAM read + write of those kernels per "
+                                     "mode (ncu, profiles/)"),
                              alg_bytes_per_launch=[int(x) for x in alg]),
             "cpu_baseline": cpu,
             "e2e": dict(value=e2e_ms, unit="ms", h2d_bytes_per_step=int(h2d / e_iters),

@@ -1,0 +1,99 @@
+"""Profiling drivers (run under ncu or alone) for the two benchmark paths.
+
+  python blocked-linearized-coordinate_b200/prof.py mttkrp --nnz N --dtype f32|f64|bf16 [--kernel K] [--reps R]
+      One MTTKRP per mode of the Zipf(1.1) 2M x 2M x 25k tensor (rank 32),
+      timed with CUDA events; factors in the requested dtype.
+  python blocked-linearized-coordinate_b200/prof.py batch --count T [--iters I]
+      Batched CP-ALS sweeps over T small tensors of the many-small-tensors
+      recipe (FP64); prints device ms per sweep.
+"""
+import argparse
+import importlib.util
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load():
+    if "blco_b200" in sys.modules:
+        return sys.modules["blco_b200"]
+    spec = importlib.util.spec_from_file_location("blco_b200", os.path.join(HERE, "__init__.py"),
+                                                  submodule_search_locations=[HERE])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["blco_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def run_mttkrp(a, pkg, torch):
+    from blco_b200 import synth
+    dims = [2_000_000, 2_000_000, 25_000]
+    X = synth.zipf_tensor_device(a.nnz, dims, 1.1, seed=0)
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"])
+    del X
+    torch.cuda.empty_cache()
+    R = a.rank
+    g = torch.Generator(device="cuda").manual_seed(1)
+    fs = [torch.rand(d, R, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    if a.dtype != "f64":
+        fs = [f.to(torch.float32 if a.dtype == "f32" else torch.bfloat16) for f in fs]
+        fd = pkg.DTYPE_F32 if a.dtype == "f32" else pkg.DTYPE_BF16
+    o = pkg.make_opts(kernel=a.kernel)
+    for m in range(3):
+        out = torch.zeros(dims[m], R, dtype=torch.float64 if a.dtype == "f64" else torch.float32, device="cuda")
+        ts = []
+        for _ in range(a.reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if a.dtype == "f64":
+                pkg.mttkrp(t, m, fs, out, o)
+            else:
+                pkg.mttkrp_ex(t, m, fs, out, fd, o)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        print(f"mode {m}: ms {['%.3f' % x for x in ts]}", flush=True)
+    t.free()
+
+
+def run_batch(a, pkg, torch):
+    from blco_b200 import synth
+    Xs = synth.batch_tensors_device(a.count, seed=0)
+    ts = [pkg.Tensor.encode_device(x["dims"], x["cidx"], x["vals"]) for x in Xs]
+    g = torch.Generator(device="cuda").manual_seed(1)
+    fs = [[torch.rand(d, x["rank"], dtype=torch.float64, device="cuda", generator=g) for d in x["dims"]] for x in Xs]
+    ls = [torch.ones(x["rank"], dtype=torch.float64, device="cuda") for x in Xs]
+    del Xs
+    b = pkg.Batch(ts, fs, ls, tol=0.0)
+    b.iterate(2)
+    b.iterate(a.iters)
+    print("batched ms/sweep %.3f" % (b.last_ms() / a.iters), flush=True)
+    b.destroy()
+    for t in ts:
+        t.free()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    m = sub.add_parser("mttkrp")
+    m.add_argument("--nnz", type=int, default=20_000_000)
+    m.add_argument("--dtype", default="f32", choices=["f64", "f32", "bf16"])
+    m.add_argument("--kernel", type=int, default=10)
+    m.add_argument("--reps", type=int, default=1)
+    m.add_argument("--rank", type=int, default=32)
+    b = sub.add_parser("batch")
+    b.add_argument("--count", type=int, default=64)
+    b.add_argument("--iters", type=int, default=1)
+    a = ap.parse_args()
+    import torch
+    pkg = load()
+    if os.environ.get("BLCO_LIB"):
+        pkg.LIB_PATH = os.environ["BLCO_LIB"]
+    (run_mttkrp if a.cmd == "mttkrp" else run_batch)(a, pkg, torch)
+
+
+if __name__ == "__main__":
+    main()
