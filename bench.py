@@ -124,6 +124,18 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(x, dist, device="cuda"):
+    """The maximum of a per-rank float over all ranks (identity without a
+    process group); `device` is where the collective's tensor lives (cuda for
+    NCCL, cpu for gloo)."""
+    if not dist:
+        return x
+    import torch
+    tt = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return tt.item()
+
+
 def run_reference(args, world, rank):
     """The reference's CPU MTTKRP on a bounded sample of the workload."""
     if rank != 0:
@@ -254,10 +266,7 @@ def time_form(pkg, torch, t, dims, rk, fs0, form, args, stream, dist):
     ms1, calls1 = plan.mttkrp_ms()
     plan.destroy()
     del fs, lam
-    if dist:
-        tt = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = tt.item()
+    elapsed = max_over_ranks(elapsed, dist)
     return dict(ms_per_step=elapsed / args.steps, mttkrp_ms=list((ms1 - ms0) / max(1, calls1 - calls0)),
                 fits=fits, launches=int(launches), clocks=ck)
 
@@ -389,10 +398,7 @@ def run_ours(args, world, rank, local):
     e2e_ms = (t3 - t0) * 1e3 / e_iters
     e2e_split = dict(encode_ms=(t1 - t0) * 1e3, cpals_ms=(t3 - t1) * 1e3)
     t2.free()
-    if dist:
-        tt = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = tt.item()
+    e2e_ms = max_over_ranks(e2e_ms, dist)
 
     peak, peak_kind = peaks()
     alg = [mttkrp_alg_bytes(dims, nnz, rk, m, 8, sv, sf, so) for m in range(3)]
