@@ -70,68 +70,11 @@ cudaStream_t pick_stream(const blco_tensor*, const blco_opts* opts)
 // src/alto_dev.cu:1979-2012, with events instead of one stream per block).
 static int mttkrp_streamed(blco_tensor* t, const MttkrpArgs& base, const blco_opts* opts, cudaStream_t s)
 {
-    const uint64_t B = t->max_block_size ? t->max_block_size : t->nnz;
-    uint64_t budget = (opts && opts->residency_bytes) ? opts->residency_bytes : (8ull << 30);
-    int nbuf = (int)std::max<uint64_t>(2, std::min<uint64_t>(8, budget / std::max<uint64_t>(1, B * 16)));
-    nbuf = (int)std::min<uint64_t>((uint64_t)nbuf, std::max<uint64_t>(1, t->block_count));
-    std::vector<uint64_t*> dc(nbuf, nullptr);
-    std::vector<double*> dv(nbuf, nullptr);
-    std::vector<cudaEvent_t> copied(nbuf, nullptr), consumed(nbuf, nullptr);
-    cudaStream_t cs = nullptr;
-    int st = BLCO_OK;
-    auto cleanup = [&]() {
-        cudaStreamSynchronize(s);
-        if (cs) cudaStreamSynchronize(cs);
-        for (int i = 0; i < nbuf; i++) {
-            cudaFree(dc[i]);
-            cudaFree(dv[i]);
-            if (copied[i]) cudaEventDestroy(copied[i]);
-            if (consumed[i]) cudaEventDestroy(consumed[i]);
-        }
-        if (cs) cudaStreamDestroy(cs);
-    };
-#define SC(call)                                                               \
-    do {                                                                       \
-        cudaError_t _e = (call);                                               \
-        if (_e != cudaSuccess) {                                               \
-            st = cuda_fail(_e, #call, __FILE__, __LINE__);                     \
-            cleanup();                                                         \
-            return st;                                                         \
-        }                                                                      \
-    } while (0)
-    SC(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    for (int i = 0; i < nbuf; i++) {
-        SC(cudaMalloc(&dc[i], B * 8));
-        SC(cudaMalloc(&dv[i], B * 8));
-        SC(cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming));
-        SC(cudaEventCreateWithFlags(&consumed[i], cudaEventDisableTiming));
-    }
-    // The copy stream must not overwrite the caller's pending work order:
-    // make it wait for everything already queued on s.
-    SC(cudaEventRecord(consumed[0], s));
-    SC(cudaStreamWaitEvent(cs, consumed[0], 0));
-    for (uint64_t b = 0; b < t->block_count; b++) {
-        const int k = (int)(b % nbuf);
-        const uint64_t beg = b * B, n = std::min(B, t->nnz - beg);
-        if (b >= (uint64_t)nbuf) SC(cudaStreamWaitEvent(cs, consumed[k], 0));
-        SC(cudaMemcpyAsync(dc[k], t->h_coords + beg, n * 8, cudaMemcpyHostToDevice, cs));
-        SC(cudaMemcpyAsync(dv[k], t->h_values + beg, n * 8, cudaMemcpyHostToDevice, cs));
-        SC(cudaEventRecord(copied[k], cs));
-        SC(cudaStreamWaitEvent(s, copied[k], 0));
-        MttkrpArgs a = base;
-        a.coords = dc[k];
-        a.vals = dv[k];
-        a.nnz = n;
-        st = mttkrp_launch(t, a, s);
-        if (st != BLCO_OK) {
-            cleanup();
-            return st;
-        }
-        SC(cudaEventRecord(consumed[k], s));
-    }
-#undef SC
-    cleanup();
-    return BLCO_OK;
+    StreamRing* ring = nullptr;
+    BLCO_TRY(stream_ring_create(t, opts ? opts->residency_bytes : 0, &ring));
+    const int st = mttkrp_streamed_ring(t, base, ring, s);
+    const int st2 = stream_ring_destroy(ring);
+    return st != BLCO_OK ? st : st2;
 }
 
 } // namespace blco

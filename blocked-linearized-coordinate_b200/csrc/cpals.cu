@@ -556,6 +556,7 @@ struct blco_cpals_plan {
     float* Mf = nullptr;              // MTTKRP result (FP32)
     const float* vals32 = nullptr;
     blco::MttkrpArgs sched[BLCO_MAX_MODES] = {}; // per-mode schedule (kernel, hot_chunk, interleave)
+    blco::StreamRing* ring = nullptr; // streamed tensors: device block buffers
     bool gram_tc = false;             // mixed form: Grams on the tensor cores
     double* tc_partials = nullptr;    // gram_tc_max_ctas x R x R
     int* d_err = nullptr;             // set by a timed-out tensor-core wait
@@ -610,6 +611,7 @@ int plan_free(blco_cpals_plan* p)
     cudaFree(p->used_eigen);
     cudaFree(p->tc_partials);
     cudaFree(p->d_err);
+    stream_ring_destroy(p->ring);
     for (auto& e : p->ev)
         if (e) cudaEventDestroy(e);
     delete p;
@@ -743,7 +745,8 @@ int mode_update(blco_cpals_plan* p, int n)
         a.factor_dtype = BLCO_DTYPE_F64;
     }
     BLCO_CUDA(cudaEventRecord(p->ev[2 * n], p->s));
-    BLCO_TRY(mttkrp_launch(t, a, p->s));
+    if (t->resident) BLCO_TRY(mttkrp_launch(t, a, p->s));
+    else BLCO_TRY(mttkrp_streamed_ring(t, a, p->ring, p->s)); // blocks copied through the plan's ring
     BLCO_CUDA(cudaEventRecord(p->ev[2 * n + 1], p->s));
 
     GramPtrs gp;
@@ -812,7 +815,8 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     *out = nullptr;
     if (!t || !d_factors || !d_lambda) return fail(BLCO_ERR_INVALID, "null argument");
     if (rank < 1 || rank > MAX_SOLVE_R) return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS rank must be 1..96");
-    if (!t->resident) return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS on a streamed tensor is not built yet");
+    if (!t->resident && opts && opts->precision != BLCO_PRECISION_FP64)
+        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS on a streamed tensor runs the FP64 form only");
     blco_cpals_plan* p = new blco_cpals_plan();
     p->t = t;
     p->R = rank;
@@ -842,6 +846,10 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
         }                                                                      \
     } while (0)
     p->mixed = p->opts.precision != BLCO_PRECISION_FP64;
+    if (!t->resident) {
+        st = stream_ring_create(t, p->opts.residency_bytes, &p->ring);
+        if (st != BLCO_OK) { plan_free(p); return st; }
+    }
     p->gather_dtype = p->opts.precision == BLCO_PRECISION_MIXED_BF16 ? BLCO_DTYPE_BF16
                       : p->mixed                                     ? BLCO_DTYPE_F32
                                                                      : BLCO_DTYPE_F64;

@@ -183,6 +183,11 @@ int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested
 // Automatic rule: the heavy-row path needs at least this many heavy nonzeros.
 constexpr uint64_t AUTO_HOT_MIN_NNZ = 1ull << 18;
 uint32_t auto_hot_chunk(uint64_t hot_nnz);
+// Streamed blocks: a reusable ring of device buffers and a copy stream.
+struct StreamRing;
+int stream_ring_create(const blco_tensor* t, uint64_t residency_bytes, StreamRing** out);
+int stream_ring_destroy(StreamRing* r);
+int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRing* r, cudaStream_t s);
 // FP32 copy of the resident values (created on first use).
 int values_f32(blco_tensor* t, cudaStream_t s, const float** out);
 

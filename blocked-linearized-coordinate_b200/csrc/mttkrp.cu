@@ -31,6 +31,8 @@
 #include <algorithm>
 #include <cstring>
 
+#include <vector>
+
 #include "internal.cuh"
 
 namespace blco {
@@ -903,6 +905,90 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     p.tiles_per_cta = (ntiles + grid - 1) / grid;
     fn<<<(unsigned)grid, MT_THREADS, smem, s>>>(p);
     BLCO_CHECK_LAUNCH("k_mttkrp");
+    return BLCO_OK;
+}
+
+// ------------------------------------------------------ streamed blocks --
+
+struct StreamRing {
+    int nbuf = 0;
+    uint64_t B = 0;
+    std::vector<uint64_t*> dc;
+    std::vector<double*> dv;
+    std::vector<cudaEvent_t> copied, consumed;
+    cudaStream_t cs = nullptr;
+};
+
+int stream_ring_destroy(StreamRing* r)
+{
+    if (!r) return BLCO_OK;
+    if (r->cs) cudaStreamSynchronize(r->cs);
+    for (int i = 0; i < r->nbuf; i++) {
+        if (r->consumed[i]) cudaEventSynchronize(r->consumed[i]);
+        cudaFree(r->dc[i]);
+        cudaFree(r->dv[i]);
+        if (r->copied[i]) cudaEventDestroy(r->copied[i]);
+        if (r->consumed[i]) cudaEventDestroy(r->consumed[i]);
+    }
+    if (r->cs) cudaStreamDestroy(r->cs);
+    delete r;
+    return BLCO_OK;
+}
+
+// A ring of device block buffers (at most residency_bytes, 8 GiB when 0,
+// between 2 and 8 buffers) and a copy stream, for tensors whose blocks stay
+// in pinned host memory.
+int stream_ring_create(const blco_tensor* t, uint64_t residency_bytes, StreamRing** out)
+{
+    *out = nullptr;
+    StreamRing* r = new StreamRing();
+    r->B = t->max_block_size ? t->max_block_size : t->nnz;
+    const uint64_t budget = residency_bytes ? residency_bytes : (8ull << 30);
+    int nbuf = (int)std::max<uint64_t>(2, std::min<uint64_t>(8, budget / std::max<uint64_t>(1, r->B * 16)));
+    nbuf = (int)std::min<uint64_t>((uint64_t)nbuf, std::max<uint64_t>(1, t->block_count));
+    r->nbuf = nbuf;
+    r->dc.assign(nbuf, nullptr);
+    r->dv.assign(nbuf, nullptr);
+    r->copied.assign(nbuf, nullptr);
+    r->consumed.assign(nbuf, nullptr);
+    cudaError_t e = cudaStreamCreateWithFlags(&r->cs, cudaStreamNonBlocking);
+    for (int i = 0; i < nbuf && e == cudaSuccess; i++) {
+        e = cudaMalloc(&r->dc[i], std::max<uint64_t>(1, r->B) * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&r->dv[i], std::max<uint64_t>(1, r->B) * 8);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->copied[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->consumed[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        stream_ring_destroy(r);
+        return cuda_fail(e, "streamed block ring", __FILE__, __LINE__);
+    }
+    *out = r;
+    return BLCO_OK;
+}
+
+// One MTTKRP over every block: block b is copied into buffer b % nbuf on the
+// copy stream (after the kernel that used that buffer before), and its
+// MTTKRP runs on s after the copy.
+int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRing* r, cudaStream_t s)
+{
+    // the copies must not overtake work already queued on s
+    BLCO_CUDA(cudaEventRecord(r->consumed[0], s));
+    BLCO_CUDA(cudaStreamWaitEvent(r->cs, r->consumed[0], 0));
+    for (uint64_t b = 0; b < t->block_count; b++) {
+        const int k = (int)(b % r->nbuf);
+        const uint64_t beg = b * r->B, n = std::min(r->B, t->nnz - beg);
+        if (b >= (uint64_t)r->nbuf) BLCO_CUDA(cudaStreamWaitEvent(r->cs, r->consumed[k], 0));
+        BLCO_CUDA(cudaMemcpyAsync(r->dc[k], t->h_coords + beg, n * 8, cudaMemcpyHostToDevice, r->cs));
+        BLCO_CUDA(cudaMemcpyAsync(r->dv[k], t->h_values + beg, n * 8, cudaMemcpyHostToDevice, r->cs));
+        BLCO_CUDA(cudaEventRecord(r->copied[k], r->cs));
+        BLCO_CUDA(cudaStreamWaitEvent(s, r->copied[k], 0));
+        MttkrpArgs a = base;
+        a.coords = r->dc[k];
+        a.vals = r->dv[k];
+        a.nnz = n;
+        BLCO_TRY(mttkrp_launch(t, a, s));
+        BLCO_CUDA(cudaEventRecord(r->consumed[k], s));
+    }
     return BLCO_OK;
 }
 

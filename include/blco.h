@@ -238,7 +238,10 @@ int blco_mttkrp_host(blco_tensor* t, int mode, int rank, const double* const* fa
  * |fit - fit_old| < tol or the fit is NaN.  factors (host, dims[n] x rank)
  * and lambda (host, rank) are read and updated in place.
  *   fit_out: last fit; fits (may be NULL): one entry per executed
- *   iteration (maxiter entries must fit); iters_out: iterations executed. */
+ *   iteration (maxiter entries must fit); iters_out: iterations executed.
+ * A streamed tensor (encoded with opts->stream_data) runs the FP64 form:
+ * every MTTKRP copies its blocks through a ring of device buffers of at most
+ * opts->residency_bytes (BLCO_ERR_UNSUPPORTED for the mixed forms). */
 int blco_cpals(blco_tensor* t, int rank, double* const* factors, double* lambda,
                int maxiter, double tol, const blco_opts* opts, double* fit_out,
                double* fits, int* iters_out);

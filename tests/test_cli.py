@@ -152,3 +152,17 @@ def test_cli_bench_and_streamed(tmp_path):
     r = run(["-i", p, "-k", "2", "-c", "-p", "-t", "1", "-r", "16", "--stream-data", "--max-block-size", "3000"])
     assert r.returncode == 0, r.stderr
     assert r.stderr.count("is correct") == 3
+    # CP-ALS with the stream in host memory follows the resident run
+    fits = []
+    for extra in ([], ["--stream-data", "--max-block-size", "3000"]):
+        r = run(["-i", p, "-k", "10", "-r", "8", "-m", "4", "-e", "0", "-x", "3"] + extra)
+        assert r.returncode == 0, r.stderr
+        fits.append([float(l.split("f = ")[1].split()[0]) for l in r.stdout.splitlines() if l.startswith("--> Iter")])
+    assert len(fits[0]) == 4 and np.allclose(fits[0], fits[1], rtol=0, atol=2e-6)
+    # CP-ALS with the stream in host memory follows the resident run
+    fits = []
+    for extra in ([], ["--stream-data", "--max-block-size", "3000"]):
+        r = run(["-i", p, "-k", "10", "-r", "8", "-m", "4", "-e", "0", "-x", "3"] + extra)
+        assert r.returncode == 0, r.stderr
+        fits.append([float(l.split("f = ")[1].split()[0]) for l in r.stdout.splitlines() if l.startswith("--> Iter")])
+    assert len(fits[0]) == 4 and np.allclose(fits[0], fits[1], rtol=0, atol=2e-6)

@@ -117,3 +117,39 @@ def test_cpals_plan_device_factors(blco):
     fo = [f.copy() for f in fs0]
     fits_o = po.cpals(X["dims"], enc, fo, np.ones(R), 5, -1.0)
     assert np.allclose(fits_a + fits_b, fits_o, atol=1e-10)
+
+
+def test_cpals_streamed_blocks_match_resident(blco):
+    """--stream-data: the stream stays in pinned host memory and every MTTKRP
+    copies its blocks through a ring of device buffers (here 3 buffers of
+    7000 nonzeros for a 40k-nonzero tensor, so buffers are reused within one
+    MTTKRP).  The FP64 fits follow the resident tensor's and the oracle's
+    (1e-10), and the mixed forms are refused on a streamed tensor."""
+    rng = np.random.default_rng(12)
+    dims = [3000, 800, 200]
+    cidx = unique_coords(rng, dims, 40_000, zipf=0.9)
+    vals = rng.random(40_000)
+    R = 8
+    fs0 = [rng.random((d, R)) for d in dims]
+    t_res = blco.Tensor.encode(dims, cidx, vals)
+    t_str = blco.Tensor.encode(dims, cidx, vals, 7000, opts=blco.make_opts(stream_data=True))
+    assert not t_str.info()["resident"] and t_str.info()["block_count"] == 6
+    f_res = [x.copy() for x in fs0]
+    _, fits_res = blco.cpals(t_res, f_res, np.ones(R), 12, 0.0)
+    f_str = [x.copy() for x in fs0]
+    lam = np.ones(R)
+    _, fits_str = blco.cpals(t_str, f_str, lam, 12, 0.0,
+                             blco.make_opts(stream_data=True, residency_bytes=3 * 7000 * 16))
+    assert np.allclose(fits_str, fits_res, rtol=0, atol=1e-10)
+    for a, b in zip(f_str, f_res):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+    enc = po.blco_encode(dims, cidx, vals)
+    fo = [x.copy() for x in fs0]
+    fits_o = po.cpals(dims, enc, fo, np.ones(R), 12, 0.0)
+    assert np.allclose(fits_str, fits_o, rtol=0, atol=1e-10)
+    with pytest.raises(blco.BlcoError) as e:
+        blco.cpals(t_str, [x.copy() for x in fs0], np.ones(R), 2, 0.0,
+                   blco.make_opts(stream_data=True, precision=blco.PRECISION_MIXED))
+    assert e.value.status == blco.ERR_UNSUPPORTED
+    t_res.free()
+    t_str.free()
