@@ -34,7 +34,7 @@ constexpr int MAX_SOLVE_R = 96; // k_solve keeps two R x R FP64 buffers in share
 // scaling the rows by inv[c] first and writing the scaled rows back.
 // Thread tile: TS x TS entries of the R x R result (TS = 4 up to R = 64,
 // 8 up to R = 128, so that 256 threads cover the result).
-constexpr int GR_CH = 32; // rows staged per step
+constexpr int GR_CH = 128; // rows staged per step
 
 __device__ __forceinline__ float round_bf16(float x, uint16_t* bits)
 {
@@ -52,16 +52,25 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t
                                                      const double* __restrict__ inv, double* __restrict__ partials,
                                                      uint16_t* __restrict__ bf16_out = nullptr)
 {
+    // The Gram is symmetric: thread tiles cover the TS x TS blocks (i, j)
+    // with i <= j only, and each is written to both halves at the end.  Rows
+    // are staged in shared memory as FP64 (converted once), so the inner
+    // loop is 2*TS shared loads per TS*TS FMAs.
     extern __shared__ __align__(16) double gs[];
     double* red = gs;                                 // R x R reduction buffer
-    T* tile = reinterpret_cast<T*>(gs + R * R);       // GR_CH x R
-    const int tpr = (R + TS - 1) / TS; // tiles per row of the result
-    const int ntile = tpr * tpr;
+    double* tile = gs + R * R;                        // GR_CH x R
+    const int nb = (R + TS - 1) / TS;                 // blocks per side
+    const int ntile = nb * (nb + 1) / 2;
     const int groups = max(1, DN_THREADS / ntile);
     const int tid = threadIdx.x;
     const int g = tid / ntile, e = tid % ntile;
     const bool active = g < groups && tid < groups * ntile;
-    const int a0 = (e / tpr) * TS, b0 = (e % tpr) * TS;
+    int bi = 0, rem = e;
+    while (rem >= nb - bi) {
+        rem -= nb - bi;
+        bi++;
+    }
+    const int a0 = bi * TS, b0 = (bi + rem) * TS;
     double acc[TS][TS];
 #pragma unroll
     for (int x = 0; x < TS; x++)
@@ -82,19 +91,19 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t
                 bf16_out[r0 * R + k] = b;
             }
             if (SCALE || BF16OUT) U[r0 * R + k] = v;
-            tile[k] = v;
+            tile[k] = (double)v;
         }
         __syncthreads();
         if (active) {
-            // Tiles that reach past R read columns clamped to R-1 and are
+            // Blocks that reach past R read columns clamped to R-1 and are
             // discarded at the end.
             for (int r = g; r < nr; r += groups) {
-                const T* row = tile + r * R;
+                const double* row = tile + r * R;
                 double va[TS], vb[TS];
 #pragma unroll
                 for (int x = 0; x < TS; x++) {
-                    va[x] = (double)row[min(a0 + x, R - 1)];
-                    vb[x] = (double)row[min(b0 + x, R - 1)];
+                    va[x] = row[min(a0 + x, R - 1)];
+                    vb[x] = row[min(b0 + x, R - 1)];
                 }
 #pragma unroll
                 for (int x = 0; x < TS; x++)
@@ -103,7 +112,7 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t
             }
         }
     }
-    // Reduce the row groups in a fixed order.
+    // Reduce the row groups in a fixed order; mirror the off-diagonal blocks.
     for (int k = tid; k < R * R; k += DN_THREADS) red[k] = 0.0;
     __syncthreads();
     for (int gg = 0; gg < groups; gg++) {
@@ -112,7 +121,10 @@ __global__ __launch_bounds__(DN_THREADS) void k_gram(T* __restrict__ U, uint64_t
             for (int x = 0; x < TS; x++)
 #pragma unroll
                 for (int y = 0; y < TS; y++)
-                    if (a0 + x < R && b0 + y < R) red[(a0 + x) * R + b0 + y] += acc[x][y];
+                    if (a0 + x < R && b0 + y < R) {
+                        red[(a0 + x) * R + b0 + y] += acc[x][y];
+                        if (a0 != b0) red[(b0 + y) * R + a0 + x] += acc[x][y];
+                    }
         }
         __syncthreads();
     }
@@ -623,7 +635,7 @@ int gram_launch(blco_cpals_plan* p, T* U, uint64_t I, const double* inv, double*
 {
     const int R = p->R;
     int grid = grid_rows(I, p->sm);
-    size_t smem = (size_t)R * R * sizeof(double) + (size_t)GR_CH * R * sizeof(T);
+    size_t smem = (size_t)R * R * sizeof(double) + (size_t)GR_CH * R * sizeof(double);
     void (*fn)(T*, uint64_t, int, const double*, double*, uint16_t*);
     if (bf16_out) {
         if (R <= 64) fn = inv ? k_gram<T, true, 4, true> : k_gram<T, false, 4, true>;
@@ -656,7 +668,7 @@ int gram_f32_impl(float* U, uint64_t I, int R, double* G, bool tensor_cores, int
             st = gram_tc_launch(U, I, R, nullptr, nullptr, parts, sm, d_err, s, &np);
         } else {
             np = grid_rows(I, sm);
-            const size_t smem = (size_t)R * R * sizeof(double) + (size_t)GR_CH * R * sizeof(float);
+            const size_t smem = (size_t)R * R * sizeof(double) + (size_t)GR_CH * R * sizeof(double);
             auto fn = R <= 64 ? k_gram<float, false, 4> : k_gram<float, false, 8>;
             e = cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e == cudaSuccess) {
