@@ -333,6 +333,7 @@ def run_ours(args, world, rank, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     pkg = load_pkg()
     from blco_b200 import synth
+    selector = pkg.default_selector(margin=0.1) if args.kernel == pkg.KERNEL_LEARNED else None
     dims, nnz, rk = WORKLOAD["dims"], args.nnz, WORKLOAD["rank"]
     X = synth.zipf_tensor_device(nnz, dims, WORKLOAD["zipf"], seed=args.seed + rank)
     stream = torch.cuda.current_stream()
@@ -404,6 +405,15 @@ def run_ours(args, world, rank, local):
     alg = [mttkrp_alg_bytes(dims, nnz, rk, m, 8, sv, sf, so) for m in range(3)]
     achieved = sum(alg) / (sum(C["mttkrp_ms"]) * 1e-3) / 1e9  # GB/s over the three launches
     traffic = traffic_from_profiles(chosen, nnz)
+    # the schedule kernel id 21 takes for each mode of the chosen form
+    schedules = None
+    if selector is not None:
+        space = pkg.tune_space()
+        dt = {"fp64": pkg.DTYPE_F64, "mixed_f32": pkg.DTYPE_F32, "mixed_bf16": pkg.DTYPE_BF16}[chosen]
+        schedules = []
+        for m in range(3):
+            k, swept = pkg.select(t, m, rk, dt, selector, 0.1)
+            schedules.append(dict(mode=m, schedule=k, **space[k], decided_by="sweep" if swept else "network"))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_quick(args, dims, rk)
@@ -425,7 +435,7 @@ def run_ours(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": C["ms_per_step"], "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": dtype, "data": "synthetic",
             "config": dict(workload=WORKLOAD["workload"], dims=dims, nnz=nnz, rank=rk, zipf=WORKLOAD["zipf"],
-                           values=WORKLOAD["values"], form=chosen, kernel=args.kernel,
+                           values=WORKLOAD["values"], form=chosen, kernel=args.kernel, schedules=schedules,
                            parallelism=("replicas" if world > 1 else "single"),
                            l2="inputs larger than L2 (3.2 GB stream, >= 0.5 GB factors)"),
             "forms": forms_out,
@@ -460,7 +470,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nnz", type=int, default=WORKLOAD["nnz"])
-    ap.add_argument("--kernel", type=int, default=10)
+    ap.add_argument("--kernel", type=int, default=21,
+                    help="MTTKRP kernel id; 21 (default) = the committed learned schedule selector")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--ref-sample", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -527,3 +527,20 @@ def gram_f32(U, tensor_cores=True):
     _check(lib().blco_gram_f32(int(U.data_ptr()), int(U.shape[0]), R, int(G.data_ptr()), int(bool(tensor_cores)),
                                U.device.index or 0, stream))
     return G
+
+
+_default_net = None
+
+
+def default_selector(margin=0.1, path=None):
+    """Load the committed trained selector (selector/selector_params.npz,
+    made by selector/train_selector.py) and make it the network kernel id
+    21 uses.  Returns the network; the module keeps it alive."""
+    global _default_net
+    path = path or os.path.join(HERE, "selector", "selector_params.npz")
+    d = np.load(path)
+    net = Mlp(hidden=int(d["hidden"]), seed=0)
+    net.set_params(d["params"])
+    selector_set(net, margin)
+    _default_net = net
+    return net

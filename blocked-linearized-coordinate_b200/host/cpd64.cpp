@@ -54,6 +54,32 @@ static void usage(const char* call)
     fprintf(stderr, "\t--stream-data        Stream data to the GPU during computation\n");
     fprintf(stderr, "\t--max-block-size     Block size (nonzeros) on the GPU\n");
     fprintf(stderr, "\t--batch              Accepted for compatibility (blocks always run in one launch)\n");
+    fprintf(stderr, "\t--selector FILE      Trained schedule selector (selector_params.bin) for -k 21\n");
+}
+
+// Reads a selector parameter file (int32 hidden width, int32 count, then
+// float32 parameters, little-endian) and makes it the network of kernel 21.
+static bool load_selector(const std::string& path, int device, blco_mlp** out, std::string* err)
+{
+    FILE* f = fopen(path.c_str(), "rb");
+    if (!f) { *err = "cannot open " + path; return false; }
+    int32_t hdr[2] = {0, 0};
+    bool ok = fread(hdr, sizeof(int32_t), 2, f) == 2 && hdr[0] > 0 && hdr[1] > 0;
+    std::vector<float> params(ok ? (size_t)hdr[1] : 0);
+    ok = ok && fread(params.data(), sizeof(float), params.size(), f) == params.size();
+    fclose(f);
+    if (!ok) { *err = "malformed selector file " + path; return false; }
+    blco_mlp* net = nullptr;
+    int n = 0;
+    if (blco_mlp_create(hdr[0], 0, device, &net) != BLCO_OK || blco_mlp_num_params(net, &n) != BLCO_OK ||
+        n != hdr[1] || blco_mlp_set_params(net, params.data(), n) != BLCO_OK) {
+        *err = std::string("selector: ") + blco_last_error();
+        if (net) blco_mlp_destroy(net);
+        return false;
+    }
+    blco_selector_set(net, 0.1f);
+    *out = net;
+    return true;
 }
 
 static void print_tensor_info(uint64_t rank, int max_iters, const Coo& X)
@@ -118,11 +144,12 @@ int main(int argc, char** argv)
         {"file", 1, nullptr, 'f'},       {"check", 0, nullptr, 'c'},       {"bench", 0, nullptr, 'p'},
         {"kernel-id", 1, nullptr, 'k'},  {"num-partitions", 1, nullptr, 'n'}, {"device", 1, nullptr, 1001},
         {"thread-cf", 1, nullptr, 1002}, {"stream-data", 0, nullptr, 1003}, {"max-block-size", 1, nullptr, 1004},
-        {"max_block_size", 1, nullptr, 1004}, {"batch", 0, nullptr, 1005}, {nullptr, 0, nullptr, 0}};
+        {"max_block_size", 1, nullptr, 1004}, {"batch", 0, nullptr, 1005}, {"selector", 1, nullptr, 1006},
+        {nullptr, 0, nullptr, 0}};
     int max_iters = 10;
     long long rank = 16;
     int target_mode = 0;
-    std::string text_file, out_file, bin_file;
+    std::string text_file, out_file, bin_file, selector_file;
     double epsilon = 1e-5;
     int seed = (int)time(nullptr);
     int save_to_file = 0;
@@ -158,6 +185,7 @@ int main(int argc, char** argv)
         case 1003: stream_data = true; break;
         case 1004: max_block_size = atoll(optarg); if (max_block_size <= 0) { fprintf(stderr, "Invalid -max-block-size: %s.\n", optarg); return 1; } break;
         case 1005: break;
+        case 1006: selector_file = optarg; break;
         default: usage(argv[0]); return 1;
         }
     }
@@ -189,6 +217,11 @@ int main(int argc, char** argv)
     if (do_check) max_iters = 1;
     if (!stream_data) max_block_size = 0; // one block (src/main.cpp:327)
 
+    blco_mlp* selector = nullptr;
+    if (!selector_file.empty() && !load_selector(selector_file, device, &selector, &err)) {
+        fprintf(stderr, "Error: %s\n", err.c_str());
+        return 1;
+    }
     blco_opts opts;
     blco_opts_init(&opts);
     opts.kernel = kernel_id;
@@ -261,5 +294,9 @@ int main(int argc, char** argv)
         }
     }
     blco_tensor_free(T);
+    if (selector) {
+        blco_selector_set(nullptr, 0.f);
+        blco_mlp_destroy(selector);
+    }
     return rc;
 }

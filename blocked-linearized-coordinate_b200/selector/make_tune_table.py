@@ -1,6 +1,7 @@
-"""Generate tests/golden/tune_table.npz: autotuner sweep timings and selector
-features for a set of synthetic tensors (runs on a B200; the table is
-committed so the selector tests train on fixed data).
+"""Generate selector/tune_table.npz: autotuner sweep timings and selector
+features for a set of synthetic tensors (runs on a B200).  The table is the
+selector's training data (train_selector.py) and the fixed data the
+selector tests train on.
 
 The tensors follow the selector workload's recipe at reduced size so the
 sweep finishes in minutes: order 3-5; mode lengths log-uniform in
@@ -15,7 +16,7 @@ Rows: one per (tensor, mode).  Arrays: X (n, 25) features, ms (n, 12)
 milliseconds per schedule (-1: not valid), tensor (n,) tensor index,
 mode, dim (mode length), rank, dtype.
 
-usage: python tests/golden/make_tune_table.py [--count 240] [--out PATH]
+usage: python blocked-linearized-coordinate_b200/selector/make_tune_table.py [--count 240] [--out PATH]
 """
 import argparse
 import importlib.util
@@ -27,8 +28,7 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-ROOT = os.path.dirname(os.path.dirname(HERE))
-PKG = os.path.join(ROOT, "blocked-linearized-coordinate_b200")
+PKG = os.path.dirname(HERE)
 
 
 def load():

@@ -68,6 +68,17 @@ def test_tns_parser_and_binary_writer(tmp_path):
     assert np.array_equal(c, cidx) and np.array_equal(v, vals)
 
 
+def test_selector_file_errors(tmp_path):
+    p = str(tmp_path / "x.tns")
+    write_tns(p, np.array([[0, 1], [1, 0], [0, 1]], dtype=np.uint64), np.array([1.0, 2.0]), comments=False)
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"\x01\x00")
+    r = run(["-i", p, "-k", "21", "--selector", str(bad)])
+    assert r.returncode == 1 and "selector" in r.stderr
+    r = run(["-i", p, "-k", "21", "--selector", str(tmp_path / "missing.bin")])
+    assert r.returncode == 1 and "cannot open" in r.stderr
+
+
 def test_tns_rejects_bad_input(tmp_path):
     p = str(tmp_path / "bad.tns")
     with open(p, "w") as f:
@@ -125,7 +136,7 @@ def test_cli_random_init_matches_reference(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel", ["1", "2", "3", "10", "13"])
+@pytest.mark.parametrize("kernel", ["1", "2", "3", "10", "13", "20", "21"])
 def test_cli_check_mode(tmp_path, kernel):
     rng = np.random.default_rng(5)
     dims = [50, 60, 70]
@@ -133,8 +144,9 @@ def test_cli_check_mode(tmp_path, kernel):
     cidx = np.array(np.unravel_index(lin, dims), dtype=np.uint64)
     p = str(tmp_path / "c.tns")
     write_tns(p, cidx, rng.random(5000), comments=False)
+    sel = ["--selector", os.path.join(PKG_DIR, "selector", "selector_params.bin")] if kernel == "21" else []
     for mode in ("0", "2"):
-        r = run(["-i", p, "-k", kernel, "-c", "-p", "-t", mode, "-r", "8", "-x", "1"])
+        r = run(["-i", p, "-k", kernel, "-c", "-p", "-t", mode, "-r", "8", "-x", "1"] + sel)
         assert r.returncode == 0, r.stderr
         assert r.stderr.count("Results of mttkrp_blco_dev is correct") == 3, r.stderr
 

@@ -1,8 +1,9 @@
 """MTTKRP schedule selection on the GPU: the autotuner sweep, every schedule
 of its space against the oracle, the selector network's kernels against the
 CPU oracle (oracle/mlp_oracle.py), and what the trained network gains over
-the fixed rules on the committed sweep table (tests/golden/tune_table.npz,
-made by tests/golden/make_tune_table.py on a B200).
+the fixed rules on the committed sweep table
+(blocked-linearized-coordinate_b200/selector/tune_table.npz, made by
+selector/make_tune_table.py on a B200), and the committed trained parameters.
 """
 import os
 import sys
@@ -12,7 +13,7 @@ import pytest
 import torch
 
 import pyoracle as po
-from conftest import GOLDEN, unique_coords
+from conftest import PKG_DIR, unique_coords
 
 sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
 import mlp_oracle as mo  # noqa: E402
@@ -140,9 +141,9 @@ def test_mlp_training_is_deterministic_and_learns(blco):
 
 
 def _table():
-    path = os.path.join(GOLDEN, "tune_table.npz")
+    path = os.path.join(PKG_DIR, "selector", "tune_table.npz")
     if not os.path.exists(path):
-        pytest.fail("tests/golden/tune_table.npz is missing (make it with tests/golden/make_tune_table.py)")
+        pytest.fail("selector/tune_table.npz is missing (make it with selector/make_tune_table.py)")
     return dict(np.load(path))
 
 
@@ -197,3 +198,42 @@ def test_tuned_kernel_in_cpals(blco):
         fits.append(np.array(fk))
     assert np.allclose(fits[0], fits[1], rtol=0, atol=1e-10)
     t.free()
+
+
+def test_committed_selector_is_reproducible_and_used(blco, tmp_path):
+    """selector/selector_params.npz is what selector/train_selector.py makes
+    on this GPU (bit for bit: training is deterministic), the binary copy
+    holds the same parameters, and the default selector drives kernel id 21
+    (MTTKRP within 1e-12 of the oracle)."""
+    import subprocess
+    import sys as _sys
+    from conftest import PKG_DIR
+    out = tmp_path / "p.npz"
+    r = subprocess.run([_sys.executable, os.path.join(PKG_DIR, "selector", "train_selector.py"), "--out", str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    mine = np.load(out)["params"]
+    committed = np.load(os.path.join(PKG_DIR, "selector", "selector_params.npz"))
+    assert np.array_equal(mine, committed["params"])
+    raw = open(os.path.join(PKG_DIR, "selector", "selector_params.bin"), "rb").read()
+    hdr = np.frombuffer(raw[:8], dtype="<i4")
+    assert hdr[0] == int(committed["hidden"]) and hdr[1] == mine.size
+    assert np.array_equal(np.frombuffer(raw[8:], dtype="<f4"), mine)
+    net = blco.default_selector(margin=0.1)
+    try:
+        dims = [30_000, 2_000, 60]
+        cidx, vals, t = _tensor(blco, dims, 200_000, 1.0, 1)
+        R = 32
+        rng = np.random.default_rng(2)
+        fs = [rng.random((d, R)) for d in dims]
+        for mode in range(3):
+            cfg, _ = blco.select(t, mode, R, blco.DTYPE_F64, net, 0.1)
+            assert 0 <= cfg < blco.TUNE_CONFIGS
+            ref = po.mttkrp_coo(cidx, vals, fs, mode)
+            out_t = torch.zeros(dims[mode], R, dtype=torch.float64, device="cuda")
+            blco.mttkrp(t, mode, [torch.from_numpy(f).cuda() for f in fs], out_t,
+                        blco.make_opts(kernel=blco.KERNEL_LEARNED))
+            assert np.linalg.norm(out_t.cpu().numpy() - ref) <= 1e-12 * np.linalg.norm(ref)
+        t.free()
+    finally:
+        blco.selector_set(None)
