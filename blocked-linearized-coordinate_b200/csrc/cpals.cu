@@ -1042,8 +1042,9 @@ int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls)
 // ==================================================================== batch
 // Batched CP-ALS: many independent tensors of uneven nnz, order (1..5 modes)
 // and rank (1..64), decomposed together.  Every step of a sweep is one launch
-// over all tensors: the MTTKRP is one persistent launch over the tiles of all
-// streams (a tile table maps a global tile to its tensor), and the dense steps
+// over all tensors: the MTTKRP is one persistent launch over the chunks of
+// every tensor's row-sorted stream copy (a chunk-offset table maps a global
+// chunk to its tensor), and the dense steps
 // use one CTA per tensor (solve, lambda, Gram reduction, fit) or per row
 // chunk (update, Gram).  Tensor t takes its k-th mode (by descending length)
 // in mode slot k.  Convergence is decided on the device per tensor (a tensor

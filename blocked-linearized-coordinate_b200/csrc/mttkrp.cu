@@ -5,23 +5,27 @@
 // The reference computes this with one-warp CTAs over 32-nonzero tiles
 // (mttkrp_lvl1/lvl2/lvl3/atomic, src/alto_dev.cu:31-1847).  This file keeps
 // the tile-level conflict resolution idea but is laid out for B200:
-//   * persistent CTAs, one per SM (grid = SM count), each owning one
-//     contiguous slice of the ALTO-ordered stream, 24 warps per CTA;
-//   * a warp takes 32 nonzeros, decodes rows with shifts and masks
-//     (alt_pext, src/alto_dev.cu:13-16), looks each output row up in the
-//     mode's heavy-row table once, groups equal output rows with
-//     __match_any_sync and writes the tile in row order into a per-warp
-//     shared staging area as packed 32-byte records (two 16-byte loads per
-//     record; the slot ranges are offset by 16 bytes so concurrent slots hit
-//     different banks);
+//   * persistent CTAs, one per SM (grid = SM count), 24 warps per CTA, each
+//     CTA owning one contiguous slice of a stream (or the tiles dealt
+//     round-robin over the grid's warps);
+//   * the tile kernel (k_mttkrp_vec): a warp takes 32 nonzeros, decodes rows
+//     with shifts and masks (alt_pext, src/alto_dev.cu:13-16), groups equal
+//     output rows with __match_any_sync and writes the tile in row order
+//     into a per-warp shared staging area as packed 32-byte records (two
+//     16-byte loads per record; the slot ranges are offset by 16 bytes so
+//     concurrent slots hit different banks);
 //   * factor rows are gathered with 128-bit loads: R/VEC lanes per nonzero
 //     (VEC = 2 FP64, 4 FP32 or 8 BF16 columns per load), several nonzeros in
 //     flight per warp;
 //   * runs of equal output rows are summed in registers and flushed once:
-//     into a per-CTA FP64 shared-memory accumulator when the row is one of
-//     the mode's heaviest rows (written back once per CTA), or into the whole
-//     output when the mode is short enough to fit (the lvl3 role), otherwise
-//     with global atomics (FP64 red, or 4-wide FP32 vector red).
+//     into a per-CTA FP64 shared-memory accumulator when the mode is short
+//     enough to fit (the lvl3 role) or for heavy rows without a row-grouped
+//     copy, otherwise with global atomics (FP64 red, or 4-wide FP32 vector
+//     red);
+//   * the heavy-row kernel (k_mttkrp_hot) walks a mode's row-grouped copy of
+//     its heaviest rows, keeping FP64 sums in registers until the row
+//     changes; the tile kernel then runs on the mode's cold copy, which is
+//     ordered by row so that a tile spans few rows.
 // Precision policies:
 //   PolicyF64   plain form: FP64 values, factors, accumulation and output;
 //   PolicyF32   mixed form: FP32 values, FP32 factor gathers, FP32 output;
