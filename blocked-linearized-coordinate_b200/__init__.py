@@ -61,7 +61,7 @@ EXPORTS = (
     "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
     "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
     "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_gram_f32",
-    "blco_launch_count",
+    "blco_encode_tns", "blco_parse_decimal", "blco_launch_count",
 )
 
 
@@ -152,6 +152,8 @@ def lib():
         L.blco_selector_set.argtypes = [vp, ctypes.c_float]
         L.blco_select.argtypes = [vp, i32, i32, i32, vp, ctypes.c_float, vp, vp, vp]
         L.blco_gram_f32.argtypes = [vp, u64, i32, vp, i32, i32, vp]
+        L.blco_encode_tns.argtypes = [ctypes.c_char_p, u64, vp, vp, vp]
+        L.blco_parse_decimal.argtypes = [ctypes.c_char_p, i32, vp, vp]
         _lib = L
     return _lib
 
@@ -196,6 +198,11 @@ def _ptrs(ptr_list):
     return (ctypes.c_void_p * len(ptr_list))(*ptr_list)
 
 
+class TnsInfo(ctypes.Structure):
+    _fields_ = [("nmodes", ctypes.c_int), ("dims", ctypes.c_uint64 * 5), ("nnz", ctypes.c_uint64),
+                ("lines", ctypes.c_uint64), ("host_parsed", ctypes.c_uint64)]
+
+
 class Tensor:
     """An encoded BLCO tensor owned by the library."""
 
@@ -232,6 +239,19 @@ class Tensor:
         _check(lib().blco_encode_device(nmodes, dims.ctypes.data, nnz, ptrs, int(d_vals.data_ptr()),
                                         max_block_size, ctypes.byref(o), ctypes.byref(h)))
         return cls(h.value)
+
+    @classmethod
+    def encode_tns(cls, path, max_block_size=0, opts=None):
+        """Parse a .tns file on the GPU and encode it (blco_encode_tns).
+        Returns (Tensor, dict(nmodes, dims, nnz, lines, host_parsed))."""
+        h = ctypes.c_void_p()
+        inf = TnsInfo()
+        o = opts if opts is not None else make_opts()
+        _check(lib().blco_encode_tns(os.fsencode(path), max_block_size, ctypes.byref(o), ctypes.byref(h),
+                                     ctypes.byref(inf)))
+        n = inf.nmodes
+        return cls(h.value), dict(nmodes=n, dims=list(inf.dims[:n]), nnz=inf.nnz, lines=inf.lines,
+                                  host_parsed=inf.host_parsed)
 
     def info(self):
         inf = TensorInfo()
@@ -544,3 +564,13 @@ def default_selector(margin=0.1, path=None):
     selector_set(net, margin)
     _default_net = net
     return net
+
+
+def parse_decimal(text):
+    """The GPU loader's decimal conversion, run on the host:
+    (status, value, consumed); status 0 decided, 1 left to strtod, 2 none."""
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    out = ctypes.c_double()
+    used = ctypes.c_int()
+    st = lib().blco_parse_decimal(b, len(b), ctypes.byref(out), ctypes.byref(used))
+    return st, out.value, used.value

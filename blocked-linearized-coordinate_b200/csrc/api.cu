@@ -489,6 +489,19 @@ int blco_gram_f32(const float* d_U, uint64_t I, int rank, double* d_G, int tenso
                     static_cast<cudaStream_t>(stream));
 }
 
+int blco_encode_tns(const char* path, uint64_t max_block_size, const blco_opts* opts, blco_tensor** out,
+                    blco_tns_info* info)
+{
+    if (!path || !out) return fail(BLCO_ERR_INVALID, "null argument");
+    return encode_tns_impl(path, max_block_size, opts, out, info);
+}
+
+int blco_parse_decimal(const char* s, int len, double* out, int* consumed)
+{
+    if (!s || !out || len < 0) return 2;
+    return parse_decimal_host(s, len, out, consumed);
+}
+
 int blco_batch_last_ms(const blco_batch* b, double* ms)
 {
     if (!b || !ms) return fail(BLCO_ERR_INVALID, "null argument");

@@ -216,6 +216,11 @@ int gram_tc_launch(float* U, uint64_t I, int R, const double* inv, uint16_t* bf1
 // cpals.cu: standalone Gram of a device FP32 matrix (tensor or CUDA cores).
 int gram_f32(float* U, uint64_t I, int R, double* G, bool tensor_cores, int sm, cudaStream_t s);
 
+// tns_parse.cu
+int encode_tns_impl(const char* path, uint64_t max_block_size, const blco_opts* opts, blco_tensor** out,
+                    blco_tns_info* info);
+int parse_decimal_host(const char* s, int len, double* out, int* consumed);
+
 // tune.cu
 int tune_features(const blco_tensor* t, int mode, int rank, int dtype, float* f);
 int tune_sweep(blco_tensor* t, int mode, int rank, int dtype, int reps, cudaStream_t s, float* ms_out);

@@ -55,6 +55,7 @@ static void usage(const char* call)
     fprintf(stderr, "\t--max-block-size     Block size (nonzeros) on the GPU\n");
     fprintf(stderr, "\t--batch              Accepted for compatibility (blocks always run in one launch)\n");
     fprintf(stderr, "\t--selector FILE      Trained schedule selector (selector_params.bin) for -k 21\n");
+    fprintf(stderr, "\t--host-load          Parse the .tns file on the host (default: on the GPU, except with -c / -f)\n");
 }
 
 // Reads a selector parameter file (int32 hidden width, int32 count, then
@@ -82,19 +83,19 @@ static bool load_selector(const std::string& path, int device, blco_mlp** out, s
     return true;
 }
 
-static void print_tensor_info(uint64_t rank, int max_iters, const Coo& X)
+static void print_tensor_info(uint64_t rank, int max_iters, const Coo& X, uint64_t nnz)
 {
     // PrintTensorInfo (src/main.cpp:756-778)
     double cells = 1.0;
     for (auto d : X.dims) cells *= (double)d;
     fprintf(stderr, "# Modes         = %u\n", (unsigned)X.nmodes);
     fprintf(stderr, "Rank            = %llu\n", (unsigned long long)rank);
-    fprintf(stderr, "Sparsity        = %f\n", (double)X.nnz() / cells);
+    fprintf(stderr, "Sparsity        = %f\n", (double)nnz / cells);
     fprintf(stderr, "Max iters       = %d\n", max_iters);
     fprintf(stderr, "Dimensions      = [%llu", (unsigned long long)X.dims[0]);
     for (int i = 1; i < X.nmodes; i++) fprintf(stderr, " X %llu", (unsigned long long)X.dims[i]);
     fprintf(stderr, "]\n");
-    fprintf(stderr, "NNZ             = %llu\n", (unsigned long long)X.nnz());
+    fprintf(stderr, "NNZ             = %llu\n", (unsigned long long)nnz);
 }
 
 // Sequential COO MTTKRP, the reference's -c ground truth
@@ -145,6 +146,7 @@ int main(int argc, char** argv)
         {"kernel-id", 1, nullptr, 'k'},  {"num-partitions", 1, nullptr, 'n'}, {"device", 1, nullptr, 1001},
         {"thread-cf", 1, nullptr, 1002}, {"stream-data", 0, nullptr, 1003}, {"max-block-size", 1, nullptr, 1004},
         {"max_block_size", 1, nullptr, 1004}, {"batch", 0, nullptr, 1005}, {"selector", 1, nullptr, 1006},
+        {"host-load", 0, nullptr, 1007},
         {nullptr, 0, nullptr, 0}};
     int max_iters = 10;
     long long rank = 16;
@@ -153,7 +155,7 @@ int main(int argc, char** argv)
     double epsilon = 1e-5;
     int seed = (int)time(nullptr);
     int save_to_file = 0;
-    bool do_check = false, do_bench = false, stream_data = false, want_dims = false;
+    bool do_check = false, do_bench = false, stream_data = false, want_dims = false, host_load = false;
     int kernel_id = 0;
     const char* omp = getenv("OMP_NUM_THREADS");
     int nthreads = omp && atoi(omp) > 0 ? atoi(omp) : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -186,13 +188,40 @@ int main(int argc, char** argv)
         case 1004: max_block_size = atoll(optarg); if (max_block_size <= 0) { fprintf(stderr, "Invalid -max-block-size: %s.\n", optarg); return 1; } break;
         case 1005: break;
         case 1006: selector_file = optarg; break;
+        case 1007: host_load = true; break;
         default: usage(argv[0]); return 1;
         }
     }
     Coo X;
     std::string err;
+    if (kernel_id != 0 && do_check) max_iters = 1;
+    if (!stream_data) max_block_size = 0; // one block (src/main.cpp:327)
+    blco_opts opts;
+    blco_opts_init(&opts);
+    opts.kernel = kernel_id;
+    opts.nprtn = num_partitions;
+    opts.thread_cf = thread_cf;
+    opts.stream_data = stream_data ? 1 : 0;
+    opts.verbose = 1;
+    opts.device = device;
+    // The text file is parsed and encoded on the GPU unless the host COO
+    // arrays are needed (-c check, -f conversion) or --host-load is given.
+    const bool gpu_load = !text_file.empty() && bin_file.empty() && !do_check && !save_to_file && !host_load &&
+                          kernel_id != 0;
+    blco_tensor* T = nullptr;
+    uint64_t nnz = 0;
     auto t0 = std::chrono::steady_clock::now();
-    if (!bin_file.empty()) {
+    if (gpu_load) {
+        blco_tns_info ti;
+        int st = blco_encode_tns(text_file.c_str(), (uint64_t)max_block_size, &opts, &T, &ti);
+        if (st) {
+            fprintf(stderr, "Error: %s\n", blco_last_error());
+            return 1;
+        }
+        X.nmodes = ti.nmodes;
+        X.dims.assign(ti.dims, ti.dims + ti.nmodes);
+        nnz = ti.nnz;
+    } else if (!bin_file.empty()) {
         if (!read_bin(bin_file, &X, &err)) { fprintf(stderr, "Error: %s\n", err.c_str()); return 1; }
         if (save_to_file && !write_tns(bin_file + ".tns", X, &err)) { fprintf(stderr, "Error: %s\n", err.c_str()); return 1; }
     } else if (!text_file.empty()) {
@@ -204,6 +233,7 @@ int main(int argc, char** argv)
         usage(argv[0]);
         return 1;
     }
+    if (!gpu_load) nnz = X.nnz();
     double t_read = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     printf("[%s]: %.6f s\n", "Reading tensor file", t_read);
     if (kernel_id == 0) {
@@ -212,37 +242,32 @@ int main(int argc, char** argv)
     }
     if (target_mode >= X.nmodes || target_mode < 0) {
         fprintf(stderr, "Invalid -target-mode: %d.\n", target_mode);
+        if (T) blco_tensor_free(T);
         return 1;
     }
-    if (do_check) max_iters = 1;
-    if (!stream_data) max_block_size = 0; // one block (src/main.cpp:327)
 
     blco_mlp* selector = nullptr;
     if (!selector_file.empty() && !load_selector(selector_file, device, &selector, &err)) {
         fprintf(stderr, "Error: %s\n", err.c_str());
         return 1;
     }
-    blco_opts opts;
-    blco_opts_init(&opts);
-    opts.kernel = kernel_id;
-    opts.nprtn = num_partitions;
-    opts.thread_cf = thread_cf;
-    opts.stream_data = stream_data ? 1 : 0;
-    opts.verbose = 1;
-    opts.device = device;
-
-    std::vector<const uint64_t*> cptr(X.nmodes);
-    for (int n = 0; n < X.nmodes; n++) cptr[n] = X.cidx[n].data();
-    blco_tensor* T = nullptr;
-    auto te = std::chrono::steady_clock::now();
-    int st = blco_encode(X.nmodes, X.dims.data(), X.nnz(), cptr.data(), X.vals.data(), (uint64_t)max_block_size, &opts, &T);
-    if (st) return die("BLCO encode", st);
+    if (gpu_load) {
+        printf("BLCO: encode time = %f (s) (parsed and encoded on the GPU with the file)\n", t_read);
+    } else {
+        std::vector<const uint64_t*> cptr(X.nmodes);
+        for (int n = 0; n < X.nmodes; n++) cptr[n] = X.cidx[n].data();
+        auto te = std::chrono::steady_clock::now();
+        int st = blco_encode(X.nmodes, X.dims.data(), X.nnz(), cptr.data(), X.vals.data(), (uint64_t)max_block_size,
+                             &opts, &T);
+        if (st) return die("BLCO encode", st);
+        printf("BLCO: encode time = %f (s)\n", std::chrono::duration<double>(std::chrono::steady_clock::now() - te).count());
+    }
     blco_tensor_info info;
     blco_tensor_get_info(T, &info);
-    printf("BLCO: encode time = %f (s)\n", std::chrono::duration<double>(std::chrono::steady_clock::now() - te).count());
     printf("Total blocks: %llu\n\n", (unsigned long long)info.block_count);
+    int st = BLCO_OK;
 
-    print_tensor_info((uint64_t)rank, max_iters, X);
+    print_tensor_info((uint64_t)rank, max_iters, X, nnz);
     Kruskal M;
     M.nmodes = X.nmodes;
     M.rank = (int)rank;

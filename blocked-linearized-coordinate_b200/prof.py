@@ -6,6 +6,10 @@
   python blocked-linearized-coordinate_b200/prof.py batch --count T [--iters I]
       Batched CP-ALS sweeps over T small tensors of the many-small-tensors
       recipe (FP64); prints device ms per sweep.
+  python blocked-linearized-coordinate_b200/prof.py tns --nnz N --dir D
+      Writes the Zipf(1.1) 2M x 2M x 25k tensor with N nonzeros as a .tns
+      file (cpd64's writer, values as %g) and times cpd64's file-to-BLCO
+      step with the GPU loader and with the host loader (--host-load).
 """
 import argparse
 import importlib.util
@@ -75,6 +79,40 @@ def run_batch(a, pkg, torch):
         t.free()
 
 
+def run_tns(a, pkg, torch):
+    import re
+    import subprocess
+    import numpy as np
+    from blco_b200 import synth
+    dims = [2_000_000, 2_000_000, 25_000]
+    X = synth.zipf_tensor_device(a.nnz, dims, 1.1, seed=0)
+    os.makedirs(a.dir, exist_ok=True)
+    binp = os.path.join(a.dir, "t.bin")
+    with open(binp, "wb") as f:
+        np.array([3], dtype=np.uint64).tofile(f)
+        np.array(dims, dtype=np.uint64).tofile(f)
+        np.array([a.nnz], dtype=np.uint64).tofile(f)
+        for c in X["cidx"]:
+            c.to(torch.int64).cpu().numpy().astype(np.uint64).tofile(f)
+        X["vals"].cpu().numpy().tofile(f)
+    del X
+    cpd = os.path.join(HERE, "bin", "cpd64")
+    subprocess.run([cpd, "-b", binp, "-f", "1"], capture_output=True, text=True)
+    tns = binp + ".tns"
+    size = os.path.getsize(tns)
+    for mode, extra in (("gpu", []), ("host", ["--host-load"])):
+        r = subprocess.run([cpd, "-i", tns, "-k", "10", "-m", "0", "-r", "8", "-x", "1"] + extra,
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            print(mode, "failed:", r.stderr[-500:])
+            continue
+        rd = float(re.search(r"Reading tensor file\]: ([0-9.]+)", r.stdout).group(1))
+        enc = float(re.search(r"encode time = ([0-9.]+)", r.stdout).group(1))
+        total = rd if mode == "gpu" else rd + enc
+        print(f"{mode} loader: {size / 1e9:.2f} GB file, {a.nnz} nonzeros: file to BLCO {total:.3f} s "
+              f"(read {rd:.3f} s, encode {enc:.3f} s)", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -87,12 +125,15 @@ def main():
     b = sub.add_parser("batch")
     b.add_argument("--count", type=int, default=64)
     b.add_argument("--iters", type=int, default=1)
+    tn = sub.add_parser("tns")
+    tn.add_argument("--nnz", type=int, default=50_000_000)
+    tn.add_argument("--dir", default="tns_prof")
     a = ap.parse_args()
     import torch
     pkg = load()
     if os.environ.get("BLCO_LIB"):
         pkg.LIB_PATH = os.environ["BLCO_LIB"]
-    (run_mttkrp if a.cmd == "mttkrp" else run_batch)(a, pkg, torch)
+    {"mttkrp": run_mttkrp, "batch": run_batch, "tns": run_tns}[a.cmd](a, pkg, torch)
 
 
 if __name__ == "__main__":

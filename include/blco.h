@@ -370,6 +370,34 @@ int blco_select(blco_tensor* t, int mode, int rank, int factor_dtype, blco_mlp* 
 int blco_gram_f32(const float* d_U, uint64_t I, int rank, double* d_G, int tensor_cores, int device,
                   void* stream);
 
+/* ---- .tns text loading on the GPU (the reference's read_tns_dims /
+ * read_tns_data, src/sptensor.cpp:74-160, feeding the encoder directly). */
+
+typedef struct blco_tns_info {
+    int nmodes;                     /* fields of the first data line minus one */
+    uint64_t dims[BLCO_MAX_MODES];  /* largest 1-based index per mode */
+    uint64_t nnz;                   /* data lines */
+    uint64_t lines;                 /* lines in the file */
+    uint64_t host_parsed;           /* lines the device left to strtoull / strtod */
+} blco_tns_info;
+
+/* Reads a FROSTT .tns file, parses it on the GPU (same line rules, indices
+ * and values as the host loader: every value is the double strtod gives)
+ * and encodes it as blco_encode_device does; the coordinates never exist on
+ * the host.  info (may be NULL) receives the mode count, lengths, nnz and
+ * line counts.  Errors: BLCO_ERR_IO (open / read), BLCO_ERR_INVALID
+ * (malformed line or index 0, with the line number in blco_last_error()). */
+int blco_encode_tns(const char* path, uint64_t max_block_size, const blco_opts* opts,
+                    blco_tensor** out, blco_tns_info* info);
+
+/* The loader's decimal-to-double conversion run on the host (the code the
+ * GPU runs): parses s[0..len) with strtod's decimal syntax.  Returns 0 with
+ * *out set when it decides the correctly rounded value, 1 when it leaves the
+ * number to strtod (over 19 significant digits, halfway cases, subnormal or
+ * overflowing values, hex / inf / nan), 2 when there is no number;
+ * *consumed = characters used. */
+int blco_parse_decimal(const char* s, int len, double* out, int* consumed);
+
 /* Number of this library's kernels launched by the calling thread since the
  * last reset (for reporting launch counts). */
 uint64_t blco_launch_count(int reset);

@@ -73,9 +73,9 @@ def test_selector_file_errors(tmp_path):
     write_tns(p, np.array([[0, 1], [1, 0], [0, 1]], dtype=np.uint64), np.array([1.0, 2.0]), comments=False)
     bad = tmp_path / "bad.bin"
     bad.write_bytes(b"\x01\x00")
-    r = run(["-i", p, "-k", "21", "--selector", str(bad)])
+    r = run(["-i", p, "-k", "21", "--host-load", "--selector", str(bad)])
     assert r.returncode == 1 and "selector" in r.stderr
-    r = run(["-i", p, "-k", "21", "--selector", str(tmp_path / "missing.bin")])
+    r = run(["-i", p, "-k", "21", "--host-load", "--selector", str(tmp_path / "missing.bin")])
     assert r.returncode == 1 and "cannot open" in r.stderr
 
 
@@ -83,9 +83,11 @@ def test_tns_rejects_bad_input(tmp_path):
     p = str(tmp_path / "bad.tns")
     with open(p, "w") as f:
         f.write("1 2 3 1.0\n0 1 1 2.0\n")
-    r = run(["-i", p, "-k", "10"])
+    r = run(["-i", p, "-k", "10", "--host-load"])
     assert r.returncode == 1 and "1-based" in r.stderr
     r = run(["-i", str(tmp_path / "missing.tns"), "-k", "10"])
+    assert r.returncode == 1 and "cannot open" in r.stderr
+    r = run(["-i", str(tmp_path / "missing.tns"), "-k", "10", "--host-load"])
     assert r.returncode == 1 and "cannot open" in r.stderr
     r = run(["-k", "10"])
     assert r.returncode == 1
@@ -113,6 +115,26 @@ def test_cli_cpals_lines_and_export(tmp_path):
         assert len(lines) == 4 + dims[n] * 4
     with open(f"{out}.lambda.out") as f:
         assert f.read().split()[:3] == ["vector", "1", "4"]
+
+
+@pytest.mark.gpu
+def test_cli_gpu_loader_matches_host_loader(tmp_path):
+    """cpd64 parses .tns files on the GPU by default; the fits equal those of
+    the host loader (--host-load) on the same file and seed."""
+    rng = np.random.default_rng(9)
+    dims = [60, 50, 40]
+    lin = rng.choice(60 * 50 * 40, size=6000, replace=False)
+    cidx = np.array(np.unravel_index(lin, dims), dtype=np.uint64)
+    p = str(tmp_path / "g.tns")
+    write_tns(p, cidx, rng.random(6000))
+    outs = []
+    for extra in ([], ["--host-load"]):
+        r = run(["-i", p, "-k", "10", "-r", "6", "-m", "5", "-e", "0", "-x", "4"] + extra)
+        assert r.returncode == 0, r.stderr
+        outs.append([l for l in r.stdout.splitlines() if l.startswith("--> Iter") or l.startswith("Final fit")])
+        assert "NNZ             = 6000" in r.stderr
+    strip = lambda ls: [l.split("time =")[0] for l in ls]
+    assert strip(outs[0]) == strip(outs[1])
 
 
 @pytest.mark.gpu
