@@ -144,6 +144,170 @@ int orc_blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
     return 0;
 }
 
+/* ---- 128-bit ALTO keys (the cpd128 build, ALTO_MASK_LENGTH=128) ---- */
+
+typedef unsigned __int128 orc_u128;
+
+/* 128-bit deposit / extract, include/bitops.hpp:89-108: the low mask word
+ * takes the first popcount(low word) bits of x, the high word the rest. */
+static orc_u128 orc_pdep128(uint64_t x, orc_u128 mask)
+{
+    uint64_t lo = (uint64_t)mask, hi = (uint64_t)(mask >> 64);
+    int shift = __builtin_popcountll(lo);
+    orc_u128 r = orc_pdep(x, lo);
+    if (shift < 64) r |= (orc_u128)orc_pdep(x >> shift, hi) << 64;
+    return r;
+}
+
+static uint64_t orc_pext128(orc_u128 x, orc_u128 mask)
+{
+    uint64_t lo = (uint64_t)mask, hi = (uint64_t)(mask >> 64);
+    int shift = __builtin_popcountll(lo);
+    uint64_t r = orc_pext((uint64_t)x, lo);
+    if (shift < 64) r |= orc_pext((uint64_t)(x >> 64), hi) << shift;
+    return r;
+}
+
+int orc_alto_masks128(int nmodes, const uint64_t* dims, uint64_t* masks_lo, uint64_t* masks_hi)
+{
+    /* include/alto.hpp:597-695 with a 128-bit LIT: the same ordering and
+     * LSB-first round robin as orc_alto_masks, over up to 128 positions. */
+    int order[ORC_MAX_MODES], bits[ORC_MAX_MODES];
+    int total = 0, maxbits = 0;
+    if (nmodes < 1 || nmodes > ORC_MAX_MODES) return -1;
+    for (int n = 0; n < nmodes; n++) {
+        bits[n] = orc_mode_bits(dims[n]);
+        order[n] = n;
+        total += bits[n];
+        if (bits[n] > maxbits) maxbits = bits[n];
+        masks_lo[n] = masks_hi[n] = 0;
+    }
+    if (total > 128) return -1;
+    for (int i = 1; i < nmodes; i++) {
+        int m = order[i], j = i - 1;
+        while (j >= 0 && bits[order[j]] > bits[m]) { order[j + 1] = order[j]; j--; }
+        order[j + 1] = m;
+    }
+    int shift = 0;
+    for (int level = 0; level < maxbits; level++)
+        for (int k = 0; k < nmodes; k++) {
+            int m = order[k];
+            if (level < bits[m]) {
+                if (shift < 64) masks_lo[m] |= (uint64_t)1 << shift;
+                else masks_hi[m] |= (uint64_t)1 << (shift - 64);
+                shift++;
+            }
+        }
+    return total;
+}
+
+typedef struct {
+    orc_u128 key;
+    uint64_t idx;
+} orc_pair128;
+
+static int orc_pair128_cmp(const void* a, const void* b)
+{
+    const orc_pair128* x = (const orc_pair128*)a;
+    const orc_pair128* y = (const orc_pair128*)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    if (x->idx != y->idx) return x->idx < y->idx ? -1 : 1;
+    return 0;
+}
+
+int orc_blco_encode128(int nmodes, const uint64_t* dims, uint64_t nnz,
+                       const uint64_t* cidx, const double* vals,
+                       uint64_t max_block_size,
+                       uint64_t* coords_out, double* vals_out,
+                       uint64_t* mode_masks_out, int* mode_pos_out,
+                       uint64_t* alto_lo_out, uint64_t* alto_hi_out,
+                       uint64_t* nblocks_out, uint64_t* block_offsets_out,
+                       uint64_t* block_coords_out)
+{
+    orc_u128 amask[ORC_MAX_MODES];
+    int tbits[ORC_MAX_MODES];
+    if (orc_alto_masks128(nmodes, dims, alto_lo_out, alto_hi_out) < 0) return -1;
+    for (int n = 0; n < nmodes; n++) {
+        if (dims[n] == 0) return -1;
+        amask[n] = ((orc_u128)alto_hi_out[n] << 64) | alto_lo_out[n];
+    }
+    /* Fields hold the bits of each mode that lie in the low key word,
+     * include/blco.hpp:222-233. */
+    for (int n = 0; n < nmodes; n++) {
+        tbits[n] = __builtin_popcountll(alto_lo_out[n]);
+        mode_masks_out[n] = (tbits[n] >= 64) ? ~(uint64_t)0 : (((uint64_t)1 << tbits[n]) - 1);
+        mode_pos_out[n] = (n == 0) ? 0 : mode_pos_out[n - 1] + tbits[n - 1];
+    }
+    orc_pair128* pairs = (orc_pair128*)malloc((nnz ? nnz : 1) * sizeof(orc_pair128));
+    if (!pairs) return -1;
+    for (uint64_t i = 0; i < nnz; i++) {
+        orc_u128 key = 0;
+        for (int n = 0; n < nmodes; n++) {
+            uint64_t c = cidx[(uint64_t)n * nnz + i];
+            if (c >= dims[n]) { free(pairs); return -1; }
+            key |= orc_pdep128(c, amask[n]);
+        }
+        pairs[i].key = key;
+        pairs[i].idx = i;
+    }
+    qsort(pairs, nnz, sizeof(orc_pair128), orc_pair128_cmp);
+    /* Re-linearize the low-word bits, include/blco.hpp:274-286. */
+    for (uint64_t i = 0; i < nnz; i++) {
+        uint64_t c = 0;
+        for (int n = 0; n < nmodes; n++)
+            c |= (orc_pext128(pairs[i].key, amask[n]) & mode_masks_out[n]) << mode_pos_out[n];
+        coords_out[i] = c;
+        vals_out[i] = vals[pairs[i].idx];
+    }
+    /* Blocks, include/blco.hpp:244-321: one histogram bucket per value of
+     * the upper key word, in increasing order (the sorted order), each split
+     * into max_block_size slices; block_coords[n] = pext(upper word, upper
+     * mask word of mode n) << (its low-word bit count). */
+    uint64_t B = max_block_size ? max_block_size : nnz;
+    uint64_t nb = 0;
+    for (uint64_t s = 0; s < nnz;) {
+        uint64_t up = (uint64_t)(pairs[s].key >> 64), e = s + 1;
+        while (e < nnz && (uint64_t)(pairs[e].key >> 64) == up) e++;
+        for (uint64_t o = s; o < e; o += B) {
+            block_offsets_out[nb] = o;
+            for (int n = 0; n < nmodes; n++) {
+                uint64_t bc = orc_pext(up, alto_hi_out[n]);
+                block_coords_out[nb * nmodes + n] = tbits[n] >= 64 ? 0 : bc << tbits[n];
+            }
+            nb++;
+        }
+        s = e;
+    }
+    block_offsets_out[nb] = nnz;
+    *nblocks_out = nb;
+    free(pairs);
+    return 0;
+}
+
+void orc_mttkrp_blco128(int nmodes, const uint64_t* mode_masks, const int* mode_pos, uint64_t nblocks,
+                        const uint64_t* block_offsets, const uint64_t* block_coords, const uint64_t* coords,
+                        const double* vals, const double* const* factors, int rank, int mode, double* out)
+{
+    /* Per block, a row index is the field plus the block's coordinate,
+     * alt_pext (src/alto_dev.cu:13-16). */
+    for (uint64_t b = 0; b < nblocks; b++) {
+        const uint64_t* bc = block_coords + b * nmodes;
+        for (uint64_t i = block_offsets[b]; i < block_offsets[b + 1]; i++) {
+            uint64_t c = coords[i];
+            double* o = out + (((c >> mode_pos[mode]) & mode_masks[mode]) | bc[mode]) * (uint64_t)rank;
+            for (int r = 0; r < rank; r++) {
+                double p = vals[i];
+                for (int m = 0; m < nmodes; m++) {
+                    if (m == mode) continue;
+                    uint64_t rid = ((c >> mode_pos[m]) & mode_masks[m]) | bc[m];
+                    p *= factors[m][rid * (uint64_t)rank + r];
+                }
+                o[r] += p;
+            }
+        }
+    }
+}
+
 void orc_mttkrp_coo(int nmodes, uint64_t nnz, const uint64_t* cidx,
                     const double* vals, int rank, const double* const* factors,
                     int mode, double* out)

@@ -62,6 +62,34 @@ int orc_blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
                     uint64_t* alto_masks_out,
                     uint64_t* nblocks_out, uint64_t* block_offsets_out);
 
+/* 128-bit ALTO masks (ALTO_MASK_LENGTH=128, include/alto.hpp:597-695):
+ * low and high mask words per mode.  Returns the total bit count, or -1
+ * above 128 bits. */
+int orc_alto_masks128(int nmodes, const uint64_t* dims, uint64_t* masks_lo, uint64_t* masks_hi);
+
+/* BLCO encoding with 128-bit ALTO keys, gen_blcotensor_host<__uint128_t>
+ * (include/blco.hpp:196-331).  Fields hold each mode's low-key-word bits
+ * (mode_masks_out[n] = (1 << t_n) - 1, t_n = popcount(low mask word));
+ * blocks are the runs of equal upper key words in sorted order, each split
+ * into max_block_size slices, with block_coords_out[b*nmodes + n] =
+ * pext(upper word, upper mask word n) << t_n.  block_offsets_out needs
+ * room for nnz + 1 entries, block_coords_out for nnz * nmodes.  With at
+ * most 64 key bits the result equals orc_blco_encode's. */
+int orc_blco_encode128(int nmodes, const uint64_t* dims, uint64_t nnz,
+                       const uint64_t* cidx, const double* vals,
+                       uint64_t max_block_size,
+                       uint64_t* coords_out, double* vals_out,
+                       uint64_t* mode_masks_out, int* mode_pos_out,
+                       uint64_t* alto_lo_out, uint64_t* alto_hi_out,
+                       uint64_t* nblocks_out, uint64_t* block_offsets_out,
+                       uint64_t* block_coords_out);
+
+/* MTTKRP over a blocked encoding: row = field | block coordinate
+ * (src/alto_dev.cu:13-16); out += (dims[mode] x rank, zeroed by caller). */
+void orc_mttkrp_blco128(int nmodes, const uint64_t* mode_masks, const int* mode_pos, uint64_t nblocks,
+                        const uint64_t* block_offsets, const uint64_t* block_coords, const uint64_t* coords,
+                        const double* vals, const double* const* factors, int rank, int mode, double* out);
+
 /* Sequential COO MTTKRP, include/cpd.hpp:510-544:
  *   out[c_mode(i), :] += val_i * prod_{m != mode} U_m[c_m(i), :]
  * factors[m] row-major dims[m] x rank.  out accumulates (not zeroed). */

@@ -42,6 +42,7 @@ def lib():
         L.orc_pext.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.orc_alto_masks.restype = ctypes.c_int
         L.orc_blco_encode.restype = ctypes.c_int
+        L.orc_blco_encode128.restype = ctypes.c_int
         L.orc_pinv_sym.restype = ctypes.c_int
         L.orc_cpals.restype = ctypes.c_int
         _lib = L
@@ -57,6 +58,7 @@ def ref_lib():
             return None
         R = ctypes.CDLL(path)
         R.ref_blco_encode.restype = ctypes.c_int
+        R.ref_blco_encode128.restype = ctypes.c_int
         R.ref_alto_create.restype = ctypes.c_void_p
         R.ref_alto_create.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int]
         R.ref_alto_mttkrp.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
@@ -123,6 +125,72 @@ def ref_blco_encode(dims, cidx, vals, max_block_size=0):
     r = _encode_with(R.ref_blco_encode, dims, cidx, vals, max_block_size, False)
     r["block_coords"] = r.pop("extra")
     return r
+
+
+def _encode128_with(fn, dims, cidx, vals, max_block_size, oracle):
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    nmodes, nnz = cidx.shape
+    coords = np.zeros(nnz, dtype=np.uint64)
+    ovals = np.zeros(nnz, dtype=np.float64)
+    masks = np.zeros(nmodes, dtype=np.uint64)
+    pos = np.zeros(nmodes, dtype=np.int32)
+    nb = np.zeros(1, dtype=np.uint64)
+    offs = np.zeros(nnz + 2, dtype=np.uint64)
+    bcoords = np.zeros((nnz + 1) * nmodes, dtype=np.uint64)
+    args = [ctypes.c_int(nmodes), _p(dims, _u64p), ctypes.c_uint64(nnz), _p(cidx, _u64p), _p(vals, _f64p),
+            ctypes.c_uint64(max_block_size), _p(coords, _u64p), _p(ovals, _f64p), _p(masks, _u64p),
+            _p(pos, _i32p)]
+    lo = np.zeros(nmodes, dtype=np.uint64)
+    hi = np.zeros(nmodes, dtype=np.uint64)
+    if oracle:
+        args += [_p(lo, _u64p), _p(hi, _u64p)]
+    args += [_p(nb, _u64p), _p(offs, _u64p), _p(bcoords, _u64p)]
+    if fn(*args) != 0:
+        raise ValueError("encode rejected the input")
+    n_blocks = int(nb[0])
+    r = dict(coords=coords, vals=ovals, mode_masks=masks, mode_pos=pos, nblocks=n_blocks,
+             block_offsets=offs[: n_blocks + 1].copy(),
+             block_coords=bcoords[: n_blocks * nmodes].reshape(-1, nmodes).copy())
+    if oracle:
+        r["alto_masks_lo"], r["alto_masks_hi"] = lo, hi
+    return r
+
+
+def blco_encode128(dims, cidx, vals, max_block_size=0):
+    """Oracle encoder with 128-bit ALTO keys (the cpd128 build): coords,
+    vals, mode_masks, mode_pos, nblocks, block_offsets, block_coords,
+    alto_masks_lo / alto_masks_hi."""
+    return _encode128_with(lib().orc_blco_encode128, dims, cidx, vals, max_block_size, True)
+
+
+def ref_blco_encode128(dims, cidx, vals, max_block_size=0):
+    """The reference encoder with 128-bit keys (oracle/_ref)."""
+    R = ref_lib()
+    if R is None:
+        raise FileNotFoundError("oracle/_ref not built")
+    return _encode128_with(R.ref_blco_encode128, dims, cidx, vals, max_block_size, False)
+
+
+def mttkrp_blco128(enc, factors, mode, out=None):
+    """MTTKRP over a blocked encoding (row = field | block coordinate)."""
+    factors = [np.ascontiguousarray(f, dtype=np.float64) for f in factors]
+    rank = factors[0].shape[1]
+    nmodes = len(factors)
+    if out is None:
+        out = np.zeros((factors[mode].shape[0], rank), dtype=np.float64)
+    masks = np.ascontiguousarray(enc["mode_masks"], dtype=np.uint64)
+    pos = np.ascontiguousarray(enc["mode_pos"], dtype=np.int32)
+    offs = np.ascontiguousarray(enc["block_offsets"], dtype=np.uint64)
+    bc = np.ascontiguousarray(enc["block_coords"], dtype=np.uint64).reshape(-1)
+    coords = np.ascontiguousarray(enc["coords"], dtype=np.uint64)
+    vals = np.ascontiguousarray(enc["vals"], dtype=np.float64)
+    lib().orc_mttkrp_blco128(ctypes.c_int(nmodes), _p(masks, _u64p), _p(pos, _i32p),
+                             ctypes.c_uint64(enc["nblocks"]), _p(offs, _u64p), _p(bc, _u64p),
+                             _p(coords, _u64p), _p(vals, _f64p), _ptr_array(factors), ctypes.c_int(rank),
+                             ctypes.c_int(mode), _p(out, _f64p))
+    return out
 
 
 def mttkrp_coo(cidx, vals, factors, mode, out=None):

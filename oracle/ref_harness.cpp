@@ -5,7 +5,8 @@
 // place from the reference checkout (oracle/Makefile, target `ref`).  It
 // exposes a small extern "C" surface so tests and bench.py's CPU-baseline
 // leg can run:
-//   * the reference BLCO encoder gen_blcotensor_host<uint64>
+//   * the reference BLCO encoder gen_blcotensor_host<uint64> and, for the
+//     cpd128 build's 128-bit keys, <unsigned __int128>
 //     (include/blco.hpp:196-331),
 //   * the reference sequential COO MTTKRP, the -c check oracle
 //     (include/cpd.hpp:510-544),
@@ -86,15 +87,16 @@ static SparseTensor* refh_make_tensor(int nmodes, const uint64_t* dims, uint64_t
     return X;
 }
 
-extern "C" int ref_blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
-                               const uint64_t* cidx, const double* vals,
-                               uint64_t max_block_size, uint64_t* coords_out,
-                               double* vals_out, uint64_t* mode_masks_out,
-                               int* mode_pos_out, uint64_t* nblocks_out,
-                               uint64_t* block_offsets_out, uint64_t* block_coords_out)
+template <typename LIT>
+static int refh_blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
+                            const uint64_t* cidx, const double* vals,
+                            uint64_t max_block_size, uint64_t* coords_out,
+                            double* vals_out, uint64_t* mode_masks_out,
+                            int* mode_pos_out, uint64_t* nblocks_out,
+                            uint64_t* block_offsets_out, uint64_t* block_coords_out)
 {
     SparseTensor* X = refh_make_tensor(nmodes, dims, nnz, cidx, vals);
-    blcotensor* T = gen_blcotensor_host<unsigned long long>(X, max_block_size);
+    blcotensor* T = gen_blcotensor_host<LIT>(X, max_block_size);
     memcpy(coords_out, T->coords, sizeof(uint64_t) * nnz);
     memcpy(vals_out, T->values, sizeof(double) * nnz);
     for (int n = 0; n < nmodes; n++) {
@@ -119,6 +121,34 @@ extern "C" int ref_blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
     delete T;
     DestroySparseTensor(X);
     return 0;
+}
+
+extern "C" int ref_blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
+                               const uint64_t* cidx, const double* vals,
+                               uint64_t max_block_size, uint64_t* coords_out,
+                               double* vals_out, uint64_t* mode_masks_out,
+                               int* mode_pos_out, uint64_t* nblocks_out,
+                               uint64_t* block_offsets_out, uint64_t* block_coords_out)
+{
+    return refh_blco_encode<unsigned long long>(nmodes, dims, nnz, cidx, vals, max_block_size, coords_out,
+                                                vals_out, mode_masks_out, mode_pos_out, nblocks_out,
+                                                block_offsets_out, block_coords_out);
+}
+
+// The cpd128 build's encoder (ALTO_MASK_LENGTH=128): gen_blcotensor_host
+// with 128-bit ALTO keys.  block_offsets_out needs nnz + 1 entries and
+// block_coords_out nnz * nmodes (one block per distinct upper key word and
+// max_block_size slice).
+extern "C" int ref_blco_encode128(int nmodes, const uint64_t* dims, uint64_t nnz,
+                                  const uint64_t* cidx, const double* vals,
+                                  uint64_t max_block_size, uint64_t* coords_out,
+                                  double* vals_out, uint64_t* mode_masks_out,
+                                  int* mode_pos_out, uint64_t* nblocks_out,
+                                  uint64_t* block_offsets_out, uint64_t* block_coords_out)
+{
+    return refh_blco_encode<unsigned __int128>(nmodes, dims, nnz, cidx, vals, max_block_size, coords_out,
+                                               vals_out, mode_masks_out, mode_pos_out, nblocks_out,
+                                               block_offsets_out, block_coords_out);
 }
 
 extern "C" void ref_mttkrp_coo(int nmodes, const uint64_t* dims, uint64_t nnz,

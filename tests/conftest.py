@@ -76,6 +76,17 @@ def unique_coords(rng, dims, nnz, zipf=None):
     return out
 
 
+def unique_coords_wide(rng, dims, nnz):
+    """nnz distinct uniform coordinates for modes whose product exceeds
+    2^63 (no linearized integer key), in first-drawn order."""
+    dims = [int(d) for d in dims]
+    c = np.stack([rng.integers(0, d, size=2 * nnz + 64, dtype=np.uint64) for d in dims])
+    _, first = np.unique(c, axis=1, return_index=True)
+    first = np.sort(first)
+    assert len(first) >= nnz
+    return np.ascontiguousarray(c[:, first[:nnz]])
+
+
 def gpu_available():
     try:
         import torch

@@ -7,11 +7,15 @@ Runs the reference's own CPU code, compiled from its sources by
   * the sequential COO MTTKRP (include/cpd.hpp:510-544) for every mode;
   * KruskalModelRandomInit (src/kruskal_model.cpp:93-110) under a stated
     OpenMP thread count.
+The w128_* cases come from the cpd128 build's encoder,
+gen_blcotensor_host<unsigned __int128>, on tensors whose coordinates need
+more than 64 key bits (several blocks with non-zero block coordinates).
 Inputs are seeded synthetic tensors (unique coordinates; the reference leaves
 the order of duplicate coordinates unspecified).  Usage, from the repo root:
 
     make -C oracle && make -C oracle ref
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py --wide     # only the w128_* fixtures
 """
 import json
 import os
@@ -76,6 +80,55 @@ CASES = [
 ]
 
 
+WIDE_CASES = [
+    # name, dims, nnz, max_block_size, rank (0: encoder only), zipf
+    ("w128_5mode", [9000, 8500, 8200, 8192, 8300], 3000, 100, 4, None),
+    ("w128_4mode", [131073, 131072, 100000, 70000], 4000, 0, 8, None),
+    ("w128_zipf5", [9000, 9000, 9000, 70000, 600], 3000, 64, 6, 0.9),
+    ("w128_long", [(1 << 31) + 5, 1 << 31, 17], 2500, 7, 0, None),
+]
+
+
+def ref_mttkrp(dims, cidx, vals, factors, m):
+    """The reference COO MTTKRP (include/cpd.hpp:510-544) of mode m; the
+    reference accumulates into U[m], so it gets a zeroed copy."""
+    import ctypes
+    fs = [f.copy() for f in factors]
+    fs[m][:] = 0.0
+    arrs = [np.ascontiguousarray(f) for f in fs]
+    ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    d64 = np.ascontiguousarray(dims, dtype=np.uint64)
+    po.ref_lib().ref_mttkrp_coo(ctypes.c_int(len(dims)), d64.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                ctypes.c_uint64(cidx.shape[1]),
+                                cidx.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                vals.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                ctypes.c_int(factors[0].shape[1]), ptrs, ctypes.c_int(m))
+    return arrs[m]
+
+
+def wide_main():
+    rng = np.random.default_rng(20240602)
+    index = []
+    for name, dims, nnz, B, rank, zipf in WIDE_CASES:
+        cidx = unique_coords(rng, dims, nnz, zipf)
+        vals = rng.uniform(0.0, 1.0, size=cidx.shape[1])
+        r = po.ref_blco_encode128(dims, cidx, vals, B)
+        payload = dict(dims=np.array(dims, dtype=np.uint64), cidx=cidx, vals=vals,
+                       max_block_size=np.uint64(B), rank=np.int64(rank),
+                       coords=r["coords"], out_vals=r["vals"], mode_masks=r["mode_masks"],
+                       mode_pos=r["mode_pos"], block_offsets=r["block_offsets"],
+                       block_coords=r["block_coords"])
+        if rank:
+            factors = formula_factors(dims, rank)
+            for m in range(len(dims)):
+                payload[f"mttkrp{m}"] = ref_mttkrp(dims, cidx, vals, factors, m)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **payload)
+        index.append(dict(name=name, dims=dims, nnz=int(cidx.shape[1]), max_block_size=B, rank=rank,
+                          zipf=zipf, nblocks=int(r["nblocks"]), key_bits=int(sum(int(d - 1).bit_length()
+                                                                                   for d in dims))))
+    return index
+
+
 def kat_inputs():
     pts = [(4, 2, 8, 1.0), (0, 0, 0, 2.0), (1, 2, 3, 3.0), (3, 1, 0, 4.0), (2, 0, 5, 5.0), (0, 1, 7, 6.0)]
     cidx = np.array([[p[n] for p in pts] for n in range(3)], dtype=np.uint64)
@@ -86,6 +139,15 @@ def kat_inputs():
 def main():
     if po.ref_lib() is None:
         sys.exit("oracle/_ref not built: run `make -C oracle ref` first")
+    if "--wide" in sys.argv[1:]:
+        path = os.path.join(HERE, "index.json")
+        with open(path) as f:
+            doc = json.load(f)
+        doc["wide_cases"] = wide_main()
+        with open(path, "w") as f:
+            json.dump(doc, f, indent=1)
+        print("wrote", len(doc["wide_cases"]), "wide cases")
+        return
     rng = np.random.default_rng(20240601)
     index = []
     for name, dims, nnz, B, rank, zipf in CASES:
@@ -142,7 +204,7 @@ def main():
                           dims=[7, 13, 5], rank=6))
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(dict(generator="tests/golden/make_golden.py", source="reference CPU code via oracle/_ref",
-                       cases=index, inits=inits), f, indent=1)
+                       cases=index, inits=inits, wide_cases=wide_main()), f, indent=1)
     print("wrote", len(index), "cases and", len(inits), "init fixtures")
 
 
