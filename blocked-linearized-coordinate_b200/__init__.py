@@ -99,6 +99,7 @@ class TensorInfo(ctypes.Structure):
         ("alto_bits", ctypes.c_int),
         ("device", ctypes.c_int),
         ("resident", ctypes.c_int),
+        ("alto_masks_hi", ctypes.c_uint64 * MAX_MODES),
     ]
 
 
@@ -260,7 +261,8 @@ class Tensor:
         return dict(nmodes=n, dims=list(inf.dims[:n]), nnz=inf.nnz, block_count=inf.block_count,
                     max_block_size=inf.max_block_size, mode_masks=list(inf.mode_masks[:n]),
                     mode_pos=list(inf.mode_pos[:n]), alto_masks=list(inf.alto_masks[:n]),
-                    alto_bits=inf.alto_bits, device=inf.device, resident=bool(inf.resident))
+                    alto_masks_hi=list(inf.alto_masks_hi[:n]), alto_bits=inf.alto_bits, device=inf.device,
+                    resident=bool(inf.resident))
 
     def copy_out(self):
         inf = self.info()

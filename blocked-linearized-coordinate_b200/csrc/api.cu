@@ -182,6 +182,12 @@ int blco_tensor_free(blco_tensor* t)
     cudaFree(t->d_coords);
     cudaFree(t->d_values);
     cudaFree(t->d_values_f32);
+    cudaFree(t->d_bfield);
+    for (auto& w : t->wide_copy) {
+        cudaFree(w.d_coords);
+        cudaFree(w.d_field);
+        cudaFree(w.d_vals);
+    }
     if (t->h_coords) cudaFreeHost(t->h_coords);
     if (t->h_values) cudaFreeHost(t->h_values);
     for (int n = 0; n < BLCO_MAX_MODES; n++) {
@@ -211,6 +217,7 @@ int blco_tensor_get_info(const blco_tensor* t, blco_tensor_info* info)
         info->mode_masks[n] = t->layout.mode_masks[n];
         info->mode_pos[n] = t->layout.mode_pos[n];
         info->alto_masks[n] = t->layout.alto_masks[n];
+        info->alto_masks_hi[n] = t->layout.alto_masks_hi[n];
     }
     info->nnz = t->nnz;
     info->block_count = t->block_count;
@@ -234,6 +241,11 @@ int blco_tensor_copy_out(const blco_tensor* t, uint64_t* coords, double* values,
             if (coords) memcpy(coords, t->h_coords, t->nnz * 8);
             if (values) memcpy(values, t->h_values, t->nnz * 8);
         }
+    }
+    if (t->layout.wide) {
+        if (block_offsets) memcpy(block_offsets, t->block_offsets.data(), (t->block_count + 1) * sizeof(uint64_t));
+        if (block_coords) memcpy(block_coords, t->block_coords.data(), t->block_coords.size() * sizeof(uint64_t));
+        return BLCO_OK;
     }
     const uint64_t B = t->max_block_size ? t->max_block_size : t->nnz;
     if (block_offsets) {
@@ -293,6 +305,7 @@ int blco_mttkrp_ex(blco_tensor* t, int mode, int rank, int factor_dtype, const v
     if (mode < 0 || mode >= t->layout.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
     if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
     if (!t->resident) return fail(BLCO_ERR_UNSUPPORTED, "mixed-precision MTTKRP needs a resident tensor");
+    if (t->layout.wide) return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits: the MTTKRP is FP64 only");
     for (int m = 0; m < t->layout.nmodes; m++)
         if (m != mode && !d_factors[m]) return fail(BLCO_ERR_INVALID, "null factor matrix");
     BLCO_CUDA(cudaSetDevice(t->device));

@@ -829,6 +829,8 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     if (rank < 1 || rank > MAX_SOLVE_R) return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS rank must be 1..96");
     if (!t->resident && opts && opts->precision != BLCO_PRECISION_FP64)
         return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS on a streamed tensor runs the FP64 form only");
+    if (t->layout.wide && opts && opts->precision != BLCO_PRECISION_FP64)
+        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS with keys above 64 bits runs the FP64 form only");
     blco_cpals_plan* p = new blco_cpals_plan();
     p->t = t;
     p->R = rank;
@@ -982,6 +984,10 @@ int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda,
                const blco_opts* opts, double* fit_out, double* fits, int* iters_out)
 {
     if (!t || !factors || !lambda) return fail(BLCO_ERR_INVALID, "null argument");
+    // forms the plan rejects are rejected before any factor is copied
+    if (opts && opts->precision != BLCO_PRECISION_FP64 && (!t->resident || t->layout.wide))
+        return fail(BLCO_ERR_UNSUPPORTED, t->layout.wide ? "CP-ALS with keys above 64 bits runs the FP64 form only"
+                                                         : "CP-ALS on a streamed tensor runs the FP64 form only");
     const int N = t->layout.nmodes;
     cudaStream_t s = pick_stream(t, opts);
     double* dU[BLCO_MAX_MODES] = {};
@@ -1632,6 +1638,8 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
     for (int t = 0; t < T; t++) {
         if (!tensors[t] || !d_factors[t] || !d_lambdas[t]) return fail(BLCO_ERR_INVALID, "null tensor or factors");
         if (!tensors[t]->resident) return fail(BLCO_ERR_UNSUPPORTED, "batched CP-ALS needs resident tensors");
+        if (tensors[t]->layout.wide)
+            return fail(BLCO_ERR_UNSUPPORTED, "batched CP-ALS takes keys of at most 64 bits");
         if (tensors[t]->device != device) return fail(BLCO_ERR_INVALID, "all tensors must be on one device");
         if (ranks[t] < 1 || ranks[t] > BATCH_MAX_R) return fail(BLCO_ERR_UNSUPPORTED, "batched rank must be 1..64");
         for (int n = 0; n < tensors[t]->layout.nmodes; n++)

@@ -37,19 +37,34 @@ int make_layout(int nmodes, const uint64_t* dims, Layout* L)
         maxbits = std::max(maxbits, bits[n]);
         order[n] = n;
     }
-    if (total > 64) return fail(BLCO_ERR_UNSUPPORTED, "coordinates need more than 64 bits (128-bit BLCO not built)");
+    // 128 bits is the widest key of the reference (ALTO_MASK_LENGTH=128,
+    // include/alto.hpp:634).
+    if (total > 128) return fail(BLCO_ERR_UNSUPPORTED, "coordinates need more than 128 key bits");
     // Shortest mode first, ties in natural order; LSB-first round robin over
-    // bit levels (include/alto.hpp:659-685).
+    // bit levels (include/alto.hpp:659-685), positions 64..127 in the upper
+    // key word.
     std::stable_sort(order, order + nmodes, [&](int a, int b) { return bits[a] < bits[b]; });
     int shift = 0;
     for (int level = 0; level < maxbits; level++)
         for (int k = 0; k < nmodes; k++)
-            if (level < bits[order[k]]) L->alto_masks[order[k]] |= 1ull << shift++;
+            if (level < bits[order[k]]) {
+                if (shift < 64) L->alto_masks[order[k]] |= 1ull << shift;
+                else L->alto_masks_hi[order[k]] |= 1ull << (shift - 64);
+                shift++;
+            }
+    // Fields of the low-word bits, include/blco.hpp:222-233 (all bits when
+    // the key fits 64 bits); block fields of the rest.
     for (int n = 0; n < nmodes; n++) {
-        L->mode_masks[n] = bits[n] >= 64 ? ~0ull : ((1ull << bits[n]) - 1);
-        L->mode_pos[n] = n == 0 ? 0 : L->mode_pos[n - 1] + bits[n - 1];
+        const int lb = __builtin_popcountll(L->alto_masks[n]);
+        const int hb = bits[n] - lb;
+        L->low_bits[n] = lb;
+        L->mode_masks[n] = lb >= 64 ? ~0ull : ((1ull << lb) - 1);
+        L->mode_pos[n] = n == 0 ? 0 : L->mode_pos[n - 1] + L->low_bits[n - 1];
+        L->bmask[n] = hb >= 64 ? ~0ull : ((1ull << hb) - 1);
+        L->bpos[n] = n == 0 ? 0 : L->bpos[n - 1] + (bits[n - 1] - L->low_bits[n - 1]);
     }
     L->alto_bits = total;
+    L->wide = total > 64;
     return BLCO_OK;
 }
 
@@ -561,7 +576,336 @@ __global__ void k_sumsq(const double* __restrict__ v, uint64_t n, double* __rest
     }
 }
 
+// ------------------------------------------------------------ wide keys --
+//
+// Keys of 65..128 bits (the reference's 128-bit build, gen_blcotensor_host
+// <unsigned __int128>, include/blco.hpp:196-331).  The key is a low and an
+// upper 64-bit word; the order is (upper, low), so two stable radix sorts
+// of an index permutation run: by the low word, then by the upper word.
+// The BLCO arrays are then gathered straight from the COO input: fields of
+// the low-word bits, the values, and the block field (Layout).  Blocks are
+// the runs of equal upper words (the reference's histogram buckets, in
+// increasing order), split into max_block_size slices.
+
+// lo[n][b][v] / hi[n][b][v]: the low / upper key word bits of coordinate
+// byte b of mode n with value v.
+struct WideTables {
+    uint64_t lo[BLCO_MAX_MODES][4][256];
+    uint64_t hi[BLCO_MAX_MODES][4][256];
+};
+
+WideTables make_wide_tables(const Layout& L)
+{
+    WideTables T;
+    memset(&T, 0, sizeof(T));
+    for (int n = 0; n < L.nmodes; n++) {
+        // key position of coordinate bit j: the j-th set bit of the 128-bit mask
+        int posn[64];
+        int j = 0;
+        for (int p = 0; p < 128; p++) {
+            const uint64_t w = p < 64 ? L.alto_masks[n] : L.alto_masks_hi[n];
+            if (w >> (p & 63) & 1) posn[j++] = p;
+        }
+        for (int b = 0; b < 4; b++)
+            for (int v = 0; v < 256; v++)
+                for (int k = 0; k < 8; k++) {
+                    const int bit = 8 * b + k;
+                    if (bit >= j || !(v >> k & 1)) continue;
+                    if (posn[bit] < 64) T.lo[n][b][v] |= 1ull << posn[bit];
+                    else T.hi[n][b][v] |= 1ull << (posn[bit] - 64);
+                }
+    }
+    return T;
+}
+
+__global__ void k_wide_keys(CooPtrs coo, uint64_t nnz, Layout L, const WideTables* __restrict__ tabs,
+                            uint64_t* __restrict__ lo, uint64_t* __restrict__ idx, uint64_t* __restrict__ hi,
+                            int* __restrict__ bad)
+{
+    extern __shared__ __align__(16) unsigned char wk_smem[];
+    WideTables* T = reinterpret_cast<WideTables*>(wk_smem);
+    const uint4* src = reinterpret_cast<const uint4*>(tabs);
+    uint4* dst = reinterpret_cast<uint4*>(wk_smem);
+    for (int i = threadIdx.x; i < (int)(sizeof(WideTables) / 16); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t kl = 0, kh = 0;
+        bool ok = true;
+#pragma unroll
+        for (int n = 0; n < BLCO_MAX_MODES; n++) {
+            if (n < L.nmodes) {
+                const uint64_t c = coo.c[n][i];
+                ok &= c < L.dims[n];
+#pragma unroll
+                for (int b = 0; b < 4; b++) {
+                    const uint32_t v = (uint32_t)(c >> (8 * b)) & 255;
+                    kl |= T->lo[n][b][v];
+                    kh |= T->hi[n][b][v];
+                }
+            }
+        }
+        if (!ok) atomicExch(bad, 1);
+        lo[i] = kl;
+        idx[i] = i;
+        hi[i] = kh;
+    }
+}
+
+__global__ void k_gather_u64(const uint64_t* __restrict__ src, const uint64_t* __restrict__ idx, uint64_t n,
+                             uint64_t* __restrict__ dst)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+
+// BLCO arrays at sorted position i from the COO entry idx[i]; flags[i] = 1
+// where a run of equal upper words starts.
+__global__ void k_wide_finish(CooPtrs coo, const double* __restrict__ vals, const uint64_t* __restrict__ idx,
+                              const uint64_t* __restrict__ hi, uint64_t nnz, Layout L, uint64_t* __restrict__ coords,
+                              double* __restrict__ vout, uint64_t* __restrict__ field, uint32_t* __restrict__ flags)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t src = idx[i];
+        uint64_t c = 0, f = 0;
+#pragma unroll
+        for (int n = 0; n < BLCO_MAX_MODES; n++) {
+            if (n < L.nmodes) {
+                const uint64_t x = coo.c[n][src];
+                c |= (x & L.mode_masks[n]) << L.mode_pos[n];
+                f |= (x >> L.low_bits[n]) << L.bpos[n];
+            }
+        }
+        coords[i] = c;
+        vout[i] = vals[src];
+        field[i] = f;
+        flags[i] = (i == 0 || hi[i] != hi[i - 1]) ? 1u : 0u;
+    }
+}
+
+__global__ void k_wide_runs(const uint32_t* __restrict__ rank, const uint64_t* __restrict__ hi,
+                            const uint64_t* __restrict__ field, uint64_t nnz, uint64_t* __restrict__ run_start,
+                            uint64_t* __restrict__ run_field)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (i == 0 || hi[i] != hi[i - 1]) {
+            run_start[rank[i]] = i;
+            run_field[rank[i]] = field[i];
+        }
+    }
+}
+
+// key[i] = row of mode n of nonzero i, idx[i] = i.
+__global__ void k_wide_row_keys(const uint64_t* __restrict__ coords, const uint64_t* __restrict__ field,
+                                uint64_t nnz, Layout L, int n, uint64_t* __restrict__ key, uint64_t* __restrict__ idx)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        key[i] = wide_row(L, n, coords[i], field[i]);
+        idx[i] = i;
+    }
+}
+
+__global__ void k_gather3(const uint64_t* __restrict__ idx, uint64_t n, const uint64_t* __restrict__ a,
+                          const uint64_t* __restrict__ b, const double* __restrict__ c, uint64_t* __restrict__ oa,
+                          uint64_t* __restrict__ ob, double* __restrict__ oc)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t j = idx[i];
+        oa[i] = a[j];
+        ob[i] = b[j];
+        oc[i] = c[j];
+    }
+}
+
 } // namespace
+
+// Per-mode copies of a wide-key stream sorted by that mode's row (stable:
+// key order inside a row), so that the MTTKRP of mode n sums each row's
+// nonzeros in registers and writes it once per warp task.
+static int build_wide_copies(blco_tensor* t, cudaStream_t s, const DeviceInfo& di)
+{
+    const uint64_t nnz = t->nnz;
+    const Layout& L = t->layout;
+    if (nnz == 0) return BLCO_OK;
+    uint64_t* tmp[4] = {};
+    auto release = [&]() {
+        cudaStreamSynchronize(s);
+        for (auto& b : tmp) { cudaFree(b); b = nullptr; }
+    };
+    for (auto& b : tmp) {
+        cudaError_t e = cudaMalloc(&b, nnz * 8);
+        if (e != cudaSuccess) { release(); return cuda_fail(e, "wide copy scratch", __FILE__, __LINE__); }
+    }
+    const int grid = (int)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)di.sm_count * 8);
+    for (int n = 0; n < L.nmodes; n++) {
+        const int bits = L.low_bits[n] + __builtin_popcountll(L.alto_masks_hi[n]);
+        k_wide_row_keys<<<grid, 256, 0, s>>>(t->d_coords, t->d_bfield, nnz, L, n, tmp[0], tmp[1]);
+        count_launch();
+        bool alt = false;
+        int st = radix_sort_pairs(tmp[0], reinterpret_cast<double*>(tmp[1]), tmp[2], reinterpret_cast<double*>(tmp[3]),
+                                  nnz, 0, bits, s, &alt);
+        if (st != BLCO_OK) { release(); return st; }
+        const uint64_t* idx = alt ? tmp[3] : tmp[1];
+        blco_tensor::WideCopy& w = t->wide_copy[n];
+        cudaError_t e = cudaMalloc(&w.d_coords, nnz * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&w.d_field, nnz * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&w.d_vals, nnz * 8);
+        if (e != cudaSuccess) { release(); return cuda_fail(e, "wide copy", __FILE__, __LINE__); }
+        k_gather3<<<grid, 256, 0, s>>>(idx, nnz, t->d_coords, t->d_bfield, t->d_values, w.d_coords, w.d_field,
+                                       w.d_vals);
+        count_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { release(); return cuda_fail(e, "k_gather3", __FILE__, __LINE__); }
+    }
+    release();
+    return BLCO_OK;
+}
+
+// Wide-key encode of the resident stream: fills t->d_coords, d_values,
+// d_bfield, block_offsets, block_coords, block_count and norm_sq.
+static int encode_wide(blco_tensor* t, const uint64_t* const* d_cidx, const double* d_vals, cudaStream_t s,
+                       const DeviceInfo& di)
+{
+    const uint64_t nnz = t->nnz;
+    const Layout& L = t->layout;
+    if (nnz == 0) return BLCO_OK;
+    uint64_t* buf[5] = {};      // k0, v0, k1, v1, hi
+    uint32_t* flags = nullptr;  // nnz + 1
+    int* d_bad = nullptr;
+    WideTables* d_tabs = nullptr;
+    uint64_t *run_start = nullptr, *run_field = nullptr;
+    int st = BLCO_OK;
+    auto release = [&]() {
+        cudaStreamSynchronize(s);
+        for (uint64_t*& b : buf) { cudaFree(b); b = nullptr; }
+        cudaFree(flags);
+        cudaFree(d_bad);
+        cudaFree(d_tabs);
+        cudaFree(run_start);
+        cudaFree(run_field);
+    };
+#define WIDE_CUDA(call)                                                         \
+    do {                                                                        \
+        cudaError_t _e = (call);                                                \
+        if (_e != cudaSuccess) {                                                \
+            int _s = cuda_fail(_e, #call, __FILE__, __LINE__);                  \
+            release();                                                          \
+            return _s;                                                          \
+        }                                                                       \
+    } while (0)
+    for (auto& b : buf) WIDE_CUDA(cudaMalloc(&b, nnz * 8));
+    WIDE_CUDA(cudaMalloc(&flags, (nnz + 1) * sizeof(uint32_t)));
+    WIDE_CUDA(cudaMalloc(&d_bad, sizeof(int)));
+    WIDE_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+    WIDE_CUDA(cudaMemsetAsync(flags + nnz, 0, sizeof(uint32_t), s));
+    {
+        WideTables* h = new WideTables(make_wide_tables(L));
+        cudaError_t e = cudaMalloc(&d_tabs, sizeof(WideTables));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_tabs, h, sizeof(WideTables), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        delete h;
+        WIDE_CUDA(e);
+    }
+    CooPtrs coo;
+    memset(&coo, 0, sizeof(coo));
+    for (int n = 0; n < L.nmodes; n++) coo.c[n] = d_cidx[n];
+    const int grid = (int)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)di.sm_count * 8);
+    WIDE_CUDA(cudaFuncSetAttribute(k_wide_keys, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WideTables)));
+    k_wide_keys<<<grid, 256, sizeof(WideTables), s>>>(coo, nnz, L, d_tabs, buf[0], buf[1], buf[4], d_bad);
+    count_launch();
+    WIDE_CUDA(cudaGetLastError());
+    int bad = 0;
+    WIDE_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    WIDE_CUDA(cudaStreamSynchronize(s));
+    if (bad) {
+        release();
+        return fail(BLCO_ERR_INVALID, "a coordinate is not below its mode length");
+    }
+    // (low word, index) by the low word, then (upper word, index) by the
+    // upper word: the index order of the 128-bit key, ties in input order.
+    bool alt = false;
+    double* v0 = reinterpret_cast<double*>(buf[1]);
+    double* v1 = reinterpret_cast<double*>(buf[3]);
+    if ((st = radix_sort_pairs(buf[0], v0, buf[2], v1, nnz, 0, 64, s, &alt)) != BLCO_OK) { release(); return st; }
+    uint64_t* kA = alt ? buf[2] : buf[0];
+    uint64_t* iA = alt ? buf[3] : buf[1];
+    uint64_t* kB = alt ? buf[0] : buf[2];
+    uint64_t* iB = alt ? buf[1] : buf[3];
+    k_gather_u64<<<grid, 256, 0, s>>>(buf[4], iA, nnz, kA);
+    count_launch();
+    WIDE_CUDA(cudaGetLastError());
+    if ((st = radix_sort_pairs(kA, reinterpret_cast<double*>(iA), kB, reinterpret_cast<double*>(iB), nnz, 0,
+                               L.alto_bits - 64, s, &alt)) != BLCO_OK) {
+        release();
+        return st;
+    }
+    uint64_t* hiF = alt ? kB : kA;  // sorted upper words
+    uint64_t* idxF = alt ? iB : iA; // sorted permutation
+    uint64_t* outC = alt ? kA : kB; // free now
+    uint64_t* outV = alt ? iA : iB;
+    uint64_t* outF = buf[4];
+    k_wide_finish<<<grid, 256, 0, s>>>(coo, d_vals, idxF, hiF, nnz, L, outC, reinterpret_cast<double*>(outV), outF,
+                                       flags);
+    count_launch();
+    WIDE_CUDA(cudaGetLastError());
+    uint32_t* sums = nullptr;
+    {
+        const uint64_t nsums = (nnz + 1 + SC_CHUNK - 1) / SC_CHUNK + 1;
+        WIDE_CUDA(cudaMallocAsync(&sums, nsums * sizeof(uint32_t), s));
+        st = scan_u32(flags, nnz + 1, sums, s);
+        cudaFreeAsync(sums, s);
+        if (st != BLCO_OK) { release(); return st; }
+    }
+    uint32_t nruns = 0;
+    WIDE_CUDA(cudaMemcpyAsync(&nruns, flags + nnz, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    WIDE_CUDA(cudaStreamSynchronize(s));
+    WIDE_CUDA(cudaMalloc(&run_start, (uint64_t)nruns * 8));
+    WIDE_CUDA(cudaMalloc(&run_field, (uint64_t)nruns * 8));
+    k_wide_runs<<<grid, 256, 0, s>>>(flags, hiF, outF, nnz, run_start, run_field);
+    count_launch();
+    WIDE_CUDA(cudaGetLastError());
+    std::vector<uint64_t> hs(nruns), hf(nruns);
+    WIDE_CUDA(cudaMemcpyAsync(hs.data(), run_start, (uint64_t)nruns * 8, cudaMemcpyDeviceToHost, s));
+    WIDE_CUDA(cudaMemcpyAsync(hf.data(), run_field, (uint64_t)nruns * 8, cudaMemcpyDeviceToHost, s));
+    // sum of squared values (the partial sums reuse the sorted-index buffer)
+    const int g2 = std::min(grid, 1024);
+    k_sumsq<<<g2, 256, 0, s>>>(reinterpret_cast<const double*>(outV), nnz, reinterpret_cast<double*>(idxF));
+    count_launch();
+    WIDE_CUDA(cudaGetLastError());
+    std::vector<double> hp(g2);
+    WIDE_CUDA(cudaMemcpyAsync(hp.data(), idxF, g2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    WIDE_CUDA(cudaStreamSynchronize(s));
+#undef WIDE_CUDA
+    double ss = 0.0;
+    for (double x : hp) ss += x;
+    t->norm_sq = ss;
+    // Blocks: each run split into max_block_size slices, block_coords[n] =
+    // (block field of mode n) << low_bits[n] (include/blco.hpp:290-321).
+    const uint64_t B = t->max_block_size ? t->max_block_size : nnz;
+    t->block_offsets.clear();
+    t->block_coords.clear();
+    for (uint32_t r = 0; r < nruns; r++) {
+        const uint64_t b0 = hs[r], b1 = r + 1 < nruns ? hs[r + 1] : nnz;
+        for (uint64_t o = b0; o < b1; o += B) {
+            t->block_offsets.push_back(o);
+            for (int n = 0; n < L.nmodes; n++)
+                t->block_coords.push_back(((hf[r] >> L.bpos[n]) & L.bmask[n]) << L.low_bits[n]);
+        }
+    }
+    t->block_count = t->block_offsets.size();
+    t->block_offsets.push_back(nnz);
+    // keep the three output arrays, release the rest
+    t->d_coords = outC;
+    t->d_values = reinterpret_cast<double*>(outV);
+    t->d_bfield = outF;
+    for (uint64_t*& b : buf)
+        if (b == outC || b == outV || b == outF) b = nullptr;
+    release();
+    return build_wide_copies(t, s, di);
+}
 
 uint32_t host_hash_row(uint32_t r) { return (r * 2654435761u) >> 7; }
 
@@ -788,11 +1132,22 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
     uint64_t B = max_block_size ? max_block_size : nnz;
     t->block_count = nnz == 0 ? 0 : (nnz + B - 1) / B;
     t->resident = !(opts && opts->stream_data);
+    if (t->layout.wide && !t->resident) {
+        delete t;
+        return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits are encoded resident only (no streamed blocks)");
+    }
 
     auto cleanup_fail = [&](int s) { blco_tensor_free(t); return s; };
     cudaError_t e = cudaSetDevice(t->device);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(e, "cudaSetDevice", __FILE__, __LINE__));
     cudaStream_t s = pick_stream(t, opts);
+    if (t->layout.wide) {
+        DeviceInfo wdi;
+        if ((st = device_info(t->device, &wdi)) != BLCO_OK) return cleanup_fail(st);
+        if ((st = encode_wide(t, d_cidx, d_vals, s, wdi)) != BLCO_OK) return cleanup_fail(st);
+        *out = t;
+        return BLCO_OK;
+    }
 
     uint64_t n_alloc = nnz ? nnz : 1;
     uint64_t *k0 = nullptr, *k1 = nullptr;
@@ -1006,6 +1361,9 @@ int encode_noalloc_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const ui
         return fail(BLCO_ERR_UNSUPPORTED, "nnz above BLCO_NOALLOC_MAX_NNZ, the limit of the allocation-free encoder");
     Layout L;
     BLCO_TRY(make_layout(nmodes, dims, &L));
+    if (L.wide)
+        return fail(BLCO_ERR_UNSUPPORTED, "the allocation-free encoder takes keys of at most 64 bits (no block "
+                                          "coordinates in its output)");
     for (int n = 0; n < nmodes; n++)
         if (nnz && !d_cidx[n]) return fail(BLCO_ERR_INVALID, "null coordinate array");
     if (nnz == 0) return BLCO_OK;

@@ -57,6 +57,16 @@ int device_info(int device, DeviceInfo* out);
 // ------------------------------------------------------------ bit layout --
 
 // Per-tensor layout constants, passed by value to kernels.
+//
+// Wide keys (alto_bits > 64, the reference's 128-bit build): the ALTO key
+// has a low word (alto_masks) and an upper word (alto_masks_hi).  A BLCO
+// coordinate holds each mode's low-word bits only (low_bits[n] of them,
+// mode_masks/mode_pos as the reference computes them), and the rest of the
+// coordinate is the block coordinate.  The engine keeps the block
+// coordinates of every nonzero as one 64-bit block field,
+//   field = OR_n (c_n >> low_bits[n]) << bpos[n],
+// so that row_n = ((coord >> mode_pos[n]) & mode_masks[n])
+//               | (((field >> bpos[n]) & bmask[n]) << low_bits[n]).
 struct Layout {
     int nmodes;
     uint64_t dims[BLCO_MAX_MODES];
@@ -64,11 +74,22 @@ struct Layout {
     int mode_pos[BLCO_MAX_MODES];
     uint64_t alto_masks[BLCO_MAX_MODES];
     int alto_bits;
+    int wide;                              // alto_bits > 64
+    uint64_t alto_masks_hi[BLCO_MAX_MODES]; // upper key word (wide only)
+    int low_bits[BLCO_MAX_MODES];          // popcount(alto_masks[n])
+    int bpos[BLCO_MAX_MODES];              // block field offsets (wide only)
+    uint64_t bmask[BLCO_MAX_MODES];        // (1 << (bits_n - low_bits[n])) - 1
 };
 
 // Computes masks/positions from dims (include/alto.hpp:597-695,
-// include/blco.hpp:221-233).  Returns BLCO_OK or BLCO_ERR_INVALID.
+// include/blco.hpp:221-233).  Keys of up to 128 bits; returns BLCO_OK,
+// BLCO_ERR_INVALID or BLCO_ERR_UNSUPPORTED.
 int make_layout(int nmodes, const uint64_t* dims, Layout* out);
+
+__host__ __device__ __forceinline__ uint64_t wide_row(const Layout& L, int n, uint64_t coord, uint64_t field)
+{
+    return ((coord >> L.mode_pos[n]) & L.mode_masks[n]) | (((field >> L.bpos[n]) & L.bmask[n]) << L.low_bits[n]);
+}
 
 // ---------------------------------------------------------------- tensor --
 
@@ -139,6 +160,18 @@ struct blco_tensor {
     // streamed blocks (pinned host)
     uint64_t* h_coords = nullptr;
     double* h_values = nullptr;
+    // wide keys: per-nonzero block field (see Layout) and the blocks
+    // (block_count + 1 offsets, block_count x nmodes block coordinates)
+    uint64_t* d_bfield = nullptr;
+    std::vector<uint64_t> block_offsets;
+    std::vector<uint64_t> block_coords;
+    // wide keys: per mode, the stream sorted by that mode's row (key order
+    // inside a row), read by that mode's MTTKRP
+    struct WideCopy {
+        uint64_t* d_coords = nullptr;
+        uint64_t* d_field = nullptr;
+        double* d_vals = nullptr;
+    } wide_copy[BLCO_MAX_MODES];
     // heavy-row tables, one per mode, built at encode time
     blco::HotTable hot[BLCO_MAX_MODES];
     blco::ModeStats stats[BLCO_MAX_MODES];
@@ -179,6 +212,8 @@ struct MttkrpArgs {
     int interleave; // tile kernel: 1 deals tiles round-robin to the grid's warps
 };
 int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
+// Wide-key tensors: FP64 MTTKRP over the BLCO stream in key order.
+int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested, int factor_dtype);
 // Automatic rule: the heavy-row path needs at least this many heavy nonzeros.
 constexpr uint64_t AUTO_HOT_MIN_NNZ = 1ull << 18;

@@ -738,6 +738,7 @@ size_t acc_elem_bytes(int) { return 8; }
 
 int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested, int factor_dtype)
 {
+    if (t->layout.wide) return BLCO_KERNEL_LVL1; // one kernel for keys above 64 bits
     DeviceInfo di;
     if (device_info(t->device, &di) != BLCO_OK) return BLCO_KERNEL_LVL1;
     size_t budget = di.smem_optin - stage_bytes(rank, policy_vec(factor_dtype)) - 2 * sizeof(uint32_t) * 4096 - 1024;
@@ -773,9 +774,161 @@ int values_f32(blco_tensor* t, cudaStream_t s, const float** out)
     return BLCO_OK;
 }
 
+// --------------------------------------------------------- wide keys --
+//
+// MTTKRP of a tensor whose keys need more than 64 bits (the reference's
+// 128-bit build).  The reference reads the stream in key order
+// (src/alto_dev.cu:31-306, alt_pext adding the block coordinate, :13-16);
+// here mode n reads its own copy of the stream sorted by the row of mode n
+// (built at encode time), and a row index is field | block coordinate,
+// taken from the per-nonzero block field.  A group of G lanes (G = 8, 16 or
+// 32 columns wide) walks a contiguous run of 4G nonzeros: lane k of the
+// group loads nonzero k of each batch of G (coalesced) and decodes its
+// rows, then the group takes the batch's nonzeros one by one through
+// shuffles, gathers the other modes' factor rows (G consecutive columns per
+// load), and keeps the running sum of an output row in registers until the
+// row changes, when it adds the sum to the output with FP64 atomics; in
+// row order that is about once per row and warp task.
+
+namespace {
+
+struct WideParams {
+    const uint64_t* coords;
+    const uint64_t* field;
+    const double* vals;
+    uint64_t nnz;
+    Layout L;
+    const double* f[BLCO_MAX_MODES];
+    double* out;
+    int mode;
+    int rank;
+    int col0; // first column of this launch's column slab
+};
+
+constexpr int WIDE_THREADS = 256;
+constexpr int WIDE_BATCHES = 4; // batches of G nonzeros per group task
+
+template <int G, int CPL>
+__global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide(const WideParams p)
+{
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % G;
+    const int grp = lane / G;
+    constexpr uint64_t WARP_TASK = (uint64_t)32 * WIDE_BATCHES;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (WIDE_THREADS / 32);
+    const uint64_t wid = (uint64_t)blockIdx.x * (WIDE_THREADS / 32) + (threadIdx.x >> 5);
+    const int nm = p.L.nmodes;
+    const int R = p.rank;
+    const uint64_t ntasks = (p.nnz + WARP_TASK - 1) / WARP_TASK;
+    for (uint64_t task = wid; task < ntasks; task += nwarps) {
+        const uint64_t g0 = task * WARP_TASK + (uint64_t)grp * (G * WIDE_BATCHES);
+        uint64_t cur = ~0ull;
+        double acc[CPL];
+#pragma unroll
+        for (int k = 0; k < CPL; k++) acc[k] = 0.0;
+        for (int b = 0; b < WIDE_BATCHES; b++) {
+            const uint64_t i = g0 + (uint64_t)b * G + sub;
+            const bool ok = i < p.nnz;
+            uint32_t row[BLCO_MAX_MODES];
+            double v = 0.0;
+            {
+                const uint64_t c = ok ? __ldg(p.coords + i) : 0;
+                const uint64_t fld = ok ? __ldg(p.field + i) : 0;
+                v = ok ? __ldg(p.vals + i) : 0.0;
+#pragma unroll
+                for (int n = 0; n < BLCO_MAX_MODES; n++)
+                    row[n] = n < nm ? (uint32_t)wide_row(p.L, n, c, fld) : 0u;
+            }
+            const uint32_t okmask = __ballot_sync(0xffffffffu, ok);
+#pragma unroll 4
+            for (int j = 0; j < G; j++) {
+                const int src = grp * G + j;
+                const bool vj = (okmask >> src) & 1u;
+                uint32_t r[BLCO_MAX_MODES];
+#pragma unroll
+                for (int n = 0; n < BLCO_MAX_MODES; n++) r[n] = __shfl_sync(0xffffffffu, row[n], j, G);
+                const double vv = __shfl_sync(0xffffffffu, v, j, G);
+                if (!vj) continue;
+                const uint64_t rt = r[p.mode];
+                if (rt != cur) {
+                    if (cur != ~0ull) {
+#pragma unroll
+                        for (int k = 0; k < CPL; k++) {
+                            const int col = p.col0 + sub + k * G;
+                            if (col < R) atomicAdd(p.out + cur * R + col, acc[k]);
+                            acc[k] = 0.0;
+                        }
+                    }
+                    cur = rt;
+                }
+#pragma unroll
+                for (int k = 0; k < CPL; k++) {
+                    const int col = p.col0 + sub + k * G;
+                    if (col < R) {
+                        double prod = vv;
+#pragma unroll
+                        for (int n = 0; n < BLCO_MAX_MODES; n++)
+                            if (n < nm && n != p.mode) prod *= __ldg(p.f[n] + (uint64_t)r[n] * R + col);
+                        acc[k] += prod;
+                    }
+                }
+            }
+        }
+        if (cur != ~0ull) {
+#pragma unroll
+            for (int k = 0; k < CPL; k++) {
+                const int col = p.col0 + sub + k * G;
+                if (col < R) atomicAdd(p.out + cur * R + col, acc[k]);
+            }
+        }
+    }
+}
+
+} // namespace
+
+int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
+{
+    if (a.nnz == 0) return BLCO_OK;
+    if (a.factor_dtype != BLCO_DTYPE_F64)
+        return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits: the MTTKRP is FP64 only (the reference's form)");
+    const blco_tensor::WideCopy& w = t->wide_copy[a.mode];
+    if (!t->resident || !w.d_coords) return fail(BLCO_ERR_STATE, "wide-key tensor without its per-mode copies");
+    DeviceInfo di;
+    BLCO_TRY(device_info(t->device, &di));
+    WideParams p;
+    memset(&p, 0, sizeof(p));
+    p.coords = w.d_coords;
+    p.field = w.d_field;
+    p.vals = w.d_vals;
+    p.nnz = a.nnz;
+    p.L = t->layout;
+    for (int m = 0; m < t->layout.nmodes; m++) p.f[m] = static_cast<const double*>(a.factors[m]);
+    p.out = static_cast<double*>(a.out);
+    p.mode = a.mode;
+    p.rank = a.rank;
+    const uint64_t ntasks = (a.nnz + 32 * WIDE_BATCHES - 1) / (32 * WIDE_BATCHES);
+    const int grid = (int)std::min<uint64_t>((ntasks + WIDE_THREADS / 32 - 1) / (WIDE_THREADS / 32),
+                                             (uint64_t)di.sm_count * 8);
+    for (int c0 = 0; c0 < a.rank; c0 += 128) {
+        p.col0 = c0;
+        const int cols = std::min(128, a.rank - c0);
+        if (a.rank <= 8) k_mttkrp_wide<8, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else if (a.rank <= 16) k_mttkrp_wide<16, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else if (cols <= 32) k_mttkrp_wide<32, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else if (cols <= 64) k_mttkrp_wide<32, 2><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else k_mttkrp_wide<32, 4><<<grid, WIDE_THREADS, 0, s>>>(p);
+        BLCO_CHECK_LAUNCH("k_mttkrp_wide");
+    }
+    return BLCO_OK;
+}
+
 int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
 {
     const Layout& L = t->layout;
+    if (L.wide) {
+        if (a.rank < 1 || a.rank > 256) return fail(BLCO_ERR_UNSUPPORTED, "rank must be 1..256");
+        return mttkrp_wide_launch(t, a, s);
+    }
     if (a.nnz == 0) return BLCO_OK;
     if (a.rank < 1 || a.rank > 256) return fail(BLCO_ERR_UNSUPPORTED, "rank must be 1..256");
     if (a.factor_dtype != BLCO_DTYPE_F64 && a.factor_dtype != BLCO_DTYPE_F32 && a.factor_dtype != BLCO_DTYPE_BF16)

@@ -275,6 +275,7 @@ int tune_features(const blco_tensor* t, int mode, int rank, int dtype, float* f)
 {
     const Layout& L = t->layout;
     if (mode < 0 || mode >= L.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
+    if (L.wide) return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits have one MTTKRP schedule (nothing to select)");
     for (int i = 0; i < BLCO_MLP_FEATURES; i++) f[i] = 0.f;
     auto lg = [](double x) { return (float)std::log2(std::max(1.0, x)); };
     const double nnz = (double)t->nnz;
@@ -324,6 +325,7 @@ int tune_sweep(blco_tensor* t, int mode, int rank, int dtype, int reps, cudaStre
 {
     const Layout& L = t->layout;
     if (!t->resident) return fail(BLCO_ERR_UNSUPPORTED, "the autotuner needs a resident tensor");
+    if (L.wide) return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits have one MTTKRP schedule (nothing to tune)");
     if (mode < 0 || mode >= L.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
     if (rank < 1 || rank > 256) return fail(BLCO_ERR_UNSUPPORTED, "rank must be 1..256");
     if (dtype < BLCO_DTYPE_F64 || dtype > BLCO_DTYPE_BF16) return fail(BLCO_ERR_INVALID, "unknown factor dtype");
@@ -659,6 +661,10 @@ int resolve_schedule(blco_tensor* t, int mode, int rank, int dtype, int requeste
 {
     a->kernel = requested;
     if (requested != BLCO_KERNEL_TUNED && requested != BLCO_KERNEL_LEARNED) return BLCO_OK;
+    if (t->layout.wide) {
+        a->kernel = BLCO_KERNEL_LVL1; // keys above 64 bits have one kernel
+        return BLCO_OK;
+    }
     if (!t->resident) {
         a->kernel = BLCO_KERNEL_AUTO; // streamed blocks: the heuristic
         return BLCO_OK;

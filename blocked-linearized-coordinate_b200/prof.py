@@ -6,6 +6,10 @@
   python blocked-linearized-coordinate_b200/prof.py batch --count T [--iters I]
       Batched CP-ALS sweeps over T small tensors of the many-small-tensors
       recipe (FP64); prints device ms per sweep.
+  python blocked-linearized-coordinate_b200/prof.py wide --nnz N [--rank R] [--reps K] [--iters I]
+      The wide-key workload: Zipf(1.1) over 2^20 x 2^20 x 2^20 x 4096
+      (72 key bits, the reference's 128-bit build), FP64: encode time and
+      block count, per-mode MTTKRP times, CP-ALS ms per iteration.
   python blocked-linearized-coordinate_b200/prof.py tns --nnz N --dir D
       Writes the Zipf(1.1) 2M x 2M x 25k tensor with N nonzeros as a .tns
       file (cpd64's writer, values as %g) and times cpd64's file-to-BLCO
@@ -59,6 +63,53 @@ def run_mttkrp(a, pkg, torch):
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         print(f"mode {m}: ms {['%.3f' % x for x in ts]}", flush=True)
+    t.free()
+
+
+WIDE_DIMS = [1 << 20, 1 << 20, 1 << 20, 1 << 12]  # 72 key bits
+
+
+def run_wide(a, pkg, torch):
+    from blco_b200 import synth
+    dims = WIDE_DIMS
+    X = synth.wide_tensor_device(a.nnz, dims, 1.1, seed=0)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"])
+    e1.record()
+    torch.cuda.synchronize()
+    del X
+    torch.cuda.empty_cache()
+    inf = t.info()
+    print(f"encode ms {e0.elapsed_time(e1):.3f} blocks {inf['block_count']} key bits {inf['alto_bits']}", flush=True)
+    R = a.rank
+    g = torch.Generator(device="cuda").manual_seed(1)
+    fs = [torch.rand(d, R, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    o = pkg.make_opts(kernel=10)
+    for m in range(len(dims)):
+        out = torch.zeros(dims[m], R, dtype=torch.float64, device="cuda")
+        pkg.mttkrp(t, m, fs, out, o)
+        ts = []
+        for _ in range(a.reps):
+            e0.record()
+            pkg.mttkrp(t, m, fs, out, o)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        alg = a.nnz * 16 + sum(d * R * 8 for d in dims)
+        best = min(ts)
+        print(f"mode {m}: ms {['%.3f' % x for x in ts]} alg GB/s {alg / best / 1e6:.0f}", flush=True)
+    if a.iters:
+        lam = torch.ones(R, dtype=torch.float64, device="cuda")
+        plan = pkg.CpalsPlan(t, fs, lam, pkg.make_opts(kernel=10))
+        plan.iterate(2, tol=-1.0)
+        e0.record()
+        fits = plan.iterate(a.iters, tol=-1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        print(f"cpals fp64 ms/iter {e0.elapsed_time(e1) / a.iters:.3f} fit {fits[-1]:.6f}", flush=True)
+        plan.destroy()
     t.free()
 
 
@@ -128,12 +179,17 @@ def main():
     tn = sub.add_parser("tns")
     tn.add_argument("--nnz", type=int, default=50_000_000)
     tn.add_argument("--dir", default="tns_prof")
+    w = sub.add_parser("wide")
+    w.add_argument("--nnz", type=int, default=50_000_000)
+    w.add_argument("--rank", type=int, default=32)
+    w.add_argument("--reps", type=int, default=3)
+    w.add_argument("--iters", type=int, default=3)
     a = ap.parse_args()
     import torch
     pkg = load()
     if os.environ.get("BLCO_LIB"):
         pkg.LIB_PATH = os.environ["BLCO_LIB"]
-    {"mttkrp": run_mttkrp, "batch": run_batch, "tns": run_tns}[a.cmd](a, pkg, torch)
+    {"mttkrp": run_mttkrp, "batch": run_batch, "tns": run_tns, "wide": run_wide}[a.cmd](a, pkg, torch)
 
 
 if __name__ == "__main__":

@@ -88,6 +88,85 @@ def zipf_tensor_device(nnz, dims, s, seed=0, device="cuda", value_dist="lognorma
     return dict(dims=dims, cidx=cidx, vals=vals.contiguous())
 
 
+def wide_tensor_device(nnz, dims, s, seed=0, device="cuda"):
+    """Distinct coordinates in a key space above 2^63 (keys of more than 64
+    bits): per-mode Zipf(s) draws (uniform for s = 0), deduplicated on a
+    pair of linear keys (the modes split into two groups whose products stay
+    below 2^62), values lognormal(0,1) drawn in FP32 and summed over
+    duplicate coordinates in FP64, exactly `nnz` nonzeros in random order.
+    Returns dict(dims, cidx=[int64 CUDA tensors], vals=float64 CUDA tensor)."""
+    import torch
+    dims = [int(d) for d in dims]
+    groups, cur, prod = [], [], 1
+    for n, d in enumerate(dims):
+        if cur and prod * d >= 2 ** 62:
+            groups.append(cur)
+            cur, prod = [], 1
+        cur.append(n)
+        prod *= d
+    groups.append(cur)
+    if len(groups) > 2:
+        raise ValueError("modes do not split into two keys below 2^62")
+    while len(groups) < 2:
+        groups.append([])
+    mults = []
+    for grp in groups:
+        m, ms = 1, {}
+        for n in reversed(grp):
+            ms[n] = m
+            m *= dims[n]
+        mults.append(ms)
+    g = torch.Generator(device=device).manual_seed(int(seed))
+    cdfs = [_zipf_cdf(torch, d, s, device) if s > 0 else None for d in dims]
+    k0 = torch.empty(0, dtype=torch.int64, device=device)
+    k1 = torch.empty(0, dtype=torch.int64, device=device)
+    vals = torch.empty(0, dtype=torch.float64, device=device)
+    draw = int(nnz * 1.02) + 1024
+    for _ in range(64):
+        a = torch.zeros(draw, dtype=torch.int64, device=device)
+        b = torch.zeros(draw, dtype=torch.int64, device=device)
+        for n, d in enumerate(dims):
+            if cdfs[n] is None:
+                c = torch.randint(0, d, (draw,), generator=g, device=device, dtype=torch.int64)
+            else:
+                u = torch.rand(draw, dtype=torch.float64, generator=g, device=device)
+                c = torch.searchsorted(cdfs[n], u).clamp_(max=d - 1)
+            if n in mults[0]:
+                a += c * mults[0][n]
+            else:
+                b += c * mults[1][n]
+            del c
+        v = torch.randn(draw, dtype=torch.float32, generator=g, device=device).exp_().double()
+        k0, k1, vals = torch.cat([k0, a]), torch.cat([k1, b]), torch.cat([vals, v])
+        del a, b, v
+        # lexicographic (k0, k1) order by two stable sorts, then runs
+        o = torch.sort(k1, stable=True)[1]
+        o = o[torch.sort(k0[o], stable=True)[1]]
+        k0, k1, vals = k0[o], k1[o], vals[o]
+        del o
+        first = torch.ones(k0.numel(), dtype=torch.bool, device=device)
+        first[1:] = (k0[1:] != k0[:-1]) | (k1[1:] != k1[:-1])
+        rid = torch.cumsum(first.to(torch.int64), 0) - 1
+        nu = int(rid[-1].item()) + 1
+        vals = torch.zeros(nu, dtype=torch.float64, device=device).index_add_(0, rid, vals)
+        k0, k1 = k0[first], k1[first]
+        del first, rid
+        if nu >= nnz:
+            break
+        draw = int((nnz - nu) * 2.0) + 1024
+    else:
+        raise RuntimeError("could not reach the requested number of distinct coordinates")
+    pick = torch.randperm(k0.numel(), generator=g, device=device)[:nnz]
+    k0, k1, vals = k0[pick], k1[pick], vals[pick]
+    cidx = [None] * len(dims)
+    for key, ms in ((k0, mults[0]), (k1, mults[1])):
+        rem = key
+        for n in sorted(ms, key=lambda q: -ms[q]):
+            cidx[n] = torch.div(rem, ms[n], rounding_mode="floor")
+            rem = rem - cidx[n] * ms[n]
+    return dict(dims=dims, cidx=cidx, vals=vals.contiguous())
+
+
 def uniform_tensor_host(nnz, dims, seed=0):
     """Distinct uniform coordinates and U(0,1) FP64 values (numpy)."""
     rng = np.random.default_rng(seed)

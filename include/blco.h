@@ -127,6 +127,12 @@ typedef struct blco_tensor_info {
     int alto_bits;                       /* sum of bits_n */
     int device;
     int resident; /* 1: stream in HBM; 0: pinned host blocks (streamed) */
+    /* Keys above 64 bits (alto_bits > 64, the reference's 128-bit build,
+     * ALTO_MASK_LENGTH=128): alto_masks holds the low key word and
+     * alto_masks_hi the upper one; mode_masks / mode_pos then cover each
+     * mode's low-word bits only, and the rest of a coordinate is its
+     * block's block_coords (include/blco.hpp:222-233, 301-319). */
+    uint64_t alto_masks_hi[BLCO_MAX_MODES];
 } blco_tensor_info;
 
 /* ---- library ------------------------------------------------------------ */
@@ -140,11 +146,16 @@ const char* blco_version(void);
 
 /* ---- encoder ------------------------------------------------------------ */
 
-/* Encode a COO tensor into 64-bit BLCO on the GPU.
- * Replaces gen_blcotensor_host<uint64> (include/blco.hpp:196) followed by
+/* Encode a COO tensor into BLCO on the GPU.
+ * Replaces gen_blcotensor_host<LIT> (include/blco.hpp:196) followed by
  * gen_blcotensor_device + send_blcotensor_over (src/blco.cu:12, 120): the
  * linearization, ALTO sort, re-linearization and block split all run as
  * sm_100a kernels and the result matches the reference bit for bit.
+ * Coordinates of up to 64 key bits give the 64-bit build's encoding (cpd64,
+ * LIT = uint64); 65 to 128 bits give the 128-bit build's (cpd128, LIT =
+ * unsigned __int128): one block per distinct upper key word, split into
+ * max_block_size slices, with non-zero block_coords.  Keys above 64 bits
+ * are resident only (opts->stream_data gives BLCO_ERR_UNSUPPORTED).
  *   cidx[n] (host): nnz 0-based coordinates of mode n; vals (host): nnz values.
  *   max_block_size: the --max-block-size of the reference (0 = nnz).
  *   opts->stream_data: keep the encoded blocks in pinned host memory instead
@@ -172,7 +183,9 @@ int blco_encode_device(int nmodes, const uint64_t* dims, uint64_t nnz,
  * Scratch: a fixed 32 MiB device array inside the library, held by every GPU
  * that loads it until the process exits; this function calls no cudaMalloc,
  * cudaFree or allocating library routine.
- *   - nnz above BLCO_NOALLOC_MAX_NNZ is rejected with BLCO_ERR_UNSUPPORTED;
+ *   - nnz above BLCO_NOALLOC_MAX_NNZ, and coordinates needing more than 64
+ *     key bits (their block coordinates have no output array here), are
+ *     rejected with BLCO_ERR_UNSUPPORTED;
  *   - every call on a device shares that one array: calls that overlap on
  *     the GPU (other streams or host threads) race, so serialise them;
  *   - the first call on a device looks up the array's address with

@@ -430,10 +430,27 @@ static void orc_gram(uint64_t rows, int R, const double* u, double* g)
     }
 }
 
-int orc_cpals(int nmodes, const uint64_t* dims, const uint64_t* mode_masks,
-              const int* mode_pos, uint64_t nnz, const uint64_t* coords,
-              const double* vals, int rank, double* const* factors,
-              double* lambda, int maxiter, double tol, double* fits)
+/* The MTTKRP of one CP-ALS step, over whichever form the caller holds. */
+typedef struct {
+    int kind; /* 0: BLCO stream, 1: COO */
+    const uint64_t* mode_masks;
+    const int* mode_pos;
+    const uint64_t* coords;
+    const uint64_t* cidx;
+} orc_mt_src;
+
+static void orc_mt(const orc_mt_src* src, int N, uint64_t nnz, const double* vals, int R,
+                   const double* const* factors, int n, double* M)
+{
+    if (src->kind == 0)
+        orc_mttkrp_blco(N, src->mode_masks, src->mode_pos, nnz, src->coords, vals, R, factors, n, M);
+    else
+        orc_mttkrp_coo(N, nnz, src->cidx, vals, R, factors, n, M);
+}
+
+static int orc_cpals_src(int nmodes, const uint64_t* dims, const orc_mt_src* src, uint64_t nnz,
+                         const double* vals, int rank, double* const* factors,
+                         double* lambda, int maxiter, double tol, double* fits)
 {
     const int R = rank, N = nmodes;
     uint64_t maxdim = 0;
@@ -474,8 +491,7 @@ int orc_cpals(int nmodes, const uint64_t* dims, const uint64_t* mode_masks,
             int n = order[k];
             uint64_t I = dims[n];
             memset(M, 0, sizeof(double) * I * (uint64_t)R);
-            orc_mttkrp_blco(N, mode_masks, mode_pos, nnz, coords, vals, R,
-                            (const double* const*)factors, n, M);
+            orc_mt(src, N, nnz, vals, R, (const double* const*)factors, n, M);
             /* V = hadamard of the other Grams (src/cpd_gpu.cu:160-163) */
             for (int e = 0; e < R * R; e++) V[e] = 1.0;
             for (int m = 0; m < N; m++)
@@ -532,6 +548,23 @@ int orc_cpals(int nmodes, const uint64_t* dims, const uint64_t* mode_masks,
     for (int n = 0; n < N; n++) free(grams[n]);
     free(M); free(V); free(P); free(W); free(colsq); free(mrow);
     return it;
+}
+
+int orc_cpals(int nmodes, const uint64_t* dims, const uint64_t* mode_masks,
+              const int* mode_pos, uint64_t nnz, const uint64_t* coords,
+              const double* vals, int rank, double* const* factors,
+              double* lambda, int maxiter, double tol, double* fits)
+{
+    orc_mt_src src = {0, mode_masks, mode_pos, coords, NULL};
+    return orc_cpals_src(nmodes, dims, &src, nnz, vals, rank, factors, lambda, maxiter, tol, fits);
+}
+
+int orc_cpals_coo(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                  const double* vals, int rank, double* const* factors,
+                  double* lambda, int maxiter, double tol, double* fits)
+{
+    orc_mt_src src = {1, NULL, NULL, NULL, cidx};
+    return orc_cpals_src(nmodes, dims, &src, nnz, vals, rank, factors, lambda, maxiter, tol, fits);
 }
 
 void orc_kruskal_random_init(int nmodes, const uint64_t* dims, int rank,

@@ -126,6 +126,12 @@ int orc_cpals(int nmodes, const uint64_t* dims, const uint64_t* mode_masks,
               const double* vals, int rank, double* const* factors,
               double* lambda, int maxiter, double tol, double* fits);
 
+/* The same CP-ALS with the MTTKRP taken from the COO tensor (cidx as in
+ * orc_blco_encode), for encodings with block coordinates. */
+int orc_cpals_coo(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                  const double* vals, int rank, double* const* factors,
+                  double* lambda, int maxiter, double tol, double* fits);
+
 /* KruskalModelRandomInit (src/kruskal_model.cpp:93-110): lambda = 1 and
  * U_n[i] = rand_r(&s_t) / RAND_MAX where thread t of nthreads owns a static
  * contiguous chunk of dims[n]*rank entries and s_t = seed + t, reset for

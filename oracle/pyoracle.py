@@ -45,6 +45,7 @@ def lib():
         L.orc_blco_encode128.restype = ctypes.c_int
         L.orc_pinv_sym.restype = ctypes.c_int
         L.orc_cpals.restype = ctypes.c_int
+        L.orc_cpals_coo.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -63,6 +64,10 @@ def ref_lib():
         R.ref_alto_create.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int]
         R.ref_alto_mttkrp.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         R.ref_alto_destroy.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        R.ref_alto_create128.restype = ctypes.c_void_p
+        R.ref_alto_create128.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int]
+        R.ref_alto_mttkrp128.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        R.ref_alto_destroy128.argtypes = [ctypes.c_void_p, ctypes.c_int]
         _ref = R
     return _ref
 
@@ -251,6 +256,22 @@ def cpals(dims, enc, factors, lam, maxiter, tol):
     return list(fits[:it])
 
 
+def cpals_coo(dims, cidx, vals, factors, lam, maxiter, tol):
+    """Oracle CP-ALS with the MTTKRP taken from the COO tensor (any key
+    width).  factors/lam are updated in place; returns the fits."""
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    for f in factors:
+        assert f.flags.c_contiguous and f.dtype == np.float64
+    rank = factors[0].shape[1]
+    fits = np.zeros(max(maxiter, 1), dtype=np.float64)
+    it = lib().orc_cpals_coo(ctypes.c_int(len(dims)), _p(dims, _u64p), ctypes.c_uint64(cidx.shape[1]),
+                             _p(cidx, _u64p), _p(vals, _f64p), ctypes.c_int(rank), _ptr_array(factors),
+                             _p(lam, _f64p), ctypes.c_int(maxiter), ctypes.c_double(tol), _p(fits, _f64p))
+    return list(fits[:it])
+
+
 def kruskal_random_init(dims, rank, seed, nthreads):
     factors = [np.zeros((int(d), rank), dtype=np.float64) for d in dims]
     lam = np.zeros(rank, dtype=np.float64)
@@ -297,22 +318,25 @@ def _req(dims, cidx, vals, factors, **kw):
     return r
 
 
-def refgpu_cpals(dims, cidx, vals, factors, lam, maxiter, tol, kernel=10, nprtn=8, thread_cf=2, log_path=None):
-    """Runs the reference cpals_blco_dev; factors/lam updated in place;
-    returns the final fit."""
+def refgpu_cpals(dims, cidx, vals, factors, lam, maxiter, tol, kernel=10, nprtn=8, thread_cf=2, log_path=None,
+                 wide=False):
+    """Runs the reference cpals_blco_dev (wide: on the 128-bit build's
+    encoding); factors/lam updated in place; returns the final fit."""
     res = _refgpu_call(_req(dims, cidx, vals, factors, op="cpals", lam=lam, maxiter=maxiter, tol=tol,
-                            kernel=kernel, nprtn=nprtn, thread_cf=thread_cf), log_path)
+                            kernel=kernel, nprtn=nprtn, thread_cf=thread_cf, wide=int(wide)), log_path)
     for m, f in enumerate(factors):
         f[:] = res[f"f{m}"]
     lam[:] = res["lam"]
     return float(res["fit"])
 
 
-def refgpu_mttkrp(dims, cidx, vals, factors, mode, kernel=1, nprtn=8, thread_cf=2, log_path=None):
-    """Runs the reference mttkrp_alto_dev once into a zeroed target factor;
-    returns the MTTKRP."""
+def refgpu_mttkrp(dims, cidx, vals, factors, mode, kernel=1, nprtn=8, thread_cf=2, log_path=None, wide=False,
+                  iters=1):
+    """Runs the reference mttkrp_alto_dev `iters` times into a zeroed target
+    factor (wide: on the 128-bit build's encoding); returns the sum of the
+    MTTKRPs.  The reference prints its per-iteration time to log_path."""
     fs = [np.array(f, dtype=np.float64) for f in factors]
     fs[mode][:] = 0.0
     res = _refgpu_call(_req(dims, cidx, vals, fs, op="mttkrp", mode=mode, kernel=kernel, nprtn=nprtn,
-                            thread_cf=thread_cf), log_path)
+                            thread_cf=thread_cf, wide=int(wide), iters=iters), log_path)
     return res[f"f{mode}"]

@@ -9,7 +9,10 @@
 //     and lambda passed in explicitly (the reference's random init depends on
 //     the host thread count), returning the final fit and the updated model;
 //   * refgpu_mttkrp: mttkrp_alto_dev (src/alto_dev.cu:1857-1952), which adds
-//     `iters` MTTKRPs into the target factor.
+//     `iters` MTTKRPs into the target factor;
+//   * refgpu_cpals128 / refgpu_mttkrp128: the same on the 128-bit build's
+//     encoding (gen_blcotensor_host<unsigned __int128>), for keys above 64
+//     bits.
 // Only the in-memory path is exposed (no --stream-data, no --batch): there
 // the swapped arguments of gen_blcotensor_device at src/cpd_gpu.cu:39 pass 0
 // and false either way.
@@ -68,12 +71,13 @@ static KruskalModel* refg_make_model(int nmodes, const uint64_t* dims, int rank,
     return M;
 }
 
-extern "C" double refgpu_cpals(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
-                               const double* vals, int rank, double* const* factors, double* lambda, int maxiter,
-                               double tol, int kernel, int nprtn, int thread_cf)
+template <typename LIT>
+static double refg_cpals(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                         const double* vals, int rank, double* const* factors, double* lambda, int maxiter,
+                         double tol, int kernel, int nprtn, int thread_cf)
 {
     SparseTensor* X = refg_make_tensor(nmodes, dims, nnz, cidx, vals);
-    blcotensor* T = gen_blcotensor_host<unsigned long long>(X, nnz);
+    blcotensor* T = gen_blcotensor_host<LIT>(X, nnz);
     KruskalModel* M = refg_make_model(nmodes, dims, rank, factors, lambda);
     double fit = cpals_blco_dev(T, M, maxiter, tol, kernel, false, false, thread_cf, nprtn);
     for (int n = 0; n < nmodes; n++) memcpy(factors[n], M->U[n], sizeof(double) * dims[n] * rank);
@@ -84,12 +88,13 @@ extern "C" double refgpu_cpals(int nmodes, const uint64_t* dims, uint64_t nnz, c
     return fit;
 }
 
-extern "C" void refgpu_mttkrp(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
-                              const double* vals, int rank, double* const* factors, int mode, int kernel,
-                              int iters, int nprtn, int thread_cf)
+template <typename LIT>
+static void refg_mttkrp(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                        const double* vals, int rank, double* const* factors, int mode, int kernel,
+                        int iters, int nprtn, int thread_cf)
 {
     SparseTensor* X = refg_make_tensor(nmodes, dims, nnz, cidx, vals);
-    blcotensor* T = gen_blcotensor_host<unsigned long long>(X, nnz);
+    blcotensor* T = gen_blcotensor_host<LIT>(X, nnz);
     std::vector<double> ones(rank, 1.0);
     KruskalModel* M = refg_make_model(nmodes, dims, rank, factors, ones.data());
     mttkrp_alto_dev<IType>(T, M, kernel, iters, mode, (IType)thread_cf, false, false, nprtn);
@@ -97,4 +102,39 @@ extern "C" void refgpu_mttkrp(int nmodes, const uint64_t* dims, uint64_t nnz, co
     DestroyKruskalModel(M);
     delete_blcotensor_host(T);
     DestroySparseTensor(X);
+}
+
+extern "C" double refgpu_cpals(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                               const double* vals, int rank, double* const* factors, double* lambda, int maxiter,
+                               double tol, int kernel, int nprtn, int thread_cf)
+{
+    return refg_cpals<unsigned long long>(nmodes, dims, nnz, cidx, vals, rank, factors, lambda, maxiter, tol,
+                                          kernel, nprtn, thread_cf);
+}
+
+extern "C" void refgpu_mttkrp(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                              const double* vals, int rank, double* const* factors, int mode, int kernel,
+                              int iters, int nprtn, int thread_cf)
+{
+    refg_mttkrp<unsigned long long>(nmodes, dims, nnz, cidx, vals, rank, factors, mode, kernel, iters, nprtn,
+                                    thread_cf);
+}
+
+// The 128-bit build (cpd128): the tensor encoded by
+// gen_blcotensor_host<unsigned __int128>, one block per distinct upper key
+// word (max_block_size = nnz), and the same GPU drivers.
+extern "C" double refgpu_cpals128(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                                  const double* vals, int rank, double* const* factors, double* lambda,
+                                  int maxiter, double tol, int kernel, int nprtn, int thread_cf)
+{
+    return refg_cpals<unsigned __int128>(nmodes, dims, nnz, cidx, vals, rank, factors, lambda, maxiter, tol,
+                                         kernel, nprtn, thread_cf);
+}
+
+extern "C" void refgpu_mttkrp128(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                                 const double* vals, int rank, double* const* factors, int mode, int kernel,
+                                 int iters, int nprtn, int thread_cf)
+{
+    refg_mttkrp<unsigned __int128>(nmodes, dims, nnz, cidx, vals, rank, factors, mode, kernel, iters, nprtn,
+                                   thread_cf);
 }

@@ -181,17 +181,19 @@ extern "C" void ref_kruskal_random_init(int nmodes, const uint64_t* dims, int ra
     DestroyKruskalModel(M);
 }
 
+template <typename LIT>
 struct refh_alto {
-    AltoTensor<unsigned long long>* at;
+    AltoTensor<LIT>* at;
     FType** ofibs;
     int target;
 };
 
-extern "C" void* ref_alto_create(int nmodes, const uint64_t* dims, uint64_t nnz,
-                                 const uint64_t* cidx, const double* vals, int nprtn)
+template <typename LIT>
+static void* refh_alto_create(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                              const double* vals, int nprtn)
 {
     SparseTensor* X = refh_make_tensor(nmodes, dims, nnz, cidx, vals);
-    refh_alto* h = new refh_alto;
+    refh_alto<LIT>* h = new refh_alto<LIT>;
     create_alto(X, &h->at, nprtn);
     h->ofibs = nullptr;
     h->target = -2;
@@ -199,10 +201,10 @@ extern "C" void* ref_alto_create(int nmodes, const uint64_t* dims, uint64_t nnz,
     return h;
 }
 
-// out-of-place wrapper of mttkrp_alto_par: factors[mode] receives += MTTKRP.
-extern "C" void ref_alto_mttkrp(void* hv, int mode, int rank, double* const* factors)
+template <typename LIT>
+static void refh_alto_mttkrp(void* hv, int mode, int rank, double* const* factors)
 {
-    refh_alto* h = (refh_alto*)hv;
+    refh_alto<LIT>* h = (refh_alto<LIT>*)hv;
     if (h->ofibs == nullptr) {
         create_da_mem(-1, rank, h->at, &h->ofibs);
         h->target = -1;
@@ -210,10 +212,35 @@ extern "C" void ref_alto_mttkrp(void* hv, int mode, int rank, double* const* fac
     mttkrp_alto_par(mode, (FType**)factors, (IType)rank, h->at, nullptr, h->ofibs);
 }
 
-extern "C" void ref_alto_destroy(void* hv, int rank)
+template <typename LIT>
+static void refh_alto_destroy(void* hv, int rank)
 {
-    refh_alto* h = (refh_alto*)hv;
+    refh_alto<LIT>* h = (refh_alto<LIT>*)hv;
     if (h->ofibs) destroy_da_mem(h->at, h->ofibs, rank, -1);
     destroy_alto(h->at);
     delete h;
 }
+
+extern "C" void* ref_alto_create(int nmodes, const uint64_t* dims, uint64_t nnz,
+                                 const uint64_t* cidx, const double* vals, int nprtn)
+{
+    return refh_alto_create<unsigned long long>(nmodes, dims, nnz, cidx, vals, nprtn);
+}
+extern "C" void ref_alto_mttkrp(void* hv, int mode, int rank, double* const* factors)
+{
+    refh_alto_mttkrp<unsigned long long>(hv, mode, rank, factors);
+}
+extern "C" void ref_alto_destroy(void* hv, int rank) { refh_alto_destroy<unsigned long long>(hv, rank); }
+
+// The 128-bit build's CPU ALTO MTTKRP (AltoTensor<unsigned __int128>), for
+// keys above 64 bits.
+extern "C" void* ref_alto_create128(int nmodes, const uint64_t* dims, uint64_t nnz,
+                                    const uint64_t* cidx, const double* vals, int nprtn)
+{
+    return refh_alto_create<unsigned __int128>(nmodes, dims, nnz, cidx, vals, nprtn);
+}
+extern "C" void ref_alto_mttkrp128(void* hv, int mode, int rank, double* const* factors)
+{
+    refh_alto_mttkrp<unsigned __int128>(hv, mode, rank, factors);
+}
+extern "C" void ref_alto_destroy128(void* hv, int rank) { refh_alto_destroy<unsigned __int128>(hv, rank); }

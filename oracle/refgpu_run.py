@@ -6,7 +6,8 @@ every call to oracle/_ref/libblco_refgpu.so runs in a fresh interpreter:
     python oracle/refgpu_run.py request.npz result.npz
 
 request.npz holds op ("cpals" | "mttkrp"), dims, cidx, vals, factors f0..fN,
-lam, rank and the reference flags; result.npz receives the outputs.  The
+lam, rank, the reference flags, optionally wide (1: the 128-bit build's
+encoding) and iters (MTTKRP repetitions); result.npz receives the outputs.  The
 reference's own printout goes to this process's stdout/stderr.
 """
 import ctypes
@@ -30,11 +31,15 @@ def main(req_path, res_path):
     fs = [np.ascontiguousarray(r[f"f{m}"], dtype=np.float64).copy() for m in range(n)]
     ptrs = (ctypes.c_void_p * n)(*[f.ctypes.data for f in fs])
     rank = int(r["rank"])
+    wide = int(r["wide"]) if "wide" in r else 0
+    cpals_fn = G.refgpu_cpals128 if wide else G.refgpu_cpals
+    mttkrp_fn = G.refgpu_mttkrp128 if wide else G.refgpu_mttkrp
+    iters = int(r["iters"]) if "iters" in r else 1
     out = {}
     if str(r["op"]) == "cpals":
         lam = np.ascontiguousarray(r["lam"], dtype=np.float64).copy()
-        G.refgpu_cpals.restype = ctypes.c_double
-        fit = G.refgpu_cpals(ctypes.c_int(n), dims.ctypes.data_as(u64p), ctypes.c_uint64(cidx.shape[1]),
+        cpals_fn.restype = ctypes.c_double
+        fit = cpals_fn(ctypes.c_int(n), dims.ctypes.data_as(u64p), ctypes.c_uint64(cidx.shape[1]),
                              cidx.ctypes.data_as(u64p), vals.ctypes.data_as(f64p), ctypes.c_int(rank), ptrs,
                              lam.ctypes.data_as(f64p), ctypes.c_int(int(r["maxiter"])),
                              ctypes.c_double(float(r["tol"])), ctypes.c_int(int(r["kernel"])),
@@ -42,10 +47,10 @@ def main(req_path, res_path):
         out["fit"] = np.float64(fit)
         out["lam"] = lam
     else:
-        G.refgpu_mttkrp(ctypes.c_int(n), dims.ctypes.data_as(u64p), ctypes.c_uint64(cidx.shape[1]),
-                        cidx.ctypes.data_as(u64p), vals.ctypes.data_as(f64p), ctypes.c_int(rank), ptrs,
-                        ctypes.c_int(int(r["mode"])), ctypes.c_int(int(r["kernel"])), ctypes.c_int(1),
-                        ctypes.c_int(int(r["nprtn"])), ctypes.c_int(int(r["thread_cf"])))
+        mttkrp_fn(ctypes.c_int(n), dims.ctypes.data_as(u64p), ctypes.c_uint64(cidx.shape[1]),
+                  cidx.ctypes.data_as(u64p), vals.ctypes.data_as(f64p), ctypes.c_int(rank), ptrs,
+                  ctypes.c_int(int(r["mode"])), ctypes.c_int(int(r["kernel"])), ctypes.c_int(iters),
+                  ctypes.c_int(int(r["nprtn"])), ctypes.c_int(int(r["thread_cf"])))
     for m in range(n):
         out[f"f{m}"] = fs[m]
     sys.stdout.flush()

@@ -200,3 +200,31 @@ def test_cli_bench_and_streamed(tmp_path):
         assert r.returncode == 0, r.stderr
         fits.append([float(l.split("f = ")[1].split()[0]) for l in r.stdout.splitlines() if l.startswith("--> Iter")])
     assert len(fits[0]) == 4 and np.allclose(fits[0], fits[1], rtol=0, atol=2e-6)
+
+
+@pytest.mark.gpu
+def test_cli_wide_keys(tmp_path):
+    """A tensor whose coordinates need 69 key bits (the reference's cpd128
+    case): CP-ALS through the GPU and the host loader give the same fits,
+    and the -c check of every mode's MTTKRP passes."""
+    rng = np.random.default_rng(17)
+    dims = [9000, 8500, 8200, 8192, 8300]
+    c = np.stack([rng.integers(0, d, size=6000, dtype=np.uint64) for d in dims])
+    cidx = np.unique(c, axis=1)
+    # every mode's largest index present, so the loaders find these lengths
+    cidx[:, 0] = np.array(dims, dtype=np.uint64) - 1
+    cidx = np.unique(cidx, axis=1)
+    p = str(tmp_path / "w.tns")
+    write_tns(p, cidx, rng.random(cidx.shape[1]))
+    outs = []
+    for extra in ([], ["--host-load"]):
+        r = run(["-i", p, "-k", "10", "-r", "4", "-m", "4", "-e", "0", "-x", "3"] + extra)
+        assert r.returncode == 0, r.stderr
+        outs.append([l.split("time =")[0] for l in r.stdout.splitlines()
+                     if l.startswith("--> Iter") or l.startswith("Final fit")])
+    assert len(outs[0]) == 5 and outs[0] == outs[1]
+    for mode in ("0", "4"):
+        r = run(["-i", p, "-k", "10", "-c", "-p", "-t", mode, "-r", "8", "-x", "1"])
+        assert r.returncode == 0, r.stderr
+        # one verification line per mode
+        assert r.stderr.count("Results of mttkrp_blco_dev is correct") == 5, r.stderr

@@ -84,7 +84,8 @@ def test_encode_errors(blco):
         blco.Tensor.encode([4, 4], np.array([[0, 4], [0, 0]], dtype=np.uint64), np.ones(2))
     assert e.value.status == blco.ERR_INVALID
     with pytest.raises(blco.BlcoError) as e:
-        blco.Tensor.encode([1 << 30, 1 << 30, 1 << 10], np.zeros((3, 1), dtype=np.uint64), np.ones(1))
+        # 160 key bits: wider than the reference's widest (128-bit) key
+        blco.Tensor.encode([(1 << 32) - 1] * 5, np.zeros((5, 1), dtype=np.uint64), np.ones(1))
     assert e.value.status == blco.ERR_UNSUPPORTED
     with pytest.raises(blco.BlcoError) as e:
         blco.Tensor.encode([4, 0], np.zeros((2, 1), dtype=np.uint64), np.ones(1))

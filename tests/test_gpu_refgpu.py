@@ -87,3 +87,55 @@ def test_cpals_skewed_matches_reference_gpu(blco):
     assert abs(fit_g - fit_r) <= 1e-10, (fit_g, fit_r)
     for a, b in zip(fg, fr):
         assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("ref_kernel", [1, 10])
+def test_wide_mttkrp_matches_reference_gpu_cpd128(blco, ref_kernel):
+    """Keys of 68 bits: the reference's 128-bit build (tensor encoded by
+    gen_blcotensor_host<unsigned __int128>, many blocks with block
+    coordinates) against this engine's wide-key path.  The reference's GPU
+    kernels take order 3 and 4 only (src/alto_dev.cu:290-304)."""
+    import torch
+    from conftest import unique_coords_wide
+    rng = np.random.default_rng(40 + ref_kernel)
+    dims = [1 << 17, 1 << 17, 100_000, 1 << 17]
+    nnz = 60_000
+    cidx = unique_coords_wide(rng, dims, nnz)
+    vals = rng.random(nnz)
+    R = 16
+    fs = [rng.random((d, R)) for d in dims]
+    t = blco.Tensor.encode(dims, cidx, vals)
+    assert t.info()["block_count"] > 1
+    dev = [torch.from_numpy(f).cuda() for f in fs]
+    for m in (0, 3):
+        ref = po.refgpu_mttkrp(dims, cidx, vals, fs, m, kernel=ref_kernel, wide=True)
+        out = torch.zeros(dims[m], R, dtype=torch.float64, device="cuda")
+        blco.mttkrp(t, m, dev, out, blco.make_opts(kernel=ref_kernel))
+        torch.cuda.synchronize()
+        o = out.cpu().numpy()
+        err = np.linalg.norm(o - ref) / np.linalg.norm(ref)
+        assert err <= 1e-12, (m, err)
+    t.free()
+
+
+def test_wide_cpals_matches_reference_gpu_cpd128(blco):
+    from conftest import unique_coords_wide
+    rng = np.random.default_rng(77)
+    dims = [1 << 17, 1 << 17, 100_000, 1 << 17]
+    nnz = 40_000
+    cidx = unique_coords_wide(rng, dims, nnz)
+    vals = rng.random(nnz)
+    R = 8
+    fs0 = [rng.random((d, R)) for d in dims]
+    fr = [f.copy() for f in fs0]
+    lr = np.ones(R)
+    fit_r = po.refgpu_cpals(dims, cidx, vals, fr, lr, 5, 0.0, kernel=10, wide=True)
+    t = blco.Tensor.encode(dims, cidx, vals)
+    fg = [f.copy() for f in fs0]
+    lg = np.ones(R)
+    fit_g, fits_g = blco.cpals(t, fg, lg, 5, 0.0, blco.make_opts(kernel=10))
+    assert len(fits_g) == 5
+    assert abs(fit_g - fit_r) <= 1e-10, (fit_g, fit_r)
+    for a, b in zip(fg, fr):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+    t.free()
