@@ -13,6 +13,11 @@ the 126 MB L2, so no flush is needed between steps.
 --impl reference times the reference's own CPU MTTKRP (mttkrp_alto_par from
 include/alto.hpp, compiled from the reference sources into oracle/_ref) on a
 bounded sample of the same workload with all host threads.
+
+Two more legs ride on the same line (skip with --no-batched / --no-wide):
+`batched`, batched CP-ALS of 512 small tensors, and `wide`, FP64 CP-ALS of a
+100M-nonzero tensor whose keys need 72 bits (the reference's 128-bit build),
+with its own roofline and CPU baseline.
 """
 import argparse
 import json
@@ -58,13 +63,13 @@ def mttkrp_alg_bytes(dims, nnz, R, mode, s_idx=8, s_val=8, s_fac=8, s_out=8):
     return b
 
 
-def traffic_from_profiles(form, nnz):
+def traffic_from_profiles(form, nnz, name=None, full_nnz=None):
     """DRAM bytes per MTTKRP (all kernels of one mode, mean over the modes)
     at the full-size workload, from the committed ncu summary of the chosen
-    form, if there is one."""
-    if nnz != WORKLOAD["nnz"]:
+    form (or the summary `name`), if there is one."""
+    if nnz != (full_nnz or WORKLOAD["nnz"]):
         return None
-    p = os.path.join(ROOT, "profiles", f"mttkrp_{form}_zipf_2Mx2Mx25k_r32.md")
+    p = os.path.join(ROOT, "profiles", name or f"mttkrp_{form}_zipf_2Mx2Mx25k_r32.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
@@ -323,6 +328,96 @@ def batched_leg(pkg, torch, args):
                      f"{k} tensors' plans (wall time), scaled by nnz")
 
 
+WIDE = dict(workload="mttkrp_wide_zipf1.1_2^20x2^20x2^20x4096_nnz100M_r32",
+            desc=("keys of 72 bits (the reference's 128-bit build): Zipf(1.1) coordinates over 2^20 x 2^20 x 2^20 "
+                  "x 4096, 100M distinct nonzeros, lognormal FP32 values, rank 32, FP64 CP-ALS"),
+            dims=[1 << 20, 1 << 20, 1 << 20, 1 << 12], nnz=100_000_000, zipf=1.1, rank=32, seed=7)
+
+
+def wide_cpu_baseline(args, X, dims, rk):
+    """The reference's 128-bit CPU ALTO MTTKRP (oracle/_ref) on a bounded
+    sample of the wide workload, all modes, scaled to its nonzeros."""
+    import ctypes
+    import pyoracle as po
+    R = po.ref_lib()
+    if R is None:
+        return None
+    sample = min(args.ref_sample, WIDE["nnz"])
+    cidx = np.ascontiguousarray(np.stack([c[:sample].cpu().numpy().astype(np.uint64) for c in X["cidx"]]))
+    vals = np.ascontiguousarray(X["vals"][:sample].cpu().numpy())
+    nthreads = os.cpu_count() or 1
+    d64 = np.ascontiguousarray(dims, dtype=np.uint64)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    f64p = ctypes.POINTER(ctypes.c_double)
+    h = R.ref_alto_create128(len(dims), d64.ctypes.data_as(u64p), sample, cidx.ctypes.data_as(u64p),
+                             vals.ctypes.data_as(f64p), nthreads)
+    rng = np.random.default_rng(0)
+    fs = [rng.random((d, rk)) for d in dims]
+    ptrs = (ctypes.c_void_p * len(dims))(*[f.ctypes.data for f in fs])
+    for m in range(len(dims)):
+        R.ref_alto_mttkrp128(h, m, rk, ptrs)
+    t0 = time.perf_counter()
+    for m in range(len(dims)):
+        R.ref_alto_mttkrp128(h, m, rk, ptrs)
+    dt = (time.perf_counter() - t0) * 1e3
+    R.ref_alto_destroy128(h, rk)
+    return dict(value=dt / sample * WIDE["nnz"], unit="ms", cores=nthreads, kind="reference",
+                sample=(f"reference mttkrp_alto_par on AltoTensor<unsigned __int128> (oracle/_ref), all "
+                        f"{len(dims)} modes on the first {sample} nonzeros, {nthreads} threads, scaled linearly "
+                        f"to {WIDE['nnz']} nonzeros; MTTKRP part of the iteration only"))
+
+
+def wide_leg(pkg, torch, args, peak, with_cpu):
+    """FP64 CP-ALS of the wide-key workload: encode, device ms per
+    iteration, per-mode MTTKRP time and its roofline, the reference's CPU
+    MTTKRP on a sample."""
+    from blco_b200 import synth
+    dims, nnz, rk = WIDE["dims"], WIDE["nnz"], WIDE["rank"]
+    X = synth.wide_tensor_device(nnz, dims, WIDE["zipf"], seed=WIDE["seed"])
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"])
+    torch.cuda.synchronize()
+    encode_ms = (time.perf_counter() - e0) * 1e3
+    cpu = wide_cpu_baseline(args, X, dims, rk) if with_cpu else None
+    del X
+    torch.cuda.empty_cache()
+    inf = t.info()
+    g = torch.Generator(device="cuda").manual_seed(4321)
+    fs = [torch.rand(d, rk, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    lam = torch.ones(rk, dtype=torch.float64, device="cuda")
+    plan = pkg.CpalsPlan(t, fs, lam, pkg.make_opts(kernel=pkg.KERNEL_AUTO))
+    plan.iterate(args.warmup, tol=-1.0)
+    ms0, c0 = plan.mttkrp_ms()
+    pkg.launch_count(reset=True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    fits = plan.iterate(args.steps, tol=-1.0)
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = pkg.launch_count(reset=True)
+    ms1, c1 = plan.mttkrp_ms()
+    per_mode = list((ms1 - ms0) / max(1, c1 - c0))
+    plan.destroy()
+    t.free()
+    del fs
+    torch.cuda.empty_cache()
+    alg = [mttkrp_alg_bytes(dims, nnz, rk, m) for m in range(len(dims))]
+    achieved = sum(alg) / (sum(per_mode) * 1e-3) / 1e9
+    return dict(workload=WIDE["workload"], desc=WIDE["desc"], key_bits=inf["alto_bits"],
+                blocks=inf["block_count"], encode_ms=encode_ms,
+                ms_per_step=ev0.elapsed_time(ev1) / args.steps, steps=args.steps, fit_last=fits[-1],
+                mttkrp_ms_per_mode=[round(x, 4) for x in per_mode], gpu_launches=int(launches), dtype="f64",
+                roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                              traffic=traffic_from_profiles("fp64", nnz, "mttkrp_wide_zipf_2p20x3x4096_r32.md",
+                                                            WIDE["nnz"]),
+                              kernel="k_mttkrp_wide (one launch per mode), mean over the 4 modes",
+                              alg_bytes_per_launch=[int(x) for x in alg]),
+                cpu_baseline=cpu)
+
+
 def run_ours(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
@@ -423,6 +518,9 @@ def run_ours(args, world, rank, local):
     batched = None
     if not args.no_batched:
         batched = batched_leg(pkg, torch, args)
+    wide = None
+    if not args.no_wide:
+        wide = wide_leg(pkg, torch, args, peaks()[0], rank == 0 and world == 1 and not args.no_cpu_baseline)
     if rank == 0:
         forms_out = {}
         for f, r in res.items():
@@ -456,6 +554,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": C["launches"],
             "clocks": C["clocks"],
             "batched": batched,
+            "wide": wide,
         }
         print(json.dumps(line))
     if dist:
@@ -476,6 +575,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=2_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched many-small-tensors leg")
+    ap.add_argument("--no-wide", action="store_true", help="skip the wide-key (128-bit BLCO) leg")
     ap.add_argument("--forms", default="fp64,mixed_f32,mixed_bf16")
     args = ap.parse_args()
     world, rank, local = dist_setup()

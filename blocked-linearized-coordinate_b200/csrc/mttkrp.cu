@@ -884,6 +884,115 @@ __global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide(const WideParams p
     }
 }
 
+// The same walk with two columns per lane (16-byte gathers of FP64 pairs),
+// the mode count fixed at compile time and every row decoded once, when
+// its batch is loaded: L = R/2 lanes per nonzero (R even, 2L >= R, column
+// slab of up to 64), 32/L nonzeros in flight per warp instruction.
+// OFF32: factor offsets row * R + col fit in 32 bits.
+struct WideParams2 {
+    const uint64_t* coords;
+    const uint64_t* field;
+    const double* vals;
+    uint64_t nnz;
+    Layout L;
+    const double* fo[BLCO_MAX_MODES - 1]; // factors of the other modes, in mode order
+    int other[BLCO_MAX_MODES - 1];        // their mode numbers
+    double* out;
+    int mode;
+    int rank;
+    int col0;
+};
+
+template <int NM, int L, bool OFF32>
+__global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide2(const WideParams2 p)
+{
+    constexpr int NO = NM - 1;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % L;
+    const int grp = lane / L;
+    constexpr uint64_t WARP_TASK = (uint64_t)32 * WIDE_BATCHES;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (WIDE_THREADS / 32);
+    const uint64_t wid = (uint64_t)blockIdx.x * (WIDE_THREADS / 32) + (threadIdx.x >> 5);
+    const int R = p.rank;
+    const int col = p.col0 + 2 * sub;
+    const bool cok = col < R; // col + 1 < R too: R is even
+    const uint64_t ntasks = (p.nnz + WARP_TASK - 1) / WARP_TASK;
+    for (uint64_t task = wid; task < ntasks; task += nwarps) {
+        const uint64_t g0 = task * WARP_TASK + (uint64_t)grp * (L * WIDE_BATCHES);
+        uint32_t cur = 0xffffffffu;
+        double a0 = 0.0, a1 = 0.0;
+        for (int b = 0; b < WIDE_BATCHES; b++) {
+            const uint64_t i = g0 + (uint64_t)b * L + sub;
+            const bool ok = i < p.nnz;
+            uint32_t rt = 0xffffffffu, ro[NO];
+            double v = 0.0;
+            {
+                const uint64_t c = ok ? __ldg(p.coords + i) : 0;
+                const uint64_t f = ok ? __ldg(p.field + i) : 0;
+                v = ok ? __ldg(p.vals + i) : 0.0;
+                if (ok) rt = (uint32_t)wide_row(p.L, p.mode, c, f);
+#pragma unroll
+                for (int k = 0; k < NO; k++) ro[k] = (uint32_t)wide_row(p.L, p.other[k], c, f);
+            }
+#pragma unroll 4
+            for (int j = 0; j < L; j++) {
+                const uint32_t r = __shfl_sync(0xffffffffu, rt, j, L);
+                const double vv = __shfl_sync(0xffffffffu, v, j, L);
+                uint32_t rr[NO];
+#pragma unroll
+                for (int k = 0; k < NO; k++) rr[k] = __shfl_sync(0xffffffffu, ro[k], j, L);
+                if (r == 0xffffffffu) continue; // past the end of the stream
+                if (r != cur) {
+                    if (cur != 0xffffffffu && cok) {
+                        double* o = p.out + (uint64_t)cur * R + col;
+                        atomicAdd(o, a0);
+                        atomicAdd(o + 1, a1);
+                    }
+                    a0 = a1 = 0.0;
+                    cur = r;
+                }
+                if (cok) {
+                    double p0 = vv, p1 = vv;
+#pragma unroll
+                    for (int k = 0; k < NO; k++) {
+                        const double2* src;
+                        if (OFF32) src = reinterpret_cast<const double2*>(p.fo[k] + (rr[k] * (uint32_t)R + (uint32_t)col));
+                        else src = reinterpret_cast<const double2*>(p.fo[k] + ((uint64_t)rr[k] * R + col));
+                        const double2 x = __ldg(src);
+                        p0 *= x.x;
+                        p1 *= x.y;
+                    }
+                    a0 += p0;
+                    a1 += p1;
+                }
+            }
+        }
+        if (cur != 0xffffffffu && cok) {
+            double* o = p.out + (uint64_t)cur * R + col;
+            atomicAdd(o, a0);
+            atomicAdd(o + 1, a1);
+        }
+    }
+}
+
+template <int NM>
+int launch_wide2(const WideParams2& p, int grid, int lanes, bool off32, cudaStream_t s)
+{
+#define WIDE2_CASE(LL)                                                                     \
+    if (lanes == LL) {                                                                     \
+        if (off32) k_mttkrp_wide2<NM, LL, true><<<grid, WIDE_THREADS, 0, s>>>(p);          \
+        else k_mttkrp_wide2<NM, LL, false><<<grid, WIDE_THREADS, 0, s>>>(p);               \
+        BLCO_CHECK_LAUNCH("k_mttkrp_wide2");                                               \
+        return BLCO_OK;                                                                    \
+    }
+    WIDE2_CASE(4)
+    WIDE2_CASE(8)
+    WIDE2_CASE(16)
+    WIDE2_CASE(32)
+#undef WIDE2_CASE
+    return fail(BLCO_ERR_INVALID, "wide MTTKRP: bad lane count");
+}
+
 } // namespace
 
 int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
@@ -909,6 +1018,43 @@ int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s
     const uint64_t ntasks = (a.nnz + 32 * WIDE_BATCHES - 1) / (32 * WIDE_BATCHES);
     const int grid = (int)std::min<uint64_t>((ntasks + WIDE_THREADS / 32 - 1) / (WIDE_THREADS / 32),
                                              (uint64_t)di.sm_count * 8);
+    // two columns per lane when every factor row starts on 16 bytes
+    bool pairs = a.rank % 2 == 0 && ((uintptr_t)a.out & 15) == 0;
+    uint64_t maxdim = 0;
+    for (int m = 0; m < t->layout.nmodes; m++) {
+        if (m != a.mode && ((uintptr_t)a.factors[m] & 15)) pairs = false;
+        maxdim = std::max(maxdim, t->layout.dims[m]);
+    }
+    const int nm = t->layout.nmodes;
+    if (pairs && nm >= 3) {
+        WideParams2 q;
+        memset(&q, 0, sizeof(q));
+        q.coords = p.coords;
+        q.field = p.field;
+        q.vals = p.vals;
+        q.nnz = p.nnz;
+        q.L = p.L;
+        q.out = p.out;
+        q.mode = p.mode;
+        q.rank = p.rank;
+        for (int m = 0, k = 0; m < nm; m++)
+            if (m != a.mode) {
+                q.fo[k] = p.f[m];
+                q.other[k++] = m;
+            }
+        const bool off32 = maxdim * (uint64_t)a.rank < (1ull << 32);
+        for (int c0 = 0; c0 < a.rank; c0 += 64) {
+            q.col0 = c0;
+            const int cols = std::min(64, a.rank - c0);
+            const int lanes = cols <= 8 ? 4 : cols <= 16 ? 8 : cols <= 32 ? 16 : 32;
+            int st;
+            if (nm == 3) st = launch_wide2<3>(q, grid, lanes, off32, s);
+            else if (nm == 4) st = launch_wide2<4>(q, grid, lanes, off32, s);
+            else st = launch_wide2<5>(q, grid, lanes, off32, s);
+            if (st != BLCO_OK) return st;
+        }
+        return BLCO_OK;
+    }
     for (int c0 = 0; c0 < a.rank; c0 += 128) {
         p.col0 = c0;
         const int cols = std::min(128, a.rank - c0);
