@@ -934,33 +934,45 @@ __global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide2(const WideParams2
 #pragma unroll
                 for (int k = 0; k < NO; k++) ro[k] = (uint32_t)wide_row(p.L, p.other[k], c, f);
             }
-#pragma unroll 4
-            for (int j = 0; j < L; j++) {
-                const uint32_t r = __shfl_sync(0xffffffffu, rt, j, L);
-                const double vv = __shfl_sync(0xffffffffu, v, j, L);
-                uint32_t rr[NO];
+            // U nonzeros at a time: every gather of the U is issued before
+            // the first product, so each lane has U x (NM-1) loads in flight
+            constexpr int U = 4;
+#pragma unroll 1
+            for (int j0 = 0; j0 < L; j0 += U) {
+                uint32_t r[U];
+                double vv[U];
+                double2 x[U][NO];
 #pragma unroll
-                for (int k = 0; k < NO; k++) rr[k] = __shfl_sync(0xffffffffu, ro[k], j, L);
-                if (r == 0xffffffffu) continue; // past the end of the stream
-                if (r != cur) {
-                    if (cur != 0xffffffffu && cok) {
-                        double* o = p.out + (uint64_t)cur * R + col;
-                        atomicAdd(o, a0);
-                        atomicAdd(o + 1, a1);
-                    }
-                    a0 = a1 = 0.0;
-                    cur = r;
-                }
-                if (cok) {
-                    double p0 = vv, p1 = vv;
+                for (int u = 0; u < U; u++) {
+                    r[u] = __shfl_sync(0xffffffffu, rt, j0 + u, L);
+                    vv[u] = __shfl_sync(0xffffffffu, v, j0 + u, L);
 #pragma unroll
                     for (int k = 0; k < NO; k++) {
+                        const uint32_t rr = __shfl_sync(0xffffffffu, ro[k], j0 + u, L);
                         const double2* src;
-                        if (OFF32) src = reinterpret_cast<const double2*>(p.fo[k] + (rr[k] * (uint32_t)R + (uint32_t)col));
-                        else src = reinterpret_cast<const double2*>(p.fo[k] + ((uint64_t)rr[k] * R + col));
-                        const double2 x = __ldg(src);
-                        p0 *= x.x;
-                        p1 *= x.y;
+                        if (OFF32) src = reinterpret_cast<const double2*>(p.fo[k] + (rr * (uint32_t)R + (uint32_t)col));
+                        else src = reinterpret_cast<const double2*>(p.fo[k] + ((uint64_t)rr * R + col));
+                        // rows of nonzeros past the end decode to row 0: in bounds
+                        x[u][k] = cok ? __ldg(src) : make_double2(0.0, 0.0);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (r[u] == 0xffffffffu) continue; // past the end of the stream
+                    if (r[u] != cur) {
+                        if (cur != 0xffffffffu && cok) {
+                            double* o = p.out + (uint64_t)cur * R + col;
+                            atomicAdd(o, a0);
+                            atomicAdd(o + 1, a1);
+                        }
+                        a0 = a1 = 0.0;
+                        cur = r[u];
+                    }
+                    double p0 = vv[u], p1 = vv[u];
+#pragma unroll
+                    for (int k = 0; k < NO; k++) {
+                        p0 *= x[u][k].x;
+                        p1 *= x[u][k].y;
                     }
                     a0 += p0;
                     a1 += p1;
