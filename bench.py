@@ -141,6 +141,73 @@ def max_over_ranks(x, dist, device="cuda"):
     return tt.item()
 
 
+def reference_gpu_leg(args):
+    """The reference's own GPU CP-ALS (cpals_blco_dev, src/cpd_gpu.cu:21-242,
+    rebuilt unchanged for sm_100a into oracle/_ref/libblco_refgpu.so) on the
+    full workload with the same initial factors as this engine's arm:
+    median of its own per-iteration times (CUDA events around each
+    iteration, src/cpd_gpu.cu:148-193) after the warm-up iterations.  The
+    reference encodes on the host first (minutes at 200M nonzeros)."""
+    import re
+    import tempfile
+    import torch
+    import pyoracle as po
+    if not po.refgpu_available():
+        return {"unavailable": "oracle/_ref/libblco_refgpu.so not built"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no GPU"}
+    from blco_b200 import synth
+    dims, nnz, rk = WORKLOAD["dims"], args.nnz, WORKLOAD["rank"]
+    X = synth.zipf_tensor_device(nnz, dims, WORKLOAD["zipf"], seed=args.seed)
+    cidx = np.ascontiguousarray(np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]]))
+    vals = np.ascontiguousarray(X["vals"].cpu().numpy())
+    del X
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    fs = [np.ascontiguousarray(torch.rand(d, rk, dtype=torch.float64, device="cuda", generator=g).cpu().numpy())
+          for d in dims]
+    torch.cuda.empty_cache()
+    out = {}
+    for kernel in (10, 2):
+        lam = np.ones(rk)
+        f = [x.copy() for x in fs]
+        with tempfile.NamedTemporaryFile("r", suffix=".log") as lf:
+            t0 = time.perf_counter()
+            fit = po.refgpu_cpals(dims, cidx, vals, f, lam, args.warmup + args.steps, -1.0, kernel=kernel,
+                                  log_path=lf.name, timeout=2400)
+            wall = time.perf_counter() - t0
+            log = open(lf.name).read()
+        its = [float(x) * 1e3 for x in re.findall(r"--> Iter +\d+: .*time = ([0-9.]+)", log)]
+        timed = its[args.warmup:]
+        out[f"k{kernel}"] = dict(ms_per_step=statistics.median(timed) if timed else None, iterations=len(its),
+                                 fit_last=fit, wall_s_including_host_encode=wall)
+    if not args.no_wide:
+        # the wide-key workload through the reference's 128-bit build (same tensor and factors as the wide leg)
+        X = synth.wide_tensor_device(WIDE["nnz"], WIDE["dims"], WIDE["zipf"], seed=WIDE["seed"])
+        wc = np.ascontiguousarray(np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]]))
+        wv = np.ascontiguousarray(X["vals"].cpu().numpy())
+        del X
+        g = torch.Generator(device="cuda").manual_seed(4321)
+        wf = [np.ascontiguousarray(torch.rand(d, WIDE["rank"], dtype=torch.float64, device="cuda",
+                                              generator=g).cpu().numpy()) for d in WIDE["dims"]]
+        torch.cuda.empty_cache()
+        lam = np.ones(WIDE["rank"])
+        with tempfile.NamedTemporaryFile("r", suffix=".log") as lf:
+            t0 = time.perf_counter()
+            fit = po.refgpu_cpals(WIDE["dims"], wc, wv, wf, lam, args.warmup + args.steps, -1.0, kernel=10,
+                                  log_path=lf.name, wide=True, timeout=2400)
+            wall = time.perf_counter() - t0
+            log = open(lf.name).read()
+        its = [float(x) * 1e3 for x in re.findall(r"--> Iter +\d+: .*time = ([0-9.]+)", log)]
+        timed = its[args.warmup:]
+        out["wide_k10"] = dict(workload=WIDE["workload"], ms_per_step=statistics.median(timed) if timed else None,
+                               iterations=len(its), fit_last=fit, wall_s_including_host_encode=wall)
+    out["note"] = ("reference cpals_blco_dev (oracle/_ref/libblco_refgpu.so, unchanged source for sm_100a), FP64, "
+                   "-k 10 (lvl1 for these mode lengths) and -k 2 (lvl2), one block, the full workload and this engine's initial factors; median of the "
+                   f"reference's own per-iteration times after {args.warmup} warm-up iterations; wide_k10: the "
+                   "wide-key workload through the reference's 128-bit encoding (one block per upper key word)")
+    return out
+
+
 def run_reference(args, world, rank):
     """The reference's CPU MTTKRP on a bounded sample of the workload."""
     if rank != 0:
@@ -194,6 +261,7 @@ def run_reference(args, world, rank):
         "config": dict(workload=WORKLOAD["workload"], parallelism="cpu", l2="inputs larger than L2"),
         "cpu_baseline": dict(value=value, unit="ms", cores=nthreads, kind="reference", sample=desc),
         "e2e": dict(value=value, unit="ms", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+        "reference_gpu": reference_gpu_leg(args) if args.ref_gpu else None,
     }))
 
 
@@ -576,6 +644,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched many-small-tensors leg")
     ap.add_argument("--no-wide", action="store_true", help="skip the wide-key (128-bit BLCO) leg")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="--impl reference: also time the reference's own GPU CP-ALS on the full workload")
     ap.add_argument("--forms", default="fp64,mixed_f32,mixed_bf16")
     args = ap.parse_args()
     world, rank, local = dist_setup()

@@ -288,7 +288,7 @@ def refgpu_available():
     return os.path.exists(os.path.join(HERE, "_ref", "libblco_refgpu.so"))
 
 
-def _refgpu_call(req, log_path=None):
+def _refgpu_call(req, log_path=None, timeout=600):
     """Runs one reference call in a child interpreter (the reference exits
     the process on CUDA errors); returns the result arrays."""
     import subprocess
@@ -298,7 +298,7 @@ def _refgpu_call(req, log_path=None):
         qp, rp = os.path.join(d, "req.npz"), os.path.join(d, "res.npz")
         np.savez(qp, **req)
         p = subprocess.run([sys.executable, os.path.join(HERE, "refgpu_run.py"), qp, rp],
-                           capture_output=True, text=True, timeout=600)
+                           capture_output=True, text=True, timeout=timeout)
         if log_path:
             with open(log_path, "a") as f:
                 f.write(p.stdout + p.stderr)
@@ -319,11 +319,11 @@ def _req(dims, cidx, vals, factors, **kw):
 
 
 def refgpu_cpals(dims, cidx, vals, factors, lam, maxiter, tol, kernel=10, nprtn=8, thread_cf=2, log_path=None,
-                 wide=False):
+                 wide=False, timeout=600):
     """Runs the reference cpals_blco_dev (wide: on the 128-bit build's
     encoding); factors/lam updated in place; returns the final fit."""
     res = _refgpu_call(_req(dims, cidx, vals, factors, op="cpals", lam=lam, maxiter=maxiter, tol=tol,
-                            kernel=kernel, nprtn=nprtn, thread_cf=thread_cf, wide=int(wide)), log_path)
+                            kernel=kernel, nprtn=nprtn, thread_cf=thread_cf, wide=int(wide)), log_path, timeout)
     for m, f in enumerate(factors):
         f[:] = res[f"f{m}"]
     lam[:] = res["lam"]
