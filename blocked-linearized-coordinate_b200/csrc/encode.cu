@@ -1111,7 +1111,10 @@ int build_hot_tables(blco_tensor* t, cudaStream_t s)
         BLCO_CUDA(cudaMemcpyAsync(ht.d_ptr, ptr.data(), (ht.nhot + 1) * 4, cudaMemcpyHostToDevice, s));
     }
     BLCO_CUDA(cudaStreamSynchronize(s));
-    BLCO_TRY(build_hot_csr(t, s));
+    // The per-mode execution copies live in HBM and serve resident streams
+    // only; a streamed tensor keeps just the statistics and hash tables, so
+    // that its device footprint stays the ring of block buffers.
+    if (t->resident) BLCO_TRY(build_hot_csr(t, s));
     return BLCO_OK;
 }
 

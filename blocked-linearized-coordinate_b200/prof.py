@@ -6,6 +6,13 @@
   python blocked-linearized-coordinate_b200/prof.py batch --count T [--iters I]
       Batched CP-ALS sweeps over T small tensors of the many-small-tensors
       recipe (FP64); prints device ms per sweep.
+  python blocked-linearized-coordinate_b200/prof.py cpals --nnz N --dtype f64|f32|bf16 [--iters I]
+      CP-ALS iterations on the Zipf(1.1) 2M x 2M x 25k tensor (rank 32):
+      ms per iteration, MTTKRP ms per mode, and the rest of the iteration.
+  python blocked-linearized-coordinate_b200/prof.py stream --nnz N [--block B] [--residency BYTES]
+      The streamed form on the 4-mode 500k x 200k x 50k x 1k Zipf(0.9) shape,
+      rank 64, FP64: ms per CP-ALS iteration and host-to-device GB/s against
+      a measured pinned copy.
   python blocked-linearized-coordinate_b200/prof.py wide --nnz N [--rank R] [--reps K] [--iters I]
       The wide-key workload: Zipf(1.1) over 2^20 x 2^20 x 2^20 x 4096
       (72 key bits, the reference's 128-bit build), FP64: encode time and
@@ -63,6 +70,85 @@ def run_mttkrp(a, pkg, torch):
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         print(f"mode {m}: ms {['%.3f' % x for x in ts]}", flush=True)
+    t.free()
+
+
+def run_cpals(a, pkg, torch):
+    from blco_b200 import synth
+    dims = [2_000_000, 2_000_000, 25_000]
+    X = synth.zipf_tensor_device(a.nnz, dims, 1.1, seed=0)
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"])
+    del X
+    torch.cuda.empty_cache()
+    R = a.rank
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    fs = [torch.rand(d, R, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    lam = torch.ones(R, dtype=torch.float64, device="cuda")
+    prec = {"f64": pkg.PRECISION_FP64, "f32": pkg.PRECISION_MIXED, "bf16": pkg.PRECISION_MIXED_BF16}[a.dtype]
+    plan = pkg.CpalsPlan(t, fs, lam, pkg.make_opts(kernel=a.kernel, precision=prec))
+    plan.iterate(3, tol=-1.0)
+    ms0, c0 = plan.mttkrp_ms()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    fits = plan.iterate(a.iters, tol=-1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms1, c1 = plan.mttkrp_ms()
+    per = (ms1 - ms0) / max(1, c1 - c0)
+    it = e0.elapsed_time(e1) / a.iters
+    print(f"cpals {a.dtype} ms/iter {it:.3f} mttkrp ms/mode {['%.3f' % x for x in per]} "
+          f"rest ms/iter {it - sum(per):.3f} fit {fits[-1]:.9f}", flush=True)
+    plan.destroy()
+    t.free()
+
+
+def run_stream(a, pkg, torch):
+    """The streamed (out-of-memory) form on the 4-mode Zipf(0.9) shape
+    500k x 200k x 50k x 1k, rank 64, FP64: blocks of --block nonzeros in
+    pinned host memory, copied through a ring of at most --residency bytes;
+    host-to-device GB/s per CP-ALS iteration against a pinned copy."""
+    from blco_b200 import synth
+    dims = [500_000, 200_000, 50_000, 1_000]
+    X = synth.zipf_tensor_device(a.nnz, dims, 0.9, seed=0, value_dist="uniform")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    # pinned host-to-device peak: 2 GiB, best of 3
+    hb = torch.empty(1 << 28, dtype=torch.float64).pin_memory()
+    db = torch.empty(1 << 28, dtype=torch.float64, device="cuda")
+    best = 0.0
+    for _ in range(3):
+        e0.record()
+        db.copy_(hb, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, hb.numel() * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del hb, db
+    o = pkg.make_opts(kernel=10, stream_data=True, residency_bytes=a.residency)
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"], a.block, o)
+    del X
+    torch.cuda.empty_cache()
+    inf = t.info()
+    R = a.rank
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    fs = [torch.rand(d, R, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    lam = torch.ones(R, dtype=torch.float64, device="cuda")
+    plan = pkg.CpalsPlan(t, fs, lam, o)
+    plan.iterate(1, tol=-1.0)
+    torch.cuda.synchronize()
+    free_b, total_b = torch.cuda.mem_get_info()
+    e0.record()
+    fits = plan.iterate(a.iters, tol=-1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    it = e0.elapsed_time(e1) / a.iters
+    h2d = len(dims) * a.nnz * 16
+    print(f"streamed fp64 nnz {a.nnz} blocks {inf['block_count']} residency {a.residency} ms/iter {it:.1f} "
+          f"h2d GB/iter {h2d / 1e9:.2f} h2d GB/s {h2d / (it * 1e-3) / 1e9:.1f} pinned peak GB/s {best:.1f} "
+          f"frac {h2d / (it * 1e-3) / 1e9 / best:.3f} device GB in use {(total_b - free_b) / 1e9:.1f} "
+          f"fit {fits[-1]:.6f}", flush=True)
+    plan.destroy()
     t.free()
 
 
@@ -179,6 +265,18 @@ def main():
     tn = sub.add_parser("tns")
     tn.add_argument("--nnz", type=int, default=50_000_000)
     tn.add_argument("--dir", default="tns_prof")
+    c = sub.add_parser("cpals")
+    c.add_argument("--nnz", type=int, default=200_000_000)
+    c.add_argument("--dtype", default="f32", choices=["f64", "f32", "bf16"])
+    c.add_argument("--kernel", type=int, default=10)
+    c.add_argument("--rank", type=int, default=32)
+    c.add_argument("--iters", type=int, default=10)
+    sm = sub.add_parser("stream")
+    sm.add_argument("--nnz", type=int, default=500_000_000)
+    sm.add_argument("--rank", type=int, default=64)
+    sm.add_argument("--block", type=int, default=64 << 20)
+    sm.add_argument("--residency", type=int, default=8 << 30)
+    sm.add_argument("--iters", type=int, default=2)
     w = sub.add_parser("wide")
     w.add_argument("--nnz", type=int, default=50_000_000)
     w.add_argument("--rank", type=int, default=32)
@@ -189,7 +287,8 @@ def main():
     pkg = load()
     if os.environ.get("BLCO_LIB"):
         pkg.LIB_PATH = os.environ["BLCO_LIB"]
-    {"mttkrp": run_mttkrp, "batch": run_batch, "tns": run_tns, "wide": run_wide}[a.cmd](a, pkg, torch)
+    {"mttkrp": run_mttkrp, "batch": run_batch, "tns": run_tns, "wide": run_wide,
+     "cpals": run_cpals, "stream": run_stream}[a.cmd](a, pkg, torch)
 
 
 if __name__ == "__main__":
