@@ -137,6 +137,13 @@ int blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
     BLCO_CUDA(cudaSetDevice(device));
     DeviceInfo di;
     BLCO_TRY(device_info(device, &di));
+    // A streamed tensor larger than one chunk is encoded chunk by chunk
+    // straight from the host arrays: the COO never sits whole on the device.
+    if (opts && opts->stream_data && nnz > stream_chunk_nnz(opts, nmodes)) {
+        for (int n = 0; n < nmodes; n++)
+            if (!cidx[n]) return fail(BLCO_ERR_INVALID, "null coordinate array");
+        return encode_impl(nmodes, dims, nnz, cidx, vals, max_block_size, opts, out);
+    }
     const uint64_t n_alloc = nnz ? nnz : 1;
     uint64_t* dc[BLCO_MAX_MODES] = {};
     double* dv = nullptr;

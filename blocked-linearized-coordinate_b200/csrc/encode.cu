@@ -14,7 +14,9 @@
 // Then per-mode row statistics and heavy-row tables for the MTTKRP kernels.
 #include <algorithm>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 
 #include "internal.cuh"
 
@@ -472,6 +474,25 @@ struct StatOut {
     unsigned long long nonempty;
     unsigned long long maxc;
 };
+
+// Nonzeros per row of every mode, from COO arrays (the chunked encoder,
+// whose stream never sits whole on the device); warp-aggregated atomics.
+// Coordinates at or above the mode length are skipped here (k_alto_keys
+// reports them; the encode then fails).
+__global__ __launch_bounds__(RC_THREADS) void k_coo_counts(CooPtrs coo, uint64_t nnz, Layout L, CountPtrs counts)
+{
+    const int lane = threadIdx.x & 31;
+    for (uint64_t b0 = blockIdx.x * (uint64_t)RC_THREADS; b0 < nnz; b0 += (uint64_t)gridDim.x * RC_THREADS) {
+        const uint64_t i = b0 + threadIdx.x;
+        for (int n = 0; n < L.nmodes; n++) {
+            const uint64_t c = i < nnz ? coo.c[n][i] : ~0ull;
+            const bool ok = c < L.dims[n];
+            const uint32_t row = ok ? (uint32_t)c : 0xffffffffu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, row);
+            if (ok && (peers & ((1u << lane) - 1)) == 0) atomicAdd(&counts.c[n][row], (uint32_t)__popc(peers));
+        }
+    }
+}
 
 __global__ void k_row_stats(const uint32_t* __restrict__ counts, uint64_t rows, StatOut* out)
 {
@@ -1006,7 +1027,10 @@ int sort_stream_by_mode(const blco_tensor* t, int mode, uint64_t* d_coords, doub
     return BLCO_OK;
 }
 
-int build_hot_tables(blco_tensor* t, cudaStream_t s)
+// Heavy-row statistics and tables.  counts_in (device, the per-row
+// nonzero counts of every mode concatenated) is used when given; otherwise
+// the counts are taken from the resident stream.
+static int build_hot_tables_impl(blco_tensor* t, cudaStream_t s, uint32_t* counts_in)
 {
     const Layout& L = t->layout;
     DeviceInfo di;
@@ -1015,15 +1039,17 @@ int build_hot_tables(blco_tensor* t, cudaStream_t s)
     memset(&cp, 0, sizeof(cp));
     uint64_t total_rows = 0;
     for (int n = 0; n < L.nmodes; n++) total_rows += L.dims[n];
-    uint32_t* counts = nullptr;
-    BLCO_CUDA(cudaMallocAsync(&counts, total_rows * sizeof(uint32_t), s));
-    BLCO_CUDA(cudaMemsetAsync(counts, 0, total_rows * sizeof(uint32_t), s));
+    uint32_t* counts = counts_in;
+    if (!counts) {
+        BLCO_CUDA(cudaMallocAsync(&counts, total_rows * sizeof(uint32_t), s));
+        BLCO_CUDA(cudaMemsetAsync(counts, 0, total_rows * sizeof(uint32_t), s));
+    }
     uint64_t off = 0;
     for (int n = 0; n < L.nmodes; n++) {
         cp.c[n] = counts + off;
         off += L.dims[n];
     }
-    if (t->nnz) {
+    if (t->nnz && !counts_in) {
         k_row_counts<<<di.sm_count * 4, RC_THREADS, 0, s>>>(t->d_coords, t->nnz, L, cp);
         BLCO_CHECK_LAUNCH("k_row_counts");
     }
@@ -1069,7 +1095,7 @@ int build_hot_tables(blco_tensor* t, cudaStream_t s)
     BLCO_CUDA(cudaMemcpyAsync(hc.data(), cand, hc.size() * 4, cudaMemcpyDeviceToHost, s));
     BLCO_CUDA(cudaMemcpyAsync(hn.data(), ncand, hn.size() * 4, cudaMemcpyDeviceToHost, s));
     BLCO_CUDA(cudaStreamSynchronize(s));
-    cudaFreeAsync(counts, s);
+    if (!counts_in) cudaFreeAsync(counts, s);
     cudaFreeAsync(d_stats, s);
     cudaFreeAsync(cand, s);
     cudaFreeAsync(ncand, s);
@@ -1118,6 +1144,238 @@ int build_hot_tables(blco_tensor* t, cudaStream_t s)
     return BLCO_OK;
 }
 
+int build_hot_tables(blco_tensor* t, cudaStream_t s) { return build_hot_tables_impl(t, s, nullptr); }
+
+// ------------------------------------------------- chunked streamed encode --
+//
+// A streamed tensor lives in pinned host memory, so it may be larger than
+// the device.  Its encode then runs in chunks that fit the residency
+// budget: per chunk, the COO slice is copied in (from host or device
+// memory), keyed (k_alto_keys), counted per row (k_coo_counts), sorted by
+// key (stable radix sort) and copied back as (key, value) runs.  The host
+// merges the runs by key, ties in chunk order, so the result is the stable
+// key order of the whole input, the same as the one-pass encoder's, and
+// writes BLCO coordinates (key re-linearized through the byte table) and
+// values into the pinned stream.
+
+uint64_t stream_chunk_nnz(const blco_opts* opts, int nmodes)
+{
+    const uint64_t budget = (opts && opts->residency_bytes) ? opts->residency_bytes : (8ull << 30);
+    // device bytes per nonzero of a chunk: COO slice, two key/value buffers
+    const uint64_t per = (uint64_t)nmodes * 8 + 8 + 32;
+    return std::max<uint64_t>(4096, budget / per);
+}
+
+static int encode_chunked(blco_tensor* t, const uint64_t* const* cidx, const double* vals, cudaStream_t s,
+                          const DeviceInfo& di, uint64_t C)
+{
+    const Layout& L = t->layout;
+    const uint64_t nnz = t->nnz;
+    const int nm = L.nmodes;
+    const uint64_t nchunks = (nnz + C - 1) / C;
+    uint64_t* dc[BLCO_MAX_MODES] = {};
+    double* dvin = nullptr;
+    uint64_t *k0 = nullptr, *k1 = nullptr;
+    double *v0 = nullptr, *v1 = nullptr, *dpart = nullptr;
+    uint32_t* counts = nullptr;
+    int* d_bad = nullptr;
+    EncTables* d_tabs = nullptr;
+    uint64_t* hk = nullptr; // sorted keys of every chunk (pinned)
+    double* hv = nullptr;
+    auto release = [&]() {
+        cudaStreamSynchronize(s);
+        for (auto& p : dc) { cudaFree(p); p = nullptr; }
+        cudaFree(dvin);
+        cudaFree(k0);
+        cudaFree(k1);
+        cudaFree(v0);
+        cudaFree(v1);
+        cudaFree(dpart);
+        cudaFree(counts);
+        cudaFree(d_bad);
+        cudaFree(d_tabs);
+        if (hk) cudaFreeHost(hk);
+        if (hv) cudaFreeHost(hv);
+    };
+#define CH_CUDA(call)                                                           \
+    do {                                                                        \
+        cudaError_t _e = (call);                                                \
+        if (_e != cudaSuccess) {                                                \
+            int _s = cuda_fail(_e, #call, __FILE__, __LINE__);                  \
+            release();                                                          \
+            return _s;                                                          \
+        }                                                                       \
+    } while (0)
+    uint64_t total_rows = 0;
+    for (int n = 0; n < nm; n++) total_rows += L.dims[n];
+    for (int n = 0; n < nm; n++) CH_CUDA(cudaMalloc(&dc[n], C * 8));
+    CH_CUDA(cudaMalloc(&dvin, C * 8));
+    CH_CUDA(cudaMalloc(&k0, C * 8));
+    CH_CUDA(cudaMalloc(&k1, C * 8));
+    CH_CUDA(cudaMalloc(&v0, C * 8));
+    CH_CUDA(cudaMalloc(&v1, C * 8));
+    const int grid = (int)std::min<uint64_t>((C + 255) / 256, (uint64_t)di.sm_count * 16);
+    const int g2 = std::min(grid, 1024);
+    CH_CUDA(cudaMalloc(&dpart, (size_t)g2 * sizeof(double)));
+    CH_CUDA(cudaMalloc(&counts, total_rows * sizeof(uint32_t)));
+    CH_CUDA(cudaMemsetAsync(counts, 0, total_rows * sizeof(uint32_t), s));
+    CH_CUDA(cudaMalloc(&d_bad, sizeof(int)));
+    CH_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), s));
+    EncTables htabs = make_tables(L);
+    CH_CUDA(cudaMalloc(&d_tabs, sizeof(EncTables)));
+    CH_CUDA(cudaMemcpyAsync(d_tabs, &htabs, sizeof(EncTables), cudaMemcpyHostToDevice, s));
+    CH_CUDA(cudaMallocHost(&hk, nnz * 8));
+    CH_CUDA(cudaMallocHost(&hv, nnz * 8));
+    CountPtrs cp;
+    memset(&cp, 0, sizeof(cp));
+    {
+        uint64_t off = 0;
+        for (int n = 0; n < nm; n++) {
+            cp.c[n] = counts + off;
+            off += L.dims[n];
+        }
+    }
+    std::vector<double> part((size_t)nchunks * g2);
+    for (uint64_t c = 0; c < nchunks; c++) {
+        const uint64_t o = c * C, n = std::min(C, nnz - o);
+        for (int m = 0; m < nm; m++)
+            CH_CUDA(cudaMemcpyAsync(dc[m], cidx[m] + o, n * 8, cudaMemcpyDefault, s));
+        CH_CUDA(cudaMemcpyAsync(dvin, vals + o, n * 8, cudaMemcpyDefault, s));
+        CooPtrs coo;
+        memset(&coo, 0, sizeof(coo));
+        for (int m = 0; m < nm; m++) coo.c[m] = dc[m];
+        const int gk = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)di.sm_count * 16);
+        k_alto_keys<<<gk, 256, 0, s>>>(coo, dvin, n, L, d_tabs, k0, v0, d_bad);
+        count_launch();
+        CH_CUDA(cudaGetLastError());
+        k_coo_counts<<<(int)std::min<uint64_t>((n + RC_THREADS - 1) / RC_THREADS, (uint64_t)di.sm_count * 8),
+                       RC_THREADS, 0, s>>>(coo, n, L, cp);
+        count_launch();
+        CH_CUDA(cudaGetLastError());
+        k_sumsq<<<g2, 256, 0, s>>>(v0, n, dpart);
+        count_launch();
+        CH_CUDA(cudaGetLastError());
+        CH_CUDA(cudaMemcpyAsync(part.data() + c * g2, dpart, g2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        bool alt = false;
+        int st = radix_sort_pairs(k0, v0, k1, v1, n, 0, L.alto_bits, s, &alt);
+        if (st != BLCO_OK) { release(); return st; }
+        CH_CUDA(cudaMemcpyAsync(hk + o, alt ? k1 : k0, n * 8, cudaMemcpyDeviceToHost, s));
+        CH_CUDA(cudaMemcpyAsync(hv + o, alt ? v1 : v0, n * 8, cudaMemcpyDeviceToHost, s));
+        // the next chunk's uploads overwrite the buffers these copies read:
+        // stream order keeps them apart
+    }
+    int bad = 0;
+    CH_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CH_CUDA(cudaStreamSynchronize(s));
+    if (bad) {
+        release();
+        return fail(BLCO_ERR_INVALID, "a coordinate is not below its mode length");
+    }
+    double ss = 0.0;
+    for (double x : part) ss += x; // fixed order: chunk by chunk
+    t->norm_sq = ss;
+    // Merge the sorted runs into the pinned stream.
+    cudaError_t e1 = cudaMallocHost(&t->h_coords, nnz * 8);
+    cudaError_t e2 = cudaMallocHost(&t->h_values, nnz * 8);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        release();
+        return fail(BLCO_ERR_NOMEM, "pinned host allocation for streamed blocks failed");
+    }
+    std::vector<uint64_t> rb(nchunks), re(nchunks);
+    for (uint64_t c = 0; c < nchunks; c++) {
+        rb[c] = c * C;
+        re[c] = std::min(nnz, (c + 1) * C);
+    }
+    const int nbytes = (L.alto_bits + 7) / 8;
+    auto relin_host = [&](uint64_t key) {
+        uint64_t v = 0;
+        for (int b = 0; b < nbytes; b++) v |= htabs.rel[b][(key >> (8 * b)) & 255];
+        return v;
+    };
+    // Output segments split at sampled keys; every key's duplicates fall in
+    // one segment (a segment holds the keys in [lo, hi)).
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::min<uint64_t>(std::max(1u, std::min(hw, 64u)), std::max<uint64_t>(1, nnz / 65536));
+    std::vector<uint64_t> sample;
+    const uint64_t step = std::max<uint64_t>(1, nnz / ((uint64_t)T * 64));
+    for (uint64_t c = 0; c < nchunks; c++)
+        for (uint64_t i = rb[c]; i < re[c]; i += step) sample.push_back(hk[i]);
+    std::sort(sample.begin(), sample.end());
+    std::vector<uint64_t> split; // T - 1 increasing keys
+    for (int k = 1; k < T; k++) {
+        const uint64_t key = sample[(size_t)((double)k / T * sample.size())];
+        if (split.empty() || key > split.back()) split.push_back(key);
+    }
+    const int S = (int)split.size() + 1;
+    // cut[c][k]: first index of run c with key >= split[k-1] (cut[c][0] = rb[c], cut[c][S] = re[c])
+    std::vector<std::vector<uint64_t>> cut(nchunks, std::vector<uint64_t>(S + 1));
+    for (uint64_t c = 0; c < nchunks; c++) {
+        cut[c][0] = rb[c];
+        cut[c][S] = re[c];
+        for (int k = 1; k < S; k++)
+            cut[c][k] = (uint64_t)(std::lower_bound(hk + rb[c], hk + re[c], split[k - 1]) - hk);
+    }
+    std::vector<uint64_t> outpos(S + 1, 0);
+    for (int k = 0; k < S; k++) {
+        uint64_t len = 0;
+        for (uint64_t c = 0; c < nchunks; c++) len += cut[c][k + 1] - cut[c][k];
+        outpos[k + 1] = outpos[k] + len;
+    }
+    auto merge_seg = [&](int k) {
+        // min-heap of (key, run): ties go to the lower run, i.e. input order
+        std::vector<std::pair<uint64_t, uint64_t>> heap;
+        std::vector<uint64_t> at(nchunks), end(nchunks);
+        for (uint64_t c = 0; c < nchunks; c++) {
+            at[c] = cut[c][k];
+            end[c] = cut[c][k + 1];
+            if (at[c] < end[c]) heap.push_back({hk[at[c]], c});
+        }
+        auto greater = [](const std::pair<uint64_t, uint64_t>& a, const std::pair<uint64_t, uint64_t>& b) {
+            return a > b;
+        };
+        std::make_heap(heap.begin(), heap.end(), greater);
+        uint64_t o = outpos[k];
+        while (!heap.empty()) {
+            std::pop_heap(heap.begin(), heap.end(), greater);
+            const uint64_t c = heap.back().second;
+            heap.pop_back();
+            // take the run's whole stretch of keys not above the next head
+            const uint64_t lim = heap.empty() ? ~0ull : heap.front().first;
+            const uint64_t limc = heap.empty() ? 0 : heap.front().second;
+            uint64_t i = at[c];
+            do {
+                t->h_coords[o] = relin_host(hk[i]);
+                t->h_values[o] = hv[i];
+                o++;
+                i++;
+            } while (i < end[c] && (hk[i] < lim || (hk[i] == lim && c < limc)));
+            at[c] = i;
+            if (i < end[c]) {
+                heap.push_back({hk[i], c});
+                std::push_heap(heap.begin(), heap.end(), greater);
+            }
+        }
+    };
+    {
+        std::vector<std::thread> th;
+        std::atomic<int> next{0};
+        for (int w = 0; w < std::min(S, (int)hw); w++)
+            th.emplace_back([&]() {
+                for (int k = next++; k < S; k = next++) merge_seg(k);
+            });
+        for (auto& x : th) x.join();
+    }
+    // heavy-row statistics and tables from the row counts
+    cudaFreeHost(hk);
+    cudaFreeHost(hv);
+    hk = nullptr;
+    hv = nullptr;
+    int st = build_hot_tables_impl(t, s, counts);
+    release();
+#undef CH_CUDA
+    return st;
+}
+
 int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* d_cidx,
                 const double* d_vals, uint64_t max_block_size, const blco_opts* opts, blco_tensor** out)
 {
@@ -1144,6 +1402,15 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
     cudaError_t e = cudaSetDevice(t->device);
     if (e != cudaSuccess) return cleanup_fail(cuda_fail(e, "cudaSetDevice", __FILE__, __LINE__));
     cudaStream_t s = pick_stream(t, opts);
+    if (!t->resident && !t->layout.wide && nnz > stream_chunk_nnz(opts, nmodes)) {
+        // streamed and larger than one chunk of the residency budget
+        DeviceInfo cdi;
+        if ((st = device_info(t->device, &cdi)) != BLCO_OK) return cleanup_fail(st);
+        if ((st = encode_chunked(t, d_cidx, d_vals, s, cdi, stream_chunk_nnz(opts, nmodes))) != BLCO_OK)
+            return cleanup_fail(st);
+        *out = t;
+        return BLCO_OK;
+    }
     if (t->layout.wide) {
         DeviceInfo wdi;
         if ((st = device_info(t->device, &wdi)) != BLCO_OK) return cleanup_fail(st);

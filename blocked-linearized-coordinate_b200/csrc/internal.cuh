@@ -188,6 +188,9 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz,
                 const uint64_t* const* d_cidx, const double* d_vals,
                 uint64_t max_block_size, const blco_opts* opts, blco_tensor** out);
 int build_hot_tables(blco_tensor* t, cudaStream_t s);
+// Nonzeros per chunk of the chunked encoder of streamed tensors (from the
+// residency budget); larger streamed tensors are encoded chunk by chunk.
+uint64_t stream_chunk_nnz(const blco_opts* opts, int nmodes);
 int sort_stream_by_mode(const blco_tensor* t, int mode, uint64_t* d_coords, double* d_vals, uint64_t* tmp_k,
                         double* tmp_v, cudaStream_t s);
 int encode_noalloc_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* d_cidx,

@@ -26,6 +26,7 @@ import argparse
 import importlib.util
 import os
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -126,7 +127,10 @@ def run_stream(a, pkg, torch):
         best = max(best, hb.numel() * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
     del hb, db
     o = pkg.make_opts(kernel=10, stream_data=True, residency_bytes=a.residency)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"], a.block, o)
+    encode_s = time.perf_counter() - t0
     del X
     torch.cuda.empty_cache()
     inf = t.info()
@@ -147,7 +151,7 @@ def run_stream(a, pkg, torch):
     print(f"streamed fp64 nnz {a.nnz} blocks {inf['block_count']} residency {a.residency} ms/iter {it:.1f} "
           f"h2d GB/iter {h2d / 1e9:.2f} h2d GB/s {h2d / (it * 1e-3) / 1e9:.1f} pinned peak GB/s {best:.1f} "
           f"frac {h2d / (it * 1e-3) / 1e9 / best:.3f} device GB in use {(total_b - free_b) / 1e9:.1f} "
-          f"fit {fits[-1]:.6f}", flush=True)
+          f"fit {fits[-1]:.6f} encode s {encode_s:.2f}", flush=True)
     plan.destroy()
     t.free()
 

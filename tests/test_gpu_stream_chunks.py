@@ -1,0 +1,96 @@
+"""The chunked encoder of streamed tensors, through the C ABI.
+
+A streamed tensor (opts.stream_data) larger than one chunk of its residency
+budget is encoded chunk by chunk: keys and a stable sort per chunk on the
+GPU, a merge of the sorted runs on the host.  The result must be the
+resident encoder's bit for bit (coordinates, values, blocks), with
+duplicate coordinates in input order; the streamed MTTKRP and CP-ALS on it
+must match the resident ones (1e-12 / 1e-10).
+"""
+import numpy as np
+import pytest
+
+from conftest import unique_coords
+
+pytestmark = pytest.mark.gpu
+
+DIMS = [3000, 2000, 90]
+
+
+def _tensor(seed, nnz=300_000, dup=20_000):
+    rng = np.random.default_rng(seed)
+    cidx = unique_coords(rng, DIMS, nnz - dup, zipf=0.9)
+    pick = rng.integers(0, nnz - dup, size=dup)
+    cidx = np.concatenate([cidx, cidx[:, pick]], axis=1)
+    perm = rng.permutation(cidx.shape[1])
+    return np.ascontiguousarray(cidx[:, perm]), rng.random(cidx.shape[1])
+
+
+def _opts(blco, residency):
+    return blco.make_opts(stream_data=True, residency_bytes=residency)
+
+
+@pytest.mark.parametrize("residency", [2 << 20, 5 << 20])
+def test_chunked_streamed_encode_is_bit_identical(blco, residency):
+    cidx, vals = _tensor(1)
+    ref = blco.Tensor.encode(DIMS, cidx, vals, 40_000)
+    t = blco.Tensor.encode(DIMS, cidx, vals, 40_000, opts=_opts(blco, residency))
+    a, b = t.copy_out(), ref.copy_out()
+    assert not a["resident"]
+    assert np.array_equal(a["coords"], b["coords"])
+    assert np.array_equal(a["vals"].view(np.uint64), b["vals"].view(np.uint64))
+    assert np.array_equal(a["block_offsets"], b["block_offsets"])
+    t.free()
+    ref.free()
+
+
+def test_chunked_streamed_encode_from_device_coo(blco):
+    import torch
+    cidx, vals = _tensor(2)
+    ref = blco.Tensor.encode(DIMS, cidx, vals, 0)
+    d_c = [torch.from_numpy(cidx[n].astype(np.int64)).cuda() for n in range(3)]
+    d_v = torch.from_numpy(vals).cuda()
+    t = blco.Tensor.encode_device(DIMS, d_c, d_v, 0, _opts(blco, 2 << 20))
+    a, b = t.copy_out(), ref.copy_out()
+    assert np.array_equal(a["coords"], b["coords"])
+    assert np.array_equal(a["vals"].view(np.uint64), b["vals"].view(np.uint64))
+    t.free()
+    ref.free()
+
+
+def test_chunked_streamed_mttkrp_and_cpals_match_resident(blco):
+    import torch
+    cidx, vals = _tensor(3)
+    R = 8
+    rng = np.random.default_rng(4)
+    fs = [rng.random((d, R)) for d in DIMS]
+    ref = blco.Tensor.encode(DIMS, cidx, vals, 50_000)
+    t = blco.Tensor.encode(DIMS, cidx, vals, 50_000, opts=_opts(blco, 2 << 20))
+    dev = [torch.from_numpy(f).cuda() for f in fs]
+    for m in range(3):
+        o1 = torch.zeros(DIMS[m], R, dtype=torch.float64, device="cuda")
+        o2 = torch.zeros(DIMS[m], R, dtype=torch.float64, device="cuda")
+        blco.mttkrp(ref, m, dev, o1)
+        blco.mttkrp(t, m, dev, o2, _opts(blco, 2 << 20))
+        torch.cuda.synchronize()
+        x, y = o1.cpu().numpy(), o2.cpu().numpy()
+        assert np.linalg.norm(x - y) <= 1e-12 * np.linalg.norm(x), m
+    f1 = [f.copy() for f in fs]
+    f2 = [f.copy() for f in fs]
+    l1, l2 = np.ones(R), np.ones(R)
+    _, fits1 = blco.cpals(ref, f1, l1, 6, 0.0)
+    _, fits2 = blco.cpals(t, f2, l2, 6, 0.0, _opts(blco, 2 << 20))
+    assert np.allclose(fits1, fits2, rtol=0, atol=1e-10)
+    for a, b in zip(f1, f2):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(a)
+    t.free()
+    ref.free()
+
+
+def test_chunked_streamed_encode_rejects_bad_coordinate_in_late_chunk(blco):
+    cidx, vals = _tensor(5)
+    cidx = cidx.copy()
+    cidx[1, -3] = DIMS[1]  # out of range, in the last chunk
+    with pytest.raises(blco.BlcoError) as e:
+        blco.Tensor.encode(DIMS, cidx, vals, 0, opts=_opts(blco, 2 << 20))
+    assert e.value.status == blco.ERR_INVALID
