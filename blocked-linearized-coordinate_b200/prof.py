@@ -9,7 +9,7 @@
   python blocked-linearized-coordinate_b200/prof.py cpals --nnz N --dtype f64|f32|bf16 [--iters I]
       CP-ALS iterations on the Zipf(1.1) 2M x 2M x 25k tensor (rank 32):
       ms per iteration, MTTKRP ms per mode, and the rest of the iteration.
-  python blocked-linearized-coordinate_b200/prof.py stream --nnz N [--block B] [--residency BYTES]
+  python blocked-linearized-coordinate_b200/prof.py stream --nnz N [--block B] [--residency BYTES] [--no-dedupe]
       The streamed form on the 4-mode 500k x 200k x 50k x 1k Zipf(0.9) shape,
       rank 64, FP64: ms per CP-ALS iteration and host-to-device GB/s against
       a measured pinned copy.
@@ -112,7 +112,10 @@ def run_stream(a, pkg, torch):
     host-to-device GB/s per CP-ALS iteration against a pinned copy."""
     from blco_b200 import synth
     dims = [500_000, 200_000, 50_000, 1_000]
-    X = synth.zipf_tensor_device(a.nnz, dims, 0.9, seed=0, value_dist="uniform")
+    if a.no_dedupe:
+        X = synth.zipf_coo_device(a.nnz, dims, 0.9, seed=0)
+    else:
+        X = synth.zipf_tensor_device(a.nnz, dims, 0.9, seed=0, value_dist="uniform")
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     # pinned host-to-device peak: 2 GiB, best of 3
@@ -282,6 +285,8 @@ def main():
     sm.add_argument("--block", type=int, default=64 << 20)
     sm.add_argument("--residency", type=int, default=8 << 30)
     sm.add_argument("--iters", type=int, default=2)
+    sm.add_argument("--no-dedupe", action="store_true",
+                    help="draw the COO chunk by chunk without removing repeated coordinates")
     w = sub.add_parser("wide")
     w.add_argument("--nnz", type=int, default=50_000_000)
     w.add_argument("--rank", type=int, default=32)

@@ -88,6 +88,35 @@ def zipf_tensor_device(nnz, dims, s, seed=0, device="cuda", value_dist="lognorma
     return dict(dims=dims, cidx=cidx, vals=vals.contiguous())
 
 
+def zipf_coo_device(nnz, dims, s, seed=0, device="cuda", chunk=1 << 28, value_dist="uniform"):
+    """Per-mode Zipf(s) coordinates drawn chunk by chunk into preallocated
+    int64 arrays, without deduplication (coordinates may repeat; the
+    MTTKRP sums repeated nonzeros), values U(0,1) (or lognormal) drawn in
+    FP32: a generator whose memory is the COO itself, for nonzero counts
+    whose deduplication would not fit the device.
+    Returns dict(dims, cidx=[int64 CUDA tensors], vals=float64 CUDA tensor)."""
+    import torch
+    dims = [int(d) for d in dims]
+    g = torch.Generator(device=device).manual_seed(int(seed))
+    cdfs = [_zipf_cdf(torch, d, s, device) if s > 0 else None for d in dims]
+    cidx = [torch.empty(nnz, dtype=torch.int64, device=device) for _ in dims]
+    vals = torch.empty(nnz, dtype=torch.float64, device=device)
+    for o in range(0, nnz, chunk):
+        n = min(chunk, nnz - o)
+        for m, d in enumerate(dims):
+            if cdfs[m] is None:
+                cidx[m][o:o + n] = torch.randint(0, d, (n,), generator=g, device=device, dtype=torch.int64)
+            else:
+                u = torch.rand(n, dtype=torch.float64, generator=g, device=device)
+                cidx[m][o:o + n] = torch.searchsorted(cdfs[m], u).clamp_(max=d - 1)
+                del u
+        if value_dist == "lognormal":
+            vals[o:o + n] = torch.randn(n, dtype=torch.float32, generator=g, device=device).exp_().double()
+        else:
+            vals[o:o + n] = torch.rand(n, dtype=torch.float32, generator=g, device=device).double()
+    return dict(dims=dims, cidx=cidx, vals=vals)
+
+
 def wide_tensor_device(nnz, dims, s, seed=0, device="cuda"):
     """Distinct coordinates in a key space above 2^63 (keys of more than 64
     bits): per-mode Zipf(s) draws (uniform for s = 0), deduplicated on a
