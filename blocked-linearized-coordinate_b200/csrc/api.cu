@@ -197,6 +197,7 @@ int blco_tensor_free(blco_tensor* t)
     }
     if (t->h_coords) cudaFreeHost(t->h_coords);
     if (t->h_values) cudaFreeHost(t->h_values);
+    if (t->h_values32) cudaFreeHost(t->h_values32);
     for (int n = 0; n < BLCO_MAX_MODES; n++) {
         cudaFree(t->hot[n].d_keys);
         cudaFree(t->hot[n].d_slot);
@@ -311,14 +312,14 @@ int blco_mttkrp_ex(blco_tensor* t, int mode, int rank, int factor_dtype, const v
         return fail(BLCO_ERR_INVALID, "factor_dtype must be BLCO_DTYPE_F32 or BLCO_DTYPE_BF16");
     if (mode < 0 || mode >= t->layout.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
     if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
-    if (!t->resident) return fail(BLCO_ERR_UNSUPPORTED, "mixed-precision MTTKRP needs a resident tensor");
     if (t->layout.wide) return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits: the MTTKRP is FP64 only");
     for (int m = 0; m < t->layout.nmodes; m++)
         if (m != mode && !d_factors[m]) return fail(BLCO_ERR_INVALID, "null factor matrix");
     BLCO_CUDA(cudaSetDevice(t->device));
     cudaStream_t s = pick_stream(t, opts);
     const float* v32 = nullptr;
-    BLCO_TRY(values_f32(t, s, &v32));
+    if (t->resident) BLCO_TRY(values_f32(t, s, &v32));
+    else BLCO_TRY(host_values_f32(t));
     MttkrpArgs a;
     memset(&a, 0, sizeof(a));
     a.coords = t->d_coords;
@@ -331,6 +332,7 @@ int blco_mttkrp_ex(blco_tensor* t, int mode, int rank, int factor_dtype, const v
     a.factor_dtype = factor_dtype;
     a.thread_cf = opts ? opts->thread_cf : 2;
     BLCO_TRY(resolve_schedule(t, mode, rank, factor_dtype, opts ? opts->kernel : BLCO_KERNEL_AUTO, s, &a));
+    if (!t->resident) return mttkrp_streamed(t, a, opts, s);
     return mttkrp_launch(t, a, s);
 }
 

@@ -827,8 +827,6 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     *out = nullptr;
     if (!t || !d_factors || !d_lambda) return fail(BLCO_ERR_INVALID, "null argument");
     if (rank < 1 || rank > MAX_SOLVE_R) return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS rank must be 1..96");
-    if (!t->resident && opts && opts->precision != BLCO_PRECISION_FP64)
-        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS on a streamed tensor runs the FP64 form only");
     if (t->layout.wide && opts && opts->precision != BLCO_PRECISION_FP64)
         return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS with keys above 64 bits runs the FP64 form only");
     blco_cpals_plan* p = new blco_cpals_plan();
@@ -893,7 +891,8 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
 #undef PC
     p->xnorm = std::sqrt(t->norm_sq);
     if (p->mixed) {
-        st = values_f32(t, p->s, &p->vals32);
+        // streamed: 4-byte values copied per block from a pinned FP32 copy
+        st = t->resident ? values_f32(t, p->s, &p->vals32) : host_values_f32(t);
         if (st != BLCO_OK) { plan_free(p); return st; }
     }
     for (int n = 0; n < p->N; n++) {
@@ -985,9 +984,8 @@ int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda,
 {
     if (!t || !factors || !lambda) return fail(BLCO_ERR_INVALID, "null argument");
     // forms the plan rejects are rejected before any factor is copied
-    if (opts && opts->precision != BLCO_PRECISION_FP64 && (!t->resident || t->layout.wide))
-        return fail(BLCO_ERR_UNSUPPORTED, t->layout.wide ? "CP-ALS with keys above 64 bits runs the FP64 form only"
-                                                         : "CP-ALS on a streamed tensor runs the FP64 form only");
+    if (opts && opts->precision != BLCO_PRECISION_FP64 && t->layout.wide)
+        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS with keys above 64 bits runs the FP64 form only");
     const int N = t->layout.nmodes;
     cudaStream_t s = pick_stream(t, opts);
     double* dU[BLCO_MAX_MODES] = {};

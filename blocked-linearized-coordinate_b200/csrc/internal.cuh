@@ -160,6 +160,7 @@ struct blco_tensor {
     // streamed blocks (pinned host)
     uint64_t* h_coords = nullptr;
     double* h_values = nullptr;
+    float* h_values32 = nullptr; // mixed forms of a streamed tensor, made on first use
     // wide keys: per-nonzero block field (see Layout) and the blocks
     // (block_count + 1 offsets, block_count x nmodes block coordinates)
     uint64_t* d_bfield = nullptr;
@@ -228,6 +229,8 @@ int stream_ring_destroy(StreamRing* r);
 int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRing* r, cudaStream_t s);
 // FP32 copy of the resident values (created on first use).
 int values_f32(blco_tensor* t, cudaStream_t s, const float** out);
+// Pinned FP32 copy of a streamed tensor's values (made once, on the host).
+int host_values_f32(blco_tensor* t);
 
 // cpals.cu
 int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_lambda, const blco_opts* opts,

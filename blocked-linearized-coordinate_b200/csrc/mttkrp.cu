@@ -37,6 +37,8 @@
 
 #include <vector>
 
+#include <thread>
+
 #include "internal.cuh"
 
 namespace blco {
@@ -774,6 +776,24 @@ int values_f32(blco_tensor* t, cudaStream_t s, const float** out)
     return BLCO_OK;
 }
 
+int host_values_f32(blco_tensor* t)
+{
+    if (t->h_values32 || !t->nnz) return BLCO_OK;
+    if (!t->h_values) return fail(BLCO_ERR_STATE, "tensor has no host values");
+    float* h = nullptr;
+    BLCO_CUDA(cudaMallocHost(&h, t->nnz * sizeof(float)));
+    const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (unsigned w = 0; w < nt; w++)
+        th.emplace_back([&, w]() {
+            const uint64_t a = t->nnz * w / nt, b = t->nnz * (w + 1) / nt;
+            for (uint64_t i = a; i < b; i++) h[i] = (float)t->h_values[i];
+        });
+    for (auto& x : th) x.join();
+    t->h_values32 = h;
+    return BLCO_OK;
+}
+
 // --------------------------------------------------------- wide keys --
 //
 // MTTKRP of a tensor whose keys need more than 64 bits (the reference's
@@ -1286,6 +1306,8 @@ int stream_ring_create(const blco_tensor* t, uint64_t residency_bytes, StreamRin
 // MTTKRP runs on s after the copy.
 int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRing* r, cudaStream_t s)
 {
+    const bool f32 = base.factor_dtype != BLCO_DTYPE_F64;
+    if (f32 && !t->h_values32) return fail(BLCO_ERR_STATE, "streamed mixed form without FP32 host values");
     // the copies must not overtake work already queued on s
     BLCO_CUDA(cudaEventRecord(r->consumed[0], s));
     BLCO_CUDA(cudaStreamWaitEvent(r->cs, r->consumed[0], 0));
@@ -1294,7 +1316,10 @@ int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRin
         const uint64_t beg = b * r->B, n = std::min(r->B, t->nnz - beg);
         if (b >= (uint64_t)r->nbuf) BLCO_CUDA(cudaStreamWaitEvent(r->cs, r->consumed[k], 0));
         BLCO_CUDA(cudaMemcpyAsync(r->dc[k], t->h_coords + beg, n * 8, cudaMemcpyHostToDevice, r->cs));
-        BLCO_CUDA(cudaMemcpyAsync(r->dv[k], t->h_values + beg, n * 8, cudaMemcpyHostToDevice, r->cs));
+        if (f32)  // the mixed forms stream 4-byte values
+            BLCO_CUDA(cudaMemcpyAsync(r->dv[k], t->h_values32 + beg, n * 4, cudaMemcpyHostToDevice, r->cs));
+        else
+            BLCO_CUDA(cudaMemcpyAsync(r->dv[k], t->h_values + beg, n * 8, cudaMemcpyHostToDevice, r->cs));
         BLCO_CUDA(cudaEventRecord(r->copied[k], r->cs));
         BLCO_CUDA(cudaStreamWaitEvent(s, r->copied[k], 0));
         MttkrpArgs a = base;

@@ -9,7 +9,7 @@
   python blocked-linearized-coordinate_b200/prof.py cpals --nnz N --dtype f64|f32|bf16 [--iters I]
       CP-ALS iterations on the Zipf(1.1) 2M x 2M x 25k tensor (rank 32):
       ms per iteration, MTTKRP ms per mode, and the rest of the iteration.
-  python blocked-linearized-coordinate_b200/prof.py stream --nnz N [--block B] [--residency BYTES] [--no-dedupe]
+  python blocked-linearized-coordinate_b200/prof.py stream --nnz N [--block B] [--residency BYTES] [--dtype f64|f32] [--no-dedupe]
       The streamed form on the 4-mode 500k x 200k x 50k x 1k Zipf(0.9) shape,
       rank 64, FP64: ms per CP-ALS iteration and host-to-device GB/s against
       a measured pinned copy.
@@ -129,7 +129,8 @@ def run_stream(a, pkg, torch):
         torch.cuda.synchronize()
         best = max(best, hb.numel() * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
     del hb, db
-    o = pkg.make_opts(kernel=10, stream_data=True, residency_bytes=a.residency)
+    prec = {"f64": pkg.PRECISION_FP64, "f32": pkg.PRECISION_MIXED}[a.dtype]
+    o = pkg.make_opts(kernel=10, stream_data=True, residency_bytes=a.residency, precision=prec)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()  # the generator's cached blocks
     t0 = time.perf_counter()
@@ -151,8 +152,8 @@ def run_stream(a, pkg, torch):
     e1.record()
     torch.cuda.synchronize()
     it = e0.elapsed_time(e1) / a.iters
-    h2d = len(dims) * a.nnz * 16
-    print(f"streamed fp64 nnz {a.nnz} blocks {inf['block_count']} residency {a.residency} ms/iter {it:.1f} "
+    h2d = len(dims) * a.nnz * (16 if a.dtype == "f64" else 12)
+    print(f"streamed {a.dtype} nnz {a.nnz} blocks {inf['block_count']} residency {a.residency} ms/iter {it:.1f} "
           f"h2d GB/iter {h2d / 1e9:.2f} h2d GB/s {h2d / (it * 1e-3) / 1e9:.1f} pinned peak GB/s {best:.1f} "
           f"frac {h2d / (it * 1e-3) / 1e9 / best:.3f} device GB in use {(total_b - free_b) / 1e9:.1f} "
           f"fit {fits[-1]:.6f} encode s {encode_s:.2f}", flush=True)
@@ -285,6 +286,7 @@ def main():
     sm.add_argument("--block", type=int, default=64 << 20)
     sm.add_argument("--residency", type=int, default=8 << 30)
     sm.add_argument("--iters", type=int, default=2)
+    sm.add_argument("--dtype", default="f64", choices=["f64", "f32"])
     sm.add_argument("--no-dedupe", action="store_true",
                     help="draw the COO chunk by chunk without removing repeated coordinates")
     w = sub.add_parser("wide")

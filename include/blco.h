@@ -159,7 +159,10 @@ const char* blco_version(void);
  *   cidx[n] (host): nnz 0-based coordinates of mode n; vals (host): nnz values.
  *   max_block_size: the --max-block-size of the reference (0 = nnz).
  *   opts->stream_data: keep the encoded blocks in pinned host memory instead
- *   of HBM, for the streamed out-of-memory path.
+ *   of HBM, for the streamed out-of-memory path; a streamed tensor of more
+ *   than opts->residency_bytes / (8 * nmodes + 40) nonzeros is encoded in
+ *   chunks of that size (the COO is never whole on the device), with the
+ *   same result.
  * Ties between equal coordinates keep input order. */
 int blco_encode(int nmodes, const uint64_t* dims, uint64_t nnz,
                 const uint64_t* const* cidx, const double* vals,
@@ -252,9 +255,10 @@ int blco_mttkrp_host(blco_tensor* t, int mode, int rank, const double* const* fa
  * and lambda (host, rank) are read and updated in place.
  *   fit_out: last fit; fits (may be NULL): one entry per executed
  *   iteration (maxiter entries must fit); iters_out: iterations executed.
- * A streamed tensor (encoded with opts->stream_data) runs the FP64 form:
- * every MTTKRP copies its blocks through a ring of device buffers of at most
- * opts->residency_bytes (BLCO_ERR_UNSUPPORTED for the mixed forms). */
+ * A streamed tensor (encoded with opts->stream_data) runs every form: each
+ * MTTKRP copies its blocks through a ring of device buffers of at most
+ * opts->residency_bytes; the mixed forms copy 4-byte values (from a pinned
+ * FP32 copy of the values made on first use). */
 int blco_cpals(blco_tensor* t, int rank, double* const* factors, double* lambda,
                int maxiter, double tol, const blco_opts* opts, double* fit_out,
                double* fits, int* iters_out);

@@ -94,3 +94,25 @@ def test_chunked_streamed_encode_rejects_bad_coordinate_in_late_chunk(blco):
     with pytest.raises(blco.BlcoError) as e:
         blco.Tensor.encode(DIMS, cidx, vals, 0, opts=_opts(blco, 2 << 20))
     assert e.value.status == blco.ERR_INVALID
+
+
+def test_streamed_mixed_mttkrp_matches_resident(blco):
+    """The mixed form on streamed blocks (4-byte values per block) against
+    the resident mixed form: FP32 sums in another order, so 1e-5 normwise."""
+    import torch
+    cidx, vals = _tensor(6)
+    R = 16
+    rng = np.random.default_rng(7)
+    fs = [torch.from_numpy(rng.random((d, R)).astype(np.float32)).cuda() for d in DIMS]
+    ref = blco.Tensor.encode(DIMS, cidx, vals, 50_000)
+    t = blco.Tensor.encode(DIMS, cidx, vals, 50_000, opts=_opts(blco, 2 << 20))
+    for m in range(3):
+        o1 = torch.zeros(DIMS[m], R, dtype=torch.float32, device="cuda")
+        o2 = torch.zeros(DIMS[m], R, dtype=torch.float32, device="cuda")
+        blco.mttkrp_ex(ref, m, fs, o1, blco.DTYPE_F32)
+        blco.mttkrp_ex(t, m, fs, o2, blco.DTYPE_F32, _opts(blco, 2 << 20))
+        torch.cuda.synchronize()
+        x, y = o1.double().cpu().numpy(), o2.double().cpu().numpy()
+        assert np.linalg.norm(x - y) <= 1e-5 * np.linalg.norm(x), m
+    t.free()
+    ref.free()
