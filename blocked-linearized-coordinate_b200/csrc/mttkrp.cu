@@ -1,4 +1,5 @@
-// mttkrp.cu -- sparse MTTKRP over the 64-bit BLCO stream.
+// mttkrp.cu -- sparse MTTKRP over the BLCO stream (64-bit keys; keys of up to
+// 128 bits in the wide-key section).
 //
 //   out[r_t(i), :] += val_i * prod_{m != t} U_m[r_m(i), :]
 //
