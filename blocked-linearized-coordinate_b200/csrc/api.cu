@@ -194,6 +194,7 @@ int blco_tensor_free(blco_tensor* t)
         cudaFree(w.d_coords);
         cudaFree(w.d_field);
         cudaFree(w.d_vals);
+        cudaFree(w.d_vals32);
     }
     if (t->h_coords) cudaFreeHost(t->h_coords);
     if (t->h_values) cudaFreeHost(t->h_values);
@@ -312,7 +313,8 @@ int blco_mttkrp_ex(blco_tensor* t, int mode, int rank, int factor_dtype, const v
         return fail(BLCO_ERR_INVALID, "factor_dtype must be BLCO_DTYPE_F32 or BLCO_DTYPE_BF16");
     if (mode < 0 || mode >= t->layout.nmodes) return fail(BLCO_ERR_INVALID, "mode out of range");
     if (rank < 1) return fail(BLCO_ERR_INVALID, "rank must be positive");
-    if (t->layout.wide) return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits: the MTTKRP is FP64 only");
+    if (t->layout.wide && factor_dtype == BLCO_DTYPE_BF16)
+        return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits: FP64 or FP32 factors (no BF16 gathers)");
     for (int m = 0; m < t->layout.nmodes; m++)
         if (m != mode && !d_factors[m]) return fail(BLCO_ERR_INVALID, "null factor matrix");
     BLCO_CUDA(cudaSetDevice(t->device));

@@ -743,12 +743,19 @@ int mode_update(blco_cpals_plan* p, int n)
     a.interleave = p->sched[n].interleave;
     a.thread_cf = p->opts.thread_cf;
     if (p->mixed) {
-        BLCO_CUDA(cudaMemsetAsync(p->Mf, 0, I * R * sizeof(float), p->s));
         a.vals = p->vals32;
         for (int m = 0; m < N; m++)
             a.factors[m] = p->gather_dtype == BLCO_DTYPE_BF16 ? (const void*)p->Ub[m] : (const void*)p->Uf[m];
-        a.out = p->Mf;
         a.factor_dtype = p->gather_dtype;
+        if (t->layout.wide) {
+            // wide keys: FP64 output (heavy rows summed in FP64), rounded once below
+            BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
+            a.out = p->M;
+            a.out64 = 1;
+        } else {
+            BLCO_CUDA(cudaMemsetAsync(p->Mf, 0, I * R * sizeof(float), p->s));
+            a.out = p->Mf;
+        }
     } else {
         BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
         a.vals = t->d_values;
@@ -759,6 +766,10 @@ int mode_update(blco_cpals_plan* p, int n)
     BLCO_CUDA(cudaEventRecord(p->ev[2 * n], p->s));
     if (t->resident) BLCO_TRY(mttkrp_launch(t, a, p->s));
     else BLCO_TRY(mttkrp_streamed_ring(t, a, p->ring, p->s)); // blocks copied through the plan's ring
+    if (p->mixed && t->layout.wide) {
+        k_f64_to_f32<<<conv_grid(I * R, p->sm), 256, 0, p->s>>>(p->M, p->Mf, I * R);
+        BLCO_CHECK_LAUNCH("k_f64_to_f32");
+    }
     BLCO_CUDA(cudaEventRecord(p->ev[2 * n + 1], p->s));
 
     GramPtrs gp;
@@ -827,8 +838,8 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     *out = nullptr;
     if (!t || !d_factors || !d_lambda) return fail(BLCO_ERR_INVALID, "null argument");
     if (rank < 1 || rank > MAX_SOLVE_R) return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS rank must be 1..96");
-    if (t->layout.wide && opts && opts->precision != BLCO_PRECISION_FP64)
-        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS with keys above 64 bits runs the FP64 form only");
+    if (t->layout.wide && opts && opts->precision == BLCO_PRECISION_MIXED_BF16)
+        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS with keys above 64 bits: FP64 or mixed FP32 (no BF16 gathers)");
     blco_cpals_plan* p = new blco_cpals_plan();
     p->t = t;
     p->R = rank;
@@ -873,6 +884,7 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
             PC(cudaMemsetAsync(p->d_err, 0, sizeof(int), p->s));
         }
         PC(cudaMalloc(&p->Mf, std::max<uint64_t>(maxdim, 1) * R * sizeof(float)));
+        if (t->layout.wide) PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
         for (int n = 0; n < p->N; n++) {
             const uint64_t len = t->layout.dims[n] * (uint64_t)R;
             PC(cudaMalloc(&p->Uf[n], len * sizeof(float)));
@@ -984,8 +996,8 @@ int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda,
 {
     if (!t || !factors || !lambda) return fail(BLCO_ERR_INVALID, "null argument");
     // forms the plan rejects are rejected before any factor is copied
-    if (opts && opts->precision != BLCO_PRECISION_FP64 && t->layout.wide)
-        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS with keys above 64 bits runs the FP64 form only");
+    if (opts && opts->precision == BLCO_PRECISION_MIXED_BF16 && t->layout.wide)
+        return fail(BLCO_ERR_UNSUPPORTED, "CP-ALS with keys above 64 bits: FP64 or mixed FP32 (no BF16 gathers)");
     const int N = t->layout.nmodes;
     cudaStream_t s = pick_stream(t, opts);
     double* dU[BLCO_MAX_MODES] = {};

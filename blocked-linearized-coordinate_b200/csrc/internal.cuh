@@ -172,6 +172,7 @@ struct blco_tensor {
         uint64_t* d_coords = nullptr;
         uint64_t* d_field = nullptr;
         double* d_vals = nullptr;
+        float* d_vals32 = nullptr; // mixed form, made on first use
     } wide_copy[BLCO_MAX_MODES];
     // heavy-row tables, one per mode, built at encode time
     blco::HotTable hot[BLCO_MAX_MODES];
@@ -214,6 +215,7 @@ struct MttkrpArgs {
     int thread_cf;
     int hot_chunk;  // positions per warp task of the heavy-row kernel (0: 512)
     int interleave; // tile kernel: 1 deals tiles round-robin to the grid's warps
+    int out64;      // wide keys, FP32 factors: out is FP64 (sums of heavy rows stay FP64)
 };
 int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 // Wide-key tensors: FP64 MTTKRP over the BLCO stream in key order.

@@ -816,11 +816,11 @@ namespace {
 struct WideParams {
     const uint64_t* coords;
     const uint64_t* field;
-    const double* vals;
+    const void* vals;             // T
     uint64_t nnz;
     Layout L;
-    const double* f[BLCO_MAX_MODES];
-    double* out;
+    const void* f[BLCO_MAX_MODES]; // T
+    void* out;                     // T
     int mode;
     int rank;
     int col0; // first column of this launch's column slab
@@ -829,9 +829,13 @@ struct WideParams {
 constexpr int WIDE_THREADS = 256;
 constexpr int WIDE_BATCHES = 4; // batches of G nonzeros per group task
 
-template <int G, int CPL>
+// T: element type of values, factors and output (FP64, or FP32 for the
+// mixed form); run sums are FP64 in both.
+template <typename T, typename TO, int G, int CPL>
 __global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide(const WideParams p)
 {
+    const T* __restrict__ vals = static_cast<const T*>(p.vals);
+    TO* __restrict__ out = static_cast<TO*>(p.out);
     const int lane = threadIdx.x & 31;
     const int sub = lane % G;
     const int grp = lane / G;
@@ -855,7 +859,7 @@ __global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide(const WideParams p
             {
                 const uint64_t c = ok ? __ldg(p.coords + i) : 0;
                 const uint64_t fld = ok ? __ldg(p.field + i) : 0;
-                v = ok ? __ldg(p.vals + i) : 0.0;
+                v = ok ? (double)__ldg(vals + i) : 0.0;
 #pragma unroll
                 for (int n = 0; n < BLCO_MAX_MODES; n++)
                     row[n] = n < nm ? (uint32_t)wide_row(p.L, n, c, fld) : 0u;
@@ -876,7 +880,7 @@ __global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide(const WideParams p
 #pragma unroll
                         for (int k = 0; k < CPL; k++) {
                             const int col = p.col0 + sub + k * G;
-                            if (col < R) atomicAdd(p.out + cur * R + col, acc[k]);
+                            if (col < R) atomicAdd(out + cur * R + col, (TO)acc[k]);
                             acc[k] = 0.0;
                         }
                     }
@@ -886,11 +890,12 @@ __global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide(const WideParams p
                 for (int k = 0; k < CPL; k++) {
                     const int col = p.col0 + sub + k * G;
                     if (col < R) {
-                        double prod = vv;
+                        T prod = (T)vv;
 #pragma unroll
                         for (int n = 0; n < BLCO_MAX_MODES; n++)
-                            if (n < nm && n != p.mode) prod *= __ldg(p.f[n] + (uint64_t)r[n] * R + col);
-                        acc[k] += prod;
+                            if (n < nm && n != p.mode)
+                                prod *= __ldg(static_cast<const T*>(p.f[n]) + (uint64_t)r[n] * R + col);
+                        acc[k] += (double)prod;
                     }
                 }
             }
@@ -899,7 +904,7 @@ __global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide(const WideParams p
 #pragma unroll
             for (int k = 0; k < CPL; k++) {
                 const int col = p.col0 + sub + k * G;
-                if (col < R) atomicAdd(p.out + cur * R + col, acc[k]);
+                if (col < R) atomicAdd(out + cur * R + col, (TO)acc[k]);
             }
         }
     }
@@ -1026,13 +1031,145 @@ int launch_wide2(const WideParams2& p, int grid, int lanes, bool off32, cudaStre
     return fail(BLCO_ERR_INVALID, "wide MTTKRP: bad lane count");
 }
 
+// Mixed form: FP32 values and factors, four columns per lane (16-byte
+// gathers), FP32 products summed in FP64 registers along a row's run and
+// added to the FP32 output when the row changes.  L = lanes per nonzero
+// (4 * L >= the columns of the slab, at most 128).
+struct WideParams4 {
+    const uint64_t* coords;
+    const uint64_t* field;
+    const float* vals;
+    uint64_t nnz;
+    Layout L;
+    const float* fo[BLCO_MAX_MODES - 1];
+    int other[BLCO_MAX_MODES - 1];
+    void* out; // TO
+    int mode;
+    int rank;
+    int col0;
+};
+
+template <int NM, int L, typename TO>
+__global__ __launch_bounds__(WIDE_THREADS) void k_mttkrp_wide4(const WideParams4 p)
+{
+    constexpr int NO = NM - 1;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane % L;
+    const int grp = lane / L;
+    constexpr uint64_t WARP_TASK = (uint64_t)32 * WIDE_BATCHES;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (WIDE_THREADS / 32);
+    const uint64_t wid = (uint64_t)blockIdx.x * (WIDE_THREADS / 32) + (threadIdx.x >> 5);
+    const int R = p.rank;
+    const int col = p.col0 + 4 * sub;
+    const bool cok = col < R; // col + 3 < R too: R is a multiple of 4
+    const uint64_t ntasks = (p.nnz + WARP_TASK - 1) / WARP_TASK;
+    for (uint64_t task = wid; task < ntasks; task += nwarps) {
+        const uint64_t g0 = task * WARP_TASK + (uint64_t)grp * (L * WIDE_BATCHES);
+        uint32_t cur = 0xffffffffu;
+        double a[4] = {0.0, 0.0, 0.0, 0.0};
+        auto flush = [&]() {
+            if (cur != 0xffffffffu && cok) {
+                TO* o = static_cast<TO*>(p.out) + (uint64_t)cur * R + col;
+#pragma unroll
+                for (int j = 0; j < 4; j++) atomicAdd(o + j, (TO)a[j]);
+            }
+        };
+        for (int b = 0; b < WIDE_BATCHES; b++) {
+            const uint64_t i = g0 + (uint64_t)b * L + sub;
+            const bool ok = i < p.nnz;
+            uint32_t rt = 0xffffffffu, ro[NO];
+            float v = 0.f;
+            {
+                const uint64_t c = ok ? __ldg(p.coords + i) : 0;
+                const uint64_t f = ok ? __ldg(p.field + i) : 0;
+                v = ok ? __ldg(p.vals + i) : 0.f;
+                if (ok) rt = (uint32_t)wide_row(p.L, p.mode, c, f);
+#pragma unroll
+                for (int k = 0; k < NO; k++) ro[k] = (uint32_t)wide_row(p.L, p.other[k], c, f);
+            }
+            constexpr int U = L >= 4 ? 4 : L;
+#pragma unroll 1
+            for (int j0 = 0; j0 < L; j0 += U) {
+                uint32_t r[U];
+                float vv[U];
+                float4 x[U][NO];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    r[u] = __shfl_sync(0xffffffffu, rt, j0 + u, L);
+                    vv[u] = __shfl_sync(0xffffffffu, v, j0 + u, L);
+#pragma unroll
+                    for (int k = 0; k < NO; k++) {
+                        const uint32_t rr = __shfl_sync(0xffffffffu, ro[k], j0 + u, L);
+                        // rows of nonzeros past the end decode to row 0: in bounds
+                        x[u][k] = cok ? __ldg(reinterpret_cast<const float4*>(p.fo[k] + ((uint64_t)rr * R + col)))
+                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (r[u] == 0xffffffffu) continue;
+                    if (r[u] != cur) {
+                        flush();
+                        a[0] = a[1] = a[2] = a[3] = 0.0;
+                        cur = r[u];
+                    }
+                    float q0 = vv[u], q1 = vv[u], q2 = vv[u], q3 = vv[u];
+#pragma unroll
+                    for (int k = 0; k < NO; k++) {
+                        q0 *= x[u][k].x;
+                        q1 *= x[u][k].y;
+                        q2 *= x[u][k].z;
+                        q3 *= x[u][k].w;
+                    }
+                    a[0] += (double)q0;
+                    a[1] += (double)q1;
+                    a[2] += (double)q2;
+                    a[3] += (double)q3;
+                }
+            }
+        }
+        flush();
+    }
+}
+
+template <int NM, typename TO>
+int launch_wide4(const WideParams4& p, int grid, int lanes, cudaStream_t s)
+{
+    switch (lanes) {
+    case 4: k_mttkrp_wide4<NM, 4, TO><<<grid, WIDE_THREADS, 0, s>>>(p); break;
+    case 8: k_mttkrp_wide4<NM, 8, TO><<<grid, WIDE_THREADS, 0, s>>>(p); break;
+    case 16: k_mttkrp_wide4<NM, 16, TO><<<grid, WIDE_THREADS, 0, s>>>(p); break;
+    case 32: k_mttkrp_wide4<NM, 32, TO><<<grid, WIDE_THREADS, 0, s>>>(p); break;
+    default: return fail(BLCO_ERR_INVALID, "wide MTTKRP: bad lane count");
+    }
+    BLCO_CHECK_LAUNCH("k_mttkrp_wide4");
+    return BLCO_OK;
+}
+
 } // namespace
+
+// FP32 copy of mode n's row-sorted values (wide keys, mixed form; made on
+// first use).
+static int wide_vals32(const blco_tensor* t, int n, cudaStream_t s, const float** out)
+{
+    blco_tensor::WideCopy& w = const_cast<blco_tensor::WideCopy&>(t->wide_copy[n]);
+    if (!w.d_vals32) {
+        BLCO_CUDA(cudaMalloc(&w.d_vals32, std::max<uint64_t>(1, t->nnz) * sizeof(float)));
+        if (t->nnz) {
+            k_to_f32<<<1024, 256, 0, s>>>(w.d_vals, w.d_vals32, t->nnz);
+            BLCO_CHECK_LAUNCH("k_to_f32");
+        }
+    }
+    *out = w.d_vals32;
+    return BLCO_OK;
+}
 
 int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
 {
     if (a.nnz == 0) return BLCO_OK;
-    if (a.factor_dtype != BLCO_DTYPE_F64)
-        return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits: the MTTKRP is FP64 only (the reference's form)");
+    if (a.factor_dtype == BLCO_DTYPE_BF16)
+        return fail(BLCO_ERR_UNSUPPORTED, "keys above 64 bits: FP64 or FP32 factors (no BF16 gathers)");
+    const bool f32 = a.factor_dtype == BLCO_DTYPE_F32;
     const blco_tensor::WideCopy& w = t->wide_copy[a.mode];
     if (!t->resident || !w.d_coords) return fail(BLCO_ERR_STATE, "wide-key tensor without its per-mode copies");
     DeviceInfo di;
@@ -1041,16 +1178,81 @@ int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s
     memset(&p, 0, sizeof(p));
     p.coords = w.d_coords;
     p.field = w.d_field;
-    p.vals = w.d_vals;
+    if (f32) {
+        const float* v32 = nullptr;
+        BLCO_TRY(wide_vals32(t, a.mode, s, &v32));
+        p.vals = v32;
+    } else {
+        p.vals = w.d_vals;
+    }
     p.nnz = a.nnz;
     p.L = t->layout;
-    for (int m = 0; m < t->layout.nmodes; m++) p.f[m] = static_cast<const double*>(a.factors[m]);
-    p.out = static_cast<double*>(a.out);
+    for (int m = 0; m < t->layout.nmodes; m++) p.f[m] = a.factors[m];
+    p.out = a.out;
     p.mode = a.mode;
     p.rank = a.rank;
     const uint64_t ntasks = (a.nnz + 32 * WIDE_BATCHES - 1) / (32 * WIDE_BATCHES);
     const int grid = (int)std::min<uint64_t>((ntasks + WIDE_THREADS / 32 - 1) / (WIDE_THREADS / 32),
                                              (uint64_t)di.sm_count * 8);
+    if (f32) {
+        bool quads = a.rank % 4 == 0 && ((uintptr_t)a.out & 15) == 0;
+        for (int m = 0; m < t->layout.nmodes; m++)
+            if (m != a.mode && ((uintptr_t)a.factors[m] & 15)) quads = false;
+        const int nm = t->layout.nmodes;
+        if (quads && nm >= 3) {
+            WideParams4 q;
+            memset(&q, 0, sizeof(q));
+            q.coords = p.coords;
+            q.field = p.field;
+            q.vals = static_cast<const float*>(p.vals);
+            q.nnz = p.nnz;
+            q.L = p.L;
+            q.out = a.out;
+            q.mode = a.mode;
+            q.rank = a.rank;
+            for (int m = 0, k = 0; m < nm; m++)
+                if (m != a.mode) {
+                    q.fo[k] = static_cast<const float*>(a.factors[m]);
+                    q.other[k++] = m;
+                }
+            for (int c0 = 0; c0 < a.rank; c0 += 128) {
+                q.col0 = c0;
+                const int cols = std::min(128, a.rank - c0);
+                const int lanes = cols <= 16 ? 4 : cols <= 32 ? 8 : cols <= 64 ? 16 : 32;
+                int st;
+                if (a.out64) {
+                    if (nm == 3) st = launch_wide4<3, double>(q, grid, lanes, s);
+                    else if (nm == 4) st = launch_wide4<4, double>(q, grid, lanes, s);
+                    else st = launch_wide4<5, double>(q, grid, lanes, s);
+                } else {
+                    if (nm == 3) st = launch_wide4<3, float>(q, grid, lanes, s);
+                    else if (nm == 4) st = launch_wide4<4, float>(q, grid, lanes, s);
+                    else st = launch_wide4<5, float>(q, grid, lanes, s);
+                }
+                if (st != BLCO_OK) return st;
+            }
+            return BLCO_OK;
+        }
+        for (int c0 = 0; c0 < a.rank; c0 += 128) {
+            p.col0 = c0;
+            const int cols = std::min(128, a.rank - c0);
+            if (a.out64) {
+                if (a.rank <= 8) k_mttkrp_wide<float, double, 8, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else if (a.rank <= 16) k_mttkrp_wide<float, double, 16, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else if (cols <= 32) k_mttkrp_wide<float, double, 32, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else if (cols <= 64) k_mttkrp_wide<float, double, 32, 2><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else k_mttkrp_wide<float, double, 32, 4><<<grid, WIDE_THREADS, 0, s>>>(p);
+            } else {
+                if (a.rank <= 8) k_mttkrp_wide<float, float, 8, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else if (a.rank <= 16) k_mttkrp_wide<float, float, 16, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else if (cols <= 32) k_mttkrp_wide<float, float, 32, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else if (cols <= 64) k_mttkrp_wide<float, float, 32, 2><<<grid, WIDE_THREADS, 0, s>>>(p);
+                else k_mttkrp_wide<float, float, 32, 4><<<grid, WIDE_THREADS, 0, s>>>(p);
+            }
+            BLCO_CHECK_LAUNCH("k_mttkrp_wide");
+        }
+        return BLCO_OK;
+    }
     // two columns per lane when every factor row starts on 16 bytes
     bool pairs = a.rank % 2 == 0 && ((uintptr_t)a.out & 15) == 0;
     uint64_t maxdim = 0;
@@ -1064,15 +1266,15 @@ int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s
         memset(&q, 0, sizeof(q));
         q.coords = p.coords;
         q.field = p.field;
-        q.vals = p.vals;
+        q.vals = static_cast<const double*>(p.vals);
         q.nnz = p.nnz;
         q.L = p.L;
-        q.out = p.out;
+        q.out = static_cast<double*>(p.out);
         q.mode = p.mode;
         q.rank = p.rank;
         for (int m = 0, k = 0; m < nm; m++)
             if (m != a.mode) {
-                q.fo[k] = p.f[m];
+                q.fo[k] = static_cast<const double*>(p.f[m]);
                 q.other[k++] = m;
             }
         const bool off32 = maxdim * (uint64_t)a.rank < (1ull << 32);
@@ -1091,11 +1293,11 @@ int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s
     for (int c0 = 0; c0 < a.rank; c0 += 128) {
         p.col0 = c0;
         const int cols = std::min(128, a.rank - c0);
-        if (a.rank <= 8) k_mttkrp_wide<8, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
-        else if (a.rank <= 16) k_mttkrp_wide<16, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
-        else if (cols <= 32) k_mttkrp_wide<32, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
-        else if (cols <= 64) k_mttkrp_wide<32, 2><<<grid, WIDE_THREADS, 0, s>>>(p);
-        else k_mttkrp_wide<32, 4><<<grid, WIDE_THREADS, 0, s>>>(p);
+        if (a.rank <= 8) k_mttkrp_wide<double, double, 8, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else if (a.rank <= 16) k_mttkrp_wide<double, double, 16, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else if (cols <= 32) k_mttkrp_wide<double, double, 32, 1><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else if (cols <= 64) k_mttkrp_wide<double, double, 32, 2><<<grid, WIDE_THREADS, 0, s>>>(p);
+        else k_mttkrp_wide<double, double, 32, 4><<<grid, WIDE_THREADS, 0, s>>>(p);
         BLCO_CHECK_LAUNCH("k_mttkrp_wide");
     }
     return BLCO_OK;

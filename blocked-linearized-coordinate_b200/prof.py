@@ -195,16 +195,32 @@ def run_wide(a, pkg, torch):
         alg = a.nnz * 16 + sum(d * R * 8 for d in dims)
         best = min(ts)
         print(f"mode {m}: ms {['%.3f' % x for x in ts]} alg GB/s {alg / best / 1e6:.0f}", flush=True)
+    f32 = [f.float() for f in fs]
+    for m in range(len(dims)):
+        out = torch.zeros(dims[m], R, dtype=torch.float32, device="cuda")
+        pkg.mttkrp_ex(t, m, f32, out, pkg.DTYPE_F32, o)
+        ts = []
+        for _ in range(a.reps):
+            e0.record()
+            pkg.mttkrp_ex(t, m, f32, out, pkg.DTYPE_F32, o)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        print(f"mode {m} f32: ms {['%.3f' % x for x in ts]}", flush=True)
+    del f32
     if a.iters:
-        lam = torch.ones(R, dtype=torch.float64, device="cuda")
-        plan = pkg.CpalsPlan(t, fs, lam, pkg.make_opts(kernel=10))
-        plan.iterate(2, tol=-1.0)
-        e0.record()
-        fits = plan.iterate(a.iters, tol=-1.0)
-        e1.record()
-        torch.cuda.synchronize()
-        print(f"cpals fp64 ms/iter {e0.elapsed_time(e1) / a.iters:.3f} fit {fits[-1]:.6f}", flush=True)
-        plan.destroy()
+        for name, prec in (("fp64", pkg.PRECISION_FP64), ("mixed_f32", pkg.PRECISION_MIXED)):
+            lam = torch.ones(R, dtype=torch.float64, device="cuda")
+            plan = pkg.CpalsPlan(t, [f.clone() for f in fs], lam, pkg.make_opts(kernel=10, precision=prec))
+            plan.iterate(2, tol=-1.0)
+            e0.record()
+            fits = plan.iterate(a.iters, tol=-1.0)
+            e1.record()
+            torch.cuda.synchronize()
+            ms, calls = plan.mttkrp_ms()
+            print(f"cpals {name} ms/iter {e0.elapsed_time(e1) / a.iters:.3f} fit {fits[-1]:.9f} "
+                  f"mttkrp ms/mode (all calls) {['%.3f' % (x / max(1, calls)) for x in ms]}", flush=True)
+            plan.destroy()
     t.free()
 
 

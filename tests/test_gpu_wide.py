@@ -197,24 +197,66 @@ def test_wide_mttkrp_large_many_blocks(blco):
     t.free()
 
 
-def test_wide_rejects_mixed_forms_and_tuner(blco):
+def test_wide_forms_and_tuner(blco):
+    """Wide keys take FP64 or FP32 factors; BF16 gathers and the tuner
+    (one schedule) answer BLCO_ERR_UNSUPPORTED."""
     torch = _torch()
     dims = [1 << 17] * 4  # 68 bits
     rng = np.random.default_rng(2)
     cidx = unique_coords_wide(rng, dims, 1000)
     t = blco.Tensor.encode(dims, cidx, rng.random(1000))
-    f32 = [torch.zeros((d, 8), dtype=torch.float32, device="cuda") for d in dims]
+    b16 = [torch.zeros((d, 8), dtype=torch.bfloat16, device="cuda") for d in dims]
     with pytest.raises(blco.BlcoError) as e:
-        blco.mttkrp_ex(t, 3, f32[:3] + [None], torch.zeros((dims[3], 8), dtype=torch.float32, device="cuda"),
-                       blco.DTYPE_F32)
+        blco.mttkrp_ex(t, 3, b16[:3] + [None], torch.zeros((dims[3], 8), dtype=torch.float32, device="cuda"),
+                       blco.DTYPE_BF16)
     assert e.value.status == blco.ERR_UNSUPPORTED
     with pytest.raises(blco.BlcoError) as e:
         blco.cpals(t, [np.ones((d, 2)) for d in dims], np.ones(2), 1, 0.0,
-                   blco.make_opts(precision=blco.PRECISION_MIXED))
+                   blco.make_opts(precision=blco.PRECISION_MIXED_BF16))
     assert e.value.status == blco.ERR_UNSUPPORTED
     with pytest.raises(blco.BlcoError) as e:
         blco.autotune(t, 0, 8)
     assert e.value.status == blco.ERR_UNSUPPORTED
+    t.free()
+
+
+@pytest.mark.parametrize("rank", [5, 8, 16, 32, 64, 96, 160])
+def test_wide_mixed_mttkrp(blco, rank):
+    """FP32 values and factors, FP64 run sums, FP32 output: within 1e-5
+    normwise of the COO oracle on the same (rounded) inputs."""
+    torch = _torch()
+    rng = np.random.default_rng(100 + rank)
+    dims = [9000, 8500, 8200, 8192, 8300] if rank % 2 else [1 << 17, 1 << 17, 100_000, 1 << 17]
+    cidx = unique_coords_wide(rng, dims, 60_000)
+    vals = rng.random(60_000).astype(np.float32).astype(np.float64)
+    fs = [rng.random((d, rank)).astype(np.float32) for d in dims]
+    t = blco.Tensor.encode(dims, cidx, vals, 7000)
+    d_f = [torch.from_numpy(f).cuda() for f in fs]
+    for m in range(len(dims)):
+        ref = po.mttkrp_coo(cidx, vals, [f.astype(np.float64) for f in fs], m)
+        out = torch.zeros((dims[m], rank), dtype=torch.float32, device="cuda")
+        blco.mttkrp_ex(t, m, d_f, out, blco.DTYPE_F32)
+        torch.cuda.synchronize()
+        o = out.double().cpu().numpy()
+        assert np.linalg.norm(o - ref) <= 1e-5 * np.linalg.norm(ref), (rank, m)
+    t.free()
+
+
+def test_wide_mixed_cpals_within_bound(blco):
+    """The chosen form on a wide-key tensor: fit within 1e-5 of FP64."""
+    rng = np.random.default_rng(31)
+    dims = [1 << 17, 1 << 17, 100_000, 1 << 17]
+    nnz = 80_000
+    cidx = unique_coords_wide(rng, dims, nnz)
+    vals = rng.random(nnz)
+    R = 16
+    fs0 = [rng.random((d, R)) for d in dims]
+    t = blco.Tensor.encode(dims, cidx, vals)
+    _, f64 = blco.cpals(t, [f.copy() for f in fs0], np.ones(R), 8, 0.0)
+    _, f32 = blco.cpals(t, [f.copy() for f in fs0], np.ones(R), 8, 0.0,
+                        blco.make_opts(precision=blco.PRECISION_MIXED))
+    assert len(f32) == 8
+    assert np.max(np.abs(np.array(f32) - np.array(f64))) <= 1e-5
     t.free()
 
 
