@@ -61,7 +61,8 @@ EXPORTS = (
     "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
     "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
     "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_gram_f32",
-    "blco_encode_tns", "blco_parse_decimal", "blco_launch_count",
+    "blco_encode_tns", "blco_parse_decimal", "blco_launch_count", "blco_cpals_plan_set_reduce",
+    "blco_cpals_plan_set_norm_sq",
 )
 
 
@@ -353,6 +354,51 @@ def cpals(t, factors, lam, maxiter, tol, opts=None):
     return fit.value, list(fits[: iters.value])
 
 
+# int fn(void* ctx, void* d_buf, uint64_t count, int dtype, void* stream)
+REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                             ctypes.c_void_p)
+
+
+class _DeviceBuf:
+    """A CUDA array view of a raw device pointer (no copy)."""
+
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = dict(shape=(int(count),), typestr=typestr, data=(int(ptr), False),
+                                             version=2)
+
+
+def dist_reduce(dist, group=None, via_host=False, view=None):
+    """A reduce hook for CpalsPlan.set_reduce from a torch.distributed
+    process group: the MTTKRP buffer is summed over the ranks on the plan's
+    stream (dist.all_reduce; NCCL puts it on that stream's timeline).  With
+    via_host the sum goes through host copies (for the gloo backend).
+    view(ptr, count, dtype) -> tensor overrides the device view (tests)."""
+    import torch
+
+    def fn(ptr, count, dtype, stream):
+        tdt = torch.float64 if dtype == DTYPE_F64 else torch.float32
+        if view is not None:
+            t = view(ptr, count, dtype)
+        else:
+            t = torch.as_tensor(_DeviceBuf(ptr, count, "<f8" if dtype == DTYPE_F64 else "<f4"), device="cuda")
+            assert t.dtype == tdt
+        ctx = torch.cuda.stream(torch.cuda.ExternalStream(stream)) if stream and t.is_cuda else None
+        if ctx is not None:
+            ctx.__enter__()
+        try:
+            if via_host and t.is_cuda:
+                h = t.cpu()
+                dist.all_reduce(h, group=group)
+                t.copy_(h)
+            else:
+                dist.all_reduce(t, group=group)
+        finally:
+            if ctx is not None:
+                ctx.__exit__(None, None, None)
+
+    return fn
+
+
 class CpalsPlan:
     """Device-resident CP-ALS over torch CUDA factors (owned by the caller)."""
 
@@ -373,6 +419,31 @@ class CpalsPlan:
         done = ctypes.c_int()
         _check(lib().blco_cpals_plan_iterate(self._h, iters, tol, fits.ctypes.data, ctypes.byref(done)))
         return list(fits[: done.value])
+
+    def set_reduce(self, fn):
+        """Sharded tensor: fn(d_ptr, count, dtype, stream) must sum the
+        MTTKRP buffer over the ranks on that stream (see dist_reduce);
+        None removes the hook."""
+        if fn is None:
+            self._reduce = None
+            _check(lib().blco_cpals_plan_set_reduce(self._h, None, None))
+            return
+
+        def cb(ctx, ptr, count, dtype, stream):
+            try:
+                fn(ptr, count, dtype, stream)
+                return 0
+            except Exception:  # reported as a failed exchange
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        self._reduce = REDUCE_FN(cb)  # kept alive with the plan
+        _check(lib().blco_cpals_plan_set_reduce(self._h, self._reduce, None))
+
+    def set_norm_sq(self, norm_sq):
+        """||X||^2 of the whole (sharded) tensor, for the fit."""
+        _check(lib().blco_cpals_plan_set_norm_sq(self._h, ctypes.c_double(float(norm_sq))))
 
     def mttkrp_ms(self):
         ms = np.zeros(self.nmodes, dtype=np.float64)

@@ -396,6 +396,10 @@ int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls) 
 
 int blco_cpals_plan_destroy(blco_cpals_plan* p) { return plan_destroy(p); }
 
+int blco_cpals_plan_set_reduce(blco_cpals_plan* p, blco_reduce_fn fn, void* ctx) { return plan_set_reduce(p, fn, ctx); }
+
+int blco_cpals_plan_set_norm_sq(blco_cpals_plan* p, double norm_sq) { return plan_set_norm_sq(p, norm_sq); }
+
 int blco_batch_create(int count, blco_tensor* const* tensors, const int* ranks, double* const* const* d_factors,
                       double* const* d_lambdas, double tol, const blco_opts* opts, blco_batch** out)
 {

@@ -557,6 +557,8 @@ int grid_rows(uint64_t I, int sm)
 struct blco_cpals_plan {
     blco_tensor* t = nullptr;
     int R = 0, N = 0;
+    blco_reduce_fn reduce = nullptr; // sharded CP-ALS: sum of the MTTKRP over the ranks
+    void* reduce_ctx = nullptr;
     double* U[BLCO_MAX_MODES] = {};   // caller's FP64 factors
     double* lambda = nullptr;         // caller's FP64 lambda
     double* M = nullptr;              // MTTKRP result (FP64, plain form)
@@ -766,6 +768,13 @@ int mode_update(blco_cpals_plan* p, int n)
     BLCO_CUDA(cudaEventRecord(p->ev[2 * n], p->s));
     if (t->resident) BLCO_TRY(mttkrp_launch(t, a, p->s));
     else BLCO_TRY(mttkrp_streamed_ring(t, a, p->ring, p->s)); // blocks copied through the plan's ring
+    if (p->reduce) {
+        // sharded tensor: sum this mode's MTTKRP over the ranks (the one exchange)
+        const bool f64 = !p->mixed || t->layout.wide;
+        if (p->reduce(p->reduce_ctx, f64 ? (void*)p->M : (void*)p->Mf, I * (uint64_t)R,
+                      f64 ? BLCO_DTYPE_F64 : BLCO_DTYPE_F32, (void*)p->s) != 0)
+            return fail(BLCO_ERR_CUDA, "the MTTKRP sum over the ranks failed");
+    }
     if (p->mixed && t->layout.wide) {
         k_f64_to_f32<<<conv_grid(I * R, p->sm), 256, 0, p->s>>>(p->M, p->Mf, I * R);
         BLCO_CHECK_LAUNCH("k_f64_to_f32");
@@ -1042,6 +1051,22 @@ int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda,
     plan_free(p);
     cleanup();
     return st;
+}
+
+int plan_set_reduce(blco_cpals_plan* p, blco_reduce_fn fn, void* ctx)
+{
+    if (!p) return fail(BLCO_ERR_INVALID, "null plan");
+    p->reduce = fn;
+    p->reduce_ctx = ctx;
+    return BLCO_OK;
+}
+
+int plan_set_norm_sq(blco_cpals_plan* p, double norm_sq)
+{
+    if (!p) return fail(BLCO_ERR_INVALID, "null plan");
+    if (!(norm_sq >= 0.0)) return fail(BLCO_ERR_INVALID, "norm_sq must be non-negative");
+    p->xnorm = std::sqrt(norm_sq);
+    return BLCO_OK;
 }
 
 int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls)

@@ -280,6 +280,26 @@ int blco_cpals_plan_iterate(blco_cpals_plan* p, int iters, double tol, double* f
 int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
 int blco_cpals_plan_destroy(blco_cpals_plan* p);
 
+/* Sharded CP-ALS (several processes, one GPU each, each holding a share of
+ * the nonzeros of one tensor and the same factors).  No reference
+ * counterpart: the reference decomposes on one GPU.  The partition of the
+ * nonzeros is free (the MTTKRP is a sum over nonzeros); the one exchange is
+ * a sum of every mode's MTTKRP over the ranks.
+ *   blco_cpals_plan_set_reduce: after each mode's MTTKRP the plan calls
+ *   fn(ctx, d_buf, count, dtype, stream) from the thread that runs
+ *   blco_cpals_plan_iterate, with the MTTKRP output (count elements of
+ *   BLCO_DTYPE_F64 or _F32 in device memory) and the plan's stream; fn
+ *   must enqueue a sum over the ranks into d_buf on that stream (for
+ *   instance ncclAllReduce) and return 0 (else the iteration stops with
+ *   BLCO_ERR_CUDA).  Every rank must get identical sums: every later step
+ *   is deterministic, so all ranks then compute the same factors and fits
+ *   and take the same convergence decision.  fn = NULL removes the hook.
+ *   blco_cpals_plan_set_norm_sq: the sum over the ranks of their tensors'
+ *   squared values (||X||^2 of the whole tensor, for the fit). */
+typedef int (*blco_reduce_fn)(void* ctx, void* d_buf, uint64_t count, int dtype, void* stream);
+int blco_cpals_plan_set_reduce(blco_cpals_plan* p, blco_reduce_fn fn, void* ctx);
+int blco_cpals_plan_set_norm_sq(blco_cpals_plan* p, double norm_sq);
+
 /* Batched CP-ALS of many independent resident tensors (no counterpart in the
  * reference, which decomposes one tensor per run).  Tensors may differ in
  * nnz, order (1..5) and rank (ranks[t] in 1..64); up to 4096 tensors, all on
