@@ -40,7 +40,7 @@ def _worker(rank, world, port, out):
 
 def test_max_over_ranks_two_gloo_ranks():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.start_processes(_worker, args=(2, port, out), nprocs=2, start_method="spawn")
         assert dict(out) == {0: 20.0, 1: 20.0}

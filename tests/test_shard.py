@@ -51,7 +51,7 @@ def _cpu_worker(rank, world, port, out):
 
 def test_dist_reduce_sums_over_two_gloo_ranks():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.start_processes(_cpu_worker, args=(2, port, out), nprocs=2, start_method="spawn")
         want = (np.arange(10) * 3.0).tolist()
@@ -118,7 +118,7 @@ def _single(blco, precision):
 def test_sharded_cpals_matches_single_process(blco, mixed):
     precision = blco.PRECISION_MIXED if mixed else blco.PRECISION_FP64
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.start_processes(_gpu_worker, args=(2, port, precision, out), nprocs=2, start_method="spawn")
         r0, r1 = dict(out[0]), dict(out[1])
