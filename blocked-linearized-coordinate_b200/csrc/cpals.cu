@@ -1,4 +1,8 @@
-// cpals.cu -- CP-ALS on the GPU (plain FP64 form).
+// cpals.cu -- CP-ALS on the GPU: the plain FP64 form and the mixed forms
+// (FP32 or BF16 gathers, FP64 solve, lambda and fit), resident or streamed
+// tensors, one tensor per plan (optionally sharded over ranks: the plan hands
+// each mode's MTTKRP to the caller's sum over the ranks), and the batched
+// CP-ALS of many small tensors (second half of the file).
 //
 // Keeps the arithmetic of cpals_blco_dev (src/cpd_gpu.cu:21-242) but runs
 // every step as this library's own kernels on one stream, with no host

@@ -12,6 +12,9 @@
 //      upper key half is always zero for 64-bit keys, so every nonzero is in
 //      histogram bucket 0, include/blco.hpp:249-321)
 // Then per-mode row statistics and heavy-row tables for the MTTKRP kernels.
+// Further sections: keys of 65-128 bits (the reference's 128-bit build,
+// blocks with block coordinates), the chunked encode of streamed tensors
+// larger than their residency budget, and the allocation-free encoder.
 #include <algorithm>
 #include <cstring>
 #include <atomic>
