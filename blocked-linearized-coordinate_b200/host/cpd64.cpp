@@ -56,6 +56,8 @@ static void usage(const char* call)
     fprintf(stderr, "\t--batch              Accepted for compatibility (blocks always run in one launch)\n");
     fprintf(stderr, "\t--selector FILE      Trained schedule selector (selector_params.bin) for -k 21\n");
     fprintf(stderr, "\t--host-load          Parse the .tns file on the host (default: on the GPU, except with -c / -f)\n");
+    fprintf(stderr, "\t--precision P        CP-ALS numeric form: fp64 (default, the reference's), mixed (FP32\n"
+                    "\t                     values and gathers, FP64 solve and fit) or mixed-bf16 (BF16 gathers)\n");
 }
 
 // Reads a selector parameter file (int32 hidden width, int32 count, then
@@ -146,7 +148,7 @@ int main(int argc, char** argv)
         {"kernel-id", 1, nullptr, 'k'},  {"num-partitions", 1, nullptr, 'n'}, {"device", 1, nullptr, 1001},
         {"thread-cf", 1, nullptr, 1002}, {"stream-data", 0, nullptr, 1003}, {"max-block-size", 1, nullptr, 1004},
         {"max_block_size", 1, nullptr, 1004}, {"batch", 0, nullptr, 1005}, {"selector", 1, nullptr, 1006},
-        {"host-load", 0, nullptr, 1007},
+        {"host-load", 0, nullptr, 1007}, {"precision", 1, nullptr, 1008},
         {nullptr, 0, nullptr, 0}};
     int max_iters = 10;
     long long rank = 16;
@@ -161,6 +163,7 @@ int main(int argc, char** argv)
     int nthreads = omp && atoi(omp) > 0 ? atoi(omp) : (int)std::max(1u, std::thread::hardware_concurrency());
     int num_partitions = nthreads;
     int device = 0, thread_cf = 2;
+    int precision = BLCO_PRECISION_FP64;
     long long max_block_size = 16777216;
     int c;
     while ((c = getopt_long(argc, argv, "hvi:o:b:r:m:x:d:t:s:e:f:cpk:n:", long_opt, nullptr)) != -1) {
@@ -189,8 +192,18 @@ int main(int argc, char** argv)
         case 1005: break;
         case 1006: selector_file = optarg; break;
         case 1007: host_load = true; break;
+        case 1008:
+            if (!strcmp(optarg, "fp64")) precision = BLCO_PRECISION_FP64;
+            else if (!strcmp(optarg, "mixed")) precision = BLCO_PRECISION_MIXED;
+            else if (!strcmp(optarg, "mixed-bf16")) precision = BLCO_PRECISION_MIXED_BF16;
+            else { fprintf(stderr, "Invalid -precision: %s (fp64, mixed or mixed-bf16).\n", optarg); return 1; }
+            break;
         default: usage(argv[0]); return 1;
         }
+    }
+    if (precision != BLCO_PRECISION_FP64 && (do_check || do_bench)) {
+        fprintf(stderr, "--precision selects the CP-ALS form; the -c / -p MTTKRP runs are FP64.\n");
+        return 1;
     }
     Coo X;
     std::string err;
@@ -202,6 +215,7 @@ int main(int argc, char** argv)
     opts.nprtn = num_partitions;
     opts.thread_cf = thread_cf;
     opts.stream_data = stream_data ? 1 : 0;
+    opts.precision = precision;
     opts.verbose = 1;
     opts.device = device;
     // The text file is parsed and encoded on the GPU unless the host COO

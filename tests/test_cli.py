@@ -79,6 +79,15 @@ def test_selector_file_errors(tmp_path):
     assert r.returncode == 1 and "cannot open" in r.stderr
 
 
+def test_precision_flag_errors():
+    r = run(["--precision", "fp16"])
+    assert r.returncode == 1 and "Invalid -precision" in r.stderr
+    r = run(["--precision", "mixed", "-c", "-i", "missing.tns"])
+    assert r.returncode == 1 and "the -c / -p MTTKRP runs are FP64" in r.stderr
+    r = run(["-h"])
+    assert "--precision" in r.stderr
+
+
 def test_tns_rejects_bad_input(tmp_path):
     p = str(tmp_path / "bad.tns")
     with open(p, "w") as f:
@@ -228,3 +237,22 @@ def test_cli_wide_keys(tmp_path):
         assert r.returncode == 0, r.stderr
         # one verification line per mode
         assert r.stderr.count("Results of mttkrp_blco_dev is correct") == 5, r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_mixed_precision_cpals(tmp_path):
+    """--precision mixed runs the chosen form: the fit follows the FP64
+    run's within the chosen form's 1e-5 bound."""
+    rng = np.random.default_rng(23)
+    dims = [80, 60, 40]
+    lin = rng.choice(80 * 60 * 40, size=20000, replace=False)
+    cidx = np.array(np.unravel_index(lin, dims), dtype=np.uint64)
+    p = str(tmp_path / "m.tns")
+    write_tns(p, cidx, rng.random(20000), comments=False)
+    fits = {}
+    for prec in ("fp64", "mixed"):
+        r = run(["-i", p, "-k", "10", "-r", "8", "-m", "6", "-e", "0", "-x", "5", "--precision", prec])
+        assert r.returncode == 0, r.stderr
+        line = [l for l in r.stdout.splitlines() if l.startswith("Final fit")][0]
+        fits[prec] = float(line.split(":")[1])
+    assert abs(fits["mixed"] - fits["fp64"]) <= 1e-5
