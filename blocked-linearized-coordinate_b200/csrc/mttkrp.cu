@@ -1480,10 +1480,15 @@ int stream_ring_create(const blco_tensor* t, uint64_t residency_bytes, StreamRin
 {
     *out = nullptr;
     StreamRing* r = new StreamRing();
-    r->B = t->max_block_size ? t->max_block_size : t->nnz;
+    // Copies are block-sized, or smaller when two blocks would not fit the
+    // budget: an MTTKRP over any contiguous range of a 64-bit stream is
+    // valid (its block coordinates are zero), so the cap always holds.
     const uint64_t budget = residency_bytes ? residency_bytes : (8ull << 30);
-    int nbuf = (int)std::max<uint64_t>(2, std::min<uint64_t>(8, budget / std::max<uint64_t>(1, r->B * 16)));
-    nbuf = (int)std::min<uint64_t>((uint64_t)nbuf, std::max<uint64_t>(1, t->block_count));
+    const uint64_t blk = t->max_block_size ? t->max_block_size : t->nnz;
+    r->B = std::max<uint64_t>(1, std::min<uint64_t>(blk, budget / (2 * 16)));
+    const uint64_t pieces = (t->nnz + r->B - 1) / r->B;
+    int nbuf = (int)std::max<uint64_t>(2, std::min<uint64_t>(8, budget / (r->B * 16)));
+    nbuf = (int)std::min<uint64_t>((uint64_t)nbuf, std::max<uint64_t>(1, pieces));
     r->nbuf = nbuf;
     r->dc.assign(nbuf, nullptr);
     r->dv.assign(nbuf, nullptr);
@@ -1504,9 +1509,10 @@ int stream_ring_create(const blco_tensor* t, uint64_t residency_bytes, StreamRin
     return BLCO_OK;
 }
 
-// One MTTKRP over every block: block b is copied into buffer b % nbuf on the
-// copy stream (after the kernel that used that buffer before), and its
-// MTTKRP runs on s after the copy.
+// One MTTKRP over every piece of the stream (a block, or a budget-sized
+// part of one): piece b is copied into buffer b % nbuf on the copy stream
+// (after the kernel that used that buffer before), and its MTTKRP runs on s
+// after the copy.
 int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRing* r, cudaStream_t s)
 {
     const bool f32 = base.factor_dtype != BLCO_DTYPE_F64;
@@ -1514,7 +1520,8 @@ int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRin
     // the copies must not overtake work already queued on s
     BLCO_CUDA(cudaEventRecord(r->consumed[0], s));
     BLCO_CUDA(cudaStreamWaitEvent(r->cs, r->consumed[0], 0));
-    for (uint64_t b = 0; b < t->block_count; b++) {
+    const uint64_t pieces = (t->nnz + r->B - 1) / r->B;
+    for (uint64_t b = 0; b < pieces; b++) {
         const int k = (int)(b % r->nbuf);
         const uint64_t beg = b * r->B, n = std::min(r->B, t->nnz - beg);
         if (b >= (uint64_t)r->nbuf) BLCO_CUDA(cudaStreamWaitEvent(r->cs, r->consumed[k], 0));

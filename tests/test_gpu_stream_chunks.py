@@ -116,3 +116,26 @@ def test_streamed_mixed_mttkrp_matches_resident(blco):
         assert np.linalg.norm(x - y) <= 1e-5 * np.linalg.norm(x), m
     t.free()
     ref.free()
+
+
+def test_streamed_blocks_larger_than_the_budget(blco):
+    """Blocks of 200k nonzeros under a 2 MiB budget: the ring copies
+    budget-sized pieces of each block, and the MTTKRP equals the resident
+    one (1e-12)."""
+    import torch
+    cidx, vals = _tensor(9)
+    R = 8
+    rng = np.random.default_rng(10)
+    fs = [torch.from_numpy(rng.random((d, R))).cuda() for d in DIMS]
+    ref = blco.Tensor.encode(DIMS, cidx, vals, 200_000)
+    t = blco.Tensor.encode(DIMS, cidx, vals, 200_000, opts=blco.make_opts(stream_data=True))
+    for m in range(3):
+        o1 = torch.zeros(DIMS[m], R, dtype=torch.float64, device="cuda")
+        o2 = torch.zeros(DIMS[m], R, dtype=torch.float64, device="cuda")
+        blco.mttkrp(ref, m, fs, o1)
+        blco.mttkrp(t, m, fs, o2, _opts(blco, 2 << 20))
+        torch.cuda.synchronize()
+        x, y = o1.cpu().numpy(), o2.cpu().numpy()
+        assert np.linalg.norm(x - y) <= 1e-12 * np.linalg.norm(x), m
+    t.free()
+    ref.free()
