@@ -35,6 +35,7 @@ KERNEL_AUTO = 10
 KERNEL_LVL1 = 1
 KERNEL_LVL2 = 2
 KERNEL_LVL3 = 3
+KERNEL_FIBRE = 4
 KERNEL_BATCHED = 11
 KERNEL_BATCHED_V2 = 12
 KERNEL_ATOMIC = 13

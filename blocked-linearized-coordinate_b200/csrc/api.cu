@@ -211,6 +211,7 @@ int blco_tensor_free(blco_tensor* t)
         cudaFree(t->hot[n].d_ccoords);
         cudaFree(t->hot[n].d_cvals);
         cudaFree(t->hot[n].d_cvals32);
+        blco::fibre_free(t->fib[n]);
     }
     delete t;
     return BLCO_OK;

@@ -157,8 +157,8 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int nblocks,
 // squares of U.  A warp computes a row; lane c owns columns c, c+32, ...
 constexpr int UP_MAXC = 4; // R <= 128
 
-template <typename T>
-__global__ __launch_bounds__(DN_THREADS) void k_update(const T* __restrict__ M, const double* __restrict__ P,
+template <typename TM, typename T>
+__global__ __launch_bounds__(DN_THREADS) void k_update(const TM* __restrict__ M, const double* __restrict__ P,
                                                        T* __restrict__ U, uint64_t I, int R,
                                                        double* __restrict__ colsq_partials)
 {
@@ -177,7 +177,7 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const T* __restrict__ M, 
     const uint64_t per = (I + gridDim.x - 1) / gridDim.x;
     const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
     for (uint64_t i = beg + warp; i < end; i += nw) {
-        const T* mrow = M + i * R;
+        const TM* mrow = M + i * R;
         double mreg[UP_MAXC];
 #pragma unroll
         for (int j = 0; j < UP_MAXC; j++) mreg[j] = (lane + 32 * j < R) ? (double)mrow[lane + 32 * j] : 0.0;
@@ -230,8 +230,8 @@ constexpr int UT_ROWS = 64;
 // The product is formed in FP64 whatever the storage type T: the
 // pseudoinverse of an ill-conditioned Hadamard product of Grams turns FP32
 // rounding in this step into fit errors well above 1e-5.
-template <typename T, int R>
-__global__ __launch_bounds__(DN_THREADS) void k_update_tiled(const T* __restrict__ M, const double* __restrict__ P,
+template <typename TM, typename T, int R>
+__global__ __launch_bounds__(DN_THREADS) void k_update_tiled(const TM* __restrict__ M, const double* __restrict__ P,
                                                              T* __restrict__ U, uint64_t I,
                                                              double* __restrict__ colsq_partials)
 {
@@ -465,8 +465,8 @@ __global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, i
 // ----------------------------------------------------------------- fit --
 // Per-block column sums of U[i][c] * M[i][c] (columnwise_inner_product,
 // src/cpd_gpu.cu:307-330).
-template <typename T>
-__global__ __launch_bounds__(DN_THREADS) void k_iprod(const T* __restrict__ U, const T* __restrict__ M,
+template <typename T, typename TM>
+__global__ __launch_bounds__(DN_THREADS) void k_iprod(const T* __restrict__ U, const TM* __restrict__ M,
                                                       uint64_t I, int R, double* __restrict__ partials)
 {
     extern __shared__ __align__(16) double ip[];
@@ -572,6 +572,7 @@ struct blco_cpals_plan {
     float* Uf[BLCO_MAX_MODES] = {};   // FP32 working factors
     void* Ub[BLCO_MAX_MODES] = {};    // BF16 gather copies (BF16 gathers only)
     float* Mf = nullptr;              // MTTKRP result (FP32)
+    bool m64[BLCO_MAX_MODES] = {};    // mixed form: this mode's MTTKRP result is in M (FP64), not Mf
     const float* vals32 = nullptr;
     blco::MttkrpArgs sched[BLCO_MAX_MODES] = {}; // per-mode schedule (kernel, hot_chunk, interleave)
     blco::StreamRing* ring = nullptr; // streamed tensors: device block buffers
@@ -712,20 +713,20 @@ int gram_launch_tc(blco_cpals_plan* p, float* U, uint64_t I, const double* inv, 
     return BLCO_OK;
 }
 
-template <typename T>
-int update_launch(blco_cpals_plan* p, const T* M, T* U, uint64_t I, int grid)
+template <typename TM, typename T>
+int update_launch(blco_cpals_plan* p, const TM* M, T* U, uint64_t I, int grid)
 {
     const int R = p->R;
     if (R == 16 || R == 32 || R == 64) {
         size_t smem = ((size_t)16 * R + (size_t)R * R + (size_t)UT_ROWS * (R + 1)) * sizeof(double);
-        void (*fn)(const T*, const double*, T*, uint64_t, double*) =
-            R == 16 ? k_update_tiled<T, 16> : R == 32 ? k_update_tiled<T, 32> : k_update_tiled<T, 64>;
+        void (*fn)(const TM*, const double*, T*, uint64_t, double*) =
+            R == 16 ? k_update_tiled<TM, T, 16> : R == 32 ? k_update_tiled<TM, T, 32> : k_update_tiled<TM, T, 64>;
         BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         fn<<<grid, DN_THREADS, smem, p->s>>>(M, p->P, U, I, p->partials);
     } else {
         size_t smem = (size_t)(R * R + (DN_THREADS / 32) * R) * sizeof(double);
-        BLCO_CUDA(cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_update<T><<<grid, DN_THREADS, smem, p->s>>>(M, p->P, U, I, R, p->partials);
+        BLCO_CUDA(cudaFuncSetAttribute(k_update<TM, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_update<TM, T><<<grid, DN_THREADS, smem, p->s>>>(M, p->P, U, I, R, p->partials);
     }
     BLCO_CHECK_LAUNCH("k_update");
     return BLCO_OK;
@@ -753,14 +754,17 @@ int mode_update(blco_cpals_plan* p, int n)
         for (int m = 0; m < N; m++)
             a.factors[m] = p->gather_dtype == BLCO_DTYPE_BF16 ? (const void*)p->Ub[m] : (const void*)p->Uf[m];
         a.factor_dtype = p->gather_dtype;
-        if (t->layout.wide) {
-            // wide keys: FP64 output (heavy rows summed in FP64), rounded once below
+        a.out = p->M;
+        a.out64 = 1;
+        // The fibre schedule sums rows in FP64 and keeps the result in FP64
+        // for the update; wide keys do the same and round once below.
+        p->m64[n] = !t->layout.wide && t->resident && a.kernel == BLCO_KERNEL_FIBRE && fibre_usable(t, a);
+        if (t->layout.wide || p->m64[n]) {
             BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
-            a.out = p->M;
-            a.out64 = 1;
         } else {
             BLCO_CUDA(cudaMemsetAsync(p->Mf, 0, I * R * sizeof(float), p->s));
             a.out = p->Mf;
+            a.out64 = 0;
         }
     } else {
         BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
@@ -774,7 +778,7 @@ int mode_update(blco_cpals_plan* p, int n)
     else BLCO_TRY(mttkrp_streamed_ring(t, a, p->ring, p->s)); // blocks copied through the plan's ring
     if (p->reduce) {
         // sharded tensor: sum this mode's MTTKRP over the ranks (the one exchange)
-        const bool f64 = !p->mixed || t->layout.wide;
+        const bool f64 = !p->mixed || a.out64;
         if (p->reduce(p->reduce_ctx, f64 ? (void*)p->M : (void*)p->Mf, I * (uint64_t)R,
                       f64 ? BLCO_DTYPE_F64 : BLCO_DTYPE_F32, (void*)p->s) != 0)
             return fail(BLCO_ERR_CUDA, "the MTTKRP sum over the ranks failed");
@@ -794,8 +798,11 @@ int mode_update(blco_cpals_plan* p, int n)
     BLCO_CHECK_LAUNCH("k_solve");
 
     int grid = grid_rows(I, p->sm);
-    if (p->mixed) BLCO_TRY(update_launch<float>(p, p->Mf, p->Uf[n], I, grid));
-    else BLCO_TRY(update_launch<double>(p, p->M, p->U[n], I, grid));
+    int ust;
+    if (p->mixed && p->m64[n]) ust = update_launch<double, float>(p, p->M, p->Uf[n], I, grid);
+    else if (p->mixed) ust = update_launch<float, float>(p, p->Mf, p->Uf[n], I, grid);
+    else ust = update_launch<double, double>(p, p->M, p->U[n], I, grid);
+    BLCO_TRY(ust);
     k_lambda<<<1, 128, 0, p->s>>>(p->partials, grid, R, p->lambda, p->inv);
     BLCO_CHECK_LAUNCH("k_lambda");
     if (p->mixed) {
@@ -815,8 +822,11 @@ int fit_launch(blco_cpals_plan* p)
     const uint64_t I = p->t->layout.dims[lm];
     int grid = grid_rows(I, p->sm);
     size_t smem = (size_t)(DN_THREADS / 32) * R * sizeof(double);
-    if (p->mixed) k_iprod<float><<<grid, DN_THREADS, smem, p->s>>>(p->Uf[lm], p->Mf, I, R, p->partials);
-    else k_iprod<double><<<grid, DN_THREADS, smem, p->s>>>(p->U[lm], p->M, I, R, p->partials);
+    if (p->mixed && p->m64[lm])
+        k_iprod<float, double><<<grid, DN_THREADS, smem, p->s>>>(p->Uf[lm], p->M, I, R, p->partials);
+    else if (p->mixed)
+        k_iprod<float, float><<<grid, DN_THREADS, smem, p->s>>>(p->Uf[lm], p->Mf, I, R, p->partials);
+    else k_iprod<double, double><<<grid, DN_THREADS, smem, p->s>>>(p->U[lm], p->M, I, R, p->partials);
     BLCO_CHECK_LAUNCH("k_iprod");
     GramPtrs gp;
     memset(&gp, 0, sizeof(gp));
@@ -897,7 +907,8 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
             PC(cudaMemsetAsync(p->d_err, 0, sizeof(int), p->s));
         }
         PC(cudaMalloc(&p->Mf, std::max<uint64_t>(maxdim, 1) * R * sizeof(float)));
-        if (t->layout.wide) PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
+        // FP64 result of the wide-key and fibre schedules
+        PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
         for (int n = 0; n < p->N; n++) {
             const uint64_t len = t->layout.dims[n] * (uint64_t)R;
             PC(cudaMalloc(&p->Uf[n], len * sizeof(float)));
@@ -937,6 +948,12 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     // the autotuner's sweep here).
     for (int n = 0; n < p->N && st == BLCO_OK; n++)
         st = resolve_schedule(t, n, R, p->gather_dtype, p->opts.kernel, p->s, &p->sched[n]);
+    if (st != BLCO_OK) { plan_free(p); return st; }
+    // compressed-fibre copies of the modes that use them, built now rather
+    // than inside the first iteration
+    for (int n = 0; n < p->N && st == BLCO_OK; n++)
+        if (p->sched[n].kernel == BLCO_KERNEL_FIBRE && fibre_eligible(t, n) && fibre_lanes(R, p->gather_dtype))
+            st = build_fibre_copy(t, n, p->s);
     if (st != BLCO_OK) { plan_free(p); return st; }
     // Descending mode length, ties in natural order (src/cpd_gpu.cu:137-139).
     for (int n = 0; n < p->N; n++) p->order[n] = n;

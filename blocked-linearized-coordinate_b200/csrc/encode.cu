@@ -746,6 +746,16 @@ __global__ void k_gather3(const uint64_t* __restrict__ idx, uint64_t n, const ui
 
 } // namespace
 
+int radix_sort_pairs_u64(uint64_t* k0, uint64_t* v0, uint64_t* k1, uint64_t* v1, uint64_t n, int end_bit,
+                         cudaStream_t s, bool* in_alt)
+{
+    // the sort moves the 8-byte payloads without reading them as numbers
+    return radix_sort_pairs(k0, reinterpret_cast<double*>(v0), k1, reinterpret_cast<double*>(v1), n, 0, end_bit, s,
+                            in_alt);
+}
+
+int scan_u32_ext(uint32_t* a, uint64_t n, uint32_t* sums, cudaStream_t s) { return scan_u32(a, n, sums, s); }
+
 // Per-mode copies of a wide-key stream sorted by that mode's row (stable:
 // key order inside a row), so that the MTTKRP of mode n sums each row's
 // nonzeros in registers and writes it once per warp task.

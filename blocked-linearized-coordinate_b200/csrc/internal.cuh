@@ -134,6 +134,31 @@ struct TuneCache {
     float ms[BLCO_TUNE_CONFIGS] = {}; // -1: schedule not valid here
 };
 
+// Compressed-fibre copy of the stream for one mode (fibre.cu, kernel id 4):
+// nonzeros grouped by (row of the mode, index of the fibre mode), fibres of
+// two or more nonzeros in the fibred stream, single-nonzero fibres in the
+// loose stream.  Built on first use; resident 64-bit-key tensors only.
+struct FibreCopy {
+    bool built = false;
+    int fmode = -1;                      // fibre mode (shortest other mode)
+    int ninner = 0;                      // other modes besides it
+    int inner[BLCO_MAX_MODES] = {};
+    uint64_t nf = 0, nl = 0;             // fibred / loose nonzeros
+    uint64_t nfib = 0, nrows_f = 0, nrows_l = 0;
+    uint32_t* d_fw[3] = {};              // fibred: inner indices (bit 31 of [0]: fibre start)
+    double* d_fv = nullptr;
+    float* d_fv32 = nullptr;             // mixed forms, made on first use
+    uint32_t* d_fib = nullptr;           // fibre-mode index per fibre (bit 31: row start)
+    uint32_t* d_frows = nullptr;         // output row per row run
+    uint32_t* d_fctab = nullptr;         // (fibre, row run) at every 256th position
+    uint32_t* d_lw[4] = {};              // loose: fibre-mode index (bit 31: row start), inner indices
+    double* d_lv = nullptr;
+    float* d_lv32 = nullptr;
+    uint32_t* d_lrows = nullptr;
+    uint32_t* d_lctab = nullptr;         // row run at every 256th position
+    uint32_t* d_counter = nullptr;       // task counter of a launch (calls on one mode run in stream order)
+};
+
 struct ModeStats {
     uint64_t max_row_nnz = 0;
     uint64_t nonempty_rows = 0;
@@ -176,6 +201,7 @@ struct blco_tensor {
     } wide_copy[BLCO_MAX_MODES];
     // heavy-row tables, one per mode, built at encode time
     blco::HotTable hot[BLCO_MAX_MODES];
+    blco::FibreCopy fib[BLCO_MAX_MODES];
     blco::ModeStats stats[BLCO_MAX_MODES];
     double norm_sq = 0.0; // sum of squared values
     blco::TuneCache tune[BLCO_MAX_MODES][3];
@@ -195,6 +221,12 @@ int build_hot_tables(blco_tensor* t, cudaStream_t s);
 uint64_t stream_chunk_nnz(const blco_opts* opts, int nmodes);
 int sort_stream_by_mode(const blco_tensor* t, int mode, uint64_t* d_coords, double* d_vals, uint64_t* tmp_k,
                         double* tmp_v, cudaStream_t s);
+// Stable LSD radix sort of (key, payload) pairs by key bits [0, end_bit);
+// *in_alt: the result is in (k1, v1).
+int radix_sort_pairs_u64(uint64_t* k0, uint64_t* v0, uint64_t* k1, uint64_t* v1, uint64_t n, int end_bit,
+                         cudaStream_t s, bool* in_alt);
+// In-place exclusive scan of n uint32 values; sums holds n / 4096 + 2 entries.
+int scan_u32_ext(uint32_t* a, uint64_t n, uint32_t* sums, cudaStream_t s);
 int encode_noalloc_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* const* d_cidx,
                         const double* d_vals, uint64_t* d_coords_out, double* d_vals_out, cudaStream_t s);
 
@@ -218,6 +250,14 @@ struct MttkrpArgs {
     int out64;      // wide keys, FP32 factors: out is FP64 (sums of heavy rows stay FP64)
 };
 int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
+// fibre.cu: the compressed-fibre schedule (kernel id 4).
+bool fibre_eligible(const blco_tensor* t, int mode);
+int fibre_lanes(int rank, int dtype); // lanes per factor row, 0 = no kernel for this rank
+int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s);
+// The fibre schedule applies to this call (else kernel id 4 takes the automatic rule).
+bool fibre_usable(const blco_tensor* t, const MttkrpArgs& a);
+void fibre_free(FibreCopy& f);
+int mttkrp_fibre_launch(blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 // Wide-key tensors: FP64 MTTKRP over the BLCO stream in key order.
 int mttkrp_wide_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested, int factor_dtype);

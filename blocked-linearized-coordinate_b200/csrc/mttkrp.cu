@@ -1312,6 +1312,8 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     }
     if (a.nnz == 0) return BLCO_OK;
     if (a.rank < 1 || a.rank > 256) return fail(BLCO_ERR_UNSUPPORTED, "rank must be 1..256");
+    if (a.kernel == BLCO_KERNEL_FIBRE && a.coords == t->d_coords && fibre_usable(t, a))
+        return mttkrp_fibre_launch(const_cast<blco_tensor*>(t), a, s);
     if (a.factor_dtype != BLCO_DTYPE_F64 && a.factor_dtype != BLCO_DTYPE_F32 && a.factor_dtype != BLCO_DTYPE_BF16)
         return fail(BLCO_ERR_INVALID, "unknown factor dtype");
     DeviceInfo di;

@@ -48,6 +48,12 @@ typedef enum blco_status {
  *   1  register/segmented conflict resolution (lvl1)
  *   2  lvl1 + shared-memory privatisation of heavy output rows (lvl2 role)
  *   3  shared-memory partial output matrix, for short modes (lvl3 role)
+ *   4  compressed fibres (no reference counterpart): the mode's copy of the
+ *      stream grouped by (output row, index of the shortest other mode),
+ *      that mode's factor row gathered once per fibre and single-nonzero
+ *      fibres in a second stream; resident tensors with 64-bit keys, 3-5
+ *      modes, every mode below 2^31, rank * element size a multiple of 16
+ *      bytes up to 512 bytes (the copy is built on first use)
  *   10 automatic selection: 3 when the mode's output fits in shared
  *      memory, else 2 when the mode has at least 2^18 nonzeros in heavy
  *      rows (heavy-row chunk 128 / 512 / 2048 below 2^20 / below 2^23 /
@@ -67,6 +73,7 @@ enum {
     BLCO_KERNEL_LVL1 = 1,
     BLCO_KERNEL_LVL2 = 2,
     BLCO_KERNEL_LVL3 = 3,
+    BLCO_KERNEL_FIBRE = 4,
     BLCO_KERNEL_BATCHED = 11,
     BLCO_KERNEL_BATCHED_V2 = 12,
     BLCO_KERNEL_ATOMIC = 13,
