@@ -46,7 +46,7 @@ PRECISION_MIXED_BF16 = 2
 
 KERNEL_TUNED = 20
 KERNEL_LEARNED = 21
-TUNE_CONFIGS = 12
+TUNE_CONFIGS = 14
 MLP_FEATURES = 25
 DTYPE_F64 = 0
 DTYPE_F32 = 1

@@ -758,7 +758,7 @@ int mode_update(blco_cpals_plan* p, int n)
         a.out64 = 1;
         // The fibre schedule sums rows in FP64 and keeps the result in FP64
         // for the update; wide keys do the same and round once below.
-        p->m64[n] = !t->layout.wide && t->resident && a.kernel == BLCO_KERNEL_FIBRE && fibre_usable(t, a);
+        p->m64[n] = !t->layout.wide && t->resident && fibre_route(t, a);
         if (t->layout.wide || p->m64[n]) {
             BLCO_CUDA(cudaMemsetAsync(p->M, 0, I * R * sizeof(double), p->s));
         } else {
@@ -952,7 +952,9 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     // compressed-fibre copies of the modes that use them, built now rather
     // than inside the first iteration
     for (int n = 0; n < p->N && st == BLCO_OK; n++)
-        if (p->sched[n].kernel == BLCO_KERNEL_FIBRE && fibre_eligible(t, n) && fibre_lanes(R, p->gather_dtype))
+        if (t->resident &&
+            mttkrp_select_kernel(t, n, R, p->sched[n].kernel, p->gather_dtype) == BLCO_KERNEL_FIBRE &&
+            (p->sched[n].kernel == BLCO_KERNEL_FIBRE || p->sched[n].kernel == BLCO_KERNEL_AUTO))
             st = build_fibre_copy(t, n, p->s);
     if (st != BLCO_OK) { plan_free(p); return st; }
     // Descending mode length, ties in natural order (src/cpd_gpu.cu:137-139).

@@ -52,26 +52,33 @@ namespace {
 constexpr uint32_t FB_FLAG = 0x80000000u;
 constexpr uint32_t FB_IDX = 0x7fffffffu;
 constexpr int FB_CHUNK = 256;    // chunk-table granularity (positions)
-constexpr int FB_SUB = 512;      // positions a lane group walks per task (a multiple of FB_CHUNK)
-constexpr int FB_FOLD = 4;       // mixed forms: steps summed in FP32 before the FP64 fold
+constexpr int FB_SUB = 256;      // positions a lane group walks per task (a multiple of FB_CHUNK)
 constexpr int FB_THREADS = 256;
+constexpr int FB_U = 4;          // nonzeros per lane-group step (their gathers are issued together)
+// Bytes of factor row per lane: one 128-bit load.  (256-bit loads gather
+// rows at the same rate on B200 but double the per-lane state: measured no
+// faster for FP32 rows and slower for FP64 rows.)
+constexpr int fb_vb(int) { return 16; }
 
 // Element types of one numeric form: value, factor, partial sum, and the
 // columns one lane holds (16 bytes of factor row).
 struct FibF64 {
     typedef double TV;
     typedef double TS;
-    static constexpr int V = 2;
+    static constexpr int V = 2; // columns per 16 bytes
+    static constexpr int VB = 16;
 };
 struct FibF32 {
     typedef float TV;
     typedef float TS;
     static constexpr int V = 4;
+    static constexpr int VB = 16;
 };
 struct FibBF16 {
     typedef float TV;
     typedef float TS;
     static constexpr int V = 8;
+    static constexpr int VB = 16;
 };
 
 struct FibParams {
@@ -99,14 +106,22 @@ struct FibParams {
     uint64_t ntask_f, ntasks, stride;
 };
 
-template <class T>
-__device__ __forceinline__ void gather(const void* F, uint32_t row, int rowvec, int sub, typename T::TS (&o)[T::V])
+// A numeric form with VB bytes of factor row per lane (16: one 128-bit
+// load, 32: one 256-bit load); V columns per lane.
+template <class B, int VBYTES>
+struct Lanes : B {
+    static constexpr int VB = VBYTES;
+    static constexpr int V = B::V * VBYTES / 16;
+};
+
+// One 16-byte piece of a factor row into E partial-type columns.
+template <class T, int E>
+__device__ __forceinline__ void unpack16(const uint4 r, typename T::TS* o)
 {
-    const uint4 r = __ldg(reinterpret_cast<const uint4*>(F) + (size_t)row * rowvec + sub);
-    if constexpr (T::V == 2) {
+    if constexpr (E == 2) {
         o[0] = __hiloint2double((int)r.y, (int)r.x);
         o[1] = __hiloint2double((int)r.w, (int)r.z);
-    } else if constexpr (T::V == 4) {
+    } else if constexpr (E == 4) {
         o[0] = __uint_as_float(r.x);
         o[1] = __uint_as_float(r.y);
         o[2] = __uint_as_float(r.z);
@@ -121,101 +136,167 @@ __device__ __forceinline__ void gather(const void* F, uint32_t row, int rowvec, 
     }
 }
 
-template <typename TV>
-__device__ __forceinline__ void load_vals(const void* v, uint64_t q, TV (&x)[4])
+// This lane's VB bytes of factor row `row` (rows of L * VB bytes).
+template <class T>
+__device__ __forceinline__ void gather(const void* F, uint32_t row, int lanes, int sub, typename T::TS (&o)[T::V])
 {
-    if constexpr (sizeof(TV) == 8) {
-        const double2 a = __ldg(reinterpret_cast<const double2*>(v) + (q >> 1));
-        const double2 b = __ldg(reinterpret_cast<const double2*>(v) + (q >> 1) + 1);
-        x[0] = a.x, x[1] = a.y, x[2] = b.x, x[3] = b.y;
+    constexpr int E = T::V * 16 / T::VB; // columns per 16 bytes
+    const char* ptr = reinterpret_cast<const char*>(F) + ((size_t)row * lanes + sub) * T::VB;
+    if constexpr (T::VB == 16) {
+        unpack16<T, E>(__ldg(reinterpret_cast<const uint4*>(ptr)), o);
     } else {
-        const float4 a = __ldg(reinterpret_cast<const float4*>(v) + (q >> 2));
-        x[0] = a.x, x[1] = a.y, x[2] = a.z, x[3] = a.w;
+        uint4 a, b;
+        asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+            : "l"(ptr));
+        unpack16<T, E>(a, o);
+        unpack16<T, E>(b, o + E);
     }
 }
 
-__device__ __forceinline__ void words4(const uint32_t* w, uint64_t q, uint32_t (&o)[4])
+// Values of positions q..q+U-1 (q a multiple of U).
+template <int U, typename TV>
+__device__ __forceinline__ void load_vals(const void* v, uint64_t q, TV (&x)[U])
 {
-    const uint4 a = __ldg(reinterpret_cast<const uint4*>(w) + (q >> 2));
-    o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w;
+    if constexpr (sizeof(TV) == 8) {
+#pragma unroll
+        for (int k = 0; k < U / 2; k++) {
+            const double2 a = __ldg(reinterpret_cast<const double2*>(v) + (q >> 1) + k);
+            x[2 * k] = a.x, x[2 * k + 1] = a.y;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < U / 4; k++) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(v) + (q >> 2) + k);
+            x[4 * k] = a.x, x[4 * k + 1] = a.y, x[4 * k + 2] = a.z, x[4 * k + 3] = a.w;
+        }
+    }
 }
 
-// Adds one lane's columns of a finished row sum to the output.
-// a[j * FB_THREADS] is column j of the lane's sum (its shared-memory slot).
+// Adds one lane's columns of a finished FP64 row sum to the output.
 template <int V, typename TO>
-__device__ __forceinline__ void flush_row(void* out, uint32_t row, int R, int sub, const double* a)
+__device__ __forceinline__ void flush_row(TO* o, const double (&a)[V])
 {
-    TO* o = reinterpret_cast<TO*>(out) + (size_t)row * R + (size_t)sub * V;
     if constexpr (sizeof(TO) == 4 && V % 4 == 0) {
 #pragma unroll
         for (int j = 0; j < V; j += 4)
             atomicAdd(reinterpret_cast<float4*>(o + j),
-                      make_float4((float)a[j * FB_THREADS], (float)a[(j + 1) * FB_THREADS],
-                                  (float)a[(j + 2) * FB_THREADS], (float)a[(j + 3) * FB_THREADS]));
+                      make_float4((float)a[j], (float)a[j + 1], (float)a[j + 2], (float)a[j + 3]));
     } else {
 #pragma unroll
-        for (int j = 0; j < V; j++) atomicAdd(o + j, (TO)a[j * FB_THREADS]);
+        for (int j = 0; j < V; j++) atomicAdd(o + j, (TO)a[j]);
     }
 }
 
-// Index words of one 4-position step.
+// This lane's columns of row `row` of a factor; b is the factor's address
+// plus this lane's byte offset, ROWB the bytes of a row.
+template <class T, int ROWB>
+__device__ __forceinline__ void gather_at(const char* b, uint32_t row, typename T::TS (&o)[T::V])
+{
+    constexpr int E = T::V * 16 / T::VB; // columns per 16 bytes
+    const char* ptr = b + (size_t)row * ROWB;
+    if constexpr (T::VB == 16) {
+        unpack16<T, E>(__ldg(reinterpret_cast<const uint4*>(ptr)), o);
+    } else {
+        uint4 u, w;
+        asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=r"(u.x), "=r"(u.y), "=r"(u.z), "=r"(u.w), "=r"(w.x), "=r"(w.y), "=r"(w.z), "=r"(w.w)
+            : "l"(ptr));
+        unpack16<T, E>(u, o);
+        unpack16<T, E>(w, o + E);
+    }
+}
+
+// Index words of one FB_U-position step.
 template <int NW>
 struct StepIn {
-    uint32_t w[NW][4];
+    uint32_t w[NW][FB_U];
 };
 
-// One lane's state while it walks the fibred stream: the fibre sum s, the
-// row sum (a in the partial type, a64 in FP64), the current and the next
-// fibre's U_f row (c, cn) and the fibre words / row ids one and two ahead.
+template <int NW>
+__device__ __forceinline__ void load_words(StepIn<NW>& in, const uint32_t* const (&wp)[NW], uint32_t i)
+{
+#pragma unroll
+    for (int m = 0; m < NW; m++)
+#pragma unroll
+        for (int k = 0; k < FB_U / 4; k++) {
+            const uint4 u = __ldg(reinterpret_cast<const uint4*>(wp[m] + (size_t)i * FB_U) + k);
+            in.w[m][4 * k] = u.x, in.w[m][4 * k + 1] = u.y, in.w[m][4 * k + 2] = u.z, in.w[m][4 * k + 3] = u.w;
+        }
+}
+
+// One lane's walk over a range of the fibred stream.  s: the current
+// fibre's sum over this step's nonzeros; c / cn: the current and the next
+// fibre's U_f row; a: the FP64 row sum.  In the mixed forms s is FP32 over at
+// most the FB_U nonzeros of a step and is folded into a after every step
+// (fibres longer than a step contribute one s * c per step).
 template <int NM, int L, class T, typename TO>
 struct FibredWalk {
     typedef typename T::TS TS;
     typedef typename T::TV TV;
-    static constexpr int V = T::V, R = L * V, NI = NM - 2;
+    static constexpr int V = T::V, R = L * V, NI = NM - 2, ROWB = L * T::VB;
     const FibParams& p;
-    const int sub;
-    double* const a64; // this lane's FP64 row sum (shared memory: read only on folds and flushes)
+    const char* fb;
+    const char* ib[NI];
+    TO* out;
+    const uint32_t* wp[NI];
+    const TV* vp;
     uint32_t fi, ri, fwn, fwnn, row, rown;
-    TS s[V], a[V], c[V], cn[V];
+    TS s[V], c[V], cn[V];
+    double a[V];
 
-    __device__ __forceinline__ FibredWalk(const FibParams& p_, int sub_, uint64_t fa, double* slot)
-        : p(p_), sub(sub_), a64(slot)
+    __device__ __forceinline__ FibredWalk(const FibParams& p_, int sub, uint64_t first) : p(p_)
     {
-        fi = p.fctab[2 * (fa / FB_CHUNK)];
-        ri = p.fctab[2 * (fa / FB_CHUNK) + 1];
+        fb = reinterpret_cast<const char*>(p.ff) + sub * T::VB;
+#pragma unroll
+        for (int m = 0; m < NI; m++) {
+            ib[m] = reinterpret_cast<const char*>(p.fi[m]) + sub * T::VB;
+            wp[m] = p.fw[m] + first;
+        }
+        out = reinterpret_cast<TO*>(p.out) + sub * V;
+        vp = reinterpret_cast<const TV*>(p.fv) + first;
+        fi = p.fctab[2 * (first / FB_CHUNK)];
+        ri = p.fctab[2 * (first / FB_CHUNK) + 1];
         fwn = p.fib[fi + 1];
         fwnn = p.fib[fi + 2];
         row = p.frows[ri];
         rown = p.frows[ri + 1];
-        gather<T>(p.ff, p.fib[fi] & FB_IDX, L, sub, c);
-        gather<T>(p.ff, fwn & FB_IDX, L, sub, cn);
+        gather_at<T, ROWB>(fb, p.fib[fi] & FB_IDX, c);
+        gather_at<T, ROWB>(fb, fwn & FB_IDX, cn);
 #pragma unroll
-        for (int v = 0; v < V; v++) s[v] = TS(0), a[v] = TS(0), a64[v * FB_THREADS] = 0.0;
+        for (int v = 0; v < V; v++) s[v] = TS(0), a[v] = 0.0;
     }
 
     __device__ __forceinline__ void flush()
     {
+        flush_row<V, TO>(out + (size_t)row * R, a);
 #pragma unroll
-        for (int v = 0; v < V; v++) {
-            a64[v * FB_THREADS] += (double)a[v];
-            a[v] = TS(0);
-        }
-        flush_row<V, TO>(p.out, row, R, sub, a64);
-#pragma unroll
-        for (int v = 0; v < V; v++) a64[v * FB_THREADS] = 0.0;
+        for (int v = 0; v < V; v++) a[v] = 0.0;
     }
 
-    // Fibre fi ends: its sum times its U_f row joins the row sum; the next
-    // fibre's row is already in cn, the one after it is gathered now.
-    __device__ __forceinline__ void close_fibre()
+    // s * c joins the row sum
+    __device__ __forceinline__ void take()
     {
 #pragma unroll
-        for (int v = 0; v < V; v++) a[v] = fma(s[v], c[v], a[v]), s[v] = TS(0), c[v] = cn[v];
+        for (int v = 0; v < V; v++) {
+            if constexpr (sizeof(TS) == 4) a[v] += (double)(s[v] * c[v]);
+            else a[v] = fma(s[v], c[v], a[v]);
+            s[v] = TS(0);
+        }
+    }
+
+    // Fibre fi ends; the next fibre's row is already in cn, the one after it
+    // is gathered now.
+    __device__ __forceinline__ void close_fibre()
+    {
+        take();
+#pragma unroll
+        for (int v = 0; v < V; v++) c[v] = cn[v];
         fi++;
         const uint32_t fw = fwn;
         fwn = fwnn;
         fwnn = p.fib[fi + 2];
-        gather<T>(p.ff, fwn & FB_IDX, L, sub, cn);
+        gather_at<T, ROWB>(fb, fwn & FB_IDX, cn);
         if (fw & FB_FLAG) { // the new fibre starts a new row run
             flush();
             row = rown;
@@ -224,40 +305,24 @@ struct FibredWalk {
         }
     }
 
-    // Partial sums of the mixed forms: FP32 over at most FB_FOLD steps, then FP64.
-    __device__ __forceinline__ void fold()
-    {
-#pragma unroll
-        for (int v = 0; v < V; v++) {
-            a[v] = fma(s[v], c[v], a[v]);
-            s[v] = TS(0);
-            a64[v * FB_THREADS] += (double)a[v];
-            a[v] = TS(0);
-        }
-    }
-
     typedef StepIn<NI> In;
 
-    __device__ __forceinline__ void load(In& in, uint64_t q0) const
-    {
-#pragma unroll
-        for (int m = 0; m < NI; m++) words4(p.fw[m], q0, in.w[m]);
-    }
+    __device__ __forceinline__ void load(In& in, uint32_t i) const { load_words<NI>(in, wp, i); }
 
-    // Four positions q0..q0+3 whose words are in `in` (values are loaded
-    // here, beside the gathers); with TAIL, positions at or past `end` are
-    // padding and take no part.
+    // Step i (positions FB_U*i.. of the range, whose words are in `in`;
+    // values are loaded here, beside the gathers).  With TAIL, positions at
+    // or past n are padding and take no part.
     template <bool TAIL>
-    __device__ __forceinline__ void process(In& in, uint64_t q0, uint64_t first, uint64_t end)
+    __device__ __forceinline__ void process(In& in, uint32_t i, uint32_t n)
     {
-        if (q0 == first) in.w[0][0] &= FB_IDX; // a range's first nonzero continues the fibre it starts in
-        TV x[4];
-        load_vals<TV>(p.fv, q0, x);
-        TS b[4][V];
+        if (i == 0) in.w[0][0] &= FB_IDX; // a range's first nonzero continues the fibre it starts in
+        TV x[FB_U];
+        load_vals<FB_U, TV>(vp, (uint64_t)FB_U * i, x);
+        TS b[FB_U][V];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (!TAIL || q0 + q < end) {
-                gather<T>(p.fi[0], in.w[0][q] & FB_IDX, L, sub, b[q]);
+        for (int q = 0; q < FB_U; q++) {
+            if (!TAIL || FB_U * i + q < n) {
+                gather_at<T, ROWB>(ib[0], in.w[0][q] & FB_IDX, b[q]);
             } else {
                 x[q] = TV(0);
                 in.w[0][q] = 0;
@@ -267,107 +332,113 @@ struct FibredWalk {
         }
 #pragma unroll
         for (int m = 1; m < NI; m++) {
-            TS e[4][V];
+            TS e[FB_U][V];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (!TAIL || q0 + q < end) gather<T>(p.fi[m], in.w[m][q], L, sub, e[q]);
+            for (int q = 0; q < FB_U; q++) {
+                if (!TAIL || FB_U * i + q < n) gather_at<T, ROWB>(ib[m], in.w[m][q], e[q]);
                 else {
 #pragma unroll
                     for (int v = 0; v < V; v++) e[q][v] = TS(0);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; q++)
+            for (int q = 0; q < FB_U; q++)
 #pragma unroll
                 for (int v = 0; v < V; v++) b[q][v] *= e[q][v];
         }
-        const uint32_t any = (in.w[0][0] | in.w[0][1] | in.w[0][2] | in.w[0][3]) & FB_FLAG;
+        uint32_t any = 0;
+#pragma unroll
+        for (int q = 0; q < FB_U; q++) any |= in.w[0][q];
+        any &= FB_FLAG;
         if (!any) {
 #pragma unroll
-            for (int q = 0; q < 4; q++)
+            for (int q = 0; q < FB_U; q++)
 #pragma unroll
                 for (int v = 0; v < V; v++) s[v] = fma((TS)x[q], b[q][v], s[v]);
         } else {
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < FB_U; q++) {
                 if (in.w[0][q] & FB_FLAG) close_fibre();
 #pragma unroll
                 for (int v = 0; v < V; v++) s[v] = fma((TS)x[q], b[q][v], s[v]);
             }
         }
+        if constexpr (sizeof(TS) == 4) take();
     }
 
     __device__ __forceinline__ void finish()
     {
-#pragma unroll
-        for (int v = 0; v < V; v++) a[v] = fma(s[v], c[v], a[v]), s[v] = TS(0);
+        take();
         flush();
     }
 };
 
-// The loose stream: every nonzero is a fibre of its own, so the row sum
-// takes x * U_f row * inner rows directly.
+// One lane's walk over a range of the loose stream: every nonzero is a
+// fibre of its own, so x * U_f row * inner rows goes straight into the row
+// sum (FP32 over a step in the mixed forms, then FP64).
 template <int NM, int L, class T, typename TO>
 struct LooseWalk {
     typedef typename T::TS TS;
     typedef typename T::TV TV;
-    static constexpr int V = T::V, R = L * V, NI = NM - 2;
+    static constexpr int V = T::V, R = L * V, NI = NM - 2, ROWB = L * T::VB;
     const FibParams& p;
-    const int sub;
-    double* const a64;
+    const char* fb;
+    const char* ib[NI];
+    TO* out;
+    const uint32_t* wp[NI + 1];
+    const TV* vp;
     uint32_t ri, row, rown;
-    TS a[V];
+    TS acc[V];
+    double a[V];
 
-    __device__ __forceinline__ LooseWalk(const FibParams& p_, int sub_, uint64_t la, double* slot)
-        : p(p_), sub(sub_), a64(slot)
+    __device__ __forceinline__ LooseWalk(const FibParams& p_, int sub, uint64_t first) : p(p_)
     {
-        ri = p.lctab[la / FB_CHUNK];
+        fb = reinterpret_cast<const char*>(p.ff) + sub * T::VB;
+#pragma unroll
+        for (int m = 0; m < NI; m++) ib[m] = reinterpret_cast<const char*>(p.fi[m]) + sub * T::VB;
+#pragma unroll
+        for (int m = 0; m <= NI; m++) wp[m] = p.lw[m] + first;
+        out = reinterpret_cast<TO*>(p.out) + sub * V;
+        vp = reinterpret_cast<const TV*>(p.lv) + first;
+        ri = p.lctab[first / FB_CHUNK];
         row = p.lrows[ri];
         rown = p.lrows[ri + 1];
 #pragma unroll
-        for (int v = 0; v < V; v++) a[v] = TS(0), a64[v * FB_THREADS] = 0.0;
-    }
-
-    __device__ __forceinline__ void flush()
-    {
-#pragma unroll
-        for (int v = 0; v < V; v++) {
-            a64[v * FB_THREADS] += (double)a[v];
-            a[v] = TS(0);
-        }
-        flush_row<V, TO>(p.out, row, R, sub, a64);
-#pragma unroll
-        for (int v = 0; v < V; v++) a64[v * FB_THREADS] = 0.0;
+        for (int v = 0; v < V; v++) acc[v] = TS(0), a[v] = 0.0;
     }
 
     __device__ __forceinline__ void fold()
     {
 #pragma unroll
         for (int v = 0; v < V; v++) {
-            a64[v * FB_THREADS] += (double)a[v];
-            a[v] = TS(0);
+            a[v] += (double)acc[v];
+            acc[v] = TS(0);
         }
+    }
+
+    __device__ __forceinline__ void flush()
+    {
+        fold();
+        flush_row<V, TO>(out + (size_t)row * R, a);
+#pragma unroll
+        for (int v = 0; v < V; v++) a[v] = 0.0;
     }
 
     typedef StepIn<NI + 1> In;
 
-    __device__ __forceinline__ void load(In& in, uint64_t q0) const
-    {
-#pragma unroll
-        for (int m = 0; m <= NI; m++) words4(p.lw[m], q0, in.w[m]);
-    }
+    __device__ __forceinline__ void load(In& in, uint32_t i) const { load_words<NI + 1>(in, wp, i); }
 
     template <bool TAIL>
-    __device__ __forceinline__ void process(In& in, uint64_t q0, uint64_t first, uint64_t end)
+    __device__ __forceinline__ void process(In& in, uint32_t i, uint32_t n)
     {
-        if (q0 == first) in.w[0][0] &= FB_IDX;
-        TV x[4];
-        load_vals<TV>(p.lv, q0, x);
-        TS b[4][V];
+        if (i == 0) in.w[0][0] &= FB_IDX;
+        TV x[FB_U];
+        load_vals<FB_U, TV>(vp, (uint64_t)FB_U * i, x);
+        TS b[FB_U][V];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            if (!TAIL || q0 + q < end) {
-                gather<T>(p.ff, in.w[0][q] & FB_IDX, L, sub, b[q]);
+        for (int q = 0; q < FB_U; q++) {
+            if (!TAIL || FB_U * i + q < n) {
+                gather_at<T, ROWB>(fb, in.w[0][q] & FB_IDX, b[q]);
             } else {
                 x[q] = TV(0);
                 in.w[0][q] = 0;
@@ -377,29 +448,32 @@ struct LooseWalk {
         }
 #pragma unroll
         for (int m = 0; m < NI; m++) {
-            TS e[4][V];
+            TS e[FB_U][V];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (!TAIL || q0 + q < end) gather<T>(p.fi[m], in.w[m + 1][q], L, sub, e[q]);
+            for (int q = 0; q < FB_U; q++) {
+                if (!TAIL || FB_U * i + q < n) gather_at<T, ROWB>(ib[m], in.w[m + 1][q], e[q]);
                 else {
 #pragma unroll
                     for (int v = 0; v < V; v++) e[q][v] = TS(0);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; q++)
+            for (int q = 0; q < FB_U; q++)
 #pragma unroll
                 for (int v = 0; v < V; v++) b[q][v] *= e[q][v];
         }
-        const uint32_t any = (in.w[0][0] | in.w[0][1] | in.w[0][2] | in.w[0][3]) & FB_FLAG;
+        uint32_t any = 0;
+#pragma unroll
+        for (int q = 0; q < FB_U; q++) any |= in.w[0][q];
+        any &= FB_FLAG;
         if (!any) {
 #pragma unroll
-            for (int q = 0; q < 4; q++)
+            for (int q = 0; q < FB_U; q++)
 #pragma unroll
-                for (int v = 0; v < V; v++) a[v] = fma((TS)x[q], b[q][v], a[v]);
+                for (int v = 0; v < V; v++) acc[v] = fma((TS)x[q], b[q][v], acc[v]);
         } else {
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < FB_U; q++) {
                 if (in.w[0][q] & FB_FLAG) { // a new row run starts here
                     flush();
                     row = rown;
@@ -407,47 +481,47 @@ struct LooseWalk {
                     rown = p.lrows[ri + 1];
                 }
 #pragma unroll
-                for (int v = 0; v < V; v++) a[v] = fma((TS)x[q], b[q][v], a[v]);
+                for (int v = 0; v < V; v++) acc[v] = fma((TS)x[q], b[q][v], acc[v]);
             }
         }
+        if constexpr (sizeof(TS) == 4) fold();
     }
 
     __device__ __forceinline__ void finish() { flush(); }
 };
 
-// Walks [first, end) four positions per step; the next step's index words
-// are loaded while this step's rows are gathered, so a step waits on one
-// memory latency (the gathers), not two.  The last step may hold padding
+// Walks the n positions of a range FB_U per step; the next step's index
+// words are loaded while this step's rows are gathered, so a step waits on
+// one memory latency (the gathers), not two.  The last step may hold padding
 // (arrays are padded by at least one step).
 template <class W>
-__device__ __forceinline__ void walk(W& wk, uint64_t first, uint64_t end)
+__device__ __forceinline__ void walk(W& wk, uint32_t n)
 {
-    constexpr bool FOLD = sizeof(typename W::TS) == 4;
     typename W::In cur, nxt;
-    wk.load(cur, first);
-    uint64_t q0 = first;
-    int step = 0;
-    for (; q0 + 4 <= end; q0 += 4) {
-        if (q0 + 4 < end) wk.load(nxt, q0 + 4);
-        wk.template process<false>(cur, q0, first, end);
-        if constexpr (FOLD)
-            if (++step % FB_FOLD == 0) wk.fold();
+    wk.load(cur, 0);
+    const uint32_t full = n / FB_U;
+    uint32_t i = 0;
+    for (; i < full; i++) {
+        if (FB_U * (i + 1) < n) wk.load(nxt, i + 1);
+        wk.template process<false>(cur, i, n);
         cur = nxt;
     }
-    if (q0 < end) wk.template process<true>(cur, q0, first, end);
+    if (FB_U * i < n) wk.template process<true>(cur, i, n);
     wk.finish();
 }
 
-// Resident CTAs per SM the register budget is sized for: three (24 warps)
-// where the walker's state fits 80 registers, else two.
+// Resident CTAs per SM the register budget is sized for.  The kernel is
+// bound by the gathers in flight, which the register file limits: for
+// 3-mode tensors with up to 4 columns per lane, four CTAs (32 warps, 64
+// registers) measured fastest (2.85 ms per FP32 mode of the 200M-nonzero
+// workload, against 3.06 ms with three CTAs and 4.1 ms with two, whatever
+// the extra gathers a wider step puts in flight); larger states take two.
 template <int NM, class T>
-constexpr int fib_min_blocks() { return (NM == 3 && T::V <= 4) ? 3 : 2; }
+constexpr int fib_min_blocks() { return (NM == 3 && T::V <= 4) ? 4 : 2; }
 
 template <int NM, int L, class T, typename TO>
 __global__ void __launch_bounds__(FB_THREADS, fib_min_blocks<NM, T>()) k_mttkrp_fib(const FibParams p)
 {
-    __shared__ double slots[T::V][FB_THREADS]; // column-major: lanes hit consecutive banks
-    double* const slot = &slots[0][threadIdx.x];
     constexpr int GPW = 32 / L; // lane groups per warp
     const int lane = threadIdx.x & 31, grp = lane / L, sub = lane % L;
     // A warp takes one task of GPW * FB_SUB positions; group g walks the g-th
@@ -460,16 +534,16 @@ __global__ void __launch_bounds__(FB_THREADS, fib_min_blocks<NM, T>()) k_mttkrp_
         if (k >= p.ntasks) break;
         const uint64_t task = (uint64_t)k * p.stride % p.ntasks;
         if (task < p.ntask_f) {
-            const uint64_t first = (task * GPW + grp) * FB_SUB, end = min(p.nf, first + FB_SUB);
-            if (first < end) {
-                FibredWalk<NM, L, T, TO> wk(p, sub, first, slot);
-                walk(wk, first, end);
+            const uint64_t first = (task * GPW + grp) * FB_SUB;
+            if (first < p.nf) {
+                FibredWalk<NM, L, T, TO> wk(p, sub, first);
+                walk(wk, (uint32_t)min((uint64_t)FB_SUB, p.nf - first));
             }
         } else {
-            const uint64_t first = ((task - p.ntask_f) * GPW + grp) * FB_SUB, end = min(p.nl, first + FB_SUB);
-            if (first < end) {
-                LooseWalk<NM, L, T, TO> wk(p, sub, first, slot);
-                walk(wk, first, end);
+            const uint64_t first = ((task - p.ntask_f) * GPW + grp) * FB_SUB;
+            if (first < p.nl) {
+                LooseWalk<NM, L, T, TO> wk(p, sub, first);
+                walk(wk, (uint32_t)min((uint64_t)FB_SUB, p.nl - first));
             }
         }
         __syncwarp();
@@ -591,7 +665,9 @@ __global__ void k_fib_to_f32(const double* __restrict__ in, float* __restrict__ 
         out[i] = (float)in[i];
 }
 
-inline uint64_t pad4(uint64_t n) { return ((n + 3) & ~3ull) + 4; }
+// Stream arrays hold a multiple of 8 positions plus one 8-position step of
+// zero padding, so a step may load whole vectors past the end.
+inline uint64_t pad4(uint64_t n) { return ((n + 7) & ~7ull) + 8; }
 
 // A stride coprime to n near n * 0.618: consecutive task numbers land far
 // apart in the streams, so lane groups working at the same time rarely share
@@ -610,10 +686,12 @@ int elem_bytes(int dtype) { return dtype == BLCO_DTYPE_F64 ? 8 : dtype == BLCO_D
 
 typedef void (*FibFn)(FibParams);
 
-template <int NM, class T, typename TO>
+template <int NM, class B, typename TO>
 FibFn pick_fib_nm(int L)
 {
+    typedef Lanes<B, B::VB> T;
     switch (L) {
+    case 1: return k_mttkrp_fib<NM, 1, T, TO>;
     case 2: return k_mttkrp_fib<NM, 2, T, TO>;
     case 4: return k_mttkrp_fib<NM, 4, T, TO>;
     case 8: return k_mttkrp_fib<NM, 8, T, TO>;
@@ -648,10 +726,10 @@ bool fibre_eligible(const blco_tensor* t, int mode)
 
 int fibre_lanes(int rank, int dtype)
 {
-    const int bytes = rank * elem_bytes(dtype);
-    if (bytes % 16) return 0;
-    const int L = bytes / 16;
-    return (L == 2 || L == 4 || L == 8 || L == 16 || L == 32) ? L : 0;
+    const int bytes = rank * elem_bytes(dtype), vb = fb_vb(dtype);
+    if (bytes % vb) return 0;
+    const int L = bytes / vb;
+    return (L == 1 || L == 2 || L == 4 || L == 8 || L == 16 || L == 32) ? L : 0;
 }
 
 void fibre_free(FibreCopy& f)
@@ -872,7 +950,7 @@ bool fibre_usable(const blco_tensor* t, const MttkrpArgs& a)
 {
     if (!fibre_eligible(t, a.mode) || !fibre_lanes(a.rank, a.factor_dtype)) return false;
     for (int m = 0; m < t->layout.nmodes; m++)
-        if (m != a.mode && ((uintptr_t)a.factors[m] & 15u)) return false;
+        if (m != a.mode && ((uintptr_t)a.factors[m] & (fb_vb(a.factor_dtype) - 1))) return false;
     return ((uintptr_t)a.out & 15u) == 0;
 }
 
@@ -881,8 +959,9 @@ int mttkrp_fibre_launch(blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     const Layout& L = t->layout;
     const int lanes = fibre_lanes(a.rank, a.factor_dtype);
     if (!fibre_usable(t, a))
-        return fail(BLCO_ERR_UNSUPPORTED, "the fibre schedule needs rank * element size a multiple of 16 bytes "
-                                          "(2 to 32 lanes), 16-byte aligned factors and output, and a resident "
+        return fail(BLCO_ERR_UNSUPPORTED, "the fibre schedule needs rank * element size of 32 bytes times a power "
+                                          "of two up to 1024, 32-byte aligned factors, a 16-byte aligned output and a "
+                                          "resident "
                                           "tensor with 64-bit keys");
     BLCO_TRY(build_fibre_copy(t, a.mode, s));
     FibreCopy& f = t->fib[a.mode];
@@ -911,7 +990,7 @@ int mttkrp_fibre_launch(blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     const uint64_t task = (uint64_t)(32 / lanes) * FB_SUB;
     p.ntask_f = (f.nf + task - 1) / task;
     p.ntasks = p.ntask_f + (f.nl + task - 1) / task;
-    p.stride = task_stride(p.ntasks);
+    p.stride = a.interleave ? 1 : task_stride(p.ntasks); // 1: tasks in stream order
     p.counter = f.d_counter;
     BLCO_CUDA(cudaMemsetAsync(f.d_counter, 0, sizeof(uint32_t), s));
     FibFn fn = nullptr;

@@ -254,8 +254,11 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 bool fibre_eligible(const blco_tensor* t, int mode);
 int fibre_lanes(int rank, int dtype); // lanes per factor row, 0 = no kernel for this rank
 int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s);
-// The fibre schedule applies to this call (else kernel id 4 takes the automatic rule).
+// The fibre kernel can serve this call (resident stream, rank, alignment).
 bool fibre_usable(const blco_tensor* t, const MttkrpArgs& a);
+// The call takes the fibre kernel: kernel id 4, or the automatic rule
+// choosing it, and fibre_usable.
+bool fibre_route(const blco_tensor* t, const MttkrpArgs& a);
 void fibre_free(FibreCopy& f);
 int mttkrp_fibre_launch(blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 // Wide-key tensors: FP64 MTTKRP over the BLCO stream in key order.

@@ -746,6 +746,9 @@ int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested
     if (device_info(t->device, &di) != BLCO_OK) return BLCO_KERNEL_LVL1;
     size_t budget = di.smem_optin - stage_bytes(rank, policy_vec(factor_dtype)) - 2 * sizeof(uint32_t) * 4096 - 1024;
     bool fits_direct = t->layout.dims[mode] * (uint64_t)rank * acc_elem_bytes(factor_dtype) <= budget;
+    const bool fibre_ok = fibre_eligible(t, mode) && fibre_lanes(rank, factor_dtype) > 0;
+    const int tiles = t->hot[mode].nhot > 0 && t->hot[mode].hot_nnz >= AUTO_HOT_MIN_NNZ ? BLCO_KERNEL_LVL2
+                                                                                      : BLCO_KERNEL_LVL1;
     switch (requested) {
     case BLCO_KERNEL_LVL1:
     case BLCO_KERNEL_BATCHED:
@@ -753,11 +756,18 @@ int mttkrp_select_kernel(const blco_tensor* t, int mode, int rank, int requested
     case BLCO_KERNEL_LVL2: return BLCO_KERNEL_LVL2;
     case BLCO_KERNEL_LVL3: return fits_direct ? BLCO_KERNEL_LVL3 : BLCO_KERNEL_LVL2;
     case BLCO_KERNEL_ATOMIC: return BLCO_KERNEL_ATOMIC;
+    case BLCO_KERNEL_FIBRE: return fibre_ok ? BLCO_KERNEL_FIBRE : fits_direct ? BLCO_KERNEL_LVL3 : tiles;
     default:
         if (fits_direct) return BLCO_KERNEL_LVL3;
-        return t->hot[mode].nhot > 0 && t->hot[mode].hot_nnz >= AUTO_HOT_MIN_NNZ ? BLCO_KERNEL_LVL2
-                                                                                : BLCO_KERNEL_LVL1;
+        return fibre_ok ? BLCO_KERNEL_FIBRE : tiles;
     }
+}
+
+bool fibre_route(const blco_tensor* t, const MttkrpArgs& a)
+{
+    if (a.kernel != BLCO_KERNEL_FIBRE && a.kernel != BLCO_KERNEL_AUTO) return false;
+    if (a.coords != t->d_coords || !fibre_usable(t, a)) return false;
+    return mttkrp_select_kernel(t, a.mode, a.rank, a.kernel, a.factor_dtype) == BLCO_KERNEL_FIBRE;
 }
 
 // Heavy-row chunk of the automatic rule: few heavy nonzeros need small
@@ -1312,8 +1322,7 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     }
     if (a.nnz == 0) return BLCO_OK;
     if (a.rank < 1 || a.rank > 256) return fail(BLCO_ERR_UNSUPPORTED, "rank must be 1..256");
-    if (a.kernel == BLCO_KERNEL_FIBRE && a.coords == t->d_coords && fibre_usable(t, a))
-        return mttkrp_fibre_launch(const_cast<blco_tensor*>(t), a, s);
+    if (fibre_route(t, a)) return mttkrp_fibre_launch(const_cast<blco_tensor*>(t), a, s);
     if (a.factor_dtype != BLCO_DTYPE_F64 && a.factor_dtype != BLCO_DTYPE_F32 && a.factor_dtype != BLCO_DTYPE_BF16)
         return fail(BLCO_ERR_INVALID, "unknown factor dtype");
     DeviceInfo di;
@@ -1334,7 +1343,10 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
     p.merge = 1;
     p.interleave = a.interleave;
     const size_t accb = acc_elem_bytes(a.factor_dtype);
-    const int kern = mttkrp_select_kernel(t, a.mode, a.rank, a.kernel, a.factor_dtype);
+    int kern = mttkrp_select_kernel(t, a.mode, a.rank, a.kernel, a.factor_dtype);
+    if (kern == BLCO_KERNEL_FIBRE) // the fibre copy does not serve this call (alignment or a streamed block)
+        kern = t->hot[a.mode].nhot > 0 && t->hot[a.mode].hot_nnz >= AUTO_HOT_MIN_NNZ ? BLCO_KERNEL_LVL2
+                                                                                      : BLCO_KERNEL_LVL1;
     // the automatic rule deals the cold tiles round-robin when heavy rows
     // are split off (a few percent faster in sweeps)
     if (a.kernel == BLCO_KERNEL_AUTO && kern == BLCO_KERNEL_LVL2) p.interleave = 1;

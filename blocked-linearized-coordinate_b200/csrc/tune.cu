@@ -31,6 +31,7 @@ const TuneCfg TUNE_SPACE[BLCO_TUNE_CONFIGS] = {
     {BLCO_KERNEL_LVL2, 512, 1},  {BLCO_KERNEL_LVL2, 2048, 0}, {BLCO_KERNEL_LVL2, 2048, 1},
     {BLCO_KERNEL_LVL2, 128, 0},  {BLCO_KERNEL_LVL2, 128, 1},  {BLCO_KERNEL_LVL3, 0, 0},
     {BLCO_KERNEL_LVL3, 0, 1},    {BLCO_KERNEL_ATOMIC, 0, 0},  {BLCO_KERNEL_ATOMIC, 0, 1},
+    {BLCO_KERNEL_FIBRE, 0, 0},   {BLCO_KERNEL_FIBRE, 0, 1},
 };
 
 namespace {
@@ -41,6 +42,8 @@ bool cfg_valid(const blco_tensor* t, int mode, int rank, int dtype, int k)
 {
     if (TUNE_SPACE[k].kernel == BLCO_KERNEL_LVL3)
         return mttkrp_select_kernel(t, mode, rank, BLCO_KERNEL_LVL3, dtype) == BLCO_KERNEL_LVL3;
+    if (TUNE_SPACE[k].kernel == BLCO_KERNEL_FIBRE)
+        return fibre_eligible(t, mode) && fibre_lanes(rank, dtype) > 0;
     return true;
 }
 

@@ -3,9 +3,11 @@ its parameters (runs on a B200: training uses this library's GPU kernels).
 
   python blocked-linearized-coordinate_b200/selector/train_selector.py [--out PATH]
 
-The network (64 hidden units) is trained on every row of tune_table.npz for
-300 epochs (batch 64, Adam lr 2e-3, seed 0), the settings whose held-out
-regret the selector tests check; the result is deterministic for the seed.
+The network (64 hidden units) is trained on the rows of tune_table.npz that
+are not held out (the table's `heldout` flags) for 300 epochs (batch 64,
+Adam lr 2e-3, seed 0), the settings whose held-out regret the selector tests
+and selector/eval_selector.py measure; the result is deterministic for the
+seed.
 selector_params.npz holds the flat parameter array, the hidden width and
 the final training loss; selector_params.bin holds the same parameters for
 C and C++ callers: int32 hidden width, int32 parameter count, then the
@@ -51,9 +53,10 @@ def main():
     a = ap.parse_args()
     pkg = load()
     T = dict(np.load(a.table))
-    Y, M = targets(T["ms"])
+    train = ~T["heldout"] if "heldout" in T else np.ones(len(T["ms"]), dtype=bool)
+    Y, M = targets(T["ms"][train])
     net = pkg.Mlp(hidden=HIDDEN, seed=1)
-    loss = net.train(T["X"], Y, M, epochs=EPOCHS, batch=BATCH, lr=LR, seed=SEED)
+    loss = net.train(T["X"][train], Y, M, epochs=EPOCHS, batch=BATCH, lr=LR, seed=SEED)
     params = net.params()
     np.savez(a.out, params=params, hidden=np.int32(HIDDEN), loss=np.float32(loss))
     binp = os.path.splitext(a.out)[0] + ".bin"

@@ -52,13 +52,15 @@ typedef enum blco_status {
  *      stream grouped by (output row, index of the shortest other mode),
  *      that mode's factor row gathered once per fibre and single-nonzero
  *      fibres in a second stream; resident tensors with 64-bit keys, 3-5
- *      modes, every mode below 2^31, rank * element size a multiple of 16
- *      bytes up to 512 bytes (the copy is built on first use)
+ *      modes, every mode below 2^31, rank * element size 32 bytes times a
+ *      power of two up to 1024 bytes, 32-byte aligned factors (the copy is
+ *      built on first use; other calls take the automatic rule)
  *   10 automatic selection: 3 when the mode's output fits in shared
- *      memory, else 2 when the mode has at least 2^18 nonzeros in heavy
- *      rows (heavy-row chunk 128 / 512 / 2048 below 2^20 / below 2^23 /
- *      above, cold tiles round-robin), else 1 (the reference's rule,
- *      src/alto_dev.cu:1975,1996-2001, is 3 for at most 100 rows, else 1)
+ *      memory, else 4 where it applies, else 2 when the mode has at least
+ *      2^18 nonzeros in heavy rows (heavy-row chunk 128 / 512 / 2048 below
+ *      2^20 / below 2^23 / above, cold tiles round-robin), else 1 (the
+ *      reference's rule, src/alto_dev.cu:1975,1996-2001, is 3 for at most
+ *      100 rows, else 1)
  *   11, 12 one launch over all blocks (always the case here; mapped to 1)
  *   13 one atomic per (nonzero, column)
  *   20 tuned: the fastest schedule of the autotuner's sweep on this tensor
@@ -82,7 +84,7 @@ enum {
 };
 
 /* Schedules of the autotuner's space, and the selector network's inputs. */
-#define BLCO_TUNE_CONFIGS 12
+#define BLCO_TUNE_CONFIGS 14
 #define BLCO_MLP_FEATURES 25
 
 /* Numeric form. */
@@ -339,10 +341,12 @@ int blco_batch_last_ms(const blco_batch* b, double* ms);
 /* ---- MTTKRP schedule selection (no counterpart in the reference, which
  * has the fixed -k 10 rule, src/alto_dev.cu:1975,1996-2001). */
 
-/* One schedule: kernel id (1, 2, 3 or 13), heavy-row chunk (kernel 2: the
- * positions of one warp task of the heavy-row kernel; 0 otherwise) and tile
- * order (1: tiles dealt round-robin over the grid's warps, 0: a contiguous
- * range of tiles per CTA). */
+/* One schedule: kernel id (1, 2, 3, 4 or 13), heavy-row chunk (kernel 2:
+ * the positions of one warp task of the heavy-row kernel; 0 otherwise) and
+ * tile order (kernels 1-3 and 13: 1 = tiles dealt round-robin over the
+ * grid's warps, 0 = a contiguous range of tiles per CTA; kernel 4: 1 = warp
+ * tasks taken in stream order, 0 = in a strided order that spreads
+ * concurrent tasks over the stream). */
 typedef struct blco_tune_config {
     int kernel;
     int hot_chunk;

@@ -16,10 +16,11 @@ tile order):
   2 (2, 512, c)  3 (2, 512, rr)  4 (2, 2048, c)  5 (2, 2048, rr)
   6 (2, 128, c)  7 (2, 128, rr)  8 (3, -, c)  9 (3, -, rr)
   10 (13, -, c)  11 (13, -, rr)
+  12 (4, -, strided tasks)  13 (4, -, tasks in stream order)
 """
 import numpy as np
 
-F, K = 25, 12
+F, K = 25, 14
 
 
 def unpack(p, H, F=F, K=K):
@@ -87,12 +88,15 @@ def reference_rule(dim_t, valid):
 
 def auto_rule(features, valid):
     """This library's kernel 10 (csrc/mttkrp.cu mttkrp_select_kernel and
-    auto_hot_chunk): 3 when the output fits in shared memory; else 2 with
+    auto_hot_chunk): 3 when the output fits in shared memory; else 4 (the
+    compressed-fibre kernel, strided tasks) where it applies; else 2 with
     round-robin cold tiles when the mode has at least 2^18 heavy nonzeros,
     with chunk 128 below 2^20 heavy nonzeros, 512 below 2^23, else 2048;
     else 1.  The heavy count is recovered from the features (share x nnz)."""
     if features[23] > 0.5 and valid[8]:
         return 8
+    if len(valid) > 12 and valid[12]:
+        return 12
     hot = float(features[13]) * 2.0 ** (float(features[0]) * 32.0)
     if features[14] <= 0 or hot < 2 ** 18:
         return 0

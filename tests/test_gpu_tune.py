@@ -30,8 +30,8 @@ def _tensor(blco, dims, nnz, zipf, seed):
 
 def test_tune_space_and_sweep(blco):
     space = blco.tune_space()
-    assert len(space) == blco.TUNE_CONFIGS == 12
-    assert {c["kernel"] for c in space} == {1, 2, 3, 13}
+    assert len(space) == blco.TUNE_CONFIGS == 14
+    assert {c["kernel"] for c in space} == {1, 2, 3, 4, 13}
     dims = [40_000, 3_000, 60]
     _, _, t = _tensor(blco, dims, 300_000, 1.0, 0)
     for mode in range(3):
@@ -39,7 +39,7 @@ def test_tune_space_and_sweep(blco):
         valid = ms > 0
         # the shared-memory schedules apply to the 60-row mode only
         assert valid[8] == valid[9] == (mode == 2)
-        assert valid.sum() == (12 if mode == 2 else 10)
+        assert valid.sum() == (14 if mode == 2 else 12)
         assert best == int(np.argmin(np.where(valid, ms, np.inf)))
         ms2, best2 = blco.autotune(t, mode, 32, blco.DTYPE_F64)  # cached
         assert np.array_equal(ms, ms2) and best2 == best
@@ -57,7 +57,7 @@ def _forcing_net(blco, k):
     return net
 
 
-@pytest.mark.parametrize("k", list(range(12)))
+@pytest.mark.parametrize("k", list(range(14)))
 def test_every_schedule_matches_oracle(blco, k):
     """Schedule k forced through the learned kernel id (21) with a network
     that proposes k with a wide margin; FP64 results within 1e-12 of the
@@ -148,13 +148,13 @@ def _table():
 
 
 def test_learned_selector_beats_fixed_rules(blco):
-    """Train on the sweep table's first tensors (GPU, this library's
-    kernels), choose schedules for the held-out tensors' modes, and compare
+    """Train on the sweep table's tensors that are not held out (GPU, this
+    library's kernels), choose schedules for the held-out tensors' modes, and compare
     the mean time / best time with the reference's -k 10 rule, this
     library's kernel-10 rule and the same network untrained."""
     T = _table()
     X, ms = T["X"], T["ms"]
-    held = T["tensor"] >= int(T["tensor"].max() * 5 // 6)
+    held = T["heldout"]
     Y, M = mo.targets(ms)
     valid = ms > 0
 

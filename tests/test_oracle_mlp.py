@@ -32,10 +32,11 @@ def test_gradient_matches_finite_differences():
 
 
 def test_targets_and_rules():
-    ms = np.array([[2.0, 1.0, -1, 4.0, 4, 4, 4, 4, -1, -1, 8, 8],
-                   [1.0, 1.0, 1, 1, 1, 1, 1, 1, 0.5, 0.25, 1, 1]], dtype=np.float32)
+    # schedules 12 and 13 (the compressed-fibre kernel) do not apply in row 0
+    ms = np.array([[2.0, 1.0, -1, 4.0, 4, 4, 4, 4, -1, -1, 8, 8, -1, -1],
+                   [1.0, 1.0, 1, 1, 1, 1, 1, 1, 0.5, 0.25, 1, 1, 0.75, 0.8]], dtype=np.float32)
     Y, M = mo.targets(ms)
-    assert M[0, 2] == 0 and M[0, 8] == 0 and M[1].all()
+    assert M[0, 2] == 0 and M[0, 8] == 0 and M[0, 12] == 0 and M[1].all()
     assert Y[0, 1] == 0 and abs(Y[0, 0] - 1.0) < 1e-7 and abs(Y[1, 0] - 2.0) < 1e-7
     valid0, valid1 = ms[0] > 0, ms[1] > 0
     assert mo.reference_rule(50, valid0) == 0          # kernel 3 not valid there
@@ -43,21 +44,22 @@ def test_targets_and_rules():
     assert mo.reference_rule(1000, valid1) == 0
     f = np.zeros(mo.F)
     f[23] = 1.0
-    assert mo.auto_rule(f, valid1) == 8
+    assert mo.auto_rule(f, valid1) == 8                # output in shared memory first
     f[23] = 0.0
+    assert mo.auto_rule(f, valid1) == 12               # then the fibre kernel where it applies
     f[14] = 0.5
     f[0] = np.log2(4e6) / 32     # 4M nonzeros, half of them heavy
     f[13] = 0.5
-    assert mo.auto_rule(f, valid1) == 3
+    assert mo.auto_rule(f, valid0) == 3
     f[13] = 0.05                 # 200k heavy: below the threshold
-    assert mo.auto_rule(f, valid1) == 0
-    pred = np.array([[0.0, 0.01, 0.5, 0.5, 1, 1, 1, 1, 1, 1, 1, 1]])
-    c, close = mo.choose(pred, np.ones((1, 12), bool))
+    assert mo.auto_rule(f, valid0) == 0
+    pred = np.array([[0.0, 0.01, 0.5, 0.5, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1]])
+    c, close = mo.choose(pred, np.ones((1, 14), bool))
     assert c[0] == 0 and not close[0]
     # the twin (same group) does not count against the margin
-    c, close = mo.choose(pred, np.ones((1, 12), bool), 0.3, ms=np.arange(12.0)[None, ::-1] + 1)
+    c, close = mo.choose(pred, np.ones((1, 14), bool), 0.3, ms=np.arange(14.0)[None, ::-1] + 1)
     assert c[0] == 0 and not close[0]
-    c, close = mo.choose(pred, np.ones((1, 12), bool), 0.6, ms=np.arange(12.0)[None, ::-1] + 1)
-    assert close[0] and c[0] == 11
+    c, close = mo.choose(pred, np.ones((1, 14), bool), 0.6, ms=np.arange(14.0)[None, ::-1] + 1)
+    assert close[0] and c[0] == 13
     assert abs(mo.regret(ms, np.array([1, 9])) - 1.0) < 1e-12
     assert abs(mo.regret(ms, np.array([0, 0])) - (2.0 + 4.0) / 2) < 1e-12
