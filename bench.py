@@ -10,9 +10,12 @@ solves, factor updates, normalisation, Grams and the fit.  Prints one JSON
 line (rank 0).  Inputs (3.2 GB stream + 1 GB of factors) are larger than
 the 126 MB L2, so no flush is needed between steps.
 
---impl reference times the reference's own CPU MTTKRP (mttkrp_alto_par from
-include/alto.hpp, compiled from the reference sources into oracle/_ref) on a
-bounded sample of the same workload with all host threads.
+--impl reference times the reference's own CPU CP-ALS (cpd_alto,
+include/cpd.hpp, compiled from the reference sources into oracle/_ref with
+scipy's OpenBLAS) on a bounded sample of the same workload with all host
+threads, and whole on the CPU-runnable workload (`c1`); it also runs the
+reference's own GPU code on the full workload (`reference_gpu`) with a
+full-size fit comparison against this engine's plain form.
 
 Two more legs ride on the same line (skip with --no-batched / --no-wide):
 `batched`, batched CP-ALS of 512 small tensors, and `wide`, FP64 CP-ALS of a
@@ -37,6 +40,20 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 WORKLOAD = dict(workload="cpals_zipf1.1_2Mx2Mx25k_nnz200M_r32", dims=[2_000_000, 2_000_000, 25_000],
                 nnz=200_000_000, rank=32, zipf=1.1, values="lognormal(0,1) fp32 summed over duplicates, fp64")
 METRIC = "CP-ALS ms/iter"
+
+
+def gather_ceiling():
+    """Random 128-byte factor-row gathers per second on this GPU's load path
+    (blocked-linearized-coordinate_b200/bin/gather_ceiling: Zipf(1.1) over 2M
+    rows, the workload's per-mode distribution), measured live."""
+    exe = os.path.join(ROOT, "blocked-linearized-coordinate_b200", "bin", "gather_ceiling")
+    if not os.path.exists(exe):
+        return None
+    try:
+        r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+        return json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else None
+    except Exception:
+        return None
 
 
 def load_pkg():
@@ -141,13 +158,21 @@ def max_over_ranks(x, dist, device="cuda"):
     return tt.item()
 
 
+def _ref_fits(log):
+    import re
+    return [float(x) for x in re.findall(r"--> Iter +\d+: f = ([0-9.eE+-]+)", log)]
+
+
 def reference_gpu_leg(args):
     """The reference's own GPU CP-ALS (cpals_blco_dev, src/cpd_gpu.cu:21-242,
     rebuilt unchanged for sm_100a into oracle/_ref/libblco_refgpu.so) on the
-    full workload with the same initial factors as this engine's arm:
-    median of its own per-iteration times (CUDA events around each
-    iteration, src/cpd_gpu.cu:148-193) after the warm-up iterations.  The
-    reference encodes on the host first (minutes at 200M nonzeros)."""
+    full workload with the same initial factors as this engine's arm, -k 10,
+    warm-up + timed iterations: median of its own per-iteration times (CUDA
+    events around each iteration, src/cpd_gpu.cu:148-193) after the warm-up
+    iterations.  The reference encodes on the host first (about a minute at
+    200M nonzeros).  Then, outside that timing, this engine's plain FP64 form
+    runs the same iterations from the same factors: the per-iteration fit
+    difference is the full-size parity record."""
     import re
     import tempfile
     import torch
@@ -166,21 +191,42 @@ def reference_gpu_leg(args):
     fs = [np.ascontiguousarray(torch.rand(d, rk, dtype=torch.float64, device="cuda", generator=g).cpu().numpy())
           for d in dims]
     torch.cuda.empty_cache()
+    iters = args.warmup + args.steps
     out = {}
-    for kernel in (10, 2):
-        lam = np.ones(rk)
-        f = [x.copy() for x in fs]
-        with tempfile.NamedTemporaryFile("r", suffix=".log") as lf:
-            t0 = time.perf_counter()
-            fit = po.refgpu_cpals(dims, cidx, vals, f, lam, args.warmup + args.steps, -1.0, kernel=kernel,
-                                  log_path=lf.name, timeout=2400)
-            wall = time.perf_counter() - t0
-            log = open(lf.name).read()
-        its = [float(x) * 1e3 for x in re.findall(r"--> Iter +\d+: .*time = ([0-9.]+)", log)]
-        timed = its[args.warmup:]
-        out[f"k{kernel}"] = dict(ms_per_step=statistics.median(timed) if timed else None, iterations=len(its),
-                                 fit_last=fit, wall_s_including_host_encode=wall)
-    if not args.no_wide:
+    lam = np.ones(rk)
+    f = [x.copy() for x in fs]
+    with tempfile.NamedTemporaryFile("r", suffix=".log") as lf:
+        t0 = time.perf_counter()
+        fit = po.refgpu_cpals(dims, cidx, vals, f, lam, iters, -1.0, kernel=10, log_path=lf.name, timeout=2400)
+        wall = time.perf_counter() - t0
+        log = open(lf.name).read()
+    its = [float(x) * 1e3 for x in re.findall(r"--> Iter +\d+: .*time = ([0-9.]+)", log)]
+    timed = its[args.warmup:]
+    ref_fits = _ref_fits(log)
+    out["k10"] = dict(ms_per_step=statistics.median(timed) if timed else None, iterations=len(its),
+                      fit_last=fit, wall_s_including_host_encode=wall)
+    # parity at full size: this engine's plain FP64 form, same tensor, factors and iterations
+    pkg = load_pkg()
+    t = pkg.Tensor.encode(dims, cidx, vals)
+    dfs = [torch.from_numpy(x.copy()).cuda() for x in fs]
+    dl = torch.ones(rk, dtype=torch.float64, device="cuda")
+    plan = pkg.CpalsPlan(t, dfs, dl, pkg.make_opts(precision=pkg.PRECISION_FP64))
+    ours = plan.iterate(iters, tol=-1.0)
+    plan.destroy()
+    ours_f = [x.cpu().numpy() for x in dfs]
+    t.free()
+    n = min(len(ours), len(ref_fits))
+    d = [abs(a - b) for a, b in zip(ours[:n], ref_fits[:n])]
+    fac = max(float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(ours_f, f))
+    out["parity_full_size"] = dict(
+        iterations=n, fit_ref_last=ref_fits[n - 1] if n else None, fit_ours_last=ours[n - 1] if n else None,
+        max_abs_fit_diff=max(d) if d else None,
+        max_rel_fit_diff=max(x / abs(b) for x, b in zip(d, ref_fits[:n])) if d else None,
+        factor_rel_diff_last=fac,
+        note=("this engine's plain FP64 CP-ALS (kernel 10) against the reference's cpals_blco_dev (-k 10) on the "
+              "full workload, same initial factors; fits of every iteration (the reference prints 6 decimals, "
+              "so the fit difference is bounded by its print rounding), factors after the last"))
+    if args.ref_gpu_wide:
         # the wide-key workload through the reference's 128-bit build (same tensor and factors as the wide leg)
         X = synth.wide_tensor_device(WIDE["nnz"], WIDE["dims"], WIDE["zipf"], seed=WIDE["seed"])
         wc = np.ascontiguousarray(np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]]))
@@ -193,7 +239,7 @@ def reference_gpu_leg(args):
         lam = np.ones(WIDE["rank"])
         with tempfile.NamedTemporaryFile("r", suffix=".log") as lf:
             t0 = time.perf_counter()
-            fit = po.refgpu_cpals(WIDE["dims"], wc, wv, wf, lam, args.warmup + args.steps, -1.0, kernel=10,
+            fit = po.refgpu_cpals(WIDE["dims"], wc, wv, wf, lam, iters, -1.0, kernel=10,
                                   log_path=lf.name, wide=True, timeout=2400)
             wall = time.perf_counter() - t0
             log = open(lf.name).read()
@@ -202,67 +248,90 @@ def reference_gpu_leg(args):
         out["wide_k10"] = dict(workload=WIDE["workload"], ms_per_step=statistics.median(timed) if timed else None,
                                iterations=len(its), fit_last=fit, wall_s_including_host_encode=wall)
     out["note"] = ("reference cpals_blco_dev (oracle/_ref/libblco_refgpu.so, unchanged source for sm_100a), FP64, "
-                   "-k 10 (lvl1 for these mode lengths) and -k 2 (lvl2), one block, the full workload and this engine's initial factors; median of the "
-                   f"reference's own per-iteration times after {args.warmup} warm-up iterations; wide_k10: the "
-                   "wide-key workload through the reference's 128-bit encoding (one block per upper key word)")
+                   "-k 10 (lvl1 for these mode lengths), one block, the full workload and this engine's initial "
+                   f"factors; median of the reference's own per-iteration times after {args.warmup} warm-up "
+                   "iterations")
+    return out
+
+
+C1 = dict(workload="cpals_uniform_1000x800x600_nnz100k_r16_20iters",
+          desc=("1000 x 800 x 600, 100k distinct uniform coordinates, U(0,1) FP64 values, rank 16, 20 iterations "
+                "with tolerance 0, factors from the reference's KruskalModelRandomInit (seed 1, one thread)"),
+          dims=[1000, 800, 600], nnz=100_000, rank=16, iters=20)
+
+
+def c1_inputs():
+    import pyoracle as po
+    from blco_b200 import synth
+    X = synth.uniform_tensor_host(C1["nnz"], C1["dims"], seed=0)
+    fs, lam = po.kruskal_random_init(C1["dims"], C1["rank"], 1, 1)
+    return X, fs, lam
+
+
+def reference_cpu_c1():
+    """The reference's CPU CP-ALS (cpd_alto) on the CPU-runnable workload,
+    measured whole (no sample): its own "Per iteration" time with all host
+    threads and with one."""
+    import pyoracle as po
+    X, fs, lam = c1_inputs()
+    out = dict(workload=C1["workload"], desc=C1["desc"])
+    for nt in sorted({os.cpu_count() or 1, 1}, reverse=True):
+        f = [x.copy() for x in fs]
+        r = po.ref_cpd_alto(C1["dims"], X["cidx"], X["vals"], f, lam.copy(), C1["iters"], 0.0, nthreads=nt)
+        out[f"threads_{nt}"] = r
+    best = min((v for k, v in out.items() if k.startswith("threads_")), key=lambda r: r["ms_per_iter"])
+    out.update(value=best["ms_per_iter"], unit="ms", cores=best["threads"], fit=best["fit"])
     return out
 
 
 def run_reference(args, world, rank):
-    """The reference's CPU MTTKRP on a bounded sample of the workload."""
+    """The reference's CPU CP-ALS (cpd_alto, include/cpd.hpp:44-187, built
+    from the reference sources into oracle/_ref with scipy's OpenBLAS) on a
+    bounded sample of the workload, all host threads, and on the CPU-runnable
+    workload whole; then the reference's GPU code on the full workload."""
     if rank != 0:
         return
-    import ctypes
     import torch
     import pyoracle as po
-    R = po.ref_lib()
-    if R is None:
+    if po.ref_lib() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libblco_ref.so not built"}))
         return
-    pkg = load_pkg()
+    load_pkg()
     from blco_b200 import synth
     sample = args.ref_sample
-    dims = WORKLOAD["dims"]
+    dims, rk = WORKLOAD["dims"], WORKLOAD["rank"]
     if torch.cuda.is_available():
         X = synth.zipf_tensor_device(sample, dims, WORKLOAD["zipf"], seed=7)
         cidx = np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]])
         vals = X["vals"].cpu().numpy()
+        del X
     else:
         X = synth.uniform_tensor_host(sample, dims, seed=7)
         cidx, vals = X["cidx"], X["vals"]
-    rk = WORKLOAD["rank"]
     nthreads = os.cpu_count() or 1
-    d64 = np.ascontiguousarray(dims, dtype=np.uint64)
-    u64p = ctypes.POINTER(ctypes.c_uint64)
-    f64p = ctypes.POINTER(ctypes.c_double)
-    h = R.ref_alto_create(3, d64.ctypes.data_as(u64p), sample, np.ascontiguousarray(cidx).ctypes.data_as(u64p),
-                          np.ascontiguousarray(vals).ctypes.data_as(f64p), nthreads)
     rng = np.random.default_rng(0)
-    fs = [rng.random((d, rk)) for d in dims]
-    ptrs = (ctypes.c_void_p * 3)(*[f.ctypes.data for f in fs])
-    step_ms = []
-    for s in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        for m in range(3):
-            R.ref_alto_mttkrp(h, m, rk, ptrs)
-        dt = (time.perf_counter() - t0) * 1e3
-        if s >= args.warmup:
-            step_ms.append(dt)
-    R.ref_alto_destroy(h, rk)
-    per_nnz = statistics.median(step_ms) / sample
-    value = per_nnz * WORKLOAD["nnz"]
-    desc = (f"reference mttkrp_alto_par (oracle/_ref) over all 3 modes, {sample} nonzeros of the same "
-            f"distribution and dims, {nthreads} threads, median of {args.steps} sweeps, scaled linearly "
-            f"to {WORKLOAD['nnz']} nonzeros; MTTKRP part of the iteration only")
-    print(json.dumps({
+    fs = [np.ascontiguousarray(rng.random((d, rk))) for d in dims]
+    r = po.ref_cpd_alto(dims, cidx, vals, fs, np.ones(rk), args.warmup + args.steps, 0.0, nthreads=nthreads)
+    scale = WORKLOAD["nnz"] / sample
+    value = r["ms_per_iter"] + r["mttkrp_ms_per_iter"] * (scale - 1.0)
+    desc = (f"reference cpd_alto (oracle/_ref, scipy OpenBLAS) on {sample} nonzeros of the same distribution with "
+            f"the full mode lengths, {nthreads} threads, {r['iters']} iterations, its own per-iteration times "
+            f"({r['ms_per_iter']:.1f} ms, of which MTTKRP {r['mttkrp_ms_per_iter']:.1f} ms); estimate for "
+            f"{WORKLOAD['nnz']} nonzeros = iteration + MTTKRP x ({scale:.0f} - 1): the dense steps already run at "
+            "full size, the MTTKRP is scaled by the nonzeros")
+    line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "higher_is_better": False,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(workload=WORKLOAD["workload"], parallelism="cpu", l2="inputs larger than L2"),
-        "cpu_baseline": dict(value=value, unit="ms", cores=nthreads, kind="reference", sample=desc),
+        "cpu_baseline": dict(value=value, unit="ms", cores=nthreads, kind="reference", sample=desc,
+                             sample_ms_per_iter=r["ms_per_iter"], sample_mttkrp_ms_per_iter=r["mttkrp_ms_per_iter"],
+                             sample_nnz=sample),
         "e2e": dict(value=value, unit="ms", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
-        "reference_gpu": reference_gpu_leg(args) if args.ref_gpu else None,
-    }))
+        "c1": reference_cpu_c1(),
+        "reference_gpu": None if args.no_ref_gpu else reference_gpu_leg(args),
+    }
+    print(json.dumps(line))
 
 
 def cpu_baseline_quick(args, dims, rk):
@@ -342,6 +411,47 @@ def time_form(pkg, torch, t, dims, rk, fs0, form, args, stream, dist):
     elapsed = max_over_ranks(elapsed, dist)
     return dict(ms_per_step=elapsed / args.steps, mttkrp_ms=list((ms1 - ms0) / max(1, calls1 - calls0)),
                 fits=fits, launches=int(launches), clocks=ck)
+
+
+def c1_leg(pkg, torch, args):
+    """This engine on the CPU-runnable workload (the reference's KruskalModel
+    initial factors, 20 iterations, tolerance 0): device ms per iteration of
+    the plain FP64 plan and the mixed plan, and blco_cpals end to end from
+    host buffers (encode + 20 iterations)."""
+    import pyoracle as po
+    X, fs, lam = c1_inputs()
+    out = dict(workload=C1["workload"], desc=C1["desc"])
+    t = pkg.Tensor.encode(C1["dims"], X["cidx"], X["vals"])
+    for name, prec in (("fp64", pkg.PRECISION_FP64), ("mixed_f32", pkg.PRECISION_MIXED)):
+        dfs = [torch.from_numpy(x.copy()).cuda() for x in fs]
+        dl = torch.from_numpy(lam.copy()).cuda()
+        plan = pkg.CpalsPlan(t, dfs, dl, pkg.make_opts(kernel=args.kernel, precision=prec))
+        plan.iterate(2, tol=-1.0)
+        plan.destroy()
+        dfs = [torch.from_numpy(x.copy()).cuda() for x in fs]
+        dl = torch.from_numpy(lam.copy()).cuda()
+        plan = pkg.CpalsPlan(t, dfs, dl, pkg.make_opts(kernel=args.kernel, precision=prec))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fits = plan.iterate(C1["iters"], tol=-1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        plan.destroy()
+        out[name] = dict(ms_per_iter=e0.elapsed_time(e1) / C1["iters"], fit=fits[-1])
+    t.free()
+    f = [x.copy() for x in fs]
+    t0 = time.perf_counter()
+    t2 = pkg.Tensor.encode(C1["dims"], X["cidx"], X["vals"])
+    fit, _ = pkg.cpals(t2, f, lam.copy(), C1["iters"], -1.0, pkg.make_opts(kernel=args.kernel))
+    out["e2e_fp64_ms_per_iter"] = (time.perf_counter() - t0) * 1e3 / C1["iters"]
+    t2.free()
+    out["fit_reference_oracle"] = float(po.cpals(C1["dims"], po.blco_encode(C1["dims"], X["cidx"], X["vals"]),
+                                                 [x.copy() for x in fs], lam.copy(), C1["iters"], -1.0)[-1])
+    out["note"] = ("device time (CUDA events) of plans whose factors start on the device; e2e: blco_encode from host "
+                   "COO + blco_cpals with host factors, wall time / iterations; fit_reference_oracle: the CPU "
+                   "restatement of the reference's GPU CP-ALS on the same inputs")
+    return out
 
 
 BATCH = dict(
@@ -580,6 +690,28 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_quick(args, dims, rk)
+    # rows each mode's MTTKRP gathers with the compressed-fibre kernel, and the rate
+    gather = None
+    used = [sc["kernel"] for sc in schedules] if schedules else None
+    if rank == 0 and (used is None or 4 in used):
+        try:
+            st = [t.fibre_stats(m) for m in range(3)]
+            rows = [x["rows_gathered"] for x in st]
+            rates = [r / (ms * 1e-3) / 1e9 for r, ms in zip(rows, C["mttkrp_ms"])]
+            ceil = None if args.no_gather_ceiling else gather_ceiling()
+            top = ceil["grows_per_s_zipf"] if ceil else None
+            gather = dict(rows_per_mode=rows, fibre_modes=[x["fibre_mode"] for x in st],
+                          fibred_share=[x["fibred_nnz"] / nnz for x in st], rows_per_nnz=[r / nnz for r in rows],
+                          grows_per_s=rates, ceiling=ceil,
+                          frac_of_ceiling=[r / top for r in rates] if top else None,
+                          note=("rows gathered by kernel 4 per mode (the inner modes' rows of every fibred "
+                                "nonzero, one fibre-mode row per fibre, every other mode's row of a single-nonzero "
+                                "fibre) over the mode's MTTKRP time, against the load-path ceiling measured by "
+                                "bin/gather_ceiling in this run; rows of rank x element bytes (128 B for the FP32 "
+                                "form at rank 32)"))
+        except Exception as e:  # modes the fibre kernel does not serve
+            gather = dict(unavailable=str(e))
+    c1 = c1_leg(pkg, torch, args) if rank == 0 and not args.no_c1 else None
     t.free()
     del fs0
     torch.cuda.empty_cache()
@@ -610,10 +742,10 @@ def run_ours(args, world, rank, local):
             "encode_ms": encode_ms,
             "roofline": dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                              traffic=traffic, peak_kind=peak_kind + " (hbm_gbs burst copy)",
-                             kernel=(f"MTTKRP of one mode, {chosen}: k_mttkrp_hot + k_mttkrp_vec (+ k_merge_hot); "
-                                     "mean over the 3 modes; traffic = DRAM read + write of those kernels per "
-                                     "mode (ncu, profiles/)"),
-                             alg_bytes_per_launch=[int(x) for x in alg]),
+                             kernel=(f"MTTKRP of one mode, {chosen}, the schedule of each mode in "
+                                     "config.schedules (kernel 4: k_mttkrp_fib); mean over the 3 modes; traffic = "
+                                     "DRAM read + write per mode (ncu, profiles/)"),
+                             alg_bytes_per_launch=[int(x) for x in alg], gather=gather),
             "cpu_baseline": cpu,
             "e2e": dict(value=e2e_ms, unit="ms", h2d_bytes_per_step=int(h2d / e_iters),
                         d2h_bytes_per_step=int(d2h / e_iters),
@@ -623,6 +755,7 @@ def run_ours(args, world, rank, local):
             "clocks": C["clocks"],
             "batched": batched,
             "wide": wide,
+            "c1": c1,
         }
         print(json.dumps(line))
     if dist:
@@ -644,8 +777,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched many-small-tensors leg")
     ap.add_argument("--no-wide", action="store_true", help="skip the wide-key (128-bit BLCO) leg")
-    ap.add_argument("--ref-gpu", action="store_true",
-                    help="--impl reference: also time the reference's own GPU CP-ALS on the full workload")
+    ap.add_argument("--no-c1", action="store_true", help="skip the CPU-runnable workload leg")
+    ap.add_argument("--no-gather-ceiling", action="store_true", help="skip the live gather-ceiling probe")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="--impl reference: skip the reference's own GPU CP-ALS on the full workload")
+    ap.add_argument("--ref-gpu-wide", action="store_true",
+                    help="--impl reference: also time the reference's GPU CP-ALS on the wide-key workload")
     ap.add_argument("--forms", default="fp64,mixed_f32,mixed_bf16")
     args = ap.parse_args()
     world, rank, local = dist_setup()

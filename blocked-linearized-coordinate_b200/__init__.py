@@ -36,6 +36,9 @@ KERNEL_LVL1 = 1
 KERNEL_LVL2 = 2
 KERNEL_LVL3 = 3
 KERNEL_FIBRE = 4
+SOLVE_AUTO = 0
+SOLVE_PINV = 1
+GUARD_COND = 3e4
 KERNEL_BATCHED = 11
 KERNEL_BATCHED_V2 = 12
 KERNEL_ATOMIC = 13
@@ -58,12 +61,13 @@ EXPORTS = (
     "blco_encode", "blco_encode_device", "blco_encode_device_noalloc", "blco_tensor_free", "blco_tensor_get_info",
     "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_ex", "blco_mttkrp_host",
     "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
-    "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_destroy", "blco_batch_create", "blco_batch_iterate",
+    "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_condition", "blco_cpals_plan_destroy", "blco_batch_create",
+    "blco_batch_iterate",
     "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
     "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
     "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_gram_f32",
     "blco_encode_tns", "blco_parse_decimal", "blco_launch_count", "blco_cpals_plan_set_reduce",
-    "blco_cpals_plan_set_norm_sq",
+    "blco_cpals_plan_set_norm_sq", "blco_tensor_fibre_stats",
 )
 
 
@@ -85,6 +89,8 @@ class Opts(ctypes.Structure):
         ("residency_bytes", ctypes.c_uint64),
         ("stream", ctypes.c_void_p),
         ("gram_tensor_cores", ctypes.c_int),
+        ("solve", ctypes.c_int),
+        ("guard_cond", ctypes.c_double),
     ]
 
 
@@ -136,6 +142,8 @@ def lib():
         L.blco_cpals_plan_create.argtypes = [vp, i32, vp, vp, vp, vp]
         L.blco_cpals_plan_iterate.argtypes = [vp, i32, f64, vp, vp]
         L.blco_cpals_plan_mttkrp_ms.argtypes = [vp, vp, vp]
+        L.blco_cpals_plan_condition.argtypes = [vp, vp, vp]
+        L.blco_tensor_fibre_stats.argtypes = [vp, i32, vp]
         L.blco_cpals_plan_destroy.argtypes = [vp]
         L.blco_batch_create.argtypes = [i32, vp, vp, vp, vp, f64, vp, vp]
         L.blco_batch_iterate.argtypes = [vp, i32, vp, vp]
@@ -175,13 +183,15 @@ def launch_count(reset=False):
 
 
 def make_opts(kernel=KERNEL_AUTO, nprtn=0, thread_cf=2, stream_data=False, precision=PRECISION_FP64,
-              verbose=False, device=0, residency_bytes=0, stream=None, gram_tensor_cores=False):
+              verbose=False, device=0, residency_bytes=0, stream=None, gram_tensor_cores=False, solve=SOLVE_AUTO,
+              guard_cond=0.0):
     o = Opts()
     lib().blco_opts_init(ctypes.byref(o))
     o.kernel, o.nprtn, o.thread_cf = kernel, nprtn, thread_cf
     o.stream_data, o.precision, o.verbose = int(stream_data), precision, int(verbose)
     o.device, o.residency_bytes = device, residency_bytes
     o.gram_tensor_cores = int(gram_tensor_cores)
+    o.solve, o.guard_cond = int(solve), float(guard_cond)
     if stream is None:
         try:
             import torch
@@ -277,6 +287,14 @@ class Tensor:
                                           bcoords.ctypes.data))
         return dict(coords=coords, vals=vals, block_offsets=offs, block_coords=bcoords[: nb * n].reshape(nb, n),
                     **inf)
+
+    def fibre_stats(self, mode):
+        """Statistics of the mode's compressed-fibre copy (kernel id 4):
+        dict(fibre_mode, fibred_nnz, single_nnz, fibres, rows_gathered)."""
+        st = np.zeros(5, dtype=np.uint64)
+        _check(lib().blco_tensor_fibre_stats(self.handle, mode, st.ctypes.data))
+        return dict(fibre_mode=int(st[0]), fibred_nnz=int(st[1]), single_nnz=int(st[2]), fibres=int(st[3]),
+                    rows_gathered=int(st[4]))
 
     def free(self):
         if self._h and self._h.value:
@@ -451,6 +469,13 @@ class CpalsPlan:
         calls = ctypes.c_int()
         _check(lib().blco_cpals_plan_mttkrp_ms(self._h, ms.ctypes.data, ctypes.byref(calls)))
         return ms, calls.value
+
+    def condition(self):
+        """(condition estimate of every mode's last solve, promoted to FP64)."""
+        c = np.zeros(self.nmodes, dtype=np.float64)
+        pr = ctypes.c_int()
+        _check(lib().blco_cpals_plan_condition(self._h, c.ctypes.data, ctypes.byref(pr)))
+        return c, bool(pr.value)
 
     def destroy(self):
         if self._h and self._h.value:

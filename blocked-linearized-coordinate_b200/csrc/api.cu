@@ -395,6 +395,26 @@ int blco_cpals_plan_iterate(blco_cpals_plan* p, int iters, double tol, double* f
 
 int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls) { return plan_mttkrp_ms(p, ms, calls); }
 
+int blco_tensor_fibre_stats(blco_tensor* t, int mode, uint64_t* stats)
+{
+    if (!t || !stats) return fail(BLCO_ERR_INVALID, "null argument");
+    if (!fibre_eligible(t, mode)) return fail(BLCO_ERR_UNSUPPORTED, "no fibre copy for this tensor and mode");
+    cudaSetDevice(t->device);
+    BLCO_TRY(build_fibre_copy(t, mode, pick_stream(t, nullptr)));
+    const FibreCopy& f = t->fib[mode];
+    stats[0] = (uint64_t)f.fmode;
+    stats[1] = f.nf;
+    stats[2] = f.nl;
+    stats[3] = f.nfib;
+    stats[4] = f.nf * (uint64_t)f.ninner + f.nfib + f.nl * (uint64_t)(f.ninner + 1);
+    return BLCO_OK;
+}
+
+int blco_cpals_plan_condition(const blco_cpals_plan* p, double* cond, int* promoted)
+{
+    return plan_condition(p, cond, promoted);
+}
+
 int blco_cpals_plan_destroy(blco_cpals_plan* p) { return plan_destroy(p); }
 
 int blco_cpals_plan_set_reduce(blco_cpals_plan* p, blco_reduce_fn fn, void* ctx) { return plan_set_reduce(p, fn, ctx); }

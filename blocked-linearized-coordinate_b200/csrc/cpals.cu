@@ -319,8 +319,14 @@ struct GramPtrs {
 // positive, the pseudoinverse is taken from a cyclic Jacobi
 // eigen-decomposition V = Q diag(w) Q^T instead, dropping |w| <= R*ulp(max|w|)
 // as the reference does for its SVD.
+//
+// cond (may be null) receives an estimate of V's condition number: the
+// squared ratio of the largest to the smallest Cholesky pivot (a lower
+// bound), or, on the eigen path, max|w| over the smallest kept |w|.  With
+// pinv, the eigen path is taken whatever the pivots (the reference's
+// pseudoinverse, src/cpd_gpu.cu:452-532, in every case).
 __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __restrict__ Pout,
-                           int* __restrict__ used_eigen)
+                           int* __restrict__ used_eigen, double* __restrict__ cond, bool pinv)
 {
     extern __shared__ __align__(16) double ss[];
     double* A = ss;          // R x R
@@ -335,7 +341,7 @@ __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __r
             if (m != skip) v *= gp.g[m][k];
         A[k] = v;
     }
-    if (tid == 0) bad = 0;
+    if (tid == 0) bad = pinv ? 1 : 0;
     __syncthreads();
     if (tid == 0) {
         double md = 0.0;
@@ -344,7 +350,7 @@ __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __r
     }
     __syncthreads();
     const double piv_tol = 64.0 * R * 2.220446049250313e-16 * maxdiag;
-    for (int k = 0; k < R; k++) {
+    for (int k = 0; k < R && !bad; k++) {
         if (tid == 0) {
             double d = A[k * R + k];
             if (!(d > piv_tol)) bad = 1;
@@ -363,6 +369,11 @@ __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __r
         __syncthreads();
     }
     if (!bad) {
+        if (cond && tid == 0) {
+            double lo = A[0], hi = A[0];
+            for (int i = 1; i < R; i++) lo = fmin(lo, A[i * R + i]), hi = fmax(hi, A[i * R + i]);
+            *cond = (hi / lo) * (hi / lo);
+        }
         // W = L^-1 (lower), column j by forward substitution.
         for (int j = tid; j < R; j += DN_THREADS) {
             for (int i = 0; i < j; i++) W[i * R + j] = 0.0;
@@ -447,6 +458,12 @@ __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __r
         fw[i] = fabs(w) > tol ? 1.0 / w : 0.0;
     }
     __syncthreads();
+    if (cond && tid == 0) {
+        double lo = smax;
+        for (int i = 0; i < R; i++)
+            if (fabs(A[i * R + i]) > tol) lo = fmin(lo, fabs(A[i * R + i]));
+        *cond = lo > 0.0 ? smax / lo : 0.0;
+    }
     for (int e = tid; e < RR; e += DN_THREADS) {
         int a = e / R, b = e % R;
         double s = 0.0;
@@ -457,9 +474,10 @@ __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __r
 }
 
 __global__ __launch_bounds__(DN_THREADS) void k_solve(GramPtrs gp, int nmodes, int skip, int R,
-                                                      double* __restrict__ Pout, int* __restrict__ used_eigen)
+                                                      double* __restrict__ Pout, int* __restrict__ used_eigen,
+                                                      double* __restrict__ cond, int pinv)
 {
-    solve_body(gp, nmodes, skip, R, Pout, used_eigen);
+    solve_body(gp, nmodes, skip, R, Pout, used_eigen, cond, pinv != 0);
 }
 
 // ----------------------------------------------------------------- fit --
@@ -586,6 +604,9 @@ struct blco_cpals_plan {
     double* fit = nullptr;      // 1
     int* used_eigen = nullptr;
     int order[BLCO_MAX_MODES] = {};
+    double cond[BLCO_MAX_MODES] = {}; // condition estimate of each mode's last solve
+    bool promoted = false;            // a mixed plan that continues in FP64
+    bool mixed_updated = false;       // a factor has been updated in the mixed form
     double xnorm = 0.0;
     double fit_old = 0.0;
     int iters_run = 0;
@@ -734,6 +755,9 @@ int update_launch(blco_cpals_plan* p, const TM* M, T* U, uint64_t I, int grid)
 
 int conv_grid(uint64_t n, int sm) { return (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm * 8)); }
 
+int promote_fp64(blco_cpals_plan* p, bool from_f32 = true);
+double guard_of(const blco_cpals_plan* p);
+
 int mode_update(blco_cpals_plan* p, int n)
 {
     blco_tensor* t = p->t;
@@ -794,11 +818,26 @@ int mode_update(blco_cpals_plan* p, int n)
     for (int m = 0; m < N; m++) gp.g[m] = p->grams[m];
     size_t ssmem = 2 * (size_t)R * R * sizeof(double);
     BLCO_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem));
-    k_solve<<<1, DN_THREADS, ssmem, p->s>>>(gp, N, n, R, p->P, p->used_eigen);
+    k_solve<<<1, DN_THREADS, ssmem, p->s>>>(gp, N, n, R, p->P, p->used_eigen, p->fit + 1 + n,
+                                            p->opts.solve == BLCO_SOLVE_PINV);
     BLCO_CHECK_LAUNCH("k_solve");
+    if (p->mixed && guard_of(p) > 0.0) {
+        // The guard reads this mode's estimate before any factor is updated
+        // with it: above the guard, the plan continues in FP64 and this mode
+        // starts again (MTTKRP and solve in FP64).
+        double c = 0.0;
+        BLCO_CUDA(cudaMemcpyAsync(&c, p->fit + 1 + n, sizeof(double), cudaMemcpyDeviceToHost, p->s));
+        BLCO_CUDA(cudaStreamSynchronize(p->s));
+        if (!(c <= guard_of(p))) {
+            // before the first mixed update the caller's FP64 factors are still current
+            BLCO_TRY(promote_fp64(p, p->mixed_updated));
+            return mode_update(p, n);
+        }
+    }
 
     int grid = grid_rows(I, p->sm);
     int ust;
+    if (p->mixed) p->mixed_updated = true;
     if (p->mixed && p->m64[n]) ust = update_launch<double, float>(p, p->M, p->Uf[n], I, grid);
     else if (p->mixed) ust = update_launch<float, float>(p, p->Mf, p->Uf[n], I, grid);
     else ust = update_launch<double, double>(p, p->M, p->U[n], I, grid);
@@ -833,6 +872,52 @@ int fit_launch(blco_cpals_plan* p)
     for (int m = 0; m < N; m++) gp.g[m] = p->grams[m];
     k_fit<<<1, DN_THREADS, 0, p->s>>>(p->partials, grid, gp, N, R, p->lambda, p->xnorm, p->fit);
     BLCO_CHECK_LAUNCH("k_fit");
+    return BLCO_OK;
+}
+
+// A mixed plan continues in FP64: the FP32 working factors are copied into
+// the caller's FP64 arrays, which the plain form works on from here, and
+// every Gram is formed again from them.  Taken when the R x R system is too
+// ill-conditioned for the FP32 working set: the rounding of the factors and
+// of the MTTKRP grows with the condition number through the solve.
+// (At plan creation the caller's arrays still hold the FP64 initial
+// factors: from_f32 = false keeps them.)
+int promote_fp64(blco_cpals_plan* p, bool from_f32)
+{
+    for (int n = 0; n < p->N && from_f32; n++) {
+        const uint64_t I = p->t->layout.dims[n];
+        k_f32_to_f64<<<conv_grid(I * p->R, p->sm), 256, 0, p->s>>>(p->Uf[n], p->U[n], I * p->R);
+        BLCO_CHECK_LAUNCH("k_f32_to_f64");
+    }
+    p->mixed = false;
+    p->gather_dtype = BLCO_DTYPE_F64;
+    p->promoted = true;
+    for (int n = 0; n < p->N; n++)
+        BLCO_TRY(gram_launch<double>(p, p->U[n], p->t->layout.dims[n], nullptr, p->grams[n]));
+    return BLCO_OK;
+}
+
+double guard_of(const blco_cpals_plan* p) { return p->opts.guard_cond == 0.0 ? BLCO_GUARD_COND : p->opts.guard_cond; }
+
+// Condition estimates of every mode's R x R system from the current Grams
+// into p->cond (the solves' P is discarded).
+int initial_condition(blco_cpals_plan* p)
+{
+    const int R = p->R, N = p->N;
+    GramPtrs gp;
+    memset(&gp, 0, sizeof(gp));
+    for (int m = 0; m < N; m++) gp.g[m] = p->grams[m];
+    size_t ssmem = 2 * (size_t)R * R * sizeof(double);
+    BLCO_CUDA(cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssmem));
+    for (int n = 0; n < N; n++) {
+        k_solve<<<1, DN_THREADS, ssmem, p->s>>>(gp, N, n, R, p->P, p->used_eigen, p->fit + 1 + n,
+                                                p->opts.solve == BLCO_SOLVE_PINV);
+        BLCO_CHECK_LAUNCH("k_solve");
+    }
+    double c[BLCO_MAX_MODES];
+    BLCO_CUDA(cudaMemcpyAsync(c, p->fit + 1, N * sizeof(double), cudaMemcpyDeviceToHost, p->s));
+    BLCO_CUDA(cudaStreamSynchronize(p->s));
+    for (int n = 0; n < N; n++) p->cond[n] = c[n];
     return BLCO_OK;
 }
 
@@ -921,7 +1006,9 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     PC(cudaMalloc(&p->P, (size_t)R * R * sizeof(double)));
     PC(cudaMalloc(&p->partials, (size_t)gmax * R * R * sizeof(double)));
     PC(cudaMalloc(&p->inv, (size_t)R * sizeof(double)));
-    PC(cudaMalloc(&p->fit, 2 * sizeof(double)));
+    // fit, then the condition estimate of every mode's solve: read together
+    PC(cudaMalloc(&p->fit, (1 + BLCO_MAX_MODES) * sizeof(double)));
+    PC(cudaMemsetAsync(p->fit, 0, (1 + BLCO_MAX_MODES) * sizeof(double), p->s));
     PC(cudaMalloc(&p->used_eigen, sizeof(int)));
     for (auto& e : p->ev) PC(cudaEventCreate(&e));
 #undef PC
@@ -942,6 +1029,15 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
         } else {
             st = gram_launch<double>(p, p->U[n], t->layout.dims[n], nullptr, p->grams[n]);
         }
+        if (st != BLCO_OK) { plan_free(p); return st; }
+    }
+    // A mixed plan whose initial R x R systems are already too ill-conditioned
+    // for its FP32 working set runs in FP64 from the start.
+    if (p->mixed && guard_of(p) > 0.0) {
+        st = initial_condition(p);
+        double worst = 0.0;
+        for (int n = 0; n < p->N; n++) worst = std::max(worst, p->cond[n]);
+        if (st == BLCO_OK && !(worst <= guard_of(p))) st = promote_fp64(p, false);
         if (st != BLCO_OK) { plan_free(p); return st; }
     }
     // Per-mode MTTKRP schedules, resolved once (kernels 20 and 21 may time
@@ -985,10 +1081,18 @@ int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* i
         if (st == BLCO_OK) st = fit_launch(p);
         if (st != BLCO_OK) break;
         cudaEventRecord(it1, p->s);
-        double fit = 0.0;
-        cudaError_t e = cudaMemcpyAsync(&fit, p->fit, sizeof(double), cudaMemcpyDeviceToHost, p->s);
+        double fc[1 + BLCO_MAX_MODES];
+        cudaError_t e = cudaMemcpyAsync(fc, p->fit, (1 + p->N) * sizeof(double), cudaMemcpyDeviceToHost, p->s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(p->s);
         if (e != cudaSuccess) { st = cuda_fail(e, "CP-ALS iteration", __FILE__, __LINE__); break; }
+        const double fit = fc[0];
+        double worst = 0.0;
+        for (int n = 0; n < p->N; n++) {
+            p->cond[n] = fc[1 + n];
+            worst = std::max(worst, fc[1 + n]);
+        }
+        const double guard = guard_of(p);
+        if (p->mixed && guard > 0.0 && !(worst <= guard) && (st = promote_fp64(p, p->mixed_updated)) != BLCO_OK) break;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, it0, it1);
         for (int n = 0; n < p->N; n++) {
@@ -1089,6 +1193,15 @@ int plan_set_norm_sq(blco_cpals_plan* p, double norm_sq)
     if (!p) return fail(BLCO_ERR_INVALID, "null plan");
     if (!(norm_sq >= 0.0)) return fail(BLCO_ERR_INVALID, "norm_sq must be non-negative");
     p->xnorm = std::sqrt(norm_sq);
+    return BLCO_OK;
+}
+
+int plan_condition(const blco_cpals_plan* p, double* cond, int* promoted)
+{
+    if (!p) return fail(BLCO_ERR_INVALID, "null plan");
+    if (cond)
+        for (int n = 0; n < p->N; n++) cond[n] = p->cond[n];
+    if (promoted) *promoted = p->promoted ? 1 : 0;
     return BLCO_OK;
 }
 
@@ -1338,7 +1451,7 @@ __global__ __launch_bounds__(DN_THREADS) void k_b_solve(BDesc* __restrict__ d, i
     if (!b.active || slot >= b.nmodes) return; // block-uniform
     GramPtrs gp;
     for (int m = 0; m < BLCO_MAX_MODES; m++) gp.g[m] = b.G[m];
-    solve_body(gp, b.nmodes, b.order[slot], b.rank, b.P, dummy);
+    solve_body(gp, b.nmodes, b.order[slot], b.rank, b.P, dummy, nullptr, false);
 }
 
 // Register tiling shared by the batched update and Gram kernels: columns

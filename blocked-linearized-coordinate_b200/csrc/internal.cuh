@@ -283,6 +283,7 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
 int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* iters_done, bool verbose);
 int plan_destroy(blco_cpals_plan* p);
 int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
+int plan_condition(const blco_cpals_plan* p, double* cond, int* promoted);
 int plan_set_reduce(blco_cpals_plan* p, blco_reduce_fn fn, void* ctx);
 int plan_set_norm_sq(blco_cpals_plan* p, double norm_sq);
 

@@ -95,6 +95,13 @@ enum {
     BLCO_PRECISION_MIXED_BF16 = 2 /* as MIXED, with BF16 factor-row gathers */
 };
 
+/* The R x R solve of CP-ALS (blco_opts.solve). */
+enum {
+    BLCO_SOLVE_AUTO = 0,
+    BLCO_SOLVE_PINV = 1
+};
+#define BLCO_GUARD_COND 3e4
+
 /* Element types of factor/output arrays for blco_mttkrp_ex. */
 enum {
     BLCO_DTYPE_F64 = 0,
@@ -120,6 +127,17 @@ typedef struct blco_opts {
                               cores' FP32 accumulation leans low (~1e-7
                               relative per 64-row tile), which moves the fit
                               of a 200M-nonzero tensor by ~1e-4 */
+    int solve;             /* BLCO_SOLVE_AUTO: Cholesky of the R x R system,
+                              the pseudoinverse when it is not positive
+                              definite; BLCO_SOLVE_PINV: the reference's
+                              pseudoinverse (eigen-decomposition, values at
+                              or below R * ulp(max) dropped,
+                              src/cpd_gpu.cu:452-532) in every case */
+    double guard_cond;     /* mixed forms: a plan whose R x R system has a
+                              condition estimate above this continues in
+                              FP64 (the FP32 working set's rounding grows
+                              with the condition number); 0 = the default
+                              (BLCO_GUARD_COND), negative = never */
 } blco_opts;
 
 typedef struct blco_tensor blco_tensor; /* opaque */
@@ -226,6 +244,13 @@ int blco_tensor_copy_out(const blco_tensor* t, uint64_t* coords, double* values,
 /* Device pointers of the resident stream (BLCO_ERR_STATE if streamed). */
 int blco_tensor_device_arrays(const blco_tensor* t, const uint64_t** d_coords,
                               const double** d_values);
+/* Statistics of the compressed-fibre copy of `mode` (kernel id 4), building
+ * it if needed: stats[0] fibre mode, [1] nonzeros in fibres of two or more,
+ * [2] single-nonzero fibres, [3] fibres of two or more, [4] factor rows one
+ * MTTKRP of the mode gathers ((nmodes - 2) per fibred nonzero, one per
+ * fibre, nmodes - 1 per single-nonzero fibre).  BLCO_ERR_UNSUPPORTED where
+ * kernel 4 does not apply.  No counterpart in the reference. */
+int blco_tensor_fibre_stats(blco_tensor* t, int mode, uint64_t* stats);
 
 /* ---- MTTKRP ------------------------------------------------------------- */
 
@@ -287,6 +312,12 @@ int blco_cpals_plan_iterate(blco_cpals_plan* p, int iters, double tol, double* f
 /* Milliseconds of device time spent in MTTKRP per mode over all iterations
  * run so far (CUDA events on the plan's stream); ms has nmodes entries. */
 int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
+/* The condition estimate of every mode's last R x R solve (cond: nmodes
+ * entries; the squared ratio of the extreme Cholesky pivots, or the ratio
+ * of the extreme kept eigenvalues) and whether a mixed plan runs in FP64
+ * (promoted: 1 when an estimate exceeded guard_cond, at plan creation or
+ * after an iteration).  No counterpart in the reference. */
+int blco_cpals_plan_condition(const blco_cpals_plan* p, double* cond, int* promoted);
 int blco_cpals_plan_destroy(blco_cpals_plan* p);
 
 /* Sharded CP-ALS (several processes, one GPU each, each holding a share of

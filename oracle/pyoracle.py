@@ -68,8 +68,36 @@ def ref_lib():
         R.ref_alto_create128.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int]
         R.ref_alto_mttkrp128.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         R.ref_alto_destroy128.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        R.ref_cpd_alto.restype = ctypes.c_int
+        R.ref_cpd_alto.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int, ctypes.c_void_p,
+                                   _f64p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _f64p, _f64p, _f64p]
         _ref = R
     return _ref
+
+
+def ref_cpd_alto(dims, cidx, vals, factors, lam, iters, epsilon=0.0, nthreads=None):
+    """The reference's CPU CP-ALS (cpd_alto, include/cpd.hpp:44-187) through
+    oracle/_ref: factors (list of FP64 arrays) and lam are updated in place.
+    Returns dict(iters, ms_per_iter, mttkrp_ms_per_iter, fit, threads) from
+    its own report (the "Per iteration" line)."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref/libblco_ref.so is not built")
+    dims = np.ascontiguousarray(dims, dtype=np.uint64)
+    cidx = np.ascontiguousarray(cidx, dtype=np.uint64)
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    nthreads = nthreads or (os.cpu_count() or 1)
+    for f in factors:
+        assert f.flags.c_contiguous and f.dtype == np.float64
+    ptrs = (ctypes.c_void_p * len(factors))(*[f.ctypes.data for f in factors])
+    out = np.zeros(3)
+    n = R.ref_cpd_alto(len(dims), _p(dims, _u64p), cidx.shape[1], _p(cidx, _u64p), _p(vals, _f64p),
+                       factors[0].shape[1], ptrs, _p(lam, _f64p), int(iters), float(epsilon), int(nthreads),
+                       _p(out[0:1], _f64p), _p(out[1:2], _f64p), _p(out[2:3], _f64p))
+    if n < 0:
+        raise RuntimeError("cpd_alto report not found")
+    return dict(iters=n, ms_per_iter=float(out[0]), mttkrp_ms_per_iter=float(out[1]), fit=float(out[2]),
+                threads=nthreads)
 
 
 def alto_masks(dims):

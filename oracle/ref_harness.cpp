@@ -12,9 +12,11 @@
 //     (include/cpd.hpp:510-544),
 //   * the reference OpenMP ALTO CPU MTTKRP mttkrp_alto_par
 //     (include/alto.hpp:544-550) on a create_alto tensor,
-//   * the reference KruskalModelRandomInit (src/kruskal_model.cpp:93-110).
-// The reference's BLAS/LAPACK CP-ALS (include/cpd.hpp) needs an external
-// BLAS and is not built: its BLAS symbols are stubs that abort.
+//   * the reference KruskalModelRandomInit (src/kruskal_model.cpp:93-110),
+//   * the reference's CPU CP-ALS cpd_alto (include/cpd.hpp:44-187), the CPU
+//     baseline: its BLAS/LAPACK calls (cblas_dsyrk, dpotrf_, dpotrs_,
+//     dgelsy_) are forwarded to the OpenBLAS that scipy bundles (exported as
+//     scipy_cblas_dsyrk, scipy_dpotrf_, ...; linked by oracle/Makefile).
 //
 // Stand-ins needed to run the reference host code without a GPU driver:
 //   * cudaHostAlloc/cudaMallocHost/cudaFreeHost map to malloc/free;
@@ -60,14 +62,34 @@ void check_cuda(cudaError_t status, std::string message)
     }
 }
 
-extern "C" void cblas_dsyrk(CBLAS_ORDER, CBLAS_UPLO, CBLAS_TRANSPOSE, long, long, double,
-                            const double*, long, double, double*, long) { abort(); }
-extern "C" void dpotrf_(char*, lapack_int*, double*, lapack_int*, lapack_int*) { abort(); }
-extern "C" void dpotrs_(char*, lapack_int*, lapack_int*, double*, lapack_int*, double*,
-                        lapack_int*, lapack_int*) { abort(); }
-extern "C" void dgelsy_(lapack_int*, lapack_int*, lapack_int*, double*, lapack_int*, double*,
-                        lapack_int*, lapack_int*, double*, lapack_int*, double*, lapack_int*,
-                        lapack_int*) { abort(); }
+// scipy's OpenBLAS (32-bit integers) under its prefixed names
+extern "C" void scipy_cblas_dsyrk(int, int, int, int, int, double, const double*, int, double, double*, int);
+extern "C" void scipy_dpotrf_(char*, lapack_int*, double*, lapack_int*, lapack_int*);
+extern "C" void scipy_dpotrs_(char*, lapack_int*, lapack_int*, double*, lapack_int*, double*, lapack_int*,
+                              lapack_int*);
+extern "C" void scipy_dgelsy_(lapack_int*, lapack_int*, lapack_int*, double*, lapack_int*, double*, lapack_int*,
+                              lapack_int*, double*, lapack_int*, double*, lapack_int*, lapack_int*);
+
+extern "C" void cblas_dsyrk(CBLAS_ORDER o, CBLAS_UPLO u, CBLAS_TRANSPOSE t, int n, int k, double alpha,
+                            const double* a, int lda, double beta, double* c, int ldc)
+{
+    scipy_cblas_dsyrk((int)o, (int)u, (int)t, n, k, alpha, a, lda, beta, c, ldc);
+}
+extern "C" void dpotrf_(char* uplo, lapack_int* n, double* a, lapack_int* lda, lapack_int* info)
+{
+    scipy_dpotrf_(uplo, n, a, lda, info);
+}
+extern "C" void dpotrs_(char* uplo, lapack_int* n, lapack_int* nrhs, double* a, lapack_int* lda, double* b,
+                        lapack_int* ldb, lapack_int* info)
+{
+    scipy_dpotrs_(uplo, n, nrhs, a, lda, b, ldb, info);
+}
+extern "C" void dgelsy_(lapack_int* m, lapack_int* n, lapack_int* nrhs, double* a, lapack_int* lda, double* b,
+                        lapack_int* ldb, lapack_int* jpvt, double* rcond, lapack_int* rank, double* work,
+                        lapack_int* lwork, lapack_int* info)
+{
+    scipy_dgelsy_(m, n, nrhs, a, lda, b, ldb, jpvt, rcond, rank, work, lwork, info);
+}
 
 static SparseTensor* refh_make_tensor(int nmodes, const uint64_t* dims, uint64_t nnz,
                                       const uint64_t* cidx, const double* vals)
@@ -244,3 +266,63 @@ extern "C" void ref_alto_mttkrp128(void* hv, int mode, int rank, double* const* 
     refh_alto_mttkrp<unsigned __int128>(hv, mode, rank, factors);
 }
 extern "C" void ref_alto_destroy128(void* hv, int rank) { refh_alto_destroy<unsigned __int128>(hv, rank); }
+
+// The reference's CPU CP-ALS (cpd_alto, include/cpd.hpp:44-187) on a COO
+// tensor with the given initial factors and lambda (overwritten with the
+// result), nthreads OpenMP threads.  cpd_alto reports on stdout; its output
+// is captured and parsed: *ms_per_iter and *mttkrp_ms_per_iter from its
+// "Per iteration" line (columns Total and MTTKRP, include/cpd.hpp:174-176),
+// *fit from its last iteration line.  Returns the iterations run, or -1.
+#include <omp.h>
+#include <unistd.h>
+extern "C" int ref_cpd_alto(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* cidx,
+                            const double* vals, int rank, double* const* factors, double* lambda,
+                            int max_iters, double epsilon, int nthreads, double* ms_per_iter,
+                            double* mttkrp_ms_per_iter, double* fit)
+{
+    omp_set_num_threads(nthreads);
+    SparseTensor* X = refh_make_tensor(nmodes, dims, nnz, cidx, vals);
+    AltoTensor<unsigned long long>* AT = nullptr;
+    create_alto(X, &AT, nthreads);
+    KruskalModel* M;
+    CreateKruskalModel(nmodes, (IType*)dims, rank, &M);
+    for (int n = 0; n < nmodes; n++) memcpy(M->U[n], factors[n], sizeof(double) * dims[n] * rank);
+    memcpy(M->lambda, lambda, sizeof(double) * rank);
+    fflush(stdout);
+    FILE* cap = tmpfile();
+    const int saved = dup(1);
+    if (!cap || saved < 0) return -1;
+    dup2(fileno(cap), 1);
+    cpd_alto(AT, M, max_iters, epsilon);
+    fflush(stdout);
+    dup2(saved, 1);
+    close(saved);
+    for (int n = 0; n < nmodes; n++) memcpy(factors[n], M->U[n], sizeof(double) * dims[n] * rank);
+    memcpy(lambda, M->lambda, sizeof(double) * rank);
+    DestroyKruskalModel(M);
+    destroy_alto(AT);
+    DestroySparseTensor(X);
+    // parse the captured report
+    fseek(cap, 0, SEEK_SET);
+    char line[512];
+    int iters = 0, per = 0;
+    while (fgets(line, sizeof(line), cap)) {
+        int it;
+        double f;
+        if (sscanf(line, "it: %d fit: %lf", &it, &f) == 2) {
+            *fit = f;
+            iters = it + 1;
+        } else if (per == 1) {
+            double tot = 0, mt = 0;
+            if (sscanf(line, "%lf %lf", &tot, &mt) == 2) {
+                *ms_per_iter = tot * 1e3;
+                *mttkrp_ms_per_iter = mt * 1e3;
+            }
+            per = 2;
+        } else if (strncmp(line, "Per iteration", 13) == 0) {
+            per = 1;
+        }
+    }
+    fclose(cap);
+    return per == 2 ? iters : -1;
+}

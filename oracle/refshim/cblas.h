@@ -1,7 +1,6 @@
 /* Declarations only, so that the reference's include/cpd.hpp compiles for
- * the oracle harness.  No BLAS is linked: the harness defines these symbols
- * as stubs that abort, because the reference's BLAS/LAPACK-based CPU CP-ALS
- * is not part of what oracle/_ref builds. */
+ * the oracle harness, with the 32-bit integers of the OpenBLAS scipy bundles;
+ * the harness forwards the calls to that library (oracle/ref_harness.cpp). */
 #ifndef REFSHIM_CBLAS_H_
 #define REFSHIM_CBLAS_H_
 typedef enum { CblasRowMajor = 101, CblasColMajor = 102 } CBLAS_ORDER;
@@ -10,8 +9,8 @@ typedef enum { CblasUpper = 121, CblasLower = 122 } CBLAS_UPLO;
 #ifdef __cplusplus
 extern "C" {
 #endif
-void cblas_dsyrk(CBLAS_ORDER, CBLAS_UPLO, CBLAS_TRANSPOSE, long n, long k, double alpha,
-                 const double* a, long lda, double beta, double* c, long ldc);
+void cblas_dsyrk(CBLAS_ORDER, CBLAS_UPLO, CBLAS_TRANSPOSE, int n, int k, double alpha,
+                 const double* a, int lda, double beta, double* c, int ldc);
 #ifdef __cplusplus
 }
 #endif

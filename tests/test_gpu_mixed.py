@@ -103,3 +103,86 @@ def test_mixed_cpals_skewed_fit_within_1e5(blco):
         _, fits_g = blco.cpals(t, fg, np.ones(R), 10, 0.0, blco.make_opts(precision=prec))
         d = np.max(np.abs(np.array(fits_g) - np.array(fits_o)))
         assert d <= bound, (prec, d, fits_g[-1], fits_o[-1])
+
+
+def test_mixed_plan_runs_fp64_when_ill_conditioned(blco):
+    """A mixed plan whose R x R systems are ill-conditioned continues in FP64
+    (the FP32 working set's rounding grows with the condition number):
+    initial factors with two nearly equal columns make the first systems'
+    condition estimates huge, so the plan is promoted; with the guard off it
+    stays mixed.  (Such a start is chaotic in FP64 as well, through the
+    order of FP64 atomics, so fits are compared in the next test.)"""
+    import torch
+    rng = np.random.default_rng(21)
+    dims = [3000, 800, 200]
+    cidx = unique_coords(rng, dims, 40_000, zipf=0.9)
+    vals = rng.random(40_000)
+    t = blco.Tensor.encode(dims, cidx, vals)
+    R = 8
+    fs0 = [rng.random((d, R)) for d in dims]
+    for f in fs0:
+        f[:, 1] = f[:, 0] * (1.0 + 1e-7 * rng.random(f.shape[0]))
+
+    def promoted(precision, guard):
+        dfs = [torch.from_numpy(f.copy()).cuda() for f in fs0]
+        lam = torch.ones(R, dtype=torch.float64, device="cuda")
+        plan = blco.CpalsPlan(t, dfs, lam, blco.make_opts(precision=precision, guard_cond=guard))
+        plan.iterate(3, tol=-1.0)
+        _, pr = plan.condition()
+        plan.destroy()
+        return pr
+
+    assert not promoted(blco.PRECISION_FP64, 0.0)  # an FP64 plan has nothing to promote
+    assert promoted(blco.PRECISION_MIXED, 0.0)
+    assert not promoted(blco.PRECISION_MIXED, -1.0)
+    t.free()
+
+
+def test_promoted_plan_follows_fp64(blco):
+    """Promotion at creation hands the caller's FP64 factors to the FP64
+    path unchanged: with a guard every system exceeds (1.5), the mixed plan
+    follows the FP64 plan's fits and factors (a well-conditioned tensor, so
+    FP64 runs agree to rounding of the atomics' order)."""
+    import torch
+    rng = np.random.default_rng(23)
+    dims = [3000, 800, 200]
+    cidx = unique_coords(rng, dims, 40_000)
+    vals = rng.random(40_000)
+    t = blco.Tensor.encode(dims, cidx, vals)
+    R = 8
+    fs0 = [rng.random((d, R)) for d in dims]
+    out = []
+    for precision, guard in ((blco.PRECISION_FP64, 0.0), (blco.PRECISION_MIXED, 1.5)):
+        dfs = [torch.from_numpy(f.copy()).cuda() for f in fs0]
+        lam = torch.ones(R, dtype=torch.float64, device="cuda")
+        plan = blco.CpalsPlan(t, dfs, lam, blco.make_opts(precision=precision, guard_cond=guard))
+        fits = plan.iterate(6, tol=-1.0)
+        _, pr = plan.condition()
+        plan.destroy()
+        out.append((np.array(fits), [d.cpu().numpy() for d in dfs], pr))
+    (f64, u64, p64), (fmix, umix, pmix) = out
+    assert not p64 and pmix
+    assert np.allclose(fmix, f64, rtol=0, atol=1e-10), np.abs(fmix - f64).max()
+    for a, b in zip(umix, u64):
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+    t.free()
+
+
+def test_mixed_plan_stays_mixed_when_well_conditioned(blco):
+    """Uniform random factors of a uniform tensor: every condition estimate
+    stays far below the guard and the plan keeps its FP32 working set."""
+    import torch
+    rng = np.random.default_rng(22)
+    dims = [3000, 800, 200]
+    cidx = unique_coords(rng, dims, 40_000)
+    vals = rng.random(40_000)
+    t = blco.Tensor.encode(dims, cidx, vals)
+    R = 8
+    dfs = [torch.from_numpy(rng.random((d, R))).cuda() for d in dims]
+    lam = torch.ones(R, dtype=torch.float64, device="cuda")
+    plan = blco.CpalsPlan(t, dfs, lam, blco.make_opts(precision=blco.PRECISION_MIXED))
+    plan.iterate(4, tol=-1.0)
+    cond, promoted = plan.condition()
+    assert not promoted and 1.0 <= cond.max() < blco.GUARD_COND
+    plan.destroy()
+    t.free()

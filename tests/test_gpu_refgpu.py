@@ -3,10 +3,12 @@ sm_100a into oracle/_ref/libblco_refgpu.so (make -C oracle ref-gpu):
 cpals_blco_dev (src/cpd_gpu.cu:21-242) and mttkrp_alto_dev
 (src/alto_dev.cu:1857-1952) on the same inputs and initial factors.
 
-Tolerances: MTTKRP normwise relative 1e-12; CP-ALS fit 1e-10 absolute and
-factors 1e-9 relative (Frobenius) after each tested iteration count.  Both
-sides sum with FP64 atomics in run-dependent order, and the reference solves
-with a Jacobi SVD (cuSOLVER gesvdj) where this engine uses Cholesky.
+Tolerances: MTTKRP normwise relative 1e-12; CP-ALS fit, factors
+(Frobenius) and lambda 1e-12 relative after each tested iteration count,
+with this engine's Cholesky solve and with its pseudoinverse solve (the
+reference solves with a Jacobi SVD, cuSOLVER gesvdj).  Both sides sum with
+FP64 atomics in run-dependent order.  Measured on a B200: fits equal or
+within 2e-14, factors within 4e-13, lambda within 2e-13.
 """
 import numpy as np
 import pytest
@@ -47,8 +49,13 @@ def test_mttkrp_matches_reference_gpu(blco, ref_kernel):
         assert err <= 1e-12, (m, err)
 
 
+def _rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b))
+
+
+@pytest.mark.parametrize("solve", [0, 1])
 @pytest.mark.parametrize("iters", [1, 5, 20])
-def test_cpals_matches_reference_gpu(blco, iters):
+def test_cpals_matches_reference_gpu(blco, iters, solve):
     """The CPU-runnable workload's shape (1000 x 800 x 600, unique uniform
     coordinates, U(0,1) values, rank 16, tolerance 0) at 100k nonzeros."""
     from blco_b200 import synth
@@ -61,15 +68,15 @@ def test_cpals_matches_reference_gpu(blco, iters):
     t = blco.Tensor.encode(X["dims"], X["cidx"], X["vals"])
     fg = [f.copy() for f in fs0]
     lg = lam0.copy()
-    fit_g, fits_g = blco.cpals(t, fg, lg, iters, 0.0)
+    fit_g, fits_g = blco.cpals(t, fg, lg, iters, 0.0, blco.make_opts(solve=solve))
     assert len(fits_g) == iters
-    assert abs(fit_g - fit_r) <= 1e-10, (fit_g, fit_r)
-    for a, b in zip(fg, fr):
-        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
-    assert np.allclose(lg, lr, rtol=1e-9)
+    errs = (abs(fit_g - fit_r) / abs(fit_r), max(_rel(a, b) for a, b in zip(fg, fr)), _rel(lg, lr))
+    print("fit, factor, lambda relative errors", errs)
+    assert max(errs) <= 1e-12, errs
 
 
-def test_cpals_skewed_matches_reference_gpu(blco):
+@pytest.mark.parametrize("solve", [0, 1])
+def test_cpals_skewed_matches_reference_gpu(blco, solve):
     rng = np.random.default_rng(17)
     dims = [20_000, 15_000, 500]
     nnz = 150_000
@@ -83,10 +90,10 @@ def test_cpals_skewed_matches_reference_gpu(blco):
     t = blco.Tensor.encode(dims, cidx, vals)
     fg = [f.copy() for f in fs0]
     lg = np.ones(R)
-    fit_g, _ = blco.cpals(t, fg, lg, 8, 0.0)
-    assert abs(fit_g - fit_r) <= 1e-10, (fit_g, fit_r)
-    for a, b in zip(fg, fr):
-        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+    fit_g, _ = blco.cpals(t, fg, lg, 8, 0.0, blco.make_opts(solve=solve))
+    errs = (abs(fit_g - fit_r) / abs(fit_r), max(_rel(a, b) for a, b in zip(fg, fr)), _rel(lg, lr))
+    print("fit, factor, lambda relative errors", errs)
+    assert max(errs) <= 1e-12, errs
 
 
 @pytest.mark.parametrize("ref_kernel", [1, 10])
@@ -135,7 +142,7 @@ def test_wide_cpals_matches_reference_gpu_cpd128(blco):
     lg = np.ones(R)
     fit_g, fits_g = blco.cpals(t, fg, lg, 5, 0.0, blco.make_opts(kernel=10))
     assert len(fits_g) == 5
-    assert abs(fit_g - fit_r) <= 1e-10, (fit_g, fit_r)
-    for a, b in zip(fg, fr):
-        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b)
+    errs = (abs(fit_g - fit_r) / abs(fit_r), max(_rel(a, b) for a, b in zip(fg, fr)), _rel(lg, lr))
+    print("fit, factor, lambda relative errors", errs)
+    assert max(errs) <= 1e-12, errs
     t.free()
