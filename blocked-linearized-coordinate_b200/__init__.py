@@ -61,7 +61,7 @@ EXPORTS = (
     "blco_encode", "blco_encode_device", "blco_encode_device_noalloc", "blco_tensor_free", "blco_tensor_get_info",
     "blco_tensor_copy_out", "blco_tensor_device_arrays", "blco_mttkrp", "blco_mttkrp_ex", "blco_mttkrp_host",
     "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
-    "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_condition", "blco_cpals_plan_destroy", "blco_batch_create",
+    "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_condition", "blco_cpals_plan_device_bytes", "blco_cpals_plan_destroy", "blco_batch_create",
     "blco_batch_iterate",
     "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
     "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
@@ -143,6 +143,7 @@ def lib():
         L.blco_cpals_plan_iterate.argtypes = [vp, i32, f64, vp, vp]
         L.blco_cpals_plan_mttkrp_ms.argtypes = [vp, vp, vp]
         L.blco_cpals_plan_condition.argtypes = [vp, vp, vp]
+        L.blco_cpals_plan_device_bytes.argtypes = [vp, vp]
         L.blco_tensor_fibre_stats.argtypes = [vp, i32, vp]
         L.blco_cpals_plan_destroy.argtypes = [vp]
         L.blco_batch_create.argtypes = [i32, vp, vp, vp, vp, f64, vp, vp]
@@ -469,6 +470,12 @@ class CpalsPlan:
         calls = ctypes.c_int()
         _check(lib().blco_cpals_plan_mttkrp_ms(self._h, ms.ctypes.data, ctypes.byref(calls)))
         return ms, calls.value
+
+    def device_bytes(self):
+        """Device bytes the plan holds (factors, workspace, streamed ring)."""
+        b = ctypes.c_uint64()
+        _check(lib().blco_cpals_plan_device_bytes(self._h, ctypes.byref(b)))
+        return b.value
 
     def condition(self):
         """(condition estimate of every mode's last solve, promoted to FP64)."""

@@ -70,8 +70,15 @@ cudaStream_t pick_stream(const blco_tensor*, const blco_opts* opts)
 // src/alto_dev.cu:1979-2012, with events instead of one stream per block).
 static int mttkrp_streamed(blco_tensor* t, const MttkrpArgs& base, const blco_opts* opts, cudaStream_t s)
 {
+    // the ring holds what the residency budget leaves after the caller's
+    // factors and output
+    const uint64_t budget = opts && opts->residency_bytes ? opts->residency_bytes : (8ull << 30);
+    const uint64_t eb = base.factor_dtype == BLCO_DTYPE_F64 ? 8 : base.factor_dtype == BLCO_DTYPE_F32 ? 4 : 2;
+    uint64_t held = t->layout.dims[base.mode] * (uint64_t)base.rank * (base.factor_dtype == BLCO_DTYPE_F64 ? 8 : 4);
+    for (int m = 0; m < t->layout.nmodes; m++) held += t->layout.dims[m] * (uint64_t)base.rank * eb;
+    if (budget <= held + 32) return fail(BLCO_ERR_NOMEM, "the residency budget does not cover the factors and output");
     StreamRing* ring = nullptr;
-    BLCO_TRY(stream_ring_create(t, opts ? opts->residency_bytes : 0, &ring));
+    BLCO_TRY(stream_ring_create(t, budget - held, &ring));
     const int st = mttkrp_streamed_ring(t, base, ring, s);
     const int st2 = stream_ring_destroy(ring);
     return st != BLCO_OK ? st : st2;
@@ -414,6 +421,8 @@ int blco_cpals_plan_condition(const blco_cpals_plan* p, double* cond, int* promo
 {
     return plan_condition(p, cond, promoted);
 }
+
+int blco_cpals_plan_device_bytes(const blco_cpals_plan* p, uint64_t* bytes) { return plan_device_bytes(p, bytes); }
 
 int blco_cpals_plan_destroy(blco_cpals_plan* p) { return plan_destroy(p); }
 

@@ -322,7 +322,8 @@ struct GramPtrs {
 //
 // cond (may be null) receives an estimate of V's condition number: the
 // squared ratio of the largest to the smallest Cholesky pivot (a lower
-// bound), or, on the eigen path, max|w| over the smallest kept |w|.  With
+// bound), or, on the eigen path, max|w| over the smallest |w| (infinity
+// when an eigenvalue is exactly zero).  With
 // pinv, the eigen path is taken whatever the pivots (the reference's
 // pseudoinverse, src/cpd_gpu.cu:452-532, in every case).
 __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __restrict__ Pout,
@@ -459,10 +460,11 @@ __device__ void solve_body(GramPtrs gp, int nmodes, int skip, int R, double* __r
     }
     __syncthreads();
     if (cond && tid == 0) {
+        // every eigenvalue counts, the dropped ones too: a numerically
+        // singular V reports (near) infinity, not the kept part's ratio
         double lo = smax;
-        for (int i = 0; i < R; i++)
-            if (fabs(A[i * R + i]) > tol) lo = fmin(lo, fabs(A[i * R + i]));
-        *cond = lo > 0.0 ? smax / lo : 0.0;
+        for (int i = 0; i < R; i++) lo = fmin(lo, fabs(A[i * R + i]));
+        *cond = smax == 0.0 ? 0.0 : lo > 0.0 ? smax / lo : HUGE_VAL;
     }
     for (int e = tid; e < RR; e += DN_THREADS) {
         int a = e / R, b = e % R;
@@ -607,6 +609,7 @@ struct blco_cpals_plan {
     double cond[BLCO_MAX_MODES] = {}; // condition estimate of each mode's last solve
     bool promoted = false;            // a mixed plan that continues in FP64
     bool mixed_updated = false;       // a factor has been updated in the mixed form
+    uint64_t dev_bytes = 0;           // device bytes: caller's factors and lambda, workspace, ring
     double xnorm = 0.0;
     double fit_old = 0.0;
     int iters_run = 0;
@@ -976,42 +979,64 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
             return _s;                                                         \
         }                                                                      \
     } while (0)
+    // device bytes of the plan: the caller's FP64 factors and lambda, then
+    // every buffer below (a streamed tensor's ring gets what the residency
+    // budget leaves)
+    for (int n = 0; n < p->N; n++) p->dev_bytes += t->layout.dims[n] * (uint64_t)R * sizeof(double);
+    p->dev_bytes += (uint64_t)R * sizeof(double);
+#define PCA(ptr, bytes)                                                        \
+    do {                                                                       \
+        PC(cudaMalloc((ptr), (bytes)));                                        \
+        p->dev_bytes += (uint64_t)(bytes);                                     \
+    } while (0)
     p->mixed = p->opts.precision != BLCO_PRECISION_FP64;
-    if (!t->resident) {
-        st = stream_ring_create(t, p->opts.residency_bytes, &p->ring);
-        if (st != BLCO_OK) { plan_free(p); return st; }
-    }
     p->gather_dtype = p->opts.precision == BLCO_PRECISION_MIXED_BF16 ? BLCO_DTYPE_BF16
                       : p->mixed                                     ? BLCO_DTYPE_F32
                                                                      : BLCO_DTYPE_F64;
     if (p->mixed) {
         p->gram_tc = R <= 64 && p->opts.gram_tensor_cores;
         if (p->gram_tc) {
-            PC(cudaMalloc(&p->tc_partials, (size_t)gram_tc_max_ctas(p->sm) * R * R * sizeof(double)));
-            PC(cudaMalloc(&p->d_err, sizeof(int)));
+            PCA(&p->tc_partials, (size_t)gram_tc_max_ctas(p->sm) * R * R * sizeof(double));
+            PCA(&p->d_err, sizeof(int));
             PC(cudaMemsetAsync(p->d_err, 0, sizeof(int), p->s));
         }
-        PC(cudaMalloc(&p->Mf, std::max<uint64_t>(maxdim, 1) * R * sizeof(float)));
+        PCA(&p->Mf, std::max<uint64_t>(maxdim, 1) * R * sizeof(float));
         // FP64 result of the wide-key and fibre schedules
-        PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
+        PCA(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double));
         for (int n = 0; n < p->N; n++) {
             const uint64_t len = t->layout.dims[n] * (uint64_t)R;
-            PC(cudaMalloc(&p->Uf[n], len * sizeof(float)));
-            if (p->gather_dtype == BLCO_DTYPE_BF16) PC(cudaMalloc(&p->Ub[n], len * 2));
+            PCA(&p->Uf[n], len * sizeof(float));
+            if (p->gather_dtype == BLCO_DTYPE_BF16) PCA(&p->Ub[n], len * 2);
         }
     } else {
-        PC(cudaMalloc(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double)));
+        PCA(&p->M, std::max<uint64_t>(maxdim, 1) * R * sizeof(double));
     }
-    for (int n = 0; n < p->N; n++) PC(cudaMalloc(&p->grams[n], (size_t)R * R * sizeof(double)));
-    PC(cudaMalloc(&p->P, (size_t)R * R * sizeof(double)));
-    PC(cudaMalloc(&p->partials, (size_t)gmax * R * R * sizeof(double)));
-    PC(cudaMalloc(&p->inv, (size_t)R * sizeof(double)));
+    for (int n = 0; n < p->N; n++) PCA(&p->grams[n], (size_t)R * R * sizeof(double));
+    PCA(&p->P, (size_t)R * R * sizeof(double));
+    PCA(&p->partials, (size_t)gmax * R * R * sizeof(double));
+    PCA(&p->inv, (size_t)R * sizeof(double));
     // fit, then the condition estimate of every mode's solve: read together
-    PC(cudaMalloc(&p->fit, (1 + BLCO_MAX_MODES) * sizeof(double)));
+    PCA(&p->fit, (1 + BLCO_MAX_MODES) * sizeof(double));
     PC(cudaMemsetAsync(p->fit, 0, (1 + BLCO_MAX_MODES) * sizeof(double), p->s));
-    PC(cudaMalloc(&p->used_eigen, sizeof(int)));
+    PCA(&p->used_eigen, sizeof(int));
     for (auto& e : p->ev) PC(cudaEventCreate(&e));
+#undef PCA
 #undef PC
+    if (!t->resident) {
+        // the ring of block buffers holds what the budget leaves
+        const uint64_t budget = p->opts.residency_bytes ? p->opts.residency_bytes : (8ull << 30);
+        // two pieces of at least 4096 nonzeros (smaller pieces are valid
+        // but leave each copy and kernel launch-bound)
+        const uint64_t min_ring = 2 * 16 * std::min<uint64_t>(t->nnz, 4096);
+        if (budget < p->dev_bytes + min_ring) {
+            plan_free(p);
+            return fail(BLCO_ERR_NOMEM, "the residency budget does not cover the plan's factors and workspace "
+                                        "and two block buffers");
+        }
+        st = stream_ring_create(t, budget - p->dev_bytes, &p->ring);
+        if (st != BLCO_OK) { plan_free(p); return st; }
+        p->dev_bytes += stream_ring_bytes(p->ring);
+    }
     p->xnorm = std::sqrt(t->norm_sq);
     if (p->mixed) {
         // streamed: 4-byte values copied per block from a pinned FP32 copy
@@ -1193,6 +1218,13 @@ int plan_set_norm_sq(blco_cpals_plan* p, double norm_sq)
     if (!p) return fail(BLCO_ERR_INVALID, "null plan");
     if (!(norm_sq >= 0.0)) return fail(BLCO_ERR_INVALID, "norm_sq must be non-negative");
     p->xnorm = std::sqrt(norm_sq);
+    return BLCO_OK;
+}
+
+int plan_device_bytes(const blco_cpals_plan* p, uint64_t* bytes)
+{
+    if (!p || !bytes) return fail(BLCO_ERR_INVALID, "null argument");
+    *bytes = p->dev_bytes;
     return BLCO_OK;
 }
 

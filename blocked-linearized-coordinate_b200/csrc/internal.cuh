@@ -271,6 +271,7 @@ uint32_t auto_hot_chunk(uint64_t hot_nnz);
 struct StreamRing;
 int stream_ring_create(const blco_tensor* t, uint64_t residency_bytes, StreamRing** out);
 int stream_ring_destroy(StreamRing* r);
+uint64_t stream_ring_bytes(const StreamRing* r);
 int mttkrp_streamed_ring(const blco_tensor* t, const MttkrpArgs& base, StreamRing* r, cudaStream_t s);
 // FP32 copy of the resident values (created on first use).
 int values_f32(blco_tensor* t, cudaStream_t s, const float** out);
@@ -284,6 +285,7 @@ int plan_iterate(blco_cpals_plan* p, int iters, double tol, double* fits, int* i
 int plan_destroy(blco_cpals_plan* p);
 int plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
 int plan_condition(const blco_cpals_plan* p, double* cond, int* promoted);
+int plan_device_bytes(const blco_cpals_plan* p, uint64_t* bytes);
 int plan_set_reduce(blco_cpals_plan* p, blco_reduce_fn fn, void* ctx);
 int plan_set_norm_sq(blco_cpals_plan* p, double norm_sq);
 

@@ -1471,6 +1471,8 @@ struct StreamRing {
     cudaStream_t cs = nullptr;
 };
 
+uint64_t stream_ring_bytes(const StreamRing* r) { return r ? (uint64_t)r->nbuf * r->B * 16 : 0; }
+
 int stream_ring_destroy(StreamRing* r)
 {
     if (!r) return BLCO_OK;
@@ -1487,9 +1489,10 @@ int stream_ring_destroy(StreamRing* r)
     return BLCO_OK;
 }
 
-// A ring of device block buffers (at most residency_bytes, 8 GiB when 0,
-// between 2 and 8 buffers) and a copy stream, for tensors whose blocks stay
-// in pinned host memory.
+// A ring of device block buffers (at most residency_bytes of them, 8 GiB
+// when 0; between 2 and 8 buffers) and a copy stream, for tensors whose
+// blocks stay in pinned host memory.  Callers pass what the device budget
+// leaves after their factors and workspace.
 int stream_ring_create(const blco_tensor* t, uint64_t residency_bytes, StreamRing** out)
 {
     *out = nullptr;

@@ -318,6 +318,11 @@ int blco_cpals_plan_mttkrp_ms(const blco_cpals_plan* p, double* ms, int* calls);
  * (promoted: 1 when an estimate exceeded guard_cond, at plan creation or
  * after an iteration).  No counterpart in the reference. */
 int blco_cpals_plan_condition(const blco_cpals_plan* p, double* cond, int* promoted);
+/* Device bytes the plan holds: the caller's FP64 factors and lambda, its
+ * workspace and, for a streamed tensor, the ring of block buffers, which is
+ * sized so that the total stays within opts.residency_bytes.  No
+ * counterpart in the reference. */
+int blco_cpals_plan_device_bytes(const blco_cpals_plan* p, uint64_t* bytes);
 int blco_cpals_plan_destroy(blco_cpals_plan* p);
 
 /* Sharded CP-ALS (several processes, one GPU each, each holding a share of

@@ -138,7 +138,7 @@ def test_mttkrp_host_entry_and_streamed_blocks(blco):
     for m in range(3):
         ref = po.mttkrp_coo(cidx, vals, fs, m)
         _close(blco.mttkrp_host(t_res, m, fs), ref)
-        _close(blco.mttkrp_host(t_str, m, fs, opts=blco.make_opts(stream_data=True, residency_bytes=3 * 7000 * 16)), ref)
+        _close(blco.mttkrp_host(t_str, m, fs, opts=blco.make_opts(stream_data=True, residency_bytes=1_200_000 + 3 * 7000 * 16)), ref)
 
 
 def test_mttkrp_argument_errors(blco):

@@ -118,24 +118,62 @@ def test_streamed_mixed_mttkrp_matches_resident(blco):
     ref.free()
 
 
-def test_streamed_blocks_larger_than_the_budget(blco):
+@pytest.mark.parametrize("dtype", ["f64", "f32", "bf16"])
+def test_streamed_blocks_larger_than_the_budget(blco, dtype):
     """Blocks of 200k nonzeros under a 2 MiB budget: the ring copies
     budget-sized pieces of each block, and the MTTKRP equals the resident
-    one (1e-12)."""
+    one (FP64 1e-12; the mixed forms stream 4-byte values into buffers sized
+    for 8 and flush their own heavy-row sums per piece: 1e-5)."""
     import torch
     cidx, vals = _tensor(9)
     R = 8
     rng = np.random.default_rng(10)
     fs = [torch.from_numpy(rng.random((d, R))).cuda() for d in DIMS]
+    tdt, code, tol = {"f64": (torch.float64, blco.DTYPE_F64, 1e-12), "f32": (torch.float32, blco.DTYPE_F32, 1e-5),
+                      "bf16": (torch.bfloat16, blco.DTYPE_BF16, 1e-5)}[dtype]
+    fs = [f.to(tdt) for f in fs]
+    otype = torch.float64 if dtype == "f64" else torch.float32
     ref = blco.Tensor.encode(DIMS, cidx, vals, 200_000)
     t = blco.Tensor.encode(DIMS, cidx, vals, 200_000, opts=blco.make_opts(stream_data=True))
     for m in range(3):
-        o1 = torch.zeros(DIMS[m], R, dtype=torch.float64, device="cuda")
-        o2 = torch.zeros(DIMS[m], R, dtype=torch.float64, device="cuda")
-        blco.mttkrp(ref, m, fs, o1)
-        blco.mttkrp(t, m, fs, o2, _opts(blco, 2 << 20))
+        o1 = torch.zeros(DIMS[m], R, dtype=otype, device="cuda")
+        o2 = torch.zeros(DIMS[m], R, dtype=otype, device="cuda")
+        blco.mttkrp_ex(ref, m, fs, o1, code)
+        blco.mttkrp_ex(t, m, fs, o2, code, _opts(blco, 2 << 20))
         torch.cuda.synchronize()
-        x, y = o1.cpu().numpy(), o2.cpu().numpy()
-        assert np.linalg.norm(x - y) <= 1e-12 * np.linalg.norm(x), m
+        x, y = o1.double().cpu().numpy(), o2.double().cpu().numpy()
+        assert np.linalg.norm(x - y) <= tol * np.linalg.norm(x), m
+    t.free()
+    ref.free()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_streamed_cpals_under_a_budget_smaller_than_two_blocks(blco, precision):
+    """A streamed CP-ALS plan whose budget leaves less than two blocks of
+    200k nonzeros for the ring: pieces of blocks stream through it, the fits
+    follow the resident plan's, and the plan's device bytes stay within the
+    budget."""
+    import torch
+    cidx, vals = _tensor(11)
+    R = 8
+    rng = np.random.default_rng(12)
+    fs0 = [rng.random((d, R)) for d in DIMS]
+    prec = blco.PRECISION_FP64 if precision == "fp64" else blco.PRECISION_MIXED
+    budget = 3 << 20
+    ref = blco.Tensor.encode(DIMS, cidx, vals, 200_000)
+    t = blco.Tensor.encode(DIMS, cidx, vals, 200_000, opts=blco.make_opts(stream_data=True))
+    fits = []
+    for tens, opts in ((ref, blco.make_opts(precision=prec)),
+                       (t, blco.make_opts(stream_data=True, precision=prec, residency_bytes=budget))):
+        dfs = [torch.from_numpy(f.copy()).cuda() for f in fs0]
+        lam = torch.ones(R, dtype=torch.float64, device="cuda")
+        plan = blco.CpalsPlan(tens, dfs, lam, opts)
+        fits.append(np.array(plan.iterate(6, tol=-1.0)))
+        if tens is t:
+            used = plan.device_bytes()
+            assert 0 < used <= budget, used
+        plan.destroy()
+    tol = 1e-10 if precision == "fp64" else 1e-6
+    assert np.allclose(fits[0], fits[1], rtol=0, atol=tol), np.abs(fits[0] - fits[1]).max()
     t.free()
     ref.free()
