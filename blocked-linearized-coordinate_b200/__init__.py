@@ -66,7 +66,7 @@ EXPORTS = (
     "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
     "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
     "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_gram_f32",
-    "blco_encode_tns", "blco_parse_decimal", "blco_launch_count", "blco_cpals_plan_set_reduce",
+    "blco_encode_tns", "blco_gram_tc_timeout_check", "blco_parse_decimal", "blco_launch_count", "blco_cpals_plan_set_reduce",
     "blco_cpals_plan_set_norm_sq", "blco_tensor_fibre_stats",
 )
 
@@ -184,14 +184,15 @@ def launch_count(reset=False):
 
 
 def make_opts(kernel=KERNEL_AUTO, nprtn=0, thread_cf=2, stream_data=False, precision=PRECISION_FP64,
-              verbose=False, device=0, residency_bytes=0, stream=None, gram_tensor_cores=False, solve=SOLVE_AUTO,
+              verbose=False, device=0, residency_bytes=0, stream=None, gram_tensor_cores=None, solve=SOLVE_AUTO,
               guard_cond=0.0):
     o = Opts()
     lib().blco_opts_init(ctypes.byref(o))
     o.kernel, o.nprtn, o.thread_cf = kernel, nprtn, thread_cf
     o.stream_data, o.precision, o.verbose = int(stream_data), precision, int(verbose)
     o.device, o.residency_bytes = device, residency_bytes
-    o.gram_tensor_cores = int(gram_tensor_cores)
+    # None: the default engine per rank; True / False: tensor / CUDA cores
+    o.gram_tensor_cores = 0 if gram_tensor_cores is None else (1 if gram_tensor_cores else -1)
     o.solve, o.guard_cond = int(solve), float(guard_cond)
     if stream is None:
         try:
@@ -641,6 +642,14 @@ def select(t, mode, rank, factor_dtype=DTYPE_F64, net=None, margin=0.1, opts=Non
     _check(lib().blco_select(t.handle, mode, rank, factor_dtype, net.handle if net is not None else None,
                              ctypes.c_float(margin), ctypes.byref(o), ctypes.byref(cfg), ctypes.byref(sw)))
     return cfg.value, bool(sw.value)
+
+
+def gram_tc_timeout_check(device=0):
+    """(status of a tensor-core Gram launch whose completion wait is made to
+    run out, status of an ordinary launch after it)."""
+    a, b = ctypes.c_int(), ctypes.c_int()
+    _check(lib().blco_gram_tc_timeout_check(device, ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
 
 
 def gram_f32(U, tensor_cores=True):

@@ -547,6 +547,13 @@ int blco_gram_f32(const float* d_U, uint64_t I, int rank, double* d_G, int tenso
                     static_cast<cudaStream_t>(stream));
 }
 
+int blco_gram_tc_timeout_check(int device, int* timeout_status, int* after_status)
+{
+    if (!timeout_status || !after_status) return fail(BLCO_ERR_INVALID, "null argument");
+    *timeout_status = *after_status = -1;
+    return gram_tc_timeout_check(device, timeout_status, after_status);
+}
+
 int blco_encode_tns(const char* path, uint64_t max_block_size, const blco_opts* opts, blco_tensor** out,
                     blco_tns_info* info)
 {

@@ -938,6 +938,71 @@ int export_factors(blco_cpals_plan* p)
 
 } // namespace
 
+// Self-check of the tensor-core Gram's bounded wait: one launch on a small
+// matrix that issues no MMA and no commit (so its wait on the completion
+// barrier runs out after 64 polls), then an ordinary launch on the same
+// device.  *timeout_status: what the first reported (BLCO_ERR_TIMEOUT
+// expected); *after_status: the second's status, BLCO_OK when it ran and its
+// Gram is exact (the first freed its TMEM and left the context usable).
+int gram_tc_timeout_check(int device, int* timeout_status, int* after_status)
+{
+    BLCO_CUDA(cudaSetDevice(device));
+    int sm = 0;
+    BLCO_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device));
+    const int R = 8;
+    const uint64_t I = 200;
+    float* U = nullptr;
+    double* parts = nullptr;
+    double* G = nullptr;
+    int* d_err = nullptr;
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&U, I * R * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&parts, (size_t)gram_tc_max_ctas(sm) * R * R * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&G, (size_t)R * R * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_err, sizeof(int));
+    std::vector<float> h(I * R);
+    for (uint64_t k = 0; k < I * R; k++) h[k] = (float)((int)(k % 7) - 3); // small integers: an exact Gram
+    if (e == cudaSuccess) e = cudaMemcpy(U, h.data(), I * R * sizeof(float), cudaMemcpyHostToDevice);
+    int st = e == cudaSuccess ? BLCO_OK : cuda_fail(e, "Gram self-check buffers", __FILE__, __LINE__);
+    for (int pass = 0; pass < 2 && st == BLCO_OK; pass++) {
+        int herr = 0, np = 0;
+        e = cudaMemsetAsync(d_err, 0, sizeof(int), s);
+        if (e != cudaSuccess) { st = cuda_fail(e, "memset", __FILE__, __LINE__); break; }
+        st = gram_tc_launch(U, I, R, nullptr, nullptr, parts, sm, d_err, s, &np, pass == 0 ? 64u : 0u,
+                            pass == 0 ? 1 : 0);
+        if (st != BLCO_OK) break;
+        k_sum_partials<<<(R * R * 32 + 255) / 256, 256, 0, s>>>(parts, np, R * R, G);
+        count_launch();
+        e = cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { st = cuda_fail(e, "Gram self-check", __FILE__, __LINE__); break; }
+        int res = herr ? BLCO_ERR_TIMEOUT : BLCO_OK;
+        if (pass == 1 && res == BLCO_OK) {
+            std::vector<double> g(R * R);
+            e = cudaMemcpy(g.data(), G, g.size() * sizeof(double), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) { st = cuda_fail(e, "Gram self-check", __FILE__, __LINE__); break; }
+            for (int a = 0; a < R && res == BLCO_OK; a++)
+                for (int c = 0; c < R; c++) {
+                    double want = 0.0;
+                    for (uint64_t k = 0; k < I; k++) want += (double)h[k * R + a] * h[k * R + c];
+                    if (g[a * R + c] != want) {
+                        res = fail(BLCO_ERR_CUDA, "tensor-core Gram self-check: the Gram after the timeout is wrong");
+                        break;
+                    }
+                }
+        }
+        *(pass == 0 ? timeout_status : after_status) = res;
+    }
+    if (s) cudaStreamSynchronize(s);
+    cudaFree(U);
+    cudaFree(parts);
+    cudaFree(G);
+    cudaFree(d_err);
+    if (s) cudaStreamDestroy(s);
+    return st;
+}
+
 int gram_f32(float* U, uint64_t I, int R, double* G, bool tensor_cores, int sm, cudaStream_t s)
 {
     return gram_f32_impl(U, I, R, G, tensor_cores, sm, s);
@@ -994,7 +1059,9 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
                       : p->mixed                                     ? BLCO_DTYPE_F32
                                                                      : BLCO_DTYPE_F64;
     if (p->mixed) {
-        p->gram_tc = R <= 64 && p->opts.gram_tensor_cores;
+        // tensor-core Grams: by default up to rank 32 (above it the CUDA-core
+        // Gram is the faster), on request up to 64
+        p->gram_tc = p->opts.gram_tensor_cores > 0 ? R <= 64 : p->opts.gram_tensor_cores == 0 && R <= 32;
         if (p->gram_tc) {
             PCA(&p->tc_partials, (size_t)gram_tc_max_ctas(p->sm) * R * R * sizeof(double));
             PCA(&p->d_err, sizeof(int));

@@ -1566,8 +1566,11 @@ int encode_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const uint64_t* 
 // Limits and sharing: at most BLCO_NOALLOC_MAX_NNZ nonzeros; one array per
 // device shared by every call, so calls that overlap on the GPU (other
 // streams, other host threads) race and must be serialised by the caller.
-// The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress; make that first call before any stream capture.
+// Every call looks up the array's device address (cudaGetSymbolAddress);
+// the first call on a device also does the library's set-up there (loading
+// its device code), so make that first call before any stream capture.
+// Every call synchronises its stream twice: after the copy of the encoder's
+// tables from pageable host memory, and to read back the range check.
 
 namespace {
 
@@ -1618,20 +1621,14 @@ int radix_sort_pairs_in(uint64_t* k0, double* v0, uint64_t* k1, double* v1, uint
 
 } // namespace
 
-// Device address of g_noalloc_scratch for the current device.
-static int noalloc_scratch(int device, unsigned char** out)
+// Device address of g_noalloc_scratch in the current context, looked up on
+// every call (a cached address would go stale after a device reset).
+static int noalloc_scratch(unsigned char** out)
 {
-    static std::mutex mu;
-    static unsigned char* ptr[64] = {};
-    if (device < 0 || device >= 64) return fail(BLCO_ERR_INVALID, "bad device ordinal");
-    std::lock_guard<std::mutex> g(mu);
-    if (!ptr[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
-        ptr[device] = static_cast<unsigned char*>(p);
-    }
-    *out = ptr[device];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+    *out = static_cast<unsigned char*>(p);
     return BLCO_OK;
 }
 
@@ -1655,7 +1652,7 @@ int encode_noalloc_impl(int nmodes, const uint64_t* dims, uint64_t nnz, const ui
     DeviceInfo di;
     BLCO_TRY(device_info(device, &di));
     unsigned char* base = nullptr;
-    BLCO_TRY(noalloc_scratch(device, &base));
+    BLCO_TRY(noalloc_scratch(&base));
     uint64_t* k1 = reinterpret_cast<uint64_t*>(base + NA_K1);
     double* v1 = reinterpret_cast<double*>(base + NA_V1);
     uint32_t* counts = reinterpret_cast<uint32_t*>(base + NA_COUNTS);

@@ -300,9 +300,13 @@ int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda,
 // gram_tc.cu: the mixed form's Gram (and optional scale / BF16 copy) on the
 // tensor cores; writes *nparts FP64 R x R partials (at most
 // gram_tc_max_ctas(sm)), sets *d_err when an MMA completion wait times out.
+// spin_max: polls per wait (0: the default, 2^24); no_commit (self-test of
+// the timeout path only): issue no MMA and no commit, so the first wait runs
+// out.
 int gram_tc_max_ctas(int sm);
 int gram_tc_launch(float* U, uint64_t I, int R, const double* inv, uint16_t* bf16_out, double* partials, int sm,
-                   int* d_err, cudaStream_t s, int* nparts);
+                   int* d_err, cudaStream_t s, int* nparts, uint32_t spin_max = 0, int no_commit = 0);
+int gram_tc_timeout_check(int device, int* timeout_status, int* after_status);
 
 // cpals.cu: standalone Gram of a device FP32 matrix (tensor or CUDA cores).
 int gram_f32(float* U, uint64_t I, int R, double* G, bool tensor_cores, int sm, cudaStream_t s);

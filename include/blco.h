@@ -121,12 +121,12 @@ typedef struct blco_opts {
     int device;            /* --device */
     uint64_t residency_bytes; /* device budget for streamed blocks; 0 = 8 GiB */
     void* stream;          /* cudaStream_t to run on; NULL = the default stream */
-    int gram_tensor_cores; /* mixed forms: 1 = Gram products on the tensor
-                              cores (tcgen05, split-BF16, rank <= 64); 0
-                              (default) = FP64 on the CUDA cores.  The tensor
-                              cores' FP32 accumulation leans low (~1e-7
-                              relative per 64-row tile), which moves the fit
-                              of a 200M-nonzero tensor by ~1e-4 */
+    int gram_tensor_cores; /* mixed forms' Grams (blco_gram_f32's two
+                              engines): 0 (default) = on the tensor cores
+                              (tcgen05, exact integer digit products) up to
+                              rank 32, FP64 on the CUDA cores above; 1 = on
+                              the tensor cores up to rank 64; -1 = on the
+                              CUDA cores */
     int solve;             /* BLCO_SOLVE_AUTO: Cholesky of the R x R system,
                               the pseudoinverse when it is not positive
                               definite; BLCO_SOLVE_PINV: the reference's
@@ -218,10 +218,14 @@ int blco_encode_device(int nmodes, const uint64_t* dims, uint64_t nnz,
  *     rejected with BLCO_ERR_UNSUPPORTED;
  *   - every call on a device shares that one array: calls that overlap on
  *     the GPU (other streams or host threads) race, so serialise them;
- *   - the first call on a device looks up the array's address with
- *     cudaGetSymbolAddress; make that first call before any stream capture.
- * Runs on `stream` (NULL = default stream) and returns after the stream has
- * finished the encode (it reads back the coordinate-range check). */
+ *   - the first call on a device does the library's set-up there (loading
+ *     its device code, looking up the array's address): make that first
+ *     call before any stream capture.
+ * Runs on `stream` (NULL = default stream) and synchronises it twice: after
+ * copying the encoder's tables from pageable host memory, and to read back
+ * the coordinate-range check, so it returns after the encode has finished.
+ * A device reset (cudaDeviceReset) between calls is allowed: every call
+ * looks up the array's address again. */
 #define BLCO_NOALLOC_MAX_NNZ 1900000ull
 int blco_encode_device_noalloc(int nmodes, const uint64_t* dims, uint64_t nnz,
                                const uint64_t* const* d_cidx, const double* d_vals,
@@ -446,13 +450,24 @@ int blco_select(blco_tensor* t, int mode, int rank, int factor_dtype, blco_mlp* 
                 float margin, const blco_opts* opts, int* config, int* used_sweep);
 
 /* G = U^T U for a device FP32 matrix U (I x rank, row-major, rank 1..64),
- * G (device, rank x rank FP64).  tensor_cores 1: split-BF16 products on the
- * tensor cores (each value as bf16 hi + bf16 lo, FP32 accumulation over
- * 64-row tiles, FP64 beyond); 0: FP64 products on the CUDA cores.  The
- * Gram of the reference's ata_gpu (src/cpd_gpu.cu:547-568) for the mixed
- * form's FP32 factors.  Synchronous on `stream` (NULL: default stream). */
+ * G (device, rank x rank FP64).  tensor_cores 1: products on the tensor
+ * cores (per 64-row tile and column, a power-of-two scale and three 8-bit
+ * integer digits per value, exact integer sums in the FP32 accumulator,
+ * FP64 beyond the tile; each value to within 2^-25 of its tile column's
+ * largest magnitude); 0: FP64 products on the CUDA cores.  The Gram of the
+ * reference's ata_gpu (src/cpd_gpu.cu:547-568) for the mixed form's FP32
+ * factors.  Synchronous on `stream` (NULL: default stream). */
 int blco_gram_f32(const float* d_U, uint64_t I, int rank, double* d_G, int tensor_cores, int device,
                   void* stream);
+
+/* Self-check of the tensor-core Gram's bounded wait on its MMA completion
+ * barrier: one launch that issues no MMA and no commit, so that its wait
+ * runs out (after 64 polls), then an ordinary launch.  *timeout_status
+ * receives the first launch's status (BLCO_ERR_TIMEOUT when the kernel
+ * reported the timeout), *after_status the second's (BLCO_OK when it ran
+ * and its Gram was exact: the first freed its tensor memory).  Returns an
+ * error only when the check itself could not run. */
+int blco_gram_tc_timeout_check(int device, int* timeout_status, int* after_status);
 
 /* ---- .tns text loading on the GPU (the reference's read_tns_dims /
  * read_tns_data, src/sptensor.cpp:74-160, feeding the encoder directly). */

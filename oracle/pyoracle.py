@@ -68,6 +68,10 @@ def ref_lib():
         R.ref_alto_create128.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int]
         R.ref_alto_mttkrp128.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         R.ref_alto_destroy128.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        R.ref_tns_import.restype = ctypes.c_void_p
+        R.ref_tns_import.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), _u64p, _u64p]
+        R.ref_tns_copy.argtypes = [ctypes.c_void_p, _u64p, _f64p]
+        R.ref_tns_free.argtypes = [ctypes.c_void_p]
         R.ref_cpd_alto.restype = ctypes.c_int
         R.ref_cpd_alto.argtypes = [ctypes.c_int, _u64p, ctypes.c_uint64, _u64p, _f64p, ctypes.c_int, ctypes.c_void_p,
                                    _f64p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _f64p, _f64p, _f64p]
@@ -98,6 +102,24 @@ def ref_cpd_alto(dims, cidx, vals, factors, lam, iters, epsilon=0.0, nthreads=No
         raise RuntimeError("cpd_alto report not found")
     return dict(iters=n, ms_per_iter=float(out[0]), mttkrp_ms_per_iter=float(out[1]), fit=float(out[2]),
                 threads=nthreads)
+
+
+def ref_import_tns(path):
+    """The reference's .tns reader (ImportSparseTensor, src/sptensor.cpp:162)
+    through oracle/_ref: (dims, cidx (nmodes x nnz, 0-based), vals)."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref/libblco_ref.so is not built")
+    nm = ctypes.c_int()
+    dims = np.zeros(8, dtype=np.uint64)
+    nnz = np.zeros(1, dtype=np.uint64)
+    h = R.ref_tns_import(os.fsencode(path), ctypes.byref(nm), _p(dims, _u64p), _p(nnz, _u64p))
+    n = int(nnz[0])
+    cidx = np.zeros((nm.value, n), dtype=np.uint64)
+    vals = np.zeros(n, dtype=np.float64)
+    R.ref_tns_copy(h, _p(cidx, _u64p), _p(vals, _f64p))
+    R.ref_tns_free(h)
+    return [int(d) for d in dims[:nm.value]], cidx, vals
 
 
 def alto_masks(dims):

@@ -326,3 +326,28 @@ extern "C" int ref_cpd_alto(int nmodes, const uint64_t* dims, uint64_t nnz, cons
     fclose(cap);
     return per == 2 ? iters : -1;
 }
+
+// The reference's .tns text reader, ImportSparseTensor with TEXT_FORMAT
+// (src/sptensor.cpp:74-207): returns its SparseTensor with the mode count,
+// lengths (largest 1-based index per mode) and nonzero count; ref_tns_copy
+// copies the 0-based coordinates (nmodes x nnz) and the values out, and
+// ref_tns_free frees the tensor.
+extern "C" void* ref_tns_import(const char* path, int* nmodes, uint64_t* dims, uint64_t* nnz)
+{
+    SparseTensor* X = nullptr;
+    ImportSparseTensor(path, TEXT_FORMAT, &X);
+    fflush(stdout);
+    *nmodes = X->nmodes;
+    for (int n = 0; n < X->nmodes; n++) dims[n] = X->dims[n];
+    *nnz = X->nnz;
+    return X;
+}
+
+extern "C" void ref_tns_copy(void* h, uint64_t* cidx, double* vals)
+{
+    const SparseTensor* X = static_cast<const SparseTensor*>(h);
+    for (int n = 0; n < X->nmodes; n++) memcpy(cidx + (size_t)n * X->nnz, X->cidx[n], sizeof(uint64_t) * X->nnz);
+    memcpy(vals, X->vals, sizeof(double) * X->nnz);
+}
+
+extern "C" void ref_tns_free(void* h) { DestroySparseTensor(static_cast<SparseTensor*>(h)); }

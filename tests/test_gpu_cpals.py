@@ -151,7 +151,7 @@ def test_cpals_streamed_blocks_match_resident(blco):
     assert np.allclose(fits_str, fits_o, rtol=0, atol=1e-10)
     _, fits_mix = blco.cpals(t_str, [x.copy() for x in fs0], np.ones(R), 12, 0.0,
                              blco.make_opts(stream_data=True, precision=blco.PRECISION_MIXED,
-                                            residency_bytes=700_000 + 3 * 7000 * 16))
+                                            residency_bytes=1_400_000 + 3 * 7000 * 16))
     _, fits_mix_res = blco.cpals(t_res, [x.copy() for x in fs0], np.ones(R), 12, 0.0,
                                  blco.make_opts(precision=blco.PRECISION_MIXED))
     assert len(fits_mix) == 12

@@ -145,3 +145,80 @@ def test_gpu_loader_errors(blco, tmp_path):
     with pytest.raises(blco.BlcoError) as e:
         blco.Tensor.encode_tns(str(tmp_path / "missing.tns"))
     assert e.value.status == blco.ERR_IO
+
+
+def _edge_files():
+    """.tns files whose every line the reference's reader defines
+    (src/sptensor.cpp:74-160): comments, empty lines, tabs and runs of
+    spaces, leading blanks, signed and exponent and hexadecimal values, long
+    significands, CRLF data lines, trailing blanks after the first data line,
+    duplicates, one file without a final newline; 3 to 5 modes."""
+    rng = np.random.default_rng(31)
+    pyr = random.Random(32)
+    files = {}
+    for name, dims, nnz in (("three", [50, 7, 300], 4000), ("five", [9, 4, 200, 3, 60], 3000),
+                            ("one", [5, 5, 5], 1)):
+        cidx = unique_coords(rng, dims, nnz)
+        if nnz > 1:
+            cidx = np.concatenate([cidx, cidx[:, :25]], axis=1)  # duplicates, later in the file
+        vals = rng.standard_normal(cidx.shape[1]) * 10.0 ** rng.integers(-12, 12, size=cidx.shape[1])
+        lines = ["# a comment line\n", "\n", "#\tanother\n"]
+        for i in range(cidx.shape[1]):
+            sep = pyr.choice([" ", "\t", "   ", " \t "])
+            lead = "" if i == 0 else pyr.choice(["", " ", "\t"])
+            idx = sep.join(str(int(c) + 1) for c in cidx[:, i])
+            v = float(vals[i])
+            s = pyr.choice(["%.17g", "%+.17e", "%.25g", "%.6E", "%r"])
+            s = repr(v) if s == "%r" else s % v
+            if i % 101 == 7:
+                s = pyr.choice(["0x1.8p-3", "-0X1P+4", "1e23", "+.5", "-0.0"])
+            eol = "\n" if i == 0 else pyr.choice(["\n", "\r\n", " \n", "\t\n"])
+            lines.append(lead + idx + sep + s + eol)
+            if pyr.random() < 0.02:
+                lines.append(pyr.choice(["# comment\n", "\n"]))
+        if name == "five":
+            lines[-1] = lines[-1].rstrip("\n").rstrip("\r")
+        files[name] = lines
+    return files
+
+
+@pytest.mark.gpu
+def test_gpu_loader_matches_reference_reader(blco, tmp_path):
+    """blco_encode_tns against the reference's own reader
+    (ImportSparseTensor, src/sptensor.cpp:162, built in oracle/_ref) on the
+    same files: mode count, lengths, nnz, and the encoding of the reference's
+    COO arrays, bit for bit."""
+    import pyoracle as po
+    if po.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    for name, lines in _edge_files().items():
+        p = str(tmp_path / f"{name}.tns")
+        _write(p, lines)
+        dims, cidx, vals = po.ref_import_tns(p)
+        t, info = blco.Tensor.encode_tns(p)
+        assert info["nmodes"] == len(dims) and info["dims"] == dims and info["nnz"] == len(vals), name
+        ref = blco.Tensor.encode(dims, cidx, vals)
+        a, b = t.copy_out(), ref.copy_out()
+        assert np.array_equal(a["coords"], b["coords"]), name
+        assert np.array_equal(a["vals"].view(np.uint64), b["vals"].view(np.uint64)), name
+        t.free()
+        ref.free()
+
+
+def test_reference_reader_on_edge_files(tmp_path):
+    """The reference reader (oracle/_ref) on the edge files against a plain
+    Python reading of the same lines (split on blanks, float() values, hex
+    through float.fromhex): pins the harness the GPU test compares with."""
+    import pyoracle as po
+    if po.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    for name, lines in _edge_files().items():
+        p = str(tmp_path / f"{name}.tns")
+        _write(p, lines)
+        dims, cidx, vals = po.ref_import_tns(p)
+        data = [l.split() for l in lines if len(l) > 1 and not l.startswith("#")]
+        want_c = np.array([[int(x) - 1 for x in f[:-1]] for f in data], dtype=np.uint64).T
+        want_v = np.array([float.fromhex(f[-1]) if "x" in f[-1].lower() else float(f[-1]) for f in data])
+        assert dims == [int(c.max()) + 1 for c in want_c], name
+        assert np.array_equal(cidx, want_c), name
+        assert np.array_equal(vals.view(np.uint64), want_v.view(np.uint64)), name

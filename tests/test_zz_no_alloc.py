@@ -44,6 +44,47 @@ def test_noalloc_encode_matches_allocating_encode_twice(blco):
         assert np.array_equal(v_na, ref["vals"])
 
 
+def test_noalloc_at_the_maximum_size_matches_the_oracle(blco):
+    """Exactly BLCO_NOALLOC_MAX_NNZ nonzeros (the scratch layout's limit),
+    skewed coordinates over four modes, against the oracle's encoder."""
+    import pyoracle as po
+    rng = np.random.default_rng(77)
+    dims = [150_000, 90_000, 4_000, 37]
+    nnz = int(blco.NOALLOC_MAX_NNZ)
+    cidx = unique_coords(rng, dims, nnz, 1.0)
+    vals = rng.standard_normal(nnz)
+    c_na, v_na = _noalloc(blco, dims, cidx, vals)
+    enc = po.blco_encode(dims, cidx, vals)
+    assert np.array_equal(c_na, enc["coords"])
+    assert np.array_equal(v_na.view(np.uint64), enc["vals"].view(np.uint64))
+
+
+def test_noalloc_allocates_no_device_memory(blco):
+    """After a first call (the library's set-up on this device), an encode
+    leaves the device's free memory unchanged: inputs and outputs are the
+    caller's, the scratch is the library's fixed array."""
+    import torch
+    rng = np.random.default_rng(78)
+    dims = [40_000, 30_000, 500]
+    nnz = 1_000_000
+    cidx = unique_coords(rng, dims, nnz, 0.8)
+    vals = rng.random(nnz)
+    d_c = [torch.from_numpy(cidx[n].astype(np.int64)).cuda() for n in range(3)]
+    d_v = torch.from_numpy(vals).cuda()
+    out_c = torch.empty(nnz, dtype=torch.int64, device="cuda")
+    out_v = torch.empty(nnz, dtype=torch.float64, device="cuda")
+    blco.encode_device_noalloc(dims, d_c, d_v, out_c, out_v)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        blco.encode_device_noalloc(dims, d_c, d_v, out_c, out_v)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    ref = blco.Tensor.encode(dims, cidx, vals).copy_out()
+    assert np.array_equal(out_c.cpu().numpy().view(np.uint64), ref["coords"])
+
+
 def test_noalloc_limits_and_errors(blco):
     import torch
     dims = [10, 10, 10]
