@@ -1,7 +1,13 @@
 """CP-ALS benchmark on the Zipf(1.1) 2M x 2M x 25k, 200M-nonzero, rank-32
 workload, one B200 per rank.  The plain FP64 form and the mixed-precision
 forms run on the same tensor and initial factors; the headline value is the
-fastest mixed form whose final fit is within 1e-5 of the FP64 form's.
+fastest mixed form whose final fit is within 1e-5 of the FP64 form's.  The
+fits are compared after --fit-iters (40) iterations of the same run (the
+timed steps, then untimed ones): while the fit still climbs steeply (about
+5e-4 per iteration near iteration 10), the mixed forms' trajectories run a
+little ahead of or behind the FP64 one, by up to a few 1e-5, and meet it
+again near convergence; the largest gap over the run and the gap at the end
+of the timed steps are reported beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -144,6 +150,18 @@ def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+def all_ranks(x, dist, device="cuda"):
+    """Every rank's value of a per-rank float, in rank order ([x] without a
+    process group)."""
+    if not dist:
+        return [float(x)]
+    import torch
+    tt = torch.zeros(dist.get_world_size(), dtype=torch.float64, device=device)
+    tt[dist.get_rank()] = float(x)
+    dist.all_reduce(tt)
+    return [float(v) for v in tt.tolist()]
 
 
 def max_over_ranks(x, dist, device="cuda"):
@@ -380,14 +398,20 @@ FORMS = {
 }
 
 
-def time_form(pkg, torch, t, dims, rk, fs0, form, args, stream, dist):
+def time_form(pkg, torch, t, dims, rk, fs0, form, args, stream, dist, norm_sq=None):
     """Warm up, then time args.steps CP-ALS iterations of one numeric form.
+    With norm_sq (a tensor sharded over the ranks), each mode's MTTKRP is
+    summed over the ranks by an all-reduce on the plan's stream and the fit
+    uses the whole tensor's norm.
     Returns dict(ms_per_step, mttkrp_ms (per mode), fits, launches, clocks)."""
     prec = getattr(pkg, FORMS[form][0])
     opts = pkg.make_opts(kernel=args.kernel, precision=prec, stream=stream.cuda_stream)
     fs = [f.clone() for f in fs0]
     lam = torch.ones(rk, dtype=torch.float64, device="cuda")
     plan = pkg.CpalsPlan(t, fs, lam, opts)
+    if norm_sq is not None:
+        plan.set_reduce(pkg.dist_reduce(dist))
+        plan.set_norm_sq(norm_sq)
     fits = plan.iterate(args.warmup, tol=-1.0)
     ms0, calls0 = plan.mttkrp_ms()
     torch.cuda.synchronize()
@@ -406,11 +430,17 @@ def time_form(pkg, torch, t, dims, rk, fs0, form, args, stream, dist):
     ck = clocks.stop()
     elapsed = ev0.elapsed_time(ev1)
     ms1, calls1 = plan.mttkrp_ms()
+    timed_end = len(fits)
+    # untimed: the same run continued to args.fit_iters iterations, where the
+    # forms' fits are compared (the decomposition's fit, near convergence)
+    if args.fit_iters > len(fits):
+        fits += plan.iterate(args.fit_iters - len(fits), tol=-1.0)
     plan.destroy()
     del fs, lam
+    per_rank = all_ranks(elapsed / args.steps, dist)
     elapsed = max_over_ranks(elapsed, dist)
     return dict(ms_per_step=elapsed / args.steps, mttkrp_ms=list((ms1 - ms0) / max(1, calls1 - calls0)),
-                fits=fits, launches=int(launches), clocks=ck)
+                fits=fits, timed_end=timed_end, launches=int(launches), clocks=ck, ms_per_step_per_rank=per_rank)
 
 
 def c1_leg(pkg, torch, args):
@@ -596,6 +626,105 @@ def wide_leg(pkg, torch, args, peak, with_cpu):
                 cpu_baseline=cpu)
 
 
+STREAMED = dict(workload="cpals_streamed_zipf0.9_500kx200kx50kx1k_r64", dims=[500_000, 200_000, 50_000, 1_000],
+                zipf=0.9, rank=64, full_nnz=2_000_000_000, residency=8_000_000_000, block=64 << 20,
+                values="uniform(0,1) fp32 as fp64, repeated coordinates kept as separate nonzeros")
+
+
+def pinned_h2d_peak(torch, gib=2, reps=3):
+    """Host-to-device GB/s of one pinned copy of `gib` GiB, best of `reps`."""
+    hb = torch.empty(gib << 27, dtype=torch.float64).pin_memory()
+    db = torch.empty(gib << 27, dtype=torch.float64, device="cuda")
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(reps):
+        e0.record()
+        db.copy_(hb, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, hb.numel() * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    del hb, db
+    return best
+
+
+def streamed_leg(pkg, torch, args):
+    """The out-of-memory streamed CP-ALS: the 4-mode Zipf(0.9) 500k x 200k x
+    50k x 1k tensor at rank 64, blocks of 64M nonzeros kept in pinned host
+    memory and copied through a ring of device buffers, with the whole
+    plan's device memory (factors, workspace, ring) capped at 8e9 bytes.
+    Each iteration copies every block once per mode, so the bound is the
+    host link: H2D bytes per iteration over the time, against a pinned copy
+    measured in the same process.  FP64 and the mixed FP32 form (4-byte
+    values streamed from a pinned FP32 copy)."""
+    from blco_b200 import synth
+    W = STREAMED
+    dims, rk, nnz = W["dims"], W["rank"], args.streamed_nnz
+    peak = pinned_h2d_peak(torch)
+    X = synth.zipf_coo_device(nnz, dims, W["zipf"], seed=args.seed)
+    torch.cuda.synchronize()
+    o = pkg.make_opts(kernel=10, stream_data=True, residency_bytes=W["residency"])
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"], W["block"], o)
+    torch.cuda.synchronize()
+    encode_s = time.perf_counter() - t0
+    del X
+    torch.cuda.empty_cache()
+    info = t.info()
+    g = torch.Generator(device="cuda").manual_seed(1234)
+    fs0 = [torch.rand(d, rk, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    forms = {}
+    for name, prec, bpn in (("fp64", pkg.PRECISION_FP64, 16), ("mixed_f32", pkg.PRECISION_MIXED, 12)):
+        fs = [f.clone() for f in fs0]
+        lam = torch.ones(rk, dtype=torch.float64, device="cuda")
+        plan = pkg.CpalsPlan(t, fs, lam, pkg.make_opts(kernel=10, stream_data=True, residency_bytes=W["residency"],
+                                                       precision=prec))
+        plan.iterate(1, tol=-1.0)
+        torch.cuda.synchronize()
+        free_b, total_b = torch.cuda.mem_get_info()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fits = plan.iterate(args.streamed_iters, tol=-1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.streamed_iters
+        h2d = len(dims) * nnz * bpn
+        forms[name] = dict(ms_per_iter=ms, h2d_bytes_per_iter=h2d, h2d_gbs=h2d / (ms * 1e-3) / 1e9,
+                           h2d_frac=h2d / (ms * 1e-3) / 1e9 / peak, fit_last=fits[-1],
+                           device_bytes_plan=int(plan.device_bytes()),
+                           device_bytes_in_use=int(total_b - free_b))
+        plan.destroy()
+        del fs, lam
+    forms["mixed_f32"]["fit_delta_vs_fp64"] = abs(forms["mixed_f32"]["fit_last"] - forms["fp64"]["fit_last"])
+    t.free()
+    del fs0
+    torch.cuda.empty_cache()
+    return dict(workload=W["workload"] + (f"_nnz{nnz // 1_000_000}M" if nnz != W["full_nnz"] else "_nnz2B"),
+                dims=dims, nnz=nnz, full_nnz=W["full_nnz"], rank=rk, zipf=W["zipf"], values=W["values"],
+                residency_bytes=W["residency"], block_nnz=W["block"], blocks=info["block_count"],
+                iters_timed=args.streamed_iters, encode_s=encode_s, pinned_h2d_peak_gbs=peak, forms=forms,
+                roofline=dict(bound="host link (H2D)", achieved=forms["mixed_f32"]["h2d_gbs"], peak=peak,
+                              unit="GB/s", frac=forms["mixed_f32"]["h2d_frac"],
+                              peak_kind="pinned 2 GiB host-to-device copy, best of 3, this process"),
+                note=("nnz below the configuration's 2B keeps the leg inside the benchmark's time budget "
+                      "(--streamed-nnz 2000000000 runs the full size); every block crosses the host link once "
+                      "per mode per iteration: 16 B per nonzero (FP64 values) or 12 B (mixed, FP32 values); "
+                      "device_bytes_plan is the plan's own count (caller's factors, workspace, ring)"))
+
+
+def shard_slice(X, world, rank):
+    """This rank's share of a tensor whose nonzeros are split over `world`
+    ranks: a contiguous range of the nonzero list (every rank draws the
+    same tensor), and ||X||^2 of the whole tensor for the fit."""
+    n = X["vals"].numel()
+    lo, hi = n * rank // world, n * (rank + 1) // world
+    norm_sq = float((X["vals"].double() ** 2).sum().item())
+    return dict(dims=X["dims"], cidx=[c[lo:hi] for c in X["cidx"]], vals=X["vals"][lo:hi], lo=lo, hi=hi,
+                norm_sq=norm_sq)
+
+
 def run_ours(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
@@ -608,14 +737,24 @@ def run_ours(args, world, rank, local):
     from blco_b200 import synth
     selector = pkg.default_selector(margin=0.1) if args.kernel == pkg.KERNEL_LEARNED else None
     dims, nnz, rk = WORKLOAD["dims"], args.nnz, WORKLOAD["rank"]
-    X = synth.zipf_tensor_device(nnz, dims, WORKLOAD["zipf"], seed=args.seed + rank)
+    # every rank draws the same tensor; with N ranks each encodes and owns a
+    # contiguous 1/N of its nonzeros, and each mode's MTTKRP is summed over
+    # the ranks (strong scaling: the job is the one tensor)
+    X = synth.zipf_tensor_device(nnz, dims, WORKLOAD["zipf"], seed=args.seed)
+    norm_sq = None
+    Xs = X
+    if world > 1:
+        Xs = shard_slice(X, world, rank)
+        norm_sq = Xs["norm_sq"]
+    nnz_local = int(Xs["vals"].numel())
     stream = torch.cuda.current_stream()
     opts = pkg.make_opts(kernel=args.kernel, stream=stream.cuda_stream)
     torch.cuda.synchronize()
     e0 = time.perf_counter()
-    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"], 0, opts)
+    t = pkg.Tensor.encode_device(dims, Xs["cidx"], Xs["vals"], 0, opts)
     torch.cuda.synchronize()
     encode_ms = (time.perf_counter() - e0) * 1e3
+    del Xs
     # host copies for the end-to-end leg (pinned)
     h_cidx = [c.to(torch.int64).cpu().pin_memory() for c in X["cidx"]]
     h_vals = X["vals"].cpu().pin_memory()
@@ -625,7 +764,7 @@ def run_ours(args, world, rank, local):
     fs0 = [torch.rand(d, rk, dtype=torch.float64, device="cuda", generator=g) for d in dims]
 
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
-    res = {f: time_form(pkg, torch, t, dims, rk, fs0, f, args, stream, dist) for f in forms}
+    res = {f: time_form(pkg, torch, t, dims, rk, fs0, f, args, stream, dist, norm_sq) for f in forms}
     plain = res.get("fp64")
     chosen = "fp64"
     best = plain["ms_per_step"] if plain else float("inf")
@@ -634,6 +773,11 @@ def run_ours(args, world, rank, local):
             continue
         dfit = abs(res[f]["fits"][-1] - plain["fits"][-1]) if plain else 0.0
         res[f]["fit_delta_vs_fp64"] = dfit
+        if plain:
+            n = min(len(res[f]["fits"]), len(plain["fits"]))
+            d = np.abs(np.array(res[f]["fits"][:n]) - np.array(plain["fits"][:n]))
+            res[f]["fit_delta_max_over_run"] = float(d.max())
+            res[f]["fit_delta_at_timed_end"] = float(d[res[f]["timed_end"] - 1])
         if dfit <= 1e-5 and res[f]["ms_per_step"] < best:
             best, chosen = res[f]["ms_per_step"], f
     C = res[chosen]
@@ -698,10 +842,11 @@ def run_ours(args, world, rank, local):
             st = [t.fibre_stats(m) for m in range(3)]
             rows = [x["rows_gathered"] for x in st]
             rates = [r / (ms * 1e-3) / 1e9 for r, ms in zip(rows, C["mttkrp_ms"])]
+            nnz_g = nnz_local
             ceil = None if args.no_gather_ceiling else gather_ceiling()
             top = ceil["grows_per_s_zipf"] if ceil else None
             gather = dict(rows_per_mode=rows, fibre_modes=[x["fibre_mode"] for x in st],
-                          fibred_share=[x["fibred_nnz"] / nnz for x in st], rows_per_nnz=[r / nnz for r in rows],
+                          fibred_share=[x["fibred_nnz"] / nnz_g for x in st], rows_per_nnz=[r / nnz_g for r in rows],
                           grows_per_s=rates, ceiling=ceil,
                           frac_of_ceiling=[r / top for r in rates] if top else None,
                           note=("rows gathered by kernel 4 per mode (the inner modes' rows of every fibred "
@@ -721,20 +866,27 @@ def run_ours(args, world, rank, local):
     wide = None
     if not args.no_wide:
         wide = wide_leg(pkg, torch, args, peaks()[0], rank == 0 and world == 1 and not args.no_cpu_baseline)
+    streamed = None
+    if not args.no_streamed and rank == 0 and world == 1:
+        streamed = streamed_leg(pkg, torch, args)
     if rank == 0:
         forms_out = {}
         for f, r in res.items():
             a_f = [mttkrp_alg_bytes(dims, nnz, rk, m, 8, FORMS[f][1], FORMS[f][2], FORMS[f][3]) for m in range(3)]
             forms_out[f] = dict(ms_per_step=r["ms_per_step"], mttkrp_ms_per_mode=[round(x, 4) for x in r["mttkrp_ms"]],
                                 mttkrp_gbs=sum(a_f) / (sum(r["mttkrp_ms"]) * 1e-3) / 1e9, fit_last=r["fits"][-1],
-                                fit_delta_vs_fp64=r.get("fit_delta_vs_fp64", 0.0))
+                                fit_delta_vs_fp64=r.get("fit_delta_vs_fp64", 0.0),
+                                fit_delta_at_timed_end=r.get("fit_delta_at_timed_end", 0.0),
+                                fit_delta_max_over_run=r.get("fit_delta_max_over_run", 0.0), fit_iters=len(r["fits"]))
         line = {
             "metric": METRIC, "value": C["ms_per_step"], "unit": "ms", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": C["ms_per_step"], "higher_is_better": False, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": C["ms_per_step"], "higher_is_better": False, "scaling": "strong",
             "vs_baseline": None, "dtype": dtype, "data": "synthetic",
             "config": dict(workload=WORKLOAD["workload"], dims=dims, nnz=nnz, rank=rk, zipf=WORKLOAD["zipf"],
                            values=WORKLOAD["values"], form=chosen, kernel=args.kernel, schedules=schedules,
-                           parallelism=("replicas" if world > 1 else "single"),
+                           parallelism=(f"nnz-sharded x{world}: each rank owns a contiguous 1/{world} of the "
+                                        "nonzeros; each mode's MTTKRP all-reduced over NCCL on the plan's stream"
+                                        if world > 1 else "single"),
                            l2="inputs larger than L2 (3.2 GB stream, >= 0.5 GB factors)"),
             "forms": forms_out,
             "plain_fp64_ms_per_step": plain["ms_per_step"] if plain else None,
@@ -750,17 +902,42 @@ def run_ours(args, world, rank, local):
             "e2e": dict(value=e2e_ms, unit="ms", h2d_bytes_per_step=int(h2d / e_iters),
                         d2h_bytes_per_step=int(d2h / e_iters),
                         note=(f"blco_encode from pinned host COO + blco_cpals({e_iters} iters, {chosen}) with pinned "
-                              "host factors; job time / iterations; bytes are per iteration"), **e2e_split),
+                              "host factors; job time / iterations; bytes are per iteration"
+                              + ("; with N ranks every rank runs the whole tensor this way (the host entry point "
+                                 "takes no exchange hook), max over ranks" if world > 1 else "")), **e2e_split),
+            "ms_per_step_per_rank": C["ms_per_step_per_rank"],
+            "allreduce": (dict(bytes_per_mode=[int(d * rk * 8) for d in dims], bytes_per_iter=int(sum(dims) * rk * 8),
+                               note="each mode's I_m x R MTTKRP result summed over the ranks (FP64: the plain "
+                                    "form, and the mixed form's fibre schedule, which sums rows in FP64; 4-byte "
+                                    "sums where a mixed mode runs a tile schedule)")
+                          if world > 1 else None),
             "gpu_launches": C["launches"],
             "clocks": C["clocks"],
             "batched": batched,
             "wide": wide,
             "c1": c1,
+            "streamed": streamed,
         }
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_only(args, local):
+    """One leg alone on one GPU (the commands of the ncu summaries)."""
+    import torch
+    torch.cuda.set_device(local)
+    pkg = load_pkg()
+    if args.only == "streamed":
+        out = streamed_leg(pkg, torch, args)
+    elif args.only == "batched":
+        out = batched_leg(pkg, torch, args)
+    elif args.only == "wide":
+        out = wide_leg(pkg, torch, args, peaks()[0], not args.no_cpu_baseline)
+    else:
+        out = c1_leg(pkg, torch, args)
+    print(json.dumps({args.only: out}))
 
 
 def main():
@@ -783,9 +960,20 @@ def main():
                     help="--impl reference: skip the reference's own GPU CP-ALS on the full workload")
     ap.add_argument("--ref-gpu-wide", action="store_true",
                     help="--impl reference: also time the reference's GPU CP-ALS on the wide-key workload")
+    ap.add_argument("--no-streamed", action="store_true", help="skip the streamed (out-of-memory) leg")
+    ap.add_argument("--streamed-nnz", type=int, default=500_000_000,
+                    help="nonzeros of the streamed leg (the configuration's full size is 2000000000)")
+    ap.add_argument("--streamed-iters", type=int, default=2)
+    ap.add_argument("--only", choices=["streamed", "batched", "wide", "c1"],
+                    help="run one leg alone and print its JSON object")
+    ap.add_argument("--fit-iters", type=int, default=40,
+                    help="iterations after which the forms' fits are compared (the timed steps, then untimed)")
     ap.add_argument("--forms", default="fp64,mixed_f32,mixed_bf16")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.only:
+        run_only(args, local)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
     else:

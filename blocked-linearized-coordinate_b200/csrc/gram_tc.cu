@@ -1,30 +1,37 @@
 // gram_tc.cu -- the mixed form's Gram U^T U on the 5th-generation tensor
 // cores (tcgen05.mma, accumulator in TMEM), exact in the accumulator.
 //
-// U is I x R FP32, row-major (R <= 64).  Rows are taken 64 at a time (a
-// tile).  In a tile every column c gets a power-of-two scale 2^e_c with
-// max |u_c| < 2^e_c, and every value becomes three integer digits:
-//   x = u * 2^(8 - e_c)  (|x| < 256),  d2 = rint(x),
-//   d1 = rint(256 (x - d2)),  d0 = rint(256 (256 (x - d2) - d1)),
-// so u = 2^(e_c - 8) (d2 + d1 / 2^8 + d0 / 2^16) to within 2^(e_c - 25)
-// (FP32's own precision at the tile's largest value).  The digits are
+// U is I x R FP32, row-major (R <= 64).  Rows are taken 256 at a time (a
+// super-tile; 64 for ranks above 32), staged in shared memory.  In a
+// super-tile every column c gets a power-of-two scale 2^e_c with
+// max |u_c| < 2^e_c, and every value becomes four integer digits, most
+// significant first:
+//   x = u * 2^(8 - e_c)  (|x| < 256),  d_0 = rint(x),
+//   d_k = rint(256^k x - sum_{l<k} 256^(k-l) d_l)  (k = 1, 2, 3),
+// so u = 2^(e_c - 8) sum_k d_k / 256^k to within 2^(e_c - 33): exact for
+// every value above 2^-9 of the column's largest in the super-tile (FP32
+// keeps 24 bits), and within 2^-33 of that largest value below it (the Gram
+// of a column whose magnitudes span many decades within a few hundred rows,
+// as Zipf-skewed factor rows do, needs those low digits).  The digits are
 // integers in [-256, 256], exact in BF16, and their products (at most 2^16)
-// summed over the 64 rows stay below 2^22: every partial sum the tensor
-// cores form in their FP32 accumulator is an integer below 2^24, hence
-// exact, whatever the accumulator's rounding.  (A split into BF16 hi + lo
-// parts, the usual scheme, is not exact there: the tensor cores' FP32
-// accumulation leans low, and that bias reached the CP-ALS fit.)
+// summed over at most 256 rows stay at or below 2^24: every partial sum the
+// tensor cores form in their FP32 accumulator is an integer of at most
+// 2^24, hence exact, whatever the accumulator's rounding.  (A split into BF16 hi + lo parts, the usual
+// scheme, is not exact there: the tensor cores' FP32 accumulation leans
+// low, and that bias reached the CP-ALS fit.)
 //
-// The digit rows form the K-major operand S of one tile: row i * RB + c
-// holds digit i of column c (RB = R rounded up to 8, 16, 32 or 64; rows of
+// The digit rows form the K-major operand S of one super-tile: row k * RB +
+// c holds digit k of column c (RB = R rounded up to 8, 16, 32 or 64; rows of
 // padding columns are zero).  One MMA chain per 128-row group of S computes
-// D = S S^T over the tile (M = 128, N = 3 RB rounded up to 16, K = 64 in 4
-// MMAs); D[i RB + a][j RB + c] = sum over the tile of d_i(a) d_j(c).  The
-// CTA reads D back (tcgen05.ld) and adds
+// D = S S^T over the super-tile (M = 128, N = 4 RB, K = 256 in 16 MMAs, 64
+// in 4 for ranks above 32);
+// D[i RB + a][j RB + c] = sum over the super-tile of d_i(a) d_j(c).  The CTA
+// reads D back (tcgen05.ld) and adds
 //   2^(e_a - 8 - 8 i) 2^(e_c - 8 - 8 j) D[i RB + a][j RB + c]
-// for i + j <= 2 (the terms of i + j >= 3 are below 2^-24 of the leading
-// one) to FP64 sums: registers for RB <= 32, shared memory for RB = 64.
-// The next tile's loads and digits overlap the previous tile's MMAs.  Each
+// for every digit pair (i, j) to FP64 sums: registers for RB <= 32, shared
+// memory for RB = 64.  (Dropping the small pairs would bias the diagonal:
+// there the dropped products are squares.)
+// The next super-tile's loads overlap the previous one's MMAs.  Each
 // CTA writes its R x R FP64 partial; the partials are summed in FP64 in a
 // fixed order.
 //
@@ -44,6 +51,7 @@
 // commit it gave up on, frees its TMEM and returns.  If that second wait
 // also runs out, the TMEM is freed with those MMAs possibly still running;
 // the host reports BLCO_ERR_TIMEOUT either way.
+#include <algorithm>
 #include <cstdint>
 
 #include "internal.cuh"
@@ -53,8 +61,6 @@ namespace blco {
 namespace {
 
 constexpr int TG_THREADS = 128;   // 4 warps: one TMEM lane quarter each
-constexpr int TG_KT = 64;         // rows of U per tile (4 MMAs of K = 16)
-constexpr int TG_CHUNKS = TG_KT / 8;
 constexpr uint32_t TG_SPIN_MAX = 1u << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -134,15 +140,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&d)[16])
 
 template <int RB>
 struct GramShape {
-    static constexpr int MG = 3 * RB > 128 ? 2 : 1;    // 128-row groups of S
+    static constexpr int ND = 4;                        // digits per value
+    static constexpr int MG = ND * RB > 128 ? 2 : 1;    // 128-row groups of S
     static constexpr int ROWS = 128 * MG;               // rows of S per K chunk
-    static constexpr int N = (3 * RB + 15) / 16 * 16;   // MMA N: digit rows of B
+    static constexpr int N = ND * RB;                   // MMA N: digit rows of B (32..256)
     static constexpr int NCOLS = MG == 2 ? 512 : N <= 32 ? 32 : N <= 64 ? 64 : 128;
-    static constexpr int NI = (TG_CHUNKS * RB + TG_THREADS - 1) / TG_THREADS; // (chunk, column) items per thread
+    static constexpr int KS = RB == 64 ? 64 : 256;      // rows per fold (a super-tile)
+    static constexpr int CH = KS / 8;                   // K chunks of S
+    static constexpr int NV = (KS * RB / 4 + TG_THREADS - 1) / TG_THREADS; // float4 loads per thread
     static constexpr bool REG = RB <= 32;               // digit-row sums in registers
+    static constexpr int MINB = RB == 64 ? 1 : 2;       // CTAs per SM the registers must allow
+    static constexpr size_t S_BYTES = (size_t)CH * ROWS * 16;
+    static constexpr size_t STAGE_BYTES = (size_t)KS * RB * 4;
+    static constexpr size_t GSM_BYTES = (size_t)ND * RB * (RB + 1) * 8;
+    // dynamic shared memory: S, the staged rows, then (RB = 64) the FP64
+    // sums; with RB <= 32 the sums reuse S's space once the last fold is done
+    static constexpr size_t SMEM = REG ? (S_BYTES + STAGE_BYTES > GSM_BYTES ? S_BYTES + STAGE_BYTES : GSM_BYTES)
+                                       : S_BYTES + STAGE_BYTES + GSM_BYTES;
 };
 
-// Adds one tile's D (scales sd[j RB + c] = 2^(e_c - 8 - 8 j)) to this
+// Adds one super-tile's D (scales sd[j RB + c] = 2^(e_c - 8 - 8 j)) to this
 // thread's digit-row sums: acc (registers, RB <= 32) or gsm (RB = 64).
 template <int RB>
 __device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, const double* sd,
@@ -153,8 +170,7 @@ __device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, cons
 #pragma unroll
     for (int g = 0; g < G::MG; g++) {
         const int q = g * 128 + tid;
-        const bool act = q < 3 * RB;
-        const int i = act ? q / RB : 3;
+        const bool act = q < G::ND * RB;
         const double wa = act ? sd[q] : 0.0;
 #pragma unroll
         for (int c0 = 0; c0 < G::N; c0 += 16) {
@@ -163,9 +179,8 @@ __device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, cons
 #pragma unroll
             for (int x = 0; x < 16; x++) {
                 const int n = c0 + x;
-                if (n >= 3 * RB) continue;
-                const int j = n / RB, c = n % RB;
-                if (i + j <= 2) {
+                const int c = n % RB;
+                if (act) {
                     const double v = (double)__uint_as_float(d[x]) * sd[n]; // exact: D times a power of two
                     if constexpr (G::REG) acc[c] = fma(wa, v, acc[c]);
                     else gsm[q * (RB + 1) + c] = fma(wa, v, gsm[q * (RB + 1) + c]);
@@ -176,29 +191,31 @@ __device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, cons
 }
 
 template <int RB, bool SCALE, bool BF16OUT>
-__global__ void __launch_bounds__(TG_THREADS) k_gram_tc(float* __restrict__ U, uint64_t I, int R,
+__global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(float* __restrict__ U, uint64_t I, int R,
                                                         const double* __restrict__ inv,
                                                         uint16_t* __restrict__ bf16_out, uint64_t rows_per_cta,
                                                         double* __restrict__ partials, int* __restrict__ err,
                                                         uint32_t spin_max, int no_commit)
 {
     using G = GramShape<RB>;
-    __shared__ __align__(1024) uint4 S[TG_CHUNKS * G::ROWS];
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    uint4* S = reinterpret_cast<uint4*>(dsm);                          // [CH][ROWS] operand chunks
+    float* stage = reinterpret_cast<float*>(dsm + G::S_BYTES);         // [KS][R] rows of U
+    double* gsm = reinterpret_cast<double*>(G::REG ? dsm : dsm + G::S_BYTES + G::STAGE_BYTES);
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
-    __shared__ uint32_t cmax[2][RB];   // per tile (double-buffered): largest |u| of each column, as bits
-    __shared__ double sdj[2][3 * RB];  // per tile: 2^(e_c - 8 - 8 j) at j RB + c
-    extern __shared__ __align__(16) double gsm[]; // [3 RB][RB + 1] FP64 digit-row sums
+    __shared__ uint32_t cmax[2][RB];      // per super-tile (double-buffered): largest |u| per column, as bits
+    __shared__ double sdj[2][G::ND * RB]; // per super-tile: 2^(e_c - 8 - 8 j) at j RB + c
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint64_t r_beg = (uint64_t)blockIdx.x * rows_per_cta;
     const uint64_t r_end = min(I, r_beg + rows_per_cta);
-    const int ntiles = r_beg < r_end ? (int)((r_end - r_beg + TG_KT - 1) / TG_KT) : 0;
-    const int items = TG_CHUNKS * R;
+    const int nsup = r_beg < r_end ? (int)((r_end - r_beg + G::KS - 1) / G::KS) : 0;
+    const int items = G::CH * R;          // (chunk j, column c): column c of 8 staged rows
 
-    for (int i = tid; i < TG_CHUNKS * G::ROWS; i += TG_THREADS) S[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < G::CH * G::ROWS; i += TG_THREADS) S[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < 2 * RB; i += TG_THREADS) (&cmax[0][0])[i] = 0u;
     if constexpr (!G::REG)
-        for (int i = tid; i < 3 * RB * (RB + 1); i += TG_THREADS) gsm[i] = 0.0;
+        for (int i = tid; i < G::ND * RB * (RB + 1); i += TG_THREADS) gsm[i] = 0.0;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -222,86 +239,107 @@ __global__ void __launch_bounds__(TG_THREADS) k_gram_tc(float* __restrict__ U, u
 
     uint32_t phase = 0; // commits issued (or, in the self-test, skipped)
     bool late = false;  // the same on every thread
-    for (int t = 0; t < ntiles; t++) {
+    for (int t = 0; t < nsup; t++) {
         const int b = t & 1;
-        const uint64_t k0 = r_beg + (uint64_t)t * TG_KT;
-        // item (j, c): column c of rows k0 + 8j .. +7
-        float v[G::NI][8];
+        const uint64_t k0 = r_beg + (uint64_t)t * G::KS;
+        // stage rows k0 .. k0 + KS - 1 (contiguous in U; 16-byte aligned as
+        // k0 is a multiple of 4), scaled / rounded and written back as asked
+        {
+            const uint64_t base = k0 * (uint64_t)R;                 // first element
+            const uint64_t valid = (min(r_end, k0 + G::KS) - k0) * (uint64_t)R;
+            const int nv4 = G::KS * R / 4;
+            float4 buf[G::NV];
 #pragma unroll
-        for (int n = 0; n < G::NI; n++) {
-            const int it = tid + n * TG_THREADS;
-            float amax = 0.f;
-#pragma unroll
-            for (int e = 0; e < 8; e++) v[n][e] = 0.f;
-            if (it < items) {
-                const int j = it / R, c = it % R;
-#pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const uint64_t row = k0 + 8 * j + e;
-                    if (row < r_end) {
-                        float x = U[row * R + c];
-                        if (SCALE) x = (float)((double)x * inv[c]);
-                        if constexpr (BF16OUT) {
-                            const uint16_t h = bf16_bits_rn(x);
-                            x = bf16_to_f32(h);
-                            bf16_out[row * R + c] = h;
-                        }
-                        if (SCALE || BF16OUT) U[row * R + c] = x;
-                        v[n][e] = x;
-                        amax = fmaxf(amax, fabsf(x));
+            for (int k = 0; k < G::NV; k++) {
+                const int f = tid + k * TG_THREADS;
+                const uint64_t e0 = 4 * (uint64_t)f;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (f < nv4 && e0 < valid) {
+                    if (e0 + 4 <= valid) {
+                        v = *reinterpret_cast<const float4*>(U + base + e0);
+                    } else { // the last rows' ragged end (at most 3 elements)
+                        v.x = U[base + e0];
+                        if (e0 + 1 < valid) v.y = U[base + e0 + 1];
+                        if (e0 + 2 < valid) v.z = U[base + e0 + 2];
                     }
                 }
-                atomicMax(&cmax[b][c], __float_as_uint(amax));
+                buf[k] = v;
+            }
+#pragma unroll
+            for (int k = 0; k < G::NV; k++) {
+                const int f = tid + k * TG_THREADS;
+                if (f >= nv4) continue;
+                if (SCALE || BF16OUT) {
+                    const uint64_t e0 = 4 * (uint64_t)f;
+                    float x[4] = {buf[k].x, buf[k].y, buf[k].z, buf[k].w};
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        if (e0 + u >= valid) continue;
+                        const uint64_t gi = base + e0 + u;
+                        float y = x[u];
+                        if (SCALE) y = (float)((double)y * inv[(int)(gi % (uint64_t)R)]);
+                        if constexpr (BF16OUT) {
+                            const uint16_t h = bf16_bits_rn(y);
+                            y = bf16_to_f32(h);
+                            bf16_out[gi] = h;
+                        }
+                        x[u] = y;
+                    }
+                    buf[k] = make_float4(x[0], x[1], x[2], x[3]);
+                    if (e0 + 4 <= valid) {
+                        *reinterpret_cast<float4*>(U + base + e0) = buf[k];
+                    } else if (e0 < valid) {
+                        U[base + e0] = x[0];
+                        if (e0 + 1 < valid) U[base + e0 + 1] = x[1];
+                        if (e0 + 2 < valid) U[base + e0 + 2] = x[2];
+                    }
+                }
+                reinterpret_cast<float4*>(stage)[f] = buf[k];
             }
         }
-        // the next tile's maxima (last read before the previous MMA issue)
+        // the next super-tile's maxima (last read before the previous MMA issue)
         if (tid < RB) cmax[b ^ 1][tid] = 0u;
         __syncthreads();
-        // digits of this tile, and its scales for the fold
-        uint4 w[G::NI][3];
+        for (int it = tid; it < items; it += TG_THREADS) {
+            const int j = it / R, c = it % R;
+            float m = 0.f;
 #pragma unroll
-        for (int n = 0; n < G::NI; n++) {
-            const int it = tid + n * TG_THREADS;
-            const int c = it < items ? it % R : 0;
-            const int ex = exponent_of(cmax[b][c]);
-            uint32_t h[3][4];
-#pragma unroll
-            for (int e = 0; e < 8; e += 2) {
-                uint32_t lohi[3][2];
-#pragma unroll
-                for (int u = 0; u < 2; u++) {
-                    const float x = scale_pow2(v[n][e + u], 8 - ex);
-                    const float d2 = rintf(x);
-                    const float r1 = (x - d2) * 256.f;
-                    const float d1 = rintf(r1);
-                    const float d0 = rintf((r1 - d1) * 256.f);
-                    lohi[0][u] = digit_bits(d2);
-                    lohi[1][u] = digit_bits(d1);
-                    lohi[2][u] = digit_bits(d0);
-                }
-#pragma unroll
-                for (int i = 0; i < 3; i++) h[i][e / 2] = lohi[i][0] | (lohi[i][1] << 16);
-            }
-#pragma unroll
-            for (int i = 0; i < 3; i++) w[n][i] = make_uint4(h[i][0], h[i][1], h[i][2], h[i][3]);
+            for (int e = 0; e < 8; e++) m = fmaxf(m, fabsf(stage[(8 * j + e) * R + c]));
+            atomicMax(&cmax[b][c], __float_as_uint(m));
         }
-        for (int k = tid; k < 3 * RB; k += TG_THREADS) {
-            const int j = k / RB, c = k % RB;
-            sdj[b][k] = pow2_f64(exponent_of(cmax[b][c]) - 8 - 8 * j);
-        }
-        // the previous tile's MMAs: complete before S is rewritten and D read
+        __syncthreads();
+        for (int k = tid; k < G::ND * RB; k += TG_THREADS)
+            sdj[b][k] = pow2_f64(exponent_of(cmax[b][k % RB]) - 8 - 8 * (k / RB));
+        // the previous super-tile's MMAs: complete before S is rewritten and D read
         if (t > 0 && cta_wait_late(bar, (phase - 1) & 1, spin_max)) {
             late = true;
             break;
         }
+        // digits of this super-tile into S
+        for (int it = tid; it < items; it += TG_THREADS) {
+            const int j = it / R, c = it % R;
+            const int ex = exponent_of(cmax[b][c]);
+            uint32_t h[G::ND][4];
 #pragma unroll
-        for (int n = 0; n < G::NI; n++) {
-            const int it = tid + n * TG_THREADS;
-            if (it < items) {
-                const int j = it / R, c = it % R;
+            for (int e = 0; e < 8; e += 2) {
+                uint32_t lohi[G::ND][2];
 #pragma unroll
-                for (int i = 0; i < 3; i++) S[j * G::ROWS + i * RB + c] = w[n][i];
+                for (int u = 0; u < 2; u++) {
+                    // every step exact: x has 24 significant bits, the
+                    // remainders shrink by 2^8 and stay in [-0.5, 0.5] * 2^8
+                    float r = scale_pow2(stage[(8 * j + e + u) * R + c], 8 - ex);
+#pragma unroll
+                    for (int k = 0; k < G::ND; k++) {
+                        const float d = rintf(r);
+                        lohi[k][u] = digit_bits(d);
+                        r = (r - d) * 256.f;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < G::ND; k++) h[k][e / 2] = lohi[k][0] | (lohi[k][1] << 16);
             }
+#pragma unroll
+            for (int k = 0; k < G::ND; k++) S[j * G::ROWS + k * RB + c] = make_uint4(h[k][0], h[k][1], h[k][2], h[k][3]);
         }
         if (t > 0) fold_tile<RB>(tmem, warp, tid, sdj[b ^ 1], acc, gsm);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -309,8 +347,8 @@ __global__ void __launch_bounds__(TG_THREADS) k_gram_tc(float* __restrict__ U, u
         __syncthreads();
         if (tid == 0 && !no_commit) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-            for (int kk = 0; kk < TG_KT / 16; kk++) {
+#pragma unroll 1
+            for (int kk = 0; kk < G::KS / 16; kk++) {
                 const uint32_t kb = s_addr + (uint32_t)(kk * 2 * G::ROWS * 16);
                 const uint64_t db = umma_desc(kb, G::ROWS * 16);
 #pragma unroll
@@ -328,10 +366,10 @@ __global__ void __launch_bounds__(TG_THREADS) k_gram_tc(float* __restrict__ U, u
         }
         phase++;
     }
-    // the last tile
-    if (!late && ntiles > 0) {
+    // the last super-tile
+    if (!late && nsup > 0) {
         if (cta_wait_late(bar, (phase - 1) & 1, spin_max)) late = true;
-        else fold_tile<RB>(tmem, warp, tid, sdj[(ntiles - 1) & 1], acc, gsm);
+        else fold_tile<RB>(tmem, warp, tid, sdj[(nsup - 1) & 1], acc, gsm);
     }
     if (late) {
         if (tid == 0) atomicExch(err, 1);
@@ -346,7 +384,8 @@ __global__ void __launch_bounds__(TG_THREADS) k_gram_tc(float* __restrict__ U, u
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::NCOLS));
     }
     if constexpr (G::REG) {
-        if (tid < 3 * RB)
+        // S and the staged rows are no longer read (barrier above): the sums go there
+        if (tid < G::ND * RB)
 #pragma unroll
             for (int c = 0; c < RB; c++) gsm[tid * (RB + 1) + c] = acc[c];
         __syncthreads();
@@ -354,8 +393,10 @@ __global__ void __launch_bounds__(TG_THREADS) k_gram_tc(float* __restrict__ U, u
     // G_cta[a][c] = sum over digits i of the rows i RB + a
     for (int e = tid; e < R * R; e += TG_THREADS) {
         const int a = e / R, c = e % R;
-        partials[(size_t)blockIdx.x * R * R + e] =
-            gsm[a * (RB + 1) + c] + gsm[(RB + a) * (RB + 1) + c] + gsm[(2 * RB + a) * (RB + 1) + c];
+        double g = 0.0;
+#pragma unroll
+        for (int i = 0; i < G::ND; i++) g += gsm[(i * RB + a) * (RB + 1) + c];
+        partials[(size_t)blockIdx.x * R * R + e] = g;
     }
 }
 
@@ -364,18 +405,30 @@ int gram_tc_dispatch(float* U, uint64_t I, int R, const double* inv, uint16_t* b
                      int* d_err, cudaStream_t s, int* nparts, uint32_t spin_max, int no_commit)
 {
     using G = GramShape<RB>;
-    // CTAs per SM: at most 8, and as many as TMEM holds (512 columns)
-    const uint64_t per_sm = (uint64_t)std::min(8, 512 / G::NCOLS);
-    const uint64_t tiles = (I + TG_KT - 1) / TG_KT;
-    const uint64_t maxc = std::min<uint64_t>((uint64_t)sm * per_sm, (uint64_t)gram_tc_max_ctas(sm));
-    const uint64_t tiles_per = std::max<uint64_t>(1, (tiles + maxc - 1) / maxc);
-    const uint64_t rows_per = tiles_per * TG_KT;
-    const int grid = (int)std::max<uint64_t>(1, (I + rows_per - 1) / rows_per);
-    const size_t smem = (size_t)3 * RB * (RB + 1) * sizeof(double);
+    const size_t smem = G::SMEM;
     void (*fn)(float*, uint64_t, int, const double*, uint16_t*, uint64_t, double*, int*, uint32_t, int);
     if (bf16_out) fn = inv ? k_gram_tc<RB, true, true> : k_gram_tc<RB, false, true>;
     else fn = inv ? k_gram_tc<RB, true, false> : k_gram_tc<RB, false, false>;
     BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   (int)cudaSharedmemCarveoutMaxShared));
+    // CTAs per SM: as many as the registers, the shared memory and TMEM
+    // (512 columns) hold at once, at most 8: one wave
+    cudaFuncAttributes fa;
+    BLCO_CUDA(cudaFuncGetAttributes(&fa, (const void*)fn));
+    int dev = 0, regs_sm = 65536, smem_sm = 0, smem_rsv = 0;
+    BLCO_CUDA(cudaGetDevice(&dev));
+    BLCO_CUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    BLCO_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    BLCO_CUDA(cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    const int by_regs = regs_sm / (std::max(1, fa.numRegs) * TG_THREADS);
+    const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + (size_t)smem_rsv);
+    const uint64_t per_sm = (uint64_t)std::max(1, std::min({8, 512 / G::NCOLS, by_regs, by_smem}));
+    const uint64_t sups = (I + G::KS - 1) / G::KS;
+    const uint64_t maxc = std::min<uint64_t>((uint64_t)sm * per_sm, (uint64_t)gram_tc_max_ctas(sm));
+    const uint64_t sups_per = std::max<uint64_t>(1, (sups + maxc - 1) / maxc);
+    const uint64_t rows_per = sups_per * G::KS;
+    const int grid = (int)std::max<uint64_t>(1, (I + rows_per - 1) / rows_per);
     fn<<<grid, TG_THREADS, smem, s>>>(U, I, R, inv, bf16_out, rows_per, partials, d_err, spin_max, no_commit);
     BLCO_CHECK_LAUNCH("k_gram_tc");
     *nparts = grid;
@@ -390,6 +443,8 @@ int gram_tc_launch(float* U, uint64_t I, int R, const double* inv, uint16_t* bf1
                    int* d_err, cudaStream_t s, int* nparts, uint32_t spin_max, int no_commit)
 {
     if (R < 1 || R > 64) return fail(BLCO_ERR_UNSUPPORTED, "tensor-core Gram takes rank 1..64");
+    if (reinterpret_cast<uintptr_t>(U) % 16)
+        return fail(BLCO_ERR_UNSUPPORTED, "tensor-core Gram stages rows with 16-byte loads: U must be 16-byte aligned");
     if (spin_max == 0) spin_max = TG_SPIN_MAX;
     if (R <= 8) return gram_tc_dispatch<8>(U, I, R, inv, bf16_out, partials, sm, d_err, s, nparts, spin_max, no_commit);
     if (R <= 16)

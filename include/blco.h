@@ -451,10 +451,11 @@ int blco_select(blco_tensor* t, int mode, int rank, int factor_dtype, blco_mlp* 
 
 /* G = U^T U for a device FP32 matrix U (I x rank, row-major, rank 1..64),
  * G (device, rank x rank FP64).  tensor_cores 1: products on the tensor
- * cores (per 64-row tile and column, a power-of-two scale and three 8-bit
+ * cores (per 64-row tile and column, a power-of-two scale and four 8-bit
  * integer digits per value, exact integer sums in the FP32 accumulator,
- * FP64 beyond the tile; each value to within 2^-25 of its tile column's
- * largest magnitude); 0: FP64 products on the CUDA cores.  The Gram of the
+ * FP64 beyond the tile; each value to within 2^-33 of its tile column's
+ * largest magnitude; U 16-byte aligned); 0: FP64 products on the CUDA
+ * cores.  The Gram of the
  * reference's ata_gpu (src/cpd_gpu.cu:547-568) for the mixed form's FP32
  * factors.  Synchronous on `stream` (NULL: default stream). */
 int blco_gram_f32(const float* d_U, uint64_t I, int rank, double* d_G, int tensor_cores, int device,
