@@ -495,7 +495,7 @@ def batched_leg(pkg, torch, args):
     sweep of the captured graph, next to per-tensor plans run one after
     another (timed on the first 32 tensors, scaled by nnz)."""
     from blco_b200 import synth
-    Xs = synth.batch_tensors_device(BATCH["count"], seed=BATCH["seed"])
+    Xs = synth.batch_tensors_device(args.batch_count, seed=BATCH["seed"])
     nnzs = [int(x["vals"].numel()) for x in Xs]
     ts = [pkg.Tensor.encode_device(x["dims"], x["cidx"], x["vals"]) for x in Xs]
     ranks = [x["rank"] for x in Xs]
@@ -512,7 +512,15 @@ def batched_leg(pkg, torch, args):
     b.iterate(args.steps)
     launches = pkg.launch_count(reset=True)
     ms = b.last_ms() / max(1, args.steps)
+    mt_ms = min(b.mttkrp_ms() for _ in range(3))
     b.destroy()
+    # algorithmic bytes of one sweep's MTTKRPs (FP64): per tensor and mode,
+    # the index and value stream once, every other factor once, the output once
+    alg = 0
+    for dd, r, nz in zip(dims, ranks, nnzs):
+        for m in range(len(dd)):
+            alg += nz * (8 + 8) + sum(d for i, d in enumerate(dd) if i != m) * r * 8 + dd[m] * r * 8
+    peak = peaks()[0]
     # per-tensor plans, one after another, on a prefix of the batch
     k = min(32, len(ts))
     seq = 0.0
@@ -531,6 +539,13 @@ def batched_leg(pkg, torch, args):
         t.free()
     return dict(workload=BATCH["workload"], tensors=len(ts), nnz=sum(nnzs), ms_per_sweep=ms, sweeps=args.steps,
                 gpu_launches=int(launches), dtype="f64", graph="one CUDA graph per sweep",
+                mttkrp_ms_per_sweep=mt_ms,
+                roofline=dict(bound="hbm", achieved=alg / (mt_ms * 1e-3) / 1e9, peak=peak, unit="GB/s",
+                              frac=alg / (mt_ms * 1e-3) / 1e9 / peak, traffic=None, alg_bytes_per_sweep=int(alg),
+                              kernel="k_b_mttkrp, every mode slot of one sweep (CUDA events, outside the graph, "
+                                     "best of 3); algorithmic bytes: per tensor and mode the BLCO coordinate "
+                                     "(8 B) and value (8 B) of each nonzero, every other factor and the output "
+                                     "once"),
                 sequential_plans_ms_per_iter_est=seq_est, speedup_vs_sequential=seq_est / ms,
                 note="device time (CUDA events on the batch stream); sequential estimate from the first "
                      f"{k} tensors' plans (wall time), scaled by nnz")
@@ -550,7 +565,8 @@ def wide_cpu_baseline(args, X, dims, rk):
     R = po.ref_lib()
     if R is None:
         return None
-    sample = min(args.ref_sample, WIDE["nnz"])
+    total = int(X["vals"].numel())
+    sample = min(args.ref_sample, total)
     cidx = np.ascontiguousarray(np.stack([c[:sample].cpu().numpy().astype(np.uint64) for c in X["cidx"]]))
     vals = np.ascontiguousarray(X["vals"][:sample].cpu().numpy())
     nthreads = os.cpu_count() or 1
@@ -569,10 +585,10 @@ def wide_cpu_baseline(args, X, dims, rk):
         R.ref_alto_mttkrp128(h, m, rk, ptrs)
     dt = (time.perf_counter() - t0) * 1e3
     R.ref_alto_destroy128(h, rk)
-    return dict(value=dt / sample * WIDE["nnz"], unit="ms", cores=nthreads, kind="reference",
+    return dict(value=dt / sample * total, unit="ms", cores=nthreads, kind="reference",
                 sample=(f"reference mttkrp_alto_par on AltoTensor<unsigned __int128> (oracle/_ref), all "
                         f"{len(dims)} modes on the first {sample} nonzeros, {nthreads} threads, scaled linearly "
-                        f"to {WIDE['nnz']} nonzeros; MTTKRP part of the iteration only"))
+                        f"to {total} nonzeros; MTTKRP part of the iteration only"))
 
 
 def wide_leg(pkg, torch, args, peak, with_cpu):
@@ -580,7 +596,7 @@ def wide_leg(pkg, torch, args, peak, with_cpu):
     iteration, per-mode MTTKRP time and its roofline, the reference's CPU
     MTTKRP on a sample."""
     from blco_b200 import synth
-    dims, nnz, rk = WIDE["dims"], WIDE["nnz"], WIDE["rank"]
+    dims, nnz, rk = WIDE["dims"], args.wide_nnz, WIDE["rank"]
     X = synth.wide_tensor_device(nnz, dims, WIDE["zipf"], seed=WIDE["seed"])
     torch.cuda.synchronize()
     e0 = time.perf_counter()
@@ -614,7 +630,8 @@ def wide_leg(pkg, torch, args, peak, with_cpu):
     torch.cuda.empty_cache()
     alg = [mttkrp_alg_bytes(dims, nnz, rk, m) for m in range(len(dims))]
     achieved = sum(alg) / (sum(per_mode) * 1e-3) / 1e9
-    return dict(workload=WIDE["workload"], desc=WIDE["desc"], key_bits=inf["alto_bits"],
+    return dict(workload=WIDE["workload"] if nnz == WIDE["nnz"] else WIDE["workload"] + f"_at_{nnz}_nnz",
+                desc=WIDE["desc"], nnz=nnz, key_bits=inf["alto_bits"],
                 blocks=inf["block_count"], encode_ms=encode_ms,
                 ms_per_step=ev0.elapsed_time(ev1) / args.steps, steps=args.steps, fit_last=fits[-1],
                 mttkrp_ms_per_mode=[round(x, 4) for x in per_mode], gpu_launches=int(launches), dtype="f64",
@@ -690,11 +707,15 @@ def streamed_leg(pkg, torch, args):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.streamed_iters
+        _, promoted = plan.condition()
         h2d = len(dims) * nnz * bpn
         forms[name] = dict(ms_per_iter=ms, h2d_bytes_per_iter=h2d, h2d_gbs=h2d / (ms * 1e-3) / 1e9,
                            h2d_frac=h2d / (ms * 1e-3) / 1e9 / peak, fit_last=fits[-1],
                            device_bytes_plan=int(plan.device_bytes()),
-                           device_bytes_in_use=int(total_b - free_b))
+                           device_bytes_in_use=int(total_b - free_b), promoted_to_fp64=bool(promoted))
+        if promoted:  # the guard moved the mixed plan to FP64: FP64 values crossed the link
+            forms[name]["h2d_bytes_per_iter"] = h2d = len(dims) * nnz * 16
+            forms[name].update(h2d_gbs=h2d / (ms * 1e-3) / 1e9, h2d_frac=h2d / (ms * 1e-3) / 1e9 / peak)
         plan.destroy()
         del fs, lam
     forms["mixed_f32"]["fit_delta_vs_fp64"] = abs(forms["mixed_f32"]["fit_last"] - forms["fp64"]["fit_last"])
@@ -924,12 +945,65 @@ def run_ours(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def mttkrp_leg(pkg, torch, args):
+    """One MTTKRP per mode of the benchmark tensor (args.nnz nonzeros) with
+    factors of --mttkrp-dtype, each mode's schedule from --kernel, timed with
+    CUDA events: the kernels the ncu summaries capture."""
+    from blco_b200 import synth
+    dims, rk = WORKLOAD["dims"], WORKLOAD["rank"]
+    X = synth.zipf_tensor_device(args.nnz, dims, WORKLOAD["zipf"], seed=args.seed)
+    t = pkg.Tensor.encode_device(dims, X["cidx"], X["vals"])
+    del X
+    torch.cuda.empty_cache()
+    g = torch.Generator(device="cuda").manual_seed(1)
+    fs = [torch.rand(d, rk, dtype=torch.float64, device="cuda", generator=g) for d in dims]
+    dt = args.mttkrp_dtype
+    if dt != "f64":
+        fs = [f.to(torch.float32 if dt == "f32" else torch.bfloat16) for f in fs]
+    code = {"f64": pkg.DTYPE_F64, "f32": pkg.DTYPE_F32, "bf16": pkg.DTYPE_BF16}[dt]
+    o = pkg.make_opts(kernel=args.kernel)
+    sv, sf, so = {"f64": (8, 8, 8), "f32": (4, 4, 4), "bf16": (4, 2, 4)}[dt]
+    modes = []
+    for m in range(3):
+        out = torch.zeros(dims[m], rk, dtype=torch.float64 if dt == "f64" else torch.float32, device="cuda")
+        ts = []
+        for _ in range(args.mttkrp_reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            pkg.mttkrp_ex(t, m, fs, out, code, o)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        alg = mttkrp_alg_bytes(dims, args.nnz, rk, m, 8, sv, sf, so)
+        modes.append(dict(mode=m, ms=ts, alg_bytes=int(alg), gbs=alg / (min(ts) * 1e-3) / 1e9))
+    t.free()
+    return dict(nnz=args.nnz, dtype=dt, kernel=args.kernel, modes=modes)
+
+
+def gram_leg(pkg, torch, args):
+    """The mixed form's Gram of a 2M x 32 FP32 factor, tensor-core and
+    CUDA-core engines (twice each: a warm-up, then the captured launch)."""
+    U = torch.rand(2_000_000, 32, dtype=torch.float32, device="cuda") - 0.3
+    ref = U.double().T @ U.double()
+    out = {}
+    for tc in (True, False):
+        for _ in range(2):
+            G = pkg.gram_f32(U, tensor_cores=tc)
+        out["tensor_cores" if tc else "cuda_cores"] = (torch.linalg.norm(G - ref) / torch.linalg.norm(ref)).item()
+    return dict(rows=2_000_000, rank=32, rel_err=out)
+
+
 def run_only(args, local):
     """One leg alone on one GPU (the commands of the ncu summaries)."""
     import torch
     torch.cuda.set_device(local)
     pkg = load_pkg()
-    if args.only == "streamed":
+    if args.only == "mttkrp":
+        out = mttkrp_leg(pkg, torch, args)
+    elif args.only == "gram":
+        out = gram_leg(pkg, torch, args)
+    elif args.only == "streamed":
         out = streamed_leg(pkg, torch, args)
     elif args.only == "batched":
         out = batched_leg(pkg, torch, args)
@@ -964,8 +1038,12 @@ def main():
     ap.add_argument("--streamed-nnz", type=int, default=500_000_000,
                     help="nonzeros of the streamed leg (the configuration's full size is 2000000000)")
     ap.add_argument("--streamed-iters", type=int, default=2)
-    ap.add_argument("--only", choices=["streamed", "batched", "wide", "c1"],
+    ap.add_argument("--only", choices=["mttkrp", "gram", "streamed", "batched", "wide", "c1"],
                     help="run one leg alone and print its JSON object")
+    ap.add_argument("--wide-nnz", type=int, default=WIDE["nnz"], help="nonzeros of the wide-key leg")
+    ap.add_argument("--batch-count", type=int, default=BATCH["count"], help="tensors of the batched leg")
+    ap.add_argument("--mttkrp-dtype", default="f32", choices=["f64", "f32", "bf16"])
+    ap.add_argument("--mttkrp-reps", type=int, default=1)
     ap.add_argument("--fit-iters", type=int, default=40,
                     help="iterations after which the forms' fits are compared (the timed steps, then untimed)")
     ap.add_argument("--forms", default="fp64,mixed_f32,mixed_bf16")

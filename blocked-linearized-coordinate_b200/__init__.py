@@ -63,7 +63,7 @@ EXPORTS = (
     "blco_cpals", "blco_cpals_plan_create", "blco_cpals_plan_iterate",
     "blco_cpals_plan_mttkrp_ms", "blco_cpals_plan_condition", "blco_cpals_plan_device_bytes", "blco_cpals_plan_destroy", "blco_batch_create",
     "blco_batch_iterate",
-    "blco_batch_destroy", "blco_batch_last_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
+    "blco_batch_destroy", "blco_batch_last_ms", "blco_batch_mttkrp_ms", "blco_tune_space", "blco_autotune", "blco_tune_features",
     "blco_mlp_create", "blco_mlp_num_params", "blco_mlp_set_params", "blco_mlp_get_params", "blco_mlp_predict",
     "blco_mlp_grad", "blco_mlp_train", "blco_mlp_destroy", "blco_selector_set", "blco_select", "blco_gram_f32",
     "blco_encode_tns", "blco_gram_tc_timeout_check", "blco_parse_decimal", "blco_launch_count", "blco_cpals_plan_set_reduce",
@@ -530,6 +530,12 @@ class Batch:
         """Device milliseconds of the sweeps of the last iterate call."""
         ms = ctypes.c_double()
         _check(lib().blco_batch_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def mttkrp_ms(self):
+        """Device milliseconds of one sweep's MTTKRP launches alone."""
+        ms = ctypes.c_double()
+        _check(lib().blco_batch_mttkrp_ms(self._h, ctypes.byref(ms)))
         return ms.value
 
     def destroy(self):

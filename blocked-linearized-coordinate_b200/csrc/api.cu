@@ -574,4 +574,10 @@ int blco_batch_last_ms(const blco_batch* b, double* ms)
     return BLCO_OK;
 }
 
+int blco_batch_mttkrp_ms(blco_batch* b, double* ms)
+{
+    if (!b || !ms) return fail(BLCO_ERR_INVALID, "null argument");
+    return batch_mttkrp_ms(b, ms);
+}
+
 } // extern "C"

@@ -2161,4 +2161,47 @@ int batch_destroy(blco_batch* b) { return batch_free(b); }
 
 double batch_last_ms(const blco_batch* b) { return b->last_ms; }
 
+// Device time of one sweep's MTTKRP launches alone (k_b_mttkrp of every mode
+// slot, each after its k_b_zero), outside the graph.  The MTTKRP results are
+// workspace that every sweep recomputes before use, so the iteration state
+// is unchanged.
+int batch_mttkrp_ms(blco_batch* b, double* ms)
+{
+    cudaEvent_t e[2 * BLCO_MAX_MODES] = {};
+    cudaError_t err = cudaSuccess;
+    for (int i = 0; i < 2 * BLCO_MAX_MODES && err == cudaSuccess; i++) err = cudaEventCreate(&e[i]);
+    int st = err == cudaSuccess ? BLCO_OK : cuda_fail(err, "cudaEventCreate", __FILE__, __LINE__);
+    int timed = 0;
+    for (int k = 0; k < b->maxN && st == BLCO_OK; k++) {
+        if (!b->mt_chunks[k]) continue;
+        k_b_zero<<<b->T * 8, 256, 0, b->s>>>(b->d_desc, b->T, k);
+        count_launch();
+        const unsigned grid =
+            (unsigned)std::min<uint64_t>((uint64_t)b->sm * BM_MINB, (b->mt_chunks[k] + BM_WARPS - 1) / BM_WARPS);
+        cudaEventRecord(e[2 * k], b->s);
+        k_b_mttkrp<<<grid, BM_THREADS, 0, b->s>>>(b->d_desc, b->T, b->d_choff + (size_t)k * (b->T + 1), k);
+        count_launch();
+        cudaEventRecord(e[2 * k + 1], b->s);
+        err = cudaGetLastError();
+        if (err != cudaSuccess) st = cuda_fail(err, "k_b_mttkrp", __FILE__, __LINE__);
+        timed |= 1 << k;
+    }
+    if (st == BLCO_OK) {
+        err = cudaStreamSynchronize(b->s);
+        if (err != cudaSuccess) st = cuda_fail(err, "batch MTTKRP timing", __FILE__, __LINE__);
+    }
+    double total = 0.0;
+    for (int k = 0; k < b->maxN && st == BLCO_OK; k++) {
+        if (!(timed & (1 << k))) continue;
+        float x = 0.f;
+        err = cudaEventElapsedTime(&x, e[2 * k], e[2 * k + 1]);
+        if (err != cudaSuccess) st = cuda_fail(err, "cudaEventElapsedTime", __FILE__, __LINE__);
+        total += x;
+    }
+    for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    if (st == BLCO_OK) *ms = total;
+    return st;
+}
+
 } // namespace blco

@@ -28,15 +28,17 @@
 //
 // Kernel: a group of L lanes holds one R-wide row, 16 bytes per lane
 // (L = R * element bytes / 16: 8 lanes for FP32 at R = 32, 16 for FP64).
-// Each group walks its own contiguous range of positions (ranges split the
-// work with loose nonzeros weighted by their extra gathers, start on
-// 256-position boundaries and are fixed per launch), four nonzeros per step
-// with all of a step's gathers issued before any product.  The fibre sum s,
-// the row sum and the fibre row c stay in registers; the next fibre's row is
-// gathered one fibre ahead.  A row's sum goes to the output with atomics when
-// the row run ends (ranges overlap rows only at their ends).
-// Partial sums in the mixed forms are FP32 over at most 64 nonzeros and are
-// folded into FP64 registers (every 16 steps, and on every flush), so a
+// Work comes in tasks of 256 positions per lane group (32 / L groups per
+// warp), fibred tasks first; warps take tasks from a counter in a strided
+// order (consecutive takers land far apart in the stream, so concurrent
+// warps share few output rows), or in stream order.  A group walks its 256
+// positions four nonzeros per step, with all of a step's gathers issued
+// before any product and the next step's index words loaded ahead.  The
+// fibre sum s, the row sum and the fibre row c stay in registers; the next
+// fibre's row is gathered one fibre ahead.  A row's sum goes to the output
+// with atomics when the row run ends (tasks overlap rows only at their
+// ends).  Partial sums in the mixed forms are FP32 over one step (at most
+// four products) and are folded into FP64 registers after every step, so a
 // heavy row's millions of terms are summed in FP64.
 #include <cuda_bf16.h>
 

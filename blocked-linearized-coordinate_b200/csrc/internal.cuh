@@ -294,6 +294,7 @@ int batch_create(int T, blco_tensor* const* tensors, const int* ranks, double* c
 int batch_iterate(blco_batch* b, int iters, double* fits, int* iters_done);
 int batch_destroy(blco_batch* b);
 double batch_last_ms(const blco_batch* b);
+int batch_mttkrp_ms(blco_batch* b, double* ms);
 int cpals_host(blco_tensor* t, int rank, double* const* factors, double* lambda, int maxiter,
                double tol, const blco_opts* opts, double* fit_out, double* fits, int* iters_out);
 

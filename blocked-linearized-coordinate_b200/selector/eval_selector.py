@@ -10,7 +10,9 @@ reference's -k 10 rule (src/alto_dev.cu:1975,1996-2001).  Fit: for the
 first --fit-tensors held-out tensors (made again from their recorded
 generator parameters), CP-ALS in the mixed form with the learned schedule
 (kernel id 21) against the FP64 form with kernel 10, same initial factors,
---iters iterations; |fit difference| per tensor.
+--iters iterations (40): |fit difference| per tensor at the end and after
+10 iterations, and whether the mixed plan's condition guard moved it to
+FP64.
 """
 import argparse
 import importlib.util
@@ -47,7 +49,7 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "eval.json"))
     ap.add_argument("--params", default=None, help="trained selector (default: the committed one)")
     ap.add_argument("--fit-tensors", type=int, default=20)
-    ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--iters", type=int, default=40)
     a = ap.parse_args()
     import torch
     pkg = load()
@@ -106,17 +108,22 @@ def main():
             w0 = time.time()
             f = plan.iterate(a.iters, tol=-1.0)
             torch.cuda.synchronize()
-            res[name] = (float(f[-1]), time.time() - w0)
+            _, promoted = plan.condition()
+            res[name] = (float(f[-1]), time.time() - w0, float(f[min(10, len(f)) - 1]), bool(promoted))
             plan.destroy()
         t.free()
         torch.cuda.empty_cache()
         d = abs(res["mixed"][0] - res["fp64"][0])
+        d10 = abs(res["mixed"][2] - res["fp64"][2])
         fits.append(dict(tensor=int(ti), dims=dims, nnz=nnz, zipf=s, rank=R, fit_fp64=res["fp64"][0],
-                         fit_mixed=res["mixed"][0], abs_diff=d))
+                         fit_mixed=res["mixed"][0], abs_diff=d, abs_diff_at_10=d10,
+                         mixed_promoted_to_fp64=res["mixed"][3]))
         print(f"tensor {ti}: dims {dims} nnz {nnz} R {R} fit fp64 {res['fp64'][0]:.9f} mixed "
-              f"{res['mixed'][0]:.9f} |diff| {d:.2e}", flush=True)
+              f"{res['mixed'][0]:.9f} |diff| {d:.2e} (at 10: {d10:.2e}) promoted {res['mixed'][3]}", flush=True)
     pkg.selector_set(None)
-    out["fit"] = dict(iters=a.iters, tensors=fits, max_abs_diff=max([x["abs_diff"] for x in fits] or [0.0]))
+    out["fit"] = dict(iters=a.iters, tensors=fits, max_abs_diff=max([x["abs_diff"] for x in fits] or [0.0]),
+                      max_abs_diff_at_10=max([x["abs_diff_at_10"] for x in fits] or [0.0]),
+                      promoted=sum(x["mixed_promoted_to_fp64"] for x in fits))
     with open(a.out, "w") as fo:
         json.dump(out, fo, indent=1)
     print("wrote", a.out, "max |fit diff|", out["fit"]["max_abs_diff"])

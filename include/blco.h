@@ -377,6 +377,11 @@ int blco_batch_destroy(blco_batch* b);
 /* Device time (CUDA events on the batch's stream) of the sweeps run by the
  * last blco_batch_iterate call, in milliseconds. */
 int blco_batch_last_ms(const blco_batch* b, double* ms);
+/* Device time of one sweep's MTTKRP launches alone (the persistent batched
+ * MTTKRP of every mode slot, outside the graph; the batch's state is
+ * unchanged: the MTTKRP results are recomputed by every sweep), in
+ * milliseconds.  Synchronous on the batch's stream. */
+int blco_batch_mttkrp_ms(blco_batch* b, double* ms);
 
 /* ---- MTTKRP schedule selection (no counterpart in the reference, which
  * has the fixed -k 10 rule, src/alto_dev.cu:1975,1996-2001). */

@@ -57,7 +57,7 @@ def _alone(blco, items, iters, tol):
     return res
 
 
-def _batched(blco, items, iters, tol, opts=None, split=None):
+def _batched(blco, items, iters, tol, opts=None, split=None, time_mttkrp=False):
     ts, fs, ls = [], [], []
     for dims, cidx, vals, R, f0 in items:
         ts.append(blco.Tensor.encode(dims, cidx, vals))
@@ -69,6 +69,8 @@ def _batched(blco, items, iters, tol, opts=None, split=None):
     for k in parts:
         fk, done = b.iterate(k)
         fits.append(fk)
+        if time_mttkrp:
+            assert b.mttkrp_ms() > 0.0
     b.destroy()
     for t in ts:
         t.free()
@@ -113,6 +115,15 @@ def test_batch_graph_and_split_calls(blco):
     fits, done, fs, ls = _batched(blco, items, 10, 0.0, opts=blco.make_opts(verbose=-1), split=[3, 0, 7])
     _compare(alone, fits, done, fs, ls)
     fits, done, fs, ls = _batched(blco, items, 10, 0.0, split=[1, 4, 5])
+    _compare(alone, fits, done, fs, ls)
+
+
+def test_batch_mttkrp_timing_leaves_the_state(blco):
+    """Timing one sweep's MTTKRP launches between calls (blco_batch_mttkrp_ms)
+    leaves the run as it was: the same fits and factors as blco_cpals."""
+    items = _make(4, CASES[:6])
+    alone = _alone(blco, items, 9, 0.0)
+    fits, done, fs, ls = _batched(blco, items, 9, 0.0, split=[2, 3, 4], time_mttkrp=True)
     _compare(alone, fits, done, fs, ls)
 
 
