@@ -221,78 +221,109 @@ __global__ __launch_bounds__(DN_THREADS) void k_update(const TM* __restrict__ M,
     }
 }
 
-// Register-tiled form of k_update for R in {16, 32, 64}: a block stages 64
-// rows of M in shared memory; thread (rg, cg) of 16 x 16 computes rows
-// 4*rg..4*rg+3 and columns cg*CPT..cg*CPT+CPT-1 (CPT = R / 16), so each
-// inner step reuses 4 M values and CPT P values for 4*CPT FMAs.
-constexpr int UT_ROWS = 64;
-
-// The product is formed in FP64 whatever the storage type T: the
+// Register-tiled form of k_update for R in {16, 32, 64} (U 16-byte
+// aligned).  The product is formed in FP64 whatever the storage type T: the
 // pseudoinverse of an ill-conditioned Hadamard product of Grams turns FP32
 // rounding in this step into fit errors well above 1e-5.
+template <int R>
+struct UpdShape {
+    static constexpr int CG = R / 4;            // column groups: 4 columns of U per thread
+    static constexpr int RG = DN_THREADS / CG;  // row groups: 4 rows of U per thread
+    static constexpr int TR = 4 * RG;           // rows of M per tile
+    static constexpr int TRP = TR + 2;          // padded row stride of the transposed tile (even: 16-byte reads)
+    static constexpr int NL = TR * R / DN_THREADS; // elements of M each thread loads per tile
+    static constexpr size_t SMEM = ((size_t)R * R + (size_t)R * TRP + (size_t)RG * R) * sizeof(double);
+};
+
 template <typename TM, typename T, int R>
-__global__ __launch_bounds__(DN_THREADS) void k_update_tiled(const TM* __restrict__ M, const double* __restrict__ P,
-                                                             T* __restrict__ U, uint64_t I,
-                                                             double* __restrict__ colsq_partials)
+__global__ __launch_bounds__(DN_THREADS, 2) void k_update_tiled(const TM* __restrict__ M, const double* __restrict__ P,
+                                                                T* __restrict__ U, uint64_t I,
+                                                                double* __restrict__ colsq_partials)
 {
-    constexpr int CPT = R / 16;
+    // U = M P^T in FP64, tile by tile: TR rows of M staged transposed in
+    // shared memory (MsT[k][row]), each thread a 4 x 4 block of U, so every
+    // k step is four 16-byte shared loads (4 rows of M, 4 columns of P^T) for
+    // 16 FMAs; the next tile's M is loaded into registers while this one is
+    // multiplied.  Column sums of squares of the stored U ride along.
+    using S = UpdShape<R>;
     extern __shared__ __align__(16) double us[];
-    double* csq = us;                                        // [16 row groups][R]
-    double* PT = us + 16 * R;                                // [R][R], PT[k][c] = P[c][k]
-    double* Ms = PT + R * R;                                 // [UT_ROWS][R + 1]
-    const int tid = threadIdx.x, rg = tid / 16, cg = tid % 16;
+    double* PT = us;                  // [R][R], PT[k][c] = P[c][k]
+    double* MsT = PT + R * R;         // [R][TRP]
+    double* csq = MsT + R * S::TRP;   // [RG][R]
+    const int tid = threadIdx.x, rg = tid / S::CG, cg = tid % S::CG;
     for (int k = tid; k < R * R; k += DN_THREADS) {
-        int c = k / R, kk = k % R;
+        const int c = k / R, kk = k % R;
         PT[kk * R + c] = P[k];
     }
-    double sq[CPT];
+    double sq[4] = {0.0, 0.0, 0.0, 0.0};
+    const uint64_t ntile = (I + S::TR - 1) / S::TR;
+    const uint64_t per = (ntile + gridDim.x - 1) / gridDim.x;
+    const uint64_t t_beg = per * blockIdx.x, t_end = min(ntile, t_beg + per);
+    double nxt[S::NL];
+    auto load = [&](uint64_t t) {
+        const uint64_t base = t * S::TR * (uint64_t)R, lim = I * (uint64_t)R;
 #pragma unroll
-    for (int j = 0; j < CPT; j++) sq[j] = 0.0;
-    const uint64_t per = (I + gridDim.x - 1) / gridDim.x;
-    const uint64_t beg = per * blockIdx.x, end = min(I, beg + per);
-    for (uint64_t r0 = beg; r0 < end; r0 += UT_ROWS) {
-        const int nr = (int)min((uint64_t)UT_ROWS, end - r0);
+        for (int i = 0; i < S::NL; i++) {
+            const uint64_t e = base + tid + (uint64_t)i * DN_THREADS;
+            nxt[i] = e < lim ? (double)M[e] : 0.0;
+        }
+    };
+    if (t_beg < t_end) load(t_beg);
+    for (uint64_t t = t_beg; t < t_end; t++) {
+        __syncthreads(); // the previous tile's MsT reads are done
+#pragma unroll
+        for (int i = 0; i < S::NL; i++) {
+            const int e = tid + i * DN_THREADS;
+            MsT[(e % R) * S::TRP + e / R] = nxt[i];
+        }
         __syncthreads();
-        for (int k = tid; k < nr * R; k += DN_THREADS) Ms[(k / R) * (R + 1) + (k % R)] = (double)M[r0 * R + k];
-        __syncthreads();
-        double acc[4][CPT];
+        if (t + 1 < t_end) load(t + 1);
+        double acc[4][4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < CPT; j++) acc[i][j] = 0.0;
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
 #pragma unroll 8
         for (int k = 0; k < R; k++) {
-            double m[4], pv[CPT];
-#pragma unroll
-            for (int i = 0; i < 4; i++) m[i] = Ms[(4 * rg + i) * (R + 1) + k];
-#pragma unroll
-            for (int j = 0; j < CPT; j++) pv[j] = PT[k * R + cg * CPT + j];
+            const double2 m01 = *reinterpret_cast<const double2*>(MsT + k * S::TRP + 4 * rg);
+            const double2 m23 = *reinterpret_cast<const double2*>(MsT + k * S::TRP + 4 * rg + 2);
+            const double2 p01 = *reinterpret_cast<const double2*>(PT + k * R + 4 * cg);
+            const double2 p23 = *reinterpret_cast<const double2*>(PT + k * R + 4 * cg + 2);
+            const double m[4] = {m01.x, m01.y, m23.x, m23.y};
+            const double pv[4] = {p01.x, p01.y, p23.x, p23.y};
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < CPT; j++) acc[i][j] += m[i] * pv[j];
+                for (int j = 0; j < 4; j++) acc[i][j] = fma(m[i], pv[j], acc[i][j]);
         }
+        const uint64_t r0 = t * S::TR + 4 * rg;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            const int r = 4 * rg + i;
-            if (r < nr) {
+            if (r0 + i < I) {
+                T u[4];
 #pragma unroll
-                for (int j = 0; j < CPT; j++) {
-                    const T u = (T)acc[i][j];
-                    U[(r0 + r) * R + cg * CPT + j] = u;
-                    sq[j] += (double)u * (double)u;
+                for (int j = 0; j < 4; j++) {
+                    u[j] = (T)acc[i][j];
+                    sq[j] += (double)u[j] * (double)u[j];
+                }
+                T* dst = U + (r0 + i) * R + 4 * cg;
+                if constexpr (sizeof(T) == 4) {
+                    *reinterpret_cast<float4*>(dst) = make_float4(u[0], u[1], u[2], u[3]);
+                } else {
+                    reinterpret_cast<double2*>(dst)[0] = make_double2(u[0], u[1]);
+                    reinterpret_cast<double2*>(dst)[1] = make_double2(u[2], u[3]);
                 }
             }
         }
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < CPT; j++) csq[rg * R + cg * CPT + j] = sq[j];
+    for (int j = 0; j < 4; j++) csq[rg * R + 4 * cg + j] = sq[j];
     __syncthreads();
     for (int c = tid; c < R; c += DN_THREADS) {
-        double t = 0.0;
-        for (int g = 0; g < 16; g++) t += csq[g * R + c];
-        colsq_partials[(size_t)blockIdx.x * R + c] = t;
+        double x = 0.0;
+        for (int g = 0; g < S::RG; g++) x += csq[g * R + c];
+        colsq_partials[(size_t)blockIdx.x * R + c] = x;
     }
 }
 
@@ -741,8 +772,8 @@ template <typename TM, typename T>
 int update_launch(blco_cpals_plan* p, const TM* M, T* U, uint64_t I, int grid)
 {
     const int R = p->R;
-    if (R == 16 || R == 32 || R == 64) {
-        size_t smem = ((size_t)16 * R + (size_t)R * R + (size_t)UT_ROWS * (R + 1)) * sizeof(double);
+    if ((R == 16 || R == 32 || R == 64) && reinterpret_cast<uintptr_t>(U) % 16 == 0) {
+        const size_t smem = R == 16 ? UpdShape<16>::SMEM : R == 32 ? UpdShape<32>::SMEM : UpdShape<64>::SMEM;
         void (*fn)(const TM*, const double*, T*, uint64_t, double*) =
             R == 16 ? k_update_tiled<TM, T, 16> : R == 32 ? k_update_tiled<TM, T, 32> : k_update_tiled<TM, T, 64>;
         BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -60,7 +60,7 @@ namespace blco {
 
 namespace {
 
-constexpr int TG_THREADS = 128;   // 4 warps: one TMEM lane quarter each
+constexpr int TG_LANES = 128;     // TMEM lanes: D rows, one quarter per warp (warp id mod 4)
 constexpr uint32_t TG_SPIN_MAX = 1u << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -147,8 +147,12 @@ struct GramShape {
     static constexpr int NCOLS = MG == 2 ? 512 : N <= 32 ? 32 : N <= 64 ? 64 : 128;
     static constexpr int KS = RB == 64 ? 64 : 256;      // rows per fold (a super-tile)
     static constexpr int CH = KS / 8;                   // K chunks of S
-    static constexpr int NV = (KS * RB / 4 + TG_THREADS - 1) / TG_THREADS; // float4 loads per thread
     static constexpr bool REG = RB <= 32;               // digit-row sums in registers
+    // threads: 8 warps with register sums (two per TMEM lane quarter, each
+    // pair splitting D's columns in halves), 4 with shared-memory sums
+    static constexpr int THREADS = REG ? 256 : 128;
+    static constexpr int HALVES = THREADS / TG_LANES;
+    static constexpr int NV = (KS * RB / 4 + THREADS - 1) / THREADS; // float4 loads per thread
     static constexpr int MINB = RB == 64 ? 1 : 2;       // CTAs per SM the registers must allow
     static constexpr size_t S_BYTES = (size_t)CH * ROWS * 16;
     static constexpr size_t STAGE_BYTES = (size_t)KS * RB * 4;
@@ -167,18 +171,21 @@ __device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, cons
 {
     using G = GramShape<RB>;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int lane_row = tid % TG_LANES, half = tid / TG_LANES;
+    const uint32_t quarter = (uint32_t)(warp % 4) * 32;
 #pragma unroll
     for (int g = 0; g < G::MG; g++) {
-        const int q = g * 128 + tid;
+        const int q = g * 128 + lane_row;
         const bool act = q < G::ND * RB;
         const double wa = act ? sd[q] : 0.0;
 #pragma unroll
-        for (int c0 = 0; c0 < G::N; c0 += 16) {
+        for (int c0 = 0; c0 < G::N / G::HALVES; c0 += 16) {
+            const int cb = half * (G::N / G::HALVES) + c0; // this half's columns of D
             uint32_t d[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(g * 256 + c0), d);
+            tmem_ld16(tmem + (quarter << 16) + (uint32_t)(g * 256 + cb), d);
 #pragma unroll
             for (int x = 0; x < 16; x++) {
-                const int n = c0 + x;
+                const int n = cb + x;
                 const int c = n % RB;
                 if (act) {
                     const double v = (double)__uint_as_float(d[x]) * sd[n]; // exact: D times a power of two
@@ -191,7 +198,7 @@ __device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, cons
 }
 
 template <int RB, bool SCALE, bool BF16OUT>
-__global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(float* __restrict__ U, uint64_t I, int R,
+__global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k_gram_tc(float* __restrict__ U, uint64_t I, int R,
                                                         const double* __restrict__ inv,
                                                         uint16_t* __restrict__ bf16_out, uint64_t rows_per_cta,
                                                         double* __restrict__ partials, int* __restrict__ err,
@@ -212,10 +219,10 @@ __global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(flo
     const int nsup = r_beg < r_end ? (int)((r_end - r_beg + G::KS - 1) / G::KS) : 0;
     const int items = G::CH * R;          // (chunk j, column c): column c of 8 staged rows
 
-    for (int i = tid; i < G::CH * G::ROWS; i += TG_THREADS) S[i] = make_uint4(0, 0, 0, 0);
-    for (int i = tid; i < 2 * RB; i += TG_THREADS) (&cmax[0][0])[i] = 0u;
+    for (int i = tid; i < G::CH * G::ROWS; i += G::THREADS) S[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < 2 * RB; i += G::THREADS) (&cmax[0][0])[i] = 0u;
     if constexpr (!G::REG)
-        for (int i = tid; i < G::ND * RB * (RB + 1); i += TG_THREADS) gsm[i] = 0.0;
+        for (int i = tid; i < G::ND * RB * (RB + 1); i += G::THREADS) gsm[i] = 0.0;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -251,7 +258,7 @@ __global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(flo
             float4 buf[G::NV];
 #pragma unroll
             for (int k = 0; k < G::NV; k++) {
-                const int f = tid + k * TG_THREADS;
+                const int f = tid + k * G::THREADS;
                 const uint64_t e0 = 4 * (uint64_t)f;
                 float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (f < nv4 && e0 < valid) {
@@ -267,7 +274,7 @@ __global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(flo
             }
 #pragma unroll
             for (int k = 0; k < G::NV; k++) {
-                const int f = tid + k * TG_THREADS;
+                const int f = tid + k * G::THREADS;
                 if (f >= nv4) continue;
                 if (SCALE || BF16OUT) {
                     const uint64_t e0 = 4 * (uint64_t)f;
@@ -300,7 +307,7 @@ __global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(flo
         // the next super-tile's maxima (last read before the previous MMA issue)
         if (tid < RB) cmax[b ^ 1][tid] = 0u;
         __syncthreads();
-        for (int it = tid; it < items; it += TG_THREADS) {
+        for (int it = tid; it < items; it += G::THREADS) {
             const int j = it / R, c = it % R;
             float m = 0.f;
 #pragma unroll
@@ -308,7 +315,7 @@ __global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(flo
             atomicMax(&cmax[b][c], __float_as_uint(m));
         }
         __syncthreads();
-        for (int k = tid; k < G::ND * RB; k += TG_THREADS)
+        for (int k = tid; k < G::ND * RB; k += G::THREADS)
             sdj[b][k] = pow2_f64(exponent_of(cmax[b][k % RB]) - 8 - 8 * (k / RB));
         // the previous super-tile's MMAs: complete before S is rewritten and D read
         if (t > 0 && cta_wait_late(bar, (phase - 1) & 1, spin_max)) {
@@ -316,7 +323,7 @@ __global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(flo
             break;
         }
         // digits of this super-tile into S
-        for (int it = tid; it < items; it += TG_THREADS) {
+        for (int it = tid; it < items; it += G::THREADS) {
             const int j = it / R, c = it % R;
             const int ex = exponent_of(cmax[b][c]);
             uint32_t h[G::ND][4];
@@ -384,14 +391,19 @@ __global__ void __launch_bounds__(TG_THREADS, GramShape<RB>::MINB) k_gram_tc(flo
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::NCOLS));
     }
     if constexpr (G::REG) {
-        // S and the staged rows are no longer read (barrier above): the sums go there
-        if (tid < G::ND * RB)
+        // S and the staged rows are no longer read (barrier above): the sums
+        // go there, the second half of the CTA adding its columns' share
+        const int q = tid % TG_LANES;
 #pragma unroll
-            for (int c = 0; c < RB; c++) gsm[tid * (RB + 1) + c] = acc[c];
-        __syncthreads();
+        for (int h = 0; h < G::HALVES; h++) {
+            if (tid / TG_LANES == h && q < G::ND * RB)
+#pragma unroll
+                for (int c = 0; c < RB; c++) gsm[q * (RB + 1) + c] = (h ? gsm[q * (RB + 1) + c] : 0.0) + acc[c];
+            __syncthreads();
+        }
     }
     // G_cta[a][c] = sum over digits i of the rows i RB + a
-    for (int e = tid; e < R * R; e += TG_THREADS) {
+    for (int e = tid; e < R * R; e += G::THREADS) {
         const int a = e / R, c = e % R;
         double g = 0.0;
 #pragma unroll
@@ -421,7 +433,7 @@ int gram_tc_dispatch(float* U, uint64_t I, int R, const double* inv, uint16_t* b
     BLCO_CUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
     BLCO_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     BLCO_CUDA(cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-    const int by_regs = regs_sm / (std::max(1, fa.numRegs) * TG_THREADS);
+    const int by_regs = regs_sm / (std::max(1, fa.numRegs) * G::THREADS);
     const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + (size_t)smem_rsv);
     const uint64_t per_sm = (uint64_t)std::max(1, std::min({8, 512 / G::NCOLS, by_regs, by_smem}));
     const uint64_t sups = (I + G::KS - 1) / G::KS;
@@ -429,7 +441,7 @@ int gram_tc_dispatch(float* U, uint64_t I, int R, const double* inv, uint16_t* b
     const uint64_t sups_per = std::max<uint64_t>(1, (sups + maxc - 1) / maxc);
     const uint64_t rows_per = sups_per * G::KS;
     const int grid = (int)std::max<uint64_t>(1, (I + rows_per - 1) / rows_per);
-    fn<<<grid, TG_THREADS, smem, s>>>(U, I, R, inv, bf16_out, rows_per, partials, d_err, spin_max, no_commit);
+    fn<<<grid, G::THREADS, smem, s>>>(U, I, R, inv, bf16_out, rows_per, partials, d_err, spin_max, no_commit);
     BLCO_CHECK_LAUNCH("k_gram_tc");
     *nparts = grid;
     return BLCO_OK;
