@@ -1168,13 +1168,18 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     for (int n = 0; n < p->N && st == BLCO_OK; n++)
         st = resolve_schedule(t, n, R, p->gather_dtype, p->opts.kernel, p->s, &p->sched[n]);
     if (st != BLCO_OK) { plan_free(p); return st; }
-    // compressed-fibre copies of the modes that use them, built now rather
-    // than inside the first iteration
-    for (int n = 0; n < p->N && st == BLCO_OK; n++)
-        if (t->resident &&
-            mttkrp_select_kernel(t, n, R, p->sched[n].kernel, p->gather_dtype) == BLCO_KERNEL_FIBRE &&
+    // the stream copies the modes' schedules read (compressed fibres, or
+    // heavy rows and cold stream), built now rather than inside the first
+    // iteration
+    for (int n = 0; n < p->N && st == BLCO_OK; n++) {
+        if (!t->resident) continue;
+        const int k = mttkrp_select_kernel(t, n, R, p->sched[n].kernel, p->gather_dtype);
+        if (k == BLCO_KERNEL_FIBRE &&
             (p->sched[n].kernel == BLCO_KERNEL_FIBRE || p->sched[n].kernel == BLCO_KERNEL_AUTO))
             st = build_fibre_copy(t, n, p->s);
+        else if (k == BLCO_KERNEL_LVL2) // the heavy-row schedule's stream copies, likewise
+            st = build_mode_copies(t, n, p->s);
+    }
     if (st != BLCO_OK) { plan_free(p); return st; }
     // Descending mode length, ties in natural order (src/cpd_gpu.cu:137-139).
     for (int n = 0; n < p->N; n++) p->order[n] = n;

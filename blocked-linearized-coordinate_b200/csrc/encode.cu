@@ -952,13 +952,14 @@ uint32_t host_hash_row(uint32_t r) { return (r * 2654435761u) >> 7; }
 // nonzero as with the BLCO stream itself.  In the row-ordered cold stream a
 // 32-nonzero tile spans few rows, so the tile kernel's segmented reduction
 // leaves few atomics (FP64 MTTKRP about 30% faster than on ALTO order).
-int build_hot_csr(blco_tensor* t, cudaStream_t s)
+// Built for one mode on its first use by a schedule that reads them (the
+// heavy-row kernel beside the tile kernel), or at plan creation for such a
+// schedule; the compressed-fibre schedule never reads them.
+int build_mode_copies(blco_tensor* t, int mode, cudaStream_t s)
 {
     const Layout& L = t->layout;
-    if (t->nnz == 0) return BLCO_OK;
-    bool any = false;
-    for (int n = 0; n < L.nmodes; n++) any |= t->hot[n].nhot > 0;
-    if (!any) return BLCO_OK;
+    if (t->nnz == 0 || !t->resident || mode < 0 || mode >= L.nmodes) return BLCO_OK;
+    if (t->hot[mode].nhot == 0 || t->hot[mode].hot_nnz == 0 || t->hot[mode].d_hcoords) return BLCO_OK;
     DeviceInfo di;
     BLCO_TRY(device_info(t->device, &di));
     uint64_t *k0 = nullptr, *k1 = nullptr;
@@ -980,9 +981,8 @@ int build_hot_csr(blco_tensor* t, cudaStream_t s)
         return cuda_fail(e, "hot-row index scratch", __FILE__, __LINE__);
     }
     const int grid = (int)std::min<uint64_t>((t->nnz + 255) / 256, (uint64_t)di.sm_count * 16);
-    for (int n = 0; n < L.nmodes && st == BLCO_OK; n++) {
+    for (int n = mode; n == mode && st == BLCO_OK; n++) {
         HotTable& ht = t->hot[n];
-        if (ht.nhot == 0 || ht.hot_nnz == 0) continue;
         k_row_keys<<<grid, 256, 0, s>>>(t->d_coords, t->nnz, L.mode_pos[n], L.mode_masks[n], k0);
         count_launch();
         bool alt0 = false;
@@ -1150,10 +1150,10 @@ static int build_hot_tables_impl(blco_tensor* t, cudaStream_t s, uint32_t* count
         BLCO_CUDA(cudaMemcpyAsync(ht.d_ptr, ptr.data(), (ht.nhot + 1) * 4, cudaMemcpyHostToDevice, s));
     }
     BLCO_CUDA(cudaStreamSynchronize(s));
-    // The per-mode execution copies live in HBM and serve resident streams
-    // only; a streamed tensor keeps just the statistics and hash tables, so
-    // that its device footprint stays the ring of block buffers.
-    if (t->resident) BLCO_TRY(build_hot_csr(t, s));
+    // The per-mode execution copies (build_mode_copies) are made on first
+    // use, for resident streams only; a streamed tensor keeps just the
+    // statistics and hash tables, so that its device footprint stays the
+    // ring of block buffers.
     return BLCO_OK;
 }
 

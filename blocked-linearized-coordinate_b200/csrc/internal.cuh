@@ -254,6 +254,10 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 bool fibre_eligible(const blco_tensor* t, int mode);
 int fibre_lanes(int rank, int dtype); // lanes per factor row, 0 = no kernel for this rank
 int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s);
+// encode.cu: the mode's heavy-row and cold stream copies (HotTable), built
+// on first use by the heavy-row schedule (no-op when built, not resident,
+// or the mode has no heavy rows).
+int build_mode_copies(blco_tensor* t, int mode, cudaStream_t s);
 // The fibre kernel can serve this call (resident stream, rank, alignment).
 bool fibre_usable(const blco_tensor* t, const MttkrpArgs& a);
 // The call takes the fibre kernel: kernel id 4, or the automatic rule

@@ -1360,6 +1360,8 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s)
         if (m != a.mode && ((uintptr_t)a.factors[m] & 15u) != 0) aligned16 = false;
     size_t hash_bytes = 0;
     HotFn hot_fn = nullptr;
+    if (kern == BLCO_KERNEL_LVL2 && ht.nhot > 0 && !ht.d_hcoords && aligned16 && a.coords == t->d_coords)
+        BLCO_TRY(build_mode_copies(const_cast<blco_tensor*>(t), a.mode, s)); // first use
     if (kern == BLCO_KERNEL_LVL2 && ht.nhot > 0 && ht.d_hcoords && aligned16 && a.coords == t->d_coords) {
         switch (a.factor_dtype) {
         case BLCO_DTYPE_F64: hot_fn = pick_hot<PolicyF64>(L.nmodes, a.rank); break;
