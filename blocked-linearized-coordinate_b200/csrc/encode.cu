@@ -18,7 +18,9 @@
 #include <algorithm>
 #include <cstring>
 #include <atomic>
+#include <memory>
 #include <mutex>
+#include <new>
 #include <thread>
 
 #include "internal.cuh"
@@ -1165,11 +1167,13 @@ int build_hot_tables(blco_tensor* t, cudaStream_t s) { return build_hot_tables_i
 // the device.  Its encode then runs in chunks that fit the residency
 // budget: per chunk, the COO slice is copied in (from host or device
 // memory), keyed (k_alto_keys), counted per row (k_coo_counts), sorted by
-// key (stable radix sort) and copied back as (key, value) runs.  The host
-// merges the runs by key, ties in chunk order, so the result is the stable
-// key order of the whole input, the same as the one-pass encoder's, and
-// writes BLCO coordinates (key re-linearized through the byte table) and
-// values into the pinned stream.
+// key (stable radix sort) and copied back as (key, value) runs.  The runs
+// are then merged on the GPU, one budget-sized output segment at a time
+// (each run's share of the segment found by a search on the host, ties in
+// chunk order), so the result is the stable key order of the whole input,
+// the same as the one-pass encoder's; the merge's last sort pass writes BLCO
+// coordinates (key re-linearized through the byte table) and the segment
+// goes to the pinned stream.
 
 uint64_t stream_chunk_nnz(const blco_opts* opts, int nmodes)
 {
@@ -1193,8 +1197,20 @@ static int encode_chunked(blco_tensor* t, const uint64_t* const* cidx, const dou
     uint32_t* counts = nullptr;
     int* d_bad = nullptr;
     EncTables* d_tabs = nullptr;
-    uint64_t* hk = nullptr; // sorted keys of every chunk (pinned)
+    // sorted keys and values of every chunk: pageable host memory (pinning
+    // 16 B per nonzero costs more than the slower copies into it save)
+    std::unique_ptr<uint64_t[]> hk_own;
+    std::unique_ptr<double[]> hv_own;
+    uint64_t* hk = nullptr;
     double* hv = nullptr;
+    // the pinned stream itself is allocated on two host threads while the
+    // chunks are sorted (page-locking is the slowest step of this encode)
+    std::thread pin_c, pin_v;
+    cudaError_t pin_e[2] = {cudaSuccess, cudaSuccess};
+    auto join_pins = [&]() {
+        if (pin_c.joinable()) pin_c.join();
+        if (pin_v.joinable()) pin_v.join();
+    };
     auto release = [&]() {
         cudaStreamSynchronize(s);
         for (auto& p : dc) { cudaFree(p); p = nullptr; }
@@ -1207,8 +1223,7 @@ static int encode_chunked(blco_tensor* t, const uint64_t* const* cidx, const dou
         cudaFree(counts);
         cudaFree(d_bad);
         cudaFree(d_tabs);
-        if (hk) cudaFreeHost(hk);
-        if (hv) cudaFreeHost(hv);
+        join_pins();
     };
 #define CH_CUDA(call)                                                           \
     do {                                                                        \
@@ -1237,8 +1252,38 @@ static int encode_chunked(blco_tensor* t, const uint64_t* const* cidx, const dou
     EncTables htabs = make_tables(L);
     CH_CUDA(cudaMalloc(&d_tabs, sizeof(EncTables)));
     CH_CUDA(cudaMemcpyAsync(d_tabs, &htabs, sizeof(EncTables), cudaMemcpyHostToDevice, s));
-    CH_CUDA(cudaMallocHost(&hk, nnz * 8));
-    CH_CUDA(cudaMallocHost(&hv, nnz * 8));
+    hk_own.reset(new (std::nothrow) uint64_t[nnz]);
+    hv_own.reset(new (std::nothrow) double[nnz]);
+    hk = hk_own.get();
+    hv = hv_own.get();
+    if (!hk || !hv) {
+        release();
+        return fail(BLCO_ERR_NOMEM, "host memory for the sorted chunks");
+    }
+    {
+        // first touch of the run buffers on many host threads, before any
+        // copy lands there (page faults dominate a copy into fresh memory)
+        const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (unsigned w = 0; w < nt; w++)
+            th.emplace_back([&, w]() {
+                const uint64_t a = nnz * w / nt, b = nnz * (w + 1) / nt;
+                memset(hk + a, 0, (b - a) * 8);
+                memset(hv + a, 0, (b - a) * 8);
+            });
+        for (auto& x : th) x.join();
+    }
+    {
+        const int dev = t->device;
+        pin_c = std::thread([&, dev]() {
+            cudaSetDevice(dev);
+            pin_e[0] = cudaMallocHost(&t->h_coords, nnz * 8);
+        });
+        pin_v = std::thread([&, dev]() {
+            cudaSetDevice(dev);
+            pin_e[1] = cudaMallocHost(&t->h_values, nnz * 8);
+        });
+    }
     CountPtrs cp;
     memset(&cp, 0, sizeof(cp));
     {
@@ -1288,9 +1333,8 @@ static int encode_chunked(blco_tensor* t, const uint64_t* const* cidx, const dou
     for (double x : part) ss += x; // fixed order: chunk by chunk
     t->norm_sq = ss;
     // Merge the sorted runs into the pinned stream.
-    cudaError_t e1 = cudaMallocHost(&t->h_coords, nnz * 8);
-    cudaError_t e2 = cudaMallocHost(&t->h_values, nnz * 8);
-    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+    join_pins();
+    if (pin_e[0] != cudaSuccess || pin_e[1] != cudaSuccess) {
         release();
         return fail(BLCO_ERR_NOMEM, "pinned host allocation for streamed blocks failed");
     }
@@ -1299,88 +1343,81 @@ static int encode_chunked(blco_tensor* t, const uint64_t* const* cidx, const dou
         rb[c] = c * C;
         re[c] = std::min(nnz, (c + 1) * C);
     }
-    const int nbytes = (L.alto_bits + 7) / 8;
-    auto relin_host = [&](uint64_t key) {
-        uint64_t v = 0;
-        for (int b = 0; b < nbytes; b++) v |= htabs.rel[b][(key >> (8 * b)) & 255];
-        return v;
-    };
-    // Output segments split at sampled keys; every key's duplicates fall in
-    // one segment (a segment holds the keys in [lo, hi)).
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const int T = (int)std::min<uint64_t>(std::max(1u, std::min(hw, 64u)), std::max<uint64_t>(1, nnz / 65536));
-    std::vector<uint64_t> sample;
-    const uint64_t step = std::max<uint64_t>(1, nnz / ((uint64_t)T * 64));
-    for (uint64_t c = 0; c < nchunks; c++)
-        for (uint64_t i = rb[c]; i < re[c]; i += step) sample.push_back(hk[i]);
-    std::sort(sample.begin(), sample.end());
-    std::vector<uint64_t> split; // T - 1 increasing keys
-    for (int k = 1; k < T; k++) {
-        const uint64_t key = sample[(size_t)((double)k / T * sample.size())];
-        if (split.empty() || key > split.back()) split.push_back(key);
-    }
-    const int S = (int)split.size() + 1;
-    // cut[c][k]: first index of run c with key >= split[k-1] (cut[c][0] = rb[c], cut[c][S] = re[c])
-    std::vector<std::vector<uint64_t>> cut(nchunks, std::vector<uint64_t>(S + 1));
-    for (uint64_t c = 0; c < nchunks; c++) {
-        cut[c][0] = rb[c];
-        cut[c][S] = re[c];
-        for (int k = 1; k < S; k++)
-            cut[c][k] = (uint64_t)(std::lower_bound(hk + rb[c], hk + re[c], split[k - 1]) - hk);
-    }
-    std::vector<uint64_t> outpos(S + 1, 0);
-    for (int k = 0; k < S; k++) {
-        uint64_t len = 0;
-        for (uint64_t c = 0; c < nchunks; c++) len += cut[c][k + 1] - cut[c][k];
-        outpos[k + 1] = outpos[k] + len;
-    }
-    auto merge_seg = [&](int k) {
-        // min-heap of (key, run): ties go to the lower run, i.e. input order
-        std::vector<std::pair<uint64_t, uint64_t>> heap;
-        std::vector<uint64_t> at(nchunks), end(nchunks);
-        for (uint64_t c = 0; c < nchunks; c++) {
-            at[c] = cut[c][k];
-            end[c] = cut[c][k + 1];
-            if (at[c] < end[c]) heap.push_back({hk[at[c]], c});
+    // The merge runs on the GPU, one output segment of at most C nonzeros at
+    // a time: the segment's slice of every run (found below) is copied in,
+    // in run order, and the stable radix sort of the concatenation is the
+    // merged order (equal keys keep run order, i.e. input order); its last
+    // pass writes BLCO coordinates through the byte table.
+    // split(o): per run, how many of its nonzeros come before output rank o:
+    // all keys below v, then keys equal to v in run order, v the smallest key
+    // with at least o keys at or below it.
+    auto split_at = [&](uint64_t o, std::vector<uint64_t>& cut) {
+        cut.assign(nchunks, 0);
+        if (o >= nnz) {
+            for (uint64_t c = 0; c < nchunks; c++) cut[c] = re[c] - rb[c];
+            return;
         }
-        auto greater = [](const std::pair<uint64_t, uint64_t>& a, const std::pair<uint64_t, uint64_t>& b) {
-            return a > b;
+        auto count_le = [&](uint64_t v) {
+            uint64_t n = 0;
+            for (uint64_t c = 0; c < nchunks; c++) n += (uint64_t)(std::upper_bound(hk + rb[c], hk + re[c], v) - (hk + rb[c]));
+            return n;
         };
-        std::make_heap(heap.begin(), heap.end(), greater);
-        uint64_t o = outpos[k];
-        while (!heap.empty()) {
-            std::pop_heap(heap.begin(), heap.end(), greater);
-            const uint64_t c = heap.back().second;
-            heap.pop_back();
-            // take the run's whole stretch of keys not above the next head
-            const uint64_t lim = heap.empty() ? ~0ull : heap.front().first;
-            const uint64_t limc = heap.empty() ? 0 : heap.front().second;
-            uint64_t i = at[c];
-            do {
-                t->h_coords[o] = relin_host(hk[i]);
-                t->h_values[o] = hv[i];
-                o++;
-                i++;
-            } while (i < end[c] && (hk[i] < lim || (hk[i] == lim && c < limc)));
-            at[c] = i;
-            if (i < end[c]) {
-                heap.push_back({hk[i], c});
-                std::push_heap(heap.begin(), heap.end(), greater);
-            }
+        uint64_t lo = 0, hi = ~0ull; // count_le(hi) = nnz >= o + 1 > o
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (count_le(mid) >= o + 1) hi = mid;
+            else lo = mid + 1;
+        }
+        // lo: the key of the nonzero at rank o; the first o nonzeros are the
+        // keys below lo and the first ones equal to lo, in run order
+        uint64_t rem = o;
+        for (uint64_t c = 0; c < nchunks; c++) {
+            cut[c] = (uint64_t)(std::lower_bound(hk + rb[c], hk + re[c], lo) - (hk + rb[c]));
+            rem -= cut[c];
+        }
+        for (uint64_t c = 0; c < nchunks && rem; c++) {
+            const uint64_t eq = (uint64_t)(std::upper_bound(hk + rb[c], hk + re[c], lo) - (hk + rb[c])) - cut[c];
+            const uint64_t take = std::min(eq, rem);
+            cut[c] += take;
+            rem -= take;
         }
     };
-    {
-        std::vector<std::thread> th;
-        std::atomic<int> next{0};
-        for (int w = 0; w < std::min(S, (int)hw); w++)
-            th.emplace_back([&]() {
-                for (int k = next++; k < S; k = next++) merge_seg(k);
-            });
-        for (auto& x : th) x.join();
+    const uint64_t nseg = (nnz + C - 1) / C;
+    std::vector<uint64_t> cut_lo, cut_hi;
+    split_at(0, cut_lo);
+    const int nbytes = (L.alto_bits + 7) / 8;
+    for (uint64_t k = 0; k < nseg; k++) {
+        const uint64_t o0 = k * C, o1 = std::min(nnz, o0 + C);
+        split_at(o1, cut_hi);
+        uint64_t n = 0;
+        for (uint64_t c = 0; c < nchunks; c++) {
+            const uint64_t len = cut_hi[c] - cut_lo[c];
+            if (!len) continue;
+            CH_CUDA(cudaMemcpyAsync(k0 + n, hk + rb[c] + cut_lo[c], len * 8, cudaMemcpyHostToDevice, s));
+            CH_CUDA(cudaMemcpyAsync(v0 + n, hv + rb[c] + cut_lo[c], len * 8, cudaMemcpyHostToDevice, s));
+            n += len;
+        }
+        if (n != o1 - o0) {
+            release();
+            return fail(BLCO_ERR_STATE, "streamed encode: merge segment sizes do not add up");
+        }
+        bool alt = false;
+        int st = BLCO_OK;
+        if (n > 1 && L.alto_bits > 0) st = radix_sort_pairs(k0, v0, k1, v1, n, 0, L.alto_bits, s, &alt, d_tabs);
+        else if (n && L.alto_bits > 0) {
+            k_relin<<<1, 32, 0, s>>>(k0, n, d_tabs, nbytes);
+            count_launch();
+            if (cudaGetLastError() != cudaSuccess) st = fail(BLCO_ERR_CUDA, "k_relin launch failed");
+        }
+        if (st != BLCO_OK) { release(); return st; }
+        CH_CUDA(cudaMemcpyAsync(t->h_coords + o0, alt ? k1 : k0, n * 8, cudaMemcpyDeviceToHost, s));
+        CH_CUDA(cudaMemcpyAsync(t->h_values + o0, alt ? v1 : v0, n * 8, cudaMemcpyDeviceToHost, s));
+        cut_lo.swap(cut_hi);
     }
+    CH_CUDA(cudaStreamSynchronize(s));
     // heavy-row statistics and tables from the row counts
-    cudaFreeHost(hk);
-    cudaFreeHost(hv);
+    hk_own.reset();
+    hv_own.reset();
     hk = nullptr;
     hv = nullptr;
     int st = build_hot_tables_impl(t, s, counts);
