@@ -2,11 +2,12 @@
 // the ceiling of the MTTKRP kernels (bench.py's roofline reports each
 // MTTKRP's gathered rows per second against it).
 //
-//   bin/gather_ceiling [--rows N] [--gathers G] [--zipf S]
+//   bin/gather_ceiling [--rows N] [--gathers G] [--zipf S] [--inflight U] [--ctas-per-sm C]
 //
 // A gather is one factor row of 128 bytes (rank 32 in FP32) loaded by 8
-// lanes with one 16-byte load each, four rows in flight per lane group, 32
-// warps per SM, the same load shape as the MTTKRP kernels.  Row indices are
+// lanes with one 16-byte load each, U rows in flight per lane group (4, the
+// MTTKRP kernels' step), C CTAs of 8 warps per SM (4: 32 warps, the MTTKRP
+// kernels' occupancy); other U and C measure how the rate scales.  Row indices are
 // drawn on the GPU: Zipf(S) over N rows by inverse CDF (the workload's
 // per-mode distribution), and uniform over a 256k-row (32 MB, L2-resident)
 // factor.  Prints one JSON line with G rows/s for each; best of 5 timed
@@ -58,8 +59,7 @@ __global__ void k_draw(uint32_t* idx, uint64_t count, const double* cdf, uint32_
     }
 }
 
-constexpr int U = 4;
-
+template <int U>
 __global__ void __launch_bounds__(256) k_gather(const float4* __restrict__ F, const uint32_t* __restrict__ idx,
                                                 uint64_t count, float4* __restrict__ sink)
 {
@@ -83,11 +83,25 @@ int main(int argc, char** argv)
     uint32_t rows = 2000000;
     uint64_t count = 64ull << 20;
     double s = 1.1;
+    int inflight = 4, per_sm = 4;
     for (int i = 1; i + 1 < argc; i += 2) {
         if (!strcmp(argv[i], "--rows")) rows = (uint32_t)strtoul(argv[i + 1], nullptr, 10);
         else if (!strcmp(argv[i], "--gathers")) count = strtoull(argv[i + 1], nullptr, 10);
         else if (!strcmp(argv[i], "--zipf")) s = strtod(argv[i + 1], nullptr);
+        else if (!strcmp(argv[i], "--inflight")) inflight = atoi(argv[i + 1]);
+        else if (!strcmp(argv[i], "--ctas-per-sm")) per_sm = atoi(argv[i + 1]);
     }
+    if (inflight != 1 && inflight != 2 && inflight != 4 && inflight != 8 && inflight != 16) {
+        fprintf(stderr, "gather_ceiling: --inflight takes 1, 2, 4, 8 or 16\n");
+        return 1;
+    }
+    if (per_sm < 1 || per_sm > 8) {
+        fprintf(stderr, "gather_ceiling: --ctas-per-sm takes 1..8\n");
+        return 1;
+    }
+    void (*kern)(const float4*, const uint32_t*, uint64_t, float4*) =
+        inflight == 1 ? k_gather<1> : inflight == 2 ? k_gather<2> : inflight == 4 ? k_gather<4>
+                                    : inflight == 8 ? k_gather<8> : k_gather<16>;
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
     const uint32_t l2rows = 262144;
@@ -99,7 +113,7 @@ int main(int argc, char** argv)
     CK(cudaMalloc(&F, (size_t)frows * 128));
     CK(cudaMemset(F, 0, (size_t)frows * 128));
     CK(cudaMalloc(&idx, count * sizeof(uint32_t)));
-    const int blocks = sms * 4;
+    const int blocks = sms * per_sm;
     CK(cudaMalloc(&sink, (size_t)blocks * 256 * sizeof(float4)));
     std::vector<double> cdf(rows);
     double acc = 0.0;
@@ -114,12 +128,12 @@ int main(int argc, char** argv)
     for (int which = 0; which < 2; which++) {
         k_draw<<<sms * 8, 256>>>(idx, count, which == 0 ? dcdf : nullptr, which == 0 ? rows : l2rows, 12345u + which);
         CK(cudaGetLastError());
-        k_gather<<<blocks, 256>>>(F, idx, count, sink);
+        kern<<<blocks, 256>>>(F, idx, count, sink);
         CK(cudaGetLastError());
         float best = 1e30f;
         for (int r = 0; r < 5; r++) {
             CK(cudaEventRecord(e0));
-            k_gather<<<blocks, 256>>>(F, idx, count, sink);
+            kern<<<blocks, 256>>>(F, idx, count, sink);
             CK(cudaEventRecord(e1));
             CK(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -129,8 +143,8 @@ int main(int argc, char** argv)
         rate[which] = (double)count / (best * 1e-3) / 1e9;
     }
     printf("{\"zipf\": %.3f, \"rows\": %u, \"grows_per_s_zipf\": %.2f, \"grows_per_s_l2_resident\": %.2f, "
-           "\"gathers\": %llu, \"row_bytes\": 128, \"sms\": %d}\n",
-           s, rows, rate[0], rate[1], (unsigned long long)count, sms);
+           "\"gathers\": %llu, \"row_bytes\": 128, \"sms\": %d, \"inflight\": %d, \"ctas_per_sm\": %d}\n",
+           s, rows, rate[0], rate[1], (unsigned long long)count, sms, inflight, per_sm);
     cudaFree(F);
     cudaFree(idx);
     cudaFree(sink);
