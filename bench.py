@@ -18,8 +18,8 @@ the 126 MB L2, so no flush is needed between steps.
 
 --impl reference times the reference's own CPU CP-ALS (cpd_alto,
 include/cpd.hpp, compiled from the reference sources into oracle/_ref with
-scipy's OpenBLAS) on a bounded sample of the same workload with all host
-threads, and whole on the CPU-runnable workload (`c1`); it also runs the
+scipy's OpenBLAS) on the whole workload with all host threads (about 2.8 s
+per iteration), and on the CPU-runnable workload (`c1`); it also runs the
 reference's own GPU code on the full workload (`reference_gpu`) with a
 full-size fit comparison against this engine's plain form.
 
@@ -304,8 +304,9 @@ def reference_cpu_c1():
 
 def run_reference(args, world, rank):
     """The reference's CPU CP-ALS (cpd_alto, include/cpd.hpp:44-187, built
-    from the reference sources into oracle/_ref with scipy's OpenBLAS) on a
-    bounded sample of the workload, all host threads, and on the CPU-runnable
+    from the reference sources into oracle/_ref with scipy's OpenBLAS) on the
+    workload (the whole tensor unless --ref-sample asks for fewer nonzeros,
+    which are then scaled), all host threads, and on the CPU-runnable
     workload whole; then the reference's GPU code on the full workload."""
     if rank != 0:
         return
@@ -316,10 +317,11 @@ def run_reference(args, world, rank):
         return
     load_pkg()
     from blco_b200 import synth
-    sample = args.ref_sample
+    sample = min(args.ref_sample, WORKLOAD["nnz"])
+    full = sample == WORKLOAD["nnz"]  # --ref-sample 200000000: the whole tensor, measured, not scaled
     dims, rk = WORKLOAD["dims"], WORKLOAD["rank"]
     if torch.cuda.is_available():
-        X = synth.zipf_tensor_device(sample, dims, WORKLOAD["zipf"], seed=7)
+        X = synth.zipf_tensor_device(sample, dims, WORKLOAD["zipf"], seed=args.seed if full else 7)
         cidx = np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]])
         vals = X["vals"].cpu().numpy()
         del X
@@ -332,11 +334,17 @@ def run_reference(args, world, rank):
     r = po.ref_cpd_alto(dims, cidx, vals, fs, np.ones(rk), args.warmup + args.steps, 0.0, nthreads=nthreads)
     scale = WORKLOAD["nnz"] / sample
     value = r["ms_per_iter"] + r["mttkrp_ms_per_iter"] * (scale - 1.0)
-    desc = (f"reference cpd_alto (oracle/_ref, scipy OpenBLAS) on {sample} nonzeros of the same distribution with "
-            f"the full mode lengths, {nthreads} threads, {r['iters']} iterations, its own per-iteration times "
-            f"({r['ms_per_iter']:.1f} ms, of which MTTKRP {r['mttkrp_ms_per_iter']:.1f} ms); estimate for "
-            f"{WORKLOAD['nnz']} nonzeros = iteration + MTTKRP x ({scale:.0f} - 1): the dense steps already run at "
-            "full size, the MTTKRP is scaled by the nonzeros")
+    if full:
+        desc = (f"reference cpd_alto (oracle/_ref, scipy OpenBLAS) on the whole {sample}-nonzero tensor, "
+                f"{nthreads} threads, {r['iters']} iterations, its own per-iteration times "
+                f"({r['ms_per_iter']:.1f} ms, of which MTTKRP {r['mttkrp_ms_per_iter']:.1f} ms): measured")
+    else:
+        desc = (f"reference cpd_alto (oracle/_ref, scipy OpenBLAS) on {sample} nonzeros of the same distribution "
+                f"with the full mode lengths, {nthreads} threads, {r['iters']} iterations, its own per-iteration "
+                f"times ({r['ms_per_iter']:.1f} ms, of which MTTKRP {r['mttkrp_ms_per_iter']:.1f} ms); estimate "
+                f"for {WORKLOAD['nnz']} nonzeros = iteration + MTTKRP x ({scale:.0f} - 1): the dense steps already "
+                "run at full size, the MTTKRP is scaled by the nonzeros (--ref-sample 200000000 measures the "
+                "whole tensor)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "higher_is_better": False,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value,
@@ -352,42 +360,24 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def cpu_baseline_quick(args, dims, rk):
-    """Reference CPU MTTKRP on a bounded sample (rank 0, N=1 only)."""
-    import ctypes
+def cpu_baseline_full(args, dims, rk, h_cidx, h_vals):
+    """The reference's CPU CP-ALS (cpd_alto, oracle/_ref) on the whole
+    benchmark tensor (its host copy), all host threads, 3 iterations: its own
+    per-iteration time (rank 0, N=1 only)."""
     import pyoracle as po
-    from blco_b200 import synth
-    R = po.ref_lib()
-    if R is None:
+    if po.ref_lib() is None:
         return None
-    sample = args.ref_sample
-    X = synth.zipf_tensor_device(sample, dims, WORKLOAD["zipf"], seed=7)
-    cidx = np.ascontiguousarray(np.stack([c.cpu().numpy().astype(np.uint64) for c in X["cidx"]]))
-    vals = np.ascontiguousarray(X["vals"].cpu().numpy())
-    del X
+    cidx = np.ascontiguousarray(np.stack([c.numpy().view(np.uint64) for c in h_cidx]))
+    vals = np.ascontiguousarray(h_vals.numpy())
     nthreads = os.cpu_count() or 1
-    d64 = np.ascontiguousarray(dims, dtype=np.uint64)
-    u64p = ctypes.POINTER(ctypes.c_uint64)
-    f64p = ctypes.POINTER(ctypes.c_double)
-    h = R.ref_alto_create(3, d64.ctypes.data_as(u64p), sample, cidx.ctypes.data_as(u64p),
-                          vals.ctypes.data_as(f64p), nthreads)
     rng = np.random.default_rng(0)
-    fs = [rng.random((d, rk)) for d in dims]
-    ptrs = (ctypes.c_void_p * 3)(*[f.ctypes.data for f in fs])
-    for m in range(3):
-        R.ref_alto_mttkrp(h, m, rk, ptrs)
-    t0 = time.perf_counter()
-    reps = 2
-    for _ in range(reps):
-        for m in range(3):
-            R.ref_alto_mttkrp(h, m, rk, ptrs)
-    dt = (time.perf_counter() - t0) * 1e3 / reps
-    R.ref_alto_destroy(h, rk)
-    value = dt / sample * WORKLOAD["nnz"]
-    return dict(value=value, unit="ms", cores=nthreads, kind="reference",
-                sample=(f"reference mttkrp_alto_par (oracle/_ref), all 3 modes on {sample} nonzeros of the "
-                        f"same distribution and dims, {nthreads} threads, scaled linearly to "
-                        f"{WORKLOAD['nnz']} nonzeros; MTTKRP part of the iteration only"))
+    fs = [np.ascontiguousarray(rng.random((d, rk))) for d in dims]
+    r = po.ref_cpd_alto(dims, cidx, vals, fs, np.ones(rk), 3, 0.0, nthreads=nthreads)
+    return dict(value=r["ms_per_iter"], unit="ms", cores=nthreads, kind="reference",
+                mttkrp_ms_per_iter=r["mttkrp_ms_per_iter"],
+                sample=(f"reference cpd_alto (oracle/_ref, scipy OpenBLAS) on the whole {cidx.shape[1]}-nonzero "
+                        f"tensor, {nthreads} threads, {r['iters']} iterations, its own per-iteration time (MTTKRP "
+                        f"{r['mttkrp_ms_per_iter']:.1f} ms of it): measured, not scaled"))
 
 
 FORMS = {
@@ -585,10 +575,11 @@ def wide_cpu_baseline(args, X, dims, rk):
         R.ref_alto_mttkrp128(h, m, rk, ptrs)
     dt = (time.perf_counter() - t0) * 1e3
     R.ref_alto_destroy128(h, rk)
+    how = ("the whole tensor, measured" if sample == total else
+           f"the first {sample} nonzeros, scaled linearly to {total} nonzeros")
     return dict(value=dt / sample * total, unit="ms", cores=nthreads, kind="reference",
                 sample=(f"reference mttkrp_alto_par on AltoTensor<unsigned __int128> (oracle/_ref), all "
-                        f"{len(dims)} modes on the first {sample} nonzeros, {nthreads} threads, scaled linearly "
-                        f"to {total} nonzeros; MTTKRP part of the iteration only"))
+                        f"{len(dims)} modes on {how}, {nthreads} threads; MTTKRP part of the iteration only"))
 
 
 def wide_leg(pkg, torch, args, peak, with_cpu):
@@ -854,7 +845,7 @@ def run_ours(args, world, rank, local):
             schedules.append(dict(mode=m, schedule=k, **space[k], decided_by="sweep" if swept else "network"))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_quick(args, dims, rk)
+        cpu = cpu_baseline_full(args, dims, rk, h_cidx, h_vals)
     # rows each mode's MTTKRP gathers with the compressed-fibre kernel, and the rate
     gather = None
     used = [sc["kernel"] for sc in schedules] if schedules else None
@@ -1024,7 +1015,9 @@ def main():
     ap.add_argument("--kernel", type=int, default=21,
                     help="MTTKRP kernel id; 21 (default) = the committed learned schedule selector")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--ref-sample", type=int, default=2_000_000)
+    ap.add_argument("--ref-sample", type=int, default=WORKLOAD["nnz"],
+                    help="--impl reference: nonzeros of the CPU CP-ALS run (the whole tensor by default; fewer are "
+                         "scaled to it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched many-small-tensors leg")
     ap.add_argument("--no-wide", action="store_true", help="skip the wide-key (128-bit BLCO) leg")
