@@ -16,9 +16,9 @@
 // integers in [-256, 256], exact in BF16, and their products (at most 2^16)
 // summed over at most 256 rows stay at or below 2^24: every partial sum the
 // tensor cores form in their FP32 accumulator is an integer of at most
-// 2^24, hence exact, whatever the accumulator's rounding.  (A split into BF16 hi + lo parts, the usual
-// scheme, is not exact there: the tensor cores' FP32 accumulation leans
-// low, and that bias reached the CP-ALS fit.)
+// 2^24, hence exact, whatever the accumulator's rounding.  (A split into
+// BF16 hi + lo parts, the usual scheme, is not exact there: the tensor
+// cores' FP32 accumulation leans low, and that bias reached the CP-ALS fit.)
 //
 // The digit rows form the K-major operand S of one super-tile: row k * RB +
 // c holds digit k of column c (RB = R rounded up to 8, 16, 32 or 64; rows of
@@ -30,10 +30,11 @@
 //   2^(e_a - 8 - 8 i) 2^(e_c - 8 - 8 j) D[i RB + a][j RB + c]
 // for every digit pair (i, j) to FP64 sums: registers for RB <= 32, shared
 // memory for RB = 64.  (Dropping the small pairs would bias the diagonal:
-// there the dropped products are squares.)
-// The next super-tile's loads overlap the previous one's MMAs.  Each
-// CTA writes its R x R FP64 partial; the partials are summed in FP64 in a
-// fixed order.
+// there the dropped products are squares.)  With register sums the CTA has
+// 8 warps, two on each TMEM lane quarter, each folding half of D's columns.
+// The next super-tile's loads overlap the previous one's MMAs.  Each CTA
+// writes its R x R FP64 partial; the partials are summed in FP64 in a fixed
+// order.
 //
 // The same pass optionally scales U by inv (columns, written back) and
 // writes the BF16 gather copy, as the CUDA-core Gram does; the Gram is then
