@@ -1090,9 +1090,9 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
                       : p->mixed                                     ? BLCO_DTYPE_F32
                                                                      : BLCO_DTYPE_F64;
     if (p->mixed) {
-        // tensor-core Grams: by default up to rank 32 (above it the CUDA-core
-        // Gram is the faster), on request up to 64
-        p->gram_tc = p->opts.gram_tensor_cores > 0 ? R <= 64 : p->opts.gram_tensor_cores == 0 && R <= 32;
+        // tensor-core Grams up to rank 64 (the kernel's limit) unless the
+        // caller asks for the CUDA cores
+        p->gram_tc = p->opts.gram_tensor_cores >= 0 && R <= 64;
         if (p->gram_tc) {
             PCA(&p->tc_partials, (size_t)gram_tc_max_ctas(p->sm) * R * R * sizeof(double));
             PCA(&p->d_err, sizeof(int));

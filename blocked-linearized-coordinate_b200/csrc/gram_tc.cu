@@ -2,7 +2,7 @@
 // cores (tcgen05.mma, accumulator in TMEM), exact in the accumulator.
 //
 // U is I x R FP32, row-major (R <= 64).  Rows are taken 256 at a time (a
-// super-tile; 64 for ranks above 32), staged in shared memory.  In a
+// super-tile), staged in shared memory.  In a
 // super-tile every column c gets a power-of-two scale 2^e_c with
 // max |u_c| < 2^e_c, and every value becomes four integer digits, most
 // significant first:
@@ -23,15 +23,15 @@
 // The digit rows form the K-major operand S of one super-tile: row k * RB +
 // c holds digit k of column c (RB = R rounded up to 8, 16, 32 or 64; rows of
 // padding columns are zero).  One MMA chain per 128-row group of S computes
-// D = S S^T over the super-tile (M = 128, N = 4 RB, K = 256 in 16 MMAs, 64
-// in 4 for ranks above 32);
+// D = S S^T over the super-tile (M = 128, N = 4 RB, K = 256 in 16 MMAs);
 // D[i RB + a][j RB + c] = sum over the super-tile of d_i(a) d_j(c).  The CTA
 // reads D back (tcgen05.ld) and adds
 //   2^(e_a - 8 - 8 i) 2^(e_c - 8 - 8 j) D[i RB + a][j RB + c]
-// for every digit pair (i, j) to FP64 sums: registers for RB <= 32, shared
-// memory for RB = 64.  (Dropping the small pairs would bias the diagonal:
-// there the dropped products are squares.)  With register sums the CTA has
-// 8 warps, two on each TMEM lane quarter, each folding half of D's columns.
+// for every digit pair (i, j) to FP64 sums in registers.  (Dropping the
+// small pairs would bias the diagonal: there the dropped products are
+// squares.)  The CTA has 8 warps, two on each TMEM lane quarter, each
+// folding half of D's columns.  Ranks above 32 split the columns in two
+// halves (k_gram_tc_halves below).
 // The next super-tile's loads overlap the previous one's MMAs.  Each CTA
 // writes its R x R FP64 partial; the partials are summed in FP64 in a fixed
 // order.
@@ -141,58 +141,49 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&d)[16])
 
 template <int RB>
 struct GramShape {
+    static_assert(RB == 8 || RB == 16 || RB == 32, "ranks above 32 take k_gram_tc_halves");
     static constexpr int ND = 4;                        // digits per value
-    static constexpr int MG = ND * RB > 128 ? 2 : 1;    // 128-row groups of S
-    static constexpr int ROWS = 128 * MG;               // rows of S per K chunk
-    static constexpr int N = ND * RB;                   // MMA N: digit rows of B (32..256)
-    static constexpr int NCOLS = MG == 2 ? 512 : N <= 32 ? 32 : N <= 64 ? 64 : 128;
-    static constexpr int KS = RB == 64 ? 64 : 256;      // rows per fold (a super-tile)
+    static constexpr int ROWS = 128;                    // rows of S per K chunk (M = 128)
+    static constexpr int N = ND * RB;                   // MMA N: digit rows of B (32..128)
+    static constexpr int NCOLS = N <= 32 ? 32 : N <= 64 ? 64 : 128;
+    static constexpr int KS = 256;                      // rows per fold (a super-tile)
     static constexpr int CH = KS / 8;                   // K chunks of S
-    static constexpr bool REG = RB <= 32;               // digit-row sums in registers
-    // threads: 8 warps with register sums (two per TMEM lane quarter, each
-    // pair splitting D's columns in halves), 4 with shared-memory sums
-    static constexpr int THREADS = REG ? 256 : 128;
+    // 8 warps: two per TMEM lane quarter, each pair splitting D's columns in halves
+    static constexpr int THREADS = 256;
     static constexpr int HALVES = THREADS / TG_LANES;
     static constexpr int NV = (KS * RB / 4 + THREADS - 1) / THREADS; // float4 loads per thread
-    static constexpr int MINB = RB == 64 ? 1 : 2;       // CTAs per SM the registers must allow
+    static constexpr int MINB = 2;                      // CTAs per SM the registers must allow
     static constexpr size_t S_BYTES = (size_t)CH * ROWS * 16;
     static constexpr size_t STAGE_BYTES = (size_t)KS * RB * 4;
     static constexpr size_t GSM_BYTES = (size_t)ND * RB * (RB + 1) * 8;
-    // dynamic shared memory: S, the staged rows, then (RB = 64) the FP64
-    // sums; with RB <= 32 the sums reuse S's space once the last fold is done
-    static constexpr size_t SMEM = REG ? (S_BYTES + STAGE_BYTES > GSM_BYTES ? S_BYTES + STAGE_BYTES : GSM_BYTES)
-                                       : S_BYTES + STAGE_BYTES + GSM_BYTES;
+    // dynamic shared memory: S and the staged rows; the FP64 sums reuse that
+    // space once the last fold is done
+    static constexpr size_t SMEM = S_BYTES + STAGE_BYTES > GSM_BYTES ? S_BYTES + STAGE_BYTES : GSM_BYTES;
 };
 
 // Adds one super-tile's D (scales sd[j RB + c] = 2^(e_c - 8 - 8 j)) to this
-// thread's digit-row sums: acc (registers, RB <= 32) or gsm (RB = 64).
+// thread's digit-row sums acc.
 template <int RB>
-__device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, const double* sd,
-                                          double (&acc)[GramShape<RB>::REG ? RB : 1], double* gsm)
+__device__ __forceinline__ void fold_tile(uint32_t tmem, int warp, int tid, const double* sd, double (&acc)[RB])
 {
     using G = GramShape<RB>;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int lane_row = tid % TG_LANES, half = tid / TG_LANES;
+    const int q = tid % TG_LANES, half = tid / TG_LANES;
     const uint32_t quarter = (uint32_t)(warp % 4) * 32;
+    const bool act = q < G::ND * RB;
+    const double wa = act ? sd[q] : 0.0;
 #pragma unroll
-    for (int g = 0; g < G::MG; g++) {
-        const int q = g * 128 + lane_row;
-        const bool act = q < G::ND * RB;
-        const double wa = act ? sd[q] : 0.0;
+    for (int c0 = 0; c0 < G::N / G::HALVES; c0 += 16) {
+        const int cb = half * (G::N / G::HALVES) + c0; // this half's columns of D
+        uint32_t d[16];
+        tmem_ld16(tmem + (quarter << 16) + (uint32_t)cb, d);
 #pragma unroll
-        for (int c0 = 0; c0 < G::N / G::HALVES; c0 += 16) {
-            const int cb = half * (G::N / G::HALVES) + c0; // this half's columns of D
-            uint32_t d[16];
-            tmem_ld16(tmem + (quarter << 16) + (uint32_t)(g * 256 + cb), d);
-#pragma unroll
-            for (int x = 0; x < 16; x++) {
-                const int n = cb + x;
-                const int c = n % RB;
-                if (act) {
-                    const double v = (double)__uint_as_float(d[x]) * sd[n]; // exact: D times a power of two
-                    if constexpr (G::REG) acc[c] = fma(wa, v, acc[c]);
-                    else gsm[q * (RB + 1) + c] = fma(wa, v, gsm[q * (RB + 1) + c]);
-                }
+        for (int x = 0; x < 16; x++) {
+            const int n = cb + x;
+            const int c = n % RB;
+            if (act) {
+                const double v = (double)__uint_as_float(d[x]) * sd[n]; // exact: D times a power of two
+                acc[c] = fma(wa, v, acc[c]);
             }
         }
     }
@@ -209,7 +200,7 @@ __global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k
     extern __shared__ __align__(1024) unsigned char dsm[];
     uint4* S = reinterpret_cast<uint4*>(dsm);                          // [CH][ROWS] operand chunks
     float* stage = reinterpret_cast<float*>(dsm + G::S_BYTES);         // [KS][R] rows of U
-    double* gsm = reinterpret_cast<double*>(G::REG ? dsm : dsm + G::S_BYTES + G::STAGE_BYTES);
+    double* gsm = reinterpret_cast<double*>(dsm);                      // sums, after the last fold
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
     __shared__ uint32_t cmax[2][RB];      // per super-tile (double-buffered): largest |u| per column, as bits
@@ -222,8 +213,6 @@ __global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k
 
     for (int i = tid; i < G::CH * G::ROWS; i += G::THREADS) S[i] = make_uint4(0, 0, 0, 0);
     for (int i = tid; i < 2 * RB; i += G::THREADS) (&cmax[0][0])[i] = 0u;
-    if constexpr (!G::REG)
-        for (int i = tid; i < G::ND * RB * (RB + 1); i += G::THREADS) gsm[i] = 0.0;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -241,9 +230,9 @@ __global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k
     const uint32_t s_addr = smem_u32(S);
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(G::N >> 3) << 17) | ((128u >> 4) << 24);
 
-    double acc[G::REG ? RB : 1];
+    double acc[RB];
 #pragma unroll
-    for (int c = 0; c < (G::REG ? RB : 1); c++) acc[c] = 0.0;
+    for (int c = 0; c < RB; c++) acc[c] = 0.0;
 
     uint32_t phase = 0; // commits issued (or, in the self-test, skipped)
     bool late = false;  // the same on every thread
@@ -349,7 +338,7 @@ __global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k
 #pragma unroll
             for (int k = 0; k < G::ND; k++) S[j * G::ROWS + k * RB + c] = make_uint4(h[k][0], h[k][1], h[k][2], h[k][3]);
         }
-        if (t > 0) fold_tile<RB>(tmem, warp, tid, sdj[b ^ 1], acc, gsm);
+        if (t > 0) fold_tile<RB>(tmem, warp, tid, sdj[b ^ 1], acc);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
@@ -357,17 +346,12 @@ __global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
             for (int kk = 0; kk < G::KS / 16; kk++) {
-                const uint32_t kb = s_addr + (uint32_t)(kk * 2 * G::ROWS * 16);
-                const uint64_t db = umma_desc(kb, G::ROWS * 16);
-#pragma unroll
-                for (int g = 0; g < G::MG; g++) {
-                    const uint64_t da = umma_desc(kb + (uint32_t)(g * 128 * 16), G::ROWS * 16);
-                    asm volatile("{\n\t.reg .pred p;\n\t"
-                                 "setp.ne.b32 p, %4, 0;\n\t"
-                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                                 :
-                                 : "r"(tmem + (uint32_t)(g * 256)), "l"(da), "l"(db), "r"(idesc), "r"(kk));
-                }
+                const uint64_t dd = umma_desc(s_addr + (uint32_t)(kk * 2 * G::ROWS * 16), G::ROWS * 16);
+                asm volatile("{\n\t.reg .pred p;\n\t"
+                             "setp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                             :
+                             : "r"(tmem), "l"(dd), "l"(dd), "r"(idesc), "r"(kk));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                          : "memory");
@@ -377,7 +361,7 @@ __global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k
     // the last super-tile
     if (!late && nsup > 0) {
         if (cta_wait_late(bar, (phase - 1) & 1, spin_max)) late = true;
-        else fold_tile<RB>(tmem, warp, tid, sdj[(nsup - 1) & 1], acc, gsm);
+        else fold_tile<RB>(tmem, warp, tid, sdj[(nsup - 1) & 1], acc);
     }
     if (late) {
         if (tid == 0) atomicExch(err, 1);
@@ -391,7 +375,7 @@ __global__ void __launch_bounds__(GramShape<RB>::THREADS, GramShape<RB>::MINB) k
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::NCOLS));
     }
-    if constexpr (G::REG) {
+    {
         // S and the staged rows are no longer read (barrier above): the sums
         // go there, the second half of the CTA adding its columns' share
         const int q = tid % TG_LANES;
@@ -448,6 +432,293 @@ int gram_tc_dispatch(float* U, uint64_t I, int R, const double* inv, uint16_t* b
     return BLCO_OK;
 }
 
+// Ranks 33..64: the columns in two halves, A = columns 0..31 and B = the
+// rest (zero-padded to 32), each with its own 128 digit rows (four digits of
+// 32 columns), so every MMA keeps M = N = 128 and the sums stay in
+// registers.  Per super-tile three MMA chains fill three TMEM regions:
+// A A^T, A B^T and B B^T (B A^T is the transpose of A B^T); warps 0-3 fold
+// the digit rows of A (the AA and AB regions), warps 4-7 those of B (BB).
+constexpr int TH_THREADS = 256;
+constexpr int TH_KS = 256;               // rows per super-tile
+constexpr int TH_CH = TH_KS / 8;         // K chunks of S
+constexpr int TH_NV = (TH_KS * 64 / 4 + TH_THREADS - 1) / TH_THREADS; // float4 loads per thread
+constexpr size_t TH_S_BYTES = (size_t)TH_CH * 128 * 16; // one half's operand
+constexpr size_t TH_STAGE_BYTES = (size_t)TH_KS * 64 * 4;
+constexpr size_t TH_SMEM = 2 * TH_S_BYTES + TH_STAGE_BYTES;
+constexpr size_t TH_GSM_BYTES = (size_t)3 * 128 * 33 * 8;  // sums, over S once the last fold is done
+static_assert(TH_GSM_BYTES <= TH_SMEM, "tensor-core Gram: the sums must fit the operand space");
+
+// Adds region d (128 columns: digit j of column c at j * 32 + c) of one
+// super-tile to acc[c]: weights wa (this row's scale) and sd[j * 64 + off + c].
+__device__ __forceinline__ void fold_half(uint32_t taddr, double wa, const double* sd, int off, double (&acc)[32])
+{
+#pragma unroll
+    for (int c0 = 0; c0 < 128; c0 += 16) {
+        uint32_t d[16];
+        tmem_ld16(taddr + (uint32_t)c0, d);
+#pragma unroll
+        for (int x = 0; x < 16; x++) {
+            const int n = c0 + x, j = n / 32, c = n % 32;
+            const double v = (double)__uint_as_float(d[x]) * sd[j * 64 + off + c]; // exact: D times a power of two
+            acc[c] = fma(wa, v, acc[c]);
+        }
+    }
+}
+
+template <bool SCALE, bool BF16OUT>
+__global__ void __launch_bounds__(TH_THREADS, 1) k_gram_tc_halves(float* __restrict__ U, uint64_t I, int R,
+                                                                const double* __restrict__ inv,
+                                                                uint16_t* __restrict__ bf16_out, uint64_t rows_per_cta,
+                                                                double* __restrict__ partials, int* __restrict__ err,
+                                                                uint32_t spin_max, int no_commit)
+{
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    uint4* SA = reinterpret_cast<uint4*>(dsm);                        // [CH][128]
+    uint4* SB = reinterpret_cast<uint4*>(dsm + TH_S_BYTES);           // [CH][128]
+    float* stage = reinterpret_cast<float*>(dsm + 2 * TH_S_BYTES);    // [KS][R]
+    double* gsm = reinterpret_cast<double*>(dsm);                     // [3][128][33] at the end
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ uint32_t cmax[2][64];
+    __shared__ double sdj[2][4 * 64];  // per super-tile: 2^(e_c - 8 - 8 j) at j 64 + c
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint64_t r_beg = (uint64_t)blockIdx.x * rows_per_cta;
+    const uint64_t r_end = min(I, r_beg + rows_per_cta);
+    const int nsup = r_beg < r_end ? (int)((r_end - r_beg + TH_KS - 1) / TH_KS) : 0;
+    const int items = TH_CH * R;
+
+    for (int i = tid; i < 2 * TH_CH * 128; i += TH_THREADS) SA[i] = make_uint4(0, 0, 0, 0); // SA and SB
+    for (int i = tid; i < 2 * 64; i += TH_THREADS) (&cmax[0][0])[i] = 0u;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t bar = smem_u32(&mbar);
+    const uint32_t sa_addr = smem_u32(SA), sb_addr = smem_u32(SB);
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) | ((128u >> 4) << 24);
+    const bool rows_a = warp < 4;  // this warp folds A's digit rows (else B's)
+    const int q = (warp % 4) * 32 + lane; // digit row: digit q / 32 of column q % 32 of the half
+    const uint32_t trow = tmem + ((uint32_t)((warp % 4) * 32) << 16);
+
+    double acc0[32], acc1[32]; // A rows: AA and AB sums; B rows: BB sums in acc0
+#pragma unroll
+    for (int c = 0; c < 32; c++) acc0[c] = 0.0, acc1[c] = 0.0;
+    auto fold = [&](const double* sd) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int i = q / 32, a = q % 32;
+        if (rows_a) {
+            const double wa = sd[i * 64 + a];
+            fold_half(trow + 0, wa, sd, 0, acc0);     // A A^T
+            fold_half(trow + 128, wa, sd, 32, acc1);  // A B^T
+        } else {
+            const double wb = sd[i * 64 + 32 + a];
+            fold_half(trow + 256, wb, sd, 32, acc0);  // B B^T
+        }
+    };
+
+    uint32_t phase = 0;
+    bool late = false;
+    for (int t = 0; t < nsup; t++) {
+        const int b = t & 1;
+        const uint64_t k0 = r_beg + (uint64_t)t * TH_KS;
+        {
+            const uint64_t base = k0 * (uint64_t)R;
+            const uint64_t valid = (min(r_end, k0 + TH_KS) - k0) * (uint64_t)R;
+            const int nv4 = TH_KS * R / 4;
+            float4 buf[TH_NV];
+#pragma unroll
+            for (int k = 0; k < TH_NV; k++) {
+                const int f = tid + k * TH_THREADS;
+                const uint64_t e0 = 4 * (uint64_t)f;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (f < nv4 && e0 < valid) {
+                    if (e0 + 4 <= valid) {
+                        v = *reinterpret_cast<const float4*>(U + base + e0);
+                    } else {
+                        v.x = U[base + e0];
+                        if (e0 + 1 < valid) v.y = U[base + e0 + 1];
+                        if (e0 + 2 < valid) v.z = U[base + e0 + 2];
+                    }
+                }
+                buf[k] = v;
+            }
+#pragma unroll
+            for (int k = 0; k < TH_NV; k++) {
+                const int f = tid + k * TH_THREADS;
+                if (f >= nv4) continue;
+                if (SCALE || BF16OUT) {
+                    const uint64_t e0 = 4 * (uint64_t)f;
+                    float x[4] = {buf[k].x, buf[k].y, buf[k].z, buf[k].w};
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        if (e0 + u >= valid) continue;
+                        const uint64_t gi = base + e0 + u;
+                        float y = x[u];
+                        if (SCALE) y = (float)((double)y * inv[(int)(gi % (uint64_t)R)]);
+                        if constexpr (BF16OUT) {
+                            const uint16_t h = bf16_bits_rn(y);
+                            y = bf16_to_f32(h);
+                            bf16_out[gi] = h;
+                        }
+                        x[u] = y;
+                    }
+                    buf[k] = make_float4(x[0], x[1], x[2], x[3]);
+                    if (e0 + 4 <= valid) {
+                        *reinterpret_cast<float4*>(U + base + e0) = buf[k];
+                    } else if (e0 < valid) {
+                        U[base + e0] = x[0];
+                        if (e0 + 1 < valid) U[base + e0 + 1] = x[1];
+                        if (e0 + 2 < valid) U[base + e0 + 2] = x[2];
+                    }
+                }
+                reinterpret_cast<float4*>(stage)[f] = buf[k];
+            }
+        }
+        if (tid < 64) cmax[b ^ 1][tid] = 0u;
+        __syncthreads();
+        for (int it = tid; it < items; it += TH_THREADS) {
+            const int j = it / R, c = it % R;
+            float m = 0.f;
+#pragma unroll
+            for (int e = 0; e < 8; e++) m = fmaxf(m, fabsf(stage[(8 * j + e) * R + c]));
+            atomicMax(&cmax[b][c], __float_as_uint(m));
+        }
+        __syncthreads();
+        for (int k = tid; k < 4 * 64; k += TH_THREADS)
+            sdj[b][k] = pow2_f64(exponent_of(cmax[b][k % 64]) - 8 - 8 * (k / 64));
+        if (t > 0 && cta_wait_late(bar, (phase - 1) & 1, spin_max)) {
+            late = true;
+            break;
+        }
+        for (int it = tid; it < items; it += TH_THREADS) {
+            const int j = it / R, c = it % R;
+            const int ex = exponent_of(cmax[b][c]);
+            uint32_t h[4][4];
+#pragma unroll
+            for (int e = 0; e < 8; e += 2) {
+                uint32_t lohi[4][2];
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    float r = scale_pow2(stage[(8 * j + e + u) * R + c], 8 - ex);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const float d = rintf(r);
+                        lohi[k][u] = digit_bits(d);
+                        r = (r - d) * 256.f;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k++) h[k][e / 2] = lohi[k][0] | (lohi[k][1] << 16);
+            }
+            uint4* S = c < 32 ? SA : SB;
+            const int cc = c % 32;
+#pragma unroll
+            for (int k = 0; k < 4; k++) S[j * 128 + k * 32 + cc] = make_uint4(h[k][0], h[k][1], h[k][2], h[k][3]);
+        }
+        if (t > 0) fold(sdj[b ^ 1]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0 && !no_commit) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int kk = 0; kk < TH_KS / 16; kk++) {
+                const uint32_t off = (uint32_t)(kk * 2 * 128 * 16);
+                const uint64_t da = umma_desc(sa_addr + off, 128 * 16);
+                const uint64_t db = umma_desc(sb_addr + off, 128 * 16);
+                asm volatile("{\n\t.reg .pred p;\n\t"
+                             "setp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                             :
+                             : "r"(tmem), "l"(da), "l"(da), "r"(idesc), "r"(kk));
+                asm volatile("{\n\t.reg .pred p;\n\t"
+                             "setp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                             :
+                             : "r"(tmem + 128u), "l"(da), "l"(db), "r"(idesc), "r"(kk));
+                asm volatile("{\n\t.reg .pred p;\n\t"
+                             "setp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                             :
+                             : "r"(tmem + 256u), "l"(db), "l"(db), "r"(idesc), "r"(kk));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        phase++;
+    }
+    if (!late && nsup > 0) {
+        if (cta_wait_late(bar, (phase - 1) & 1, spin_max)) late = true;
+        else fold(sdj[(nsup - 1) & 1]);
+    }
+    if (late) {
+        if (tid == 0) atomicExch(err, 1);
+        if (!no_commit) (void)cta_wait_late(bar, (phase - 1) & 1, spin_max);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+    }
+    // sums into shared memory (over the operands, no longer read): AA and AB
+    // rows of A, BB rows of B
+    double* gAA = gsm;
+    double* gAB = gsm + 128 * 33;
+    double* gBB = gsm + 2 * 128 * 33;
+#pragma unroll
+    for (int c = 0; c < 32; c++) {
+        if (rows_a) {
+            gAA[q * 33 + c] = acc0[c];
+            gAB[q * 33 + c] = acc1[c];
+        } else {
+            gBB[q * 33 + c] = acc0[c];
+        }
+    }
+    __syncthreads();
+    // G_cta: sum over digits i of the rows i * 32 + a of the right block
+    for (int e = tid; e < R * R; e += TH_THREADS) {
+        const int a = e / R, c = e % R;
+        double g = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (a < 32 && c < 32) g += gAA[(i * 32 + a) * 33 + c];
+            else if (a < 32) g += gAB[(i * 32 + a) * 33 + (c - 32)];
+            else if (c < 32) g += gAB[(i * 32 + c) * 33 + (a - 32)];
+            else g += gBB[(i * 32 + a - 32) * 33 + (c - 32)];
+        }
+        partials[(size_t)blockIdx.x * R * R + e] = g;
+    }
+}
+
+int gram_tc_halves_launch(float* U, uint64_t I, int R, const double* inv, uint16_t* bf16_out, double* partials,
+                          int sm, int* d_err, cudaStream_t s, int* nparts, uint32_t spin_max, int no_commit)
+{
+    void (*fn)(float*, uint64_t, int, const double*, uint16_t*, uint64_t, double*, int*, uint32_t, int);
+    if (bf16_out) fn = inv ? k_gram_tc_halves<true, true> : k_gram_tc_halves<false, true>;
+    else fn = inv ? k_gram_tc_halves<true, false> : k_gram_tc_halves<false, false>;
+    BLCO_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TH_SMEM));
+    // one CTA per SM: it holds the whole TMEM (three 128-column regions)
+    const uint64_t sups = (I + TH_KS - 1) / TH_KS;
+    const uint64_t maxc = std::min<uint64_t>((uint64_t)sm, (uint64_t)gram_tc_max_ctas(sm));
+    const uint64_t sups_per = std::max<uint64_t>(1, (sups + maxc - 1) / maxc);
+    const uint64_t rows_per = sups_per * TH_KS;
+    const int grid = (int)std::max<uint64_t>(1, (I + rows_per - 1) / rows_per);
+    fn<<<grid, TH_THREADS, TH_SMEM, s>>>(U, I, R, inv, bf16_out, rows_per, partials, d_err, spin_max, no_commit);
+    BLCO_CHECK_LAUNCH("k_gram_tc_halves");
+    *nparts = grid;
+    return BLCO_OK;
+}
+
 } // namespace
 
 int gram_tc_max_ctas(int sm) { return sm * 8; }
@@ -464,7 +735,7 @@ int gram_tc_launch(float* U, uint64_t I, int R, const double* inv, uint16_t* bf1
         return gram_tc_dispatch<16>(U, I, R, inv, bf16_out, partials, sm, d_err, s, nparts, spin_max, no_commit);
     if (R <= 32)
         return gram_tc_dispatch<32>(U, I, R, inv, bf16_out, partials, sm, d_err, s, nparts, spin_max, no_commit);
-    return gram_tc_dispatch<64>(U, I, R, inv, bf16_out, partials, sm, d_err, s, nparts, spin_max, no_commit);
+    return gram_tc_halves_launch(U, I, R, inv, bf16_out, partials, sm, d_err, s, nparts, spin_max, no_commit);
 }
 
 } // namespace blco

@@ -122,11 +122,10 @@ typedef struct blco_opts {
     uint64_t residency_bytes; /* device budget for streamed blocks; 0 = 8 GiB */
     void* stream;          /* cudaStream_t to run on; NULL = the default stream */
     int gram_tensor_cores; /* mixed forms' Grams (blco_gram_f32's two
-                              engines): 0 (default) = on the tensor cores
-                              (tcgen05, exact integer digit products) up to
-                              rank 32, FP64 on the CUDA cores above; 1 = on
-                              the tensor cores up to rank 64; -1 = on the
-                              CUDA cores */
+                              engines): 0 (default) or 1 = on the tensor
+                              cores (tcgen05, exact integer digit products)
+                              up to rank 64, FP64 on the CUDA cores above;
+                              -1 = on the CUDA cores */
     int solve;             /* BLCO_SOLVE_AUTO: Cholesky of the R x R system,
                               the pseudoinverse when it is not positive
                               definite; BLCO_SOLVE_PINV: the reference's

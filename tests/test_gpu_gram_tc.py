@@ -90,14 +90,16 @@ def test_gram_tc_rejects_large_rank(blco):
     assert e.value.status == blco.ERR_UNSUPPORTED
 
 
+@pytest.mark.parametrize("R", [16, 48])
 @pytest.mark.parametrize("prec", ["PRECISION_MIXED", "PRECISION_MIXED_BF16"])
-def test_mixed_cpals_tensor_core_grams(blco, prec):
+def test_mixed_cpals_tensor_core_grams(blco, prec, R):
+    """Rank 16 runs the per-super-tile kernel, rank 48 the two-halves one,
+    each with the column scaling (and, in the BF16 form, the BF16 copy)."""
     rng = np.random.default_rng(8)
     dims = [4000, 3000, 90]
     cidx = unique_coords(rng, dims, 80_000, zipf=0.9)
     vals = rng.random(80_000)
     t = blco.Tensor.encode(dims, cidx, vals)
-    R = 16
     fs0 = [rng.random((d, R)) for d in dims]
     out = {}
     for name, o in [("fp64", blco.make_opts()),
@@ -112,8 +114,8 @@ def test_mixed_cpals_tensor_core_grams(blco, prec):
     # ~1e-3 away from FP64 and its trajectory follows small changes more.
     bound = 1e-6 if prec == "PRECISION_MIXED" else 1e-4
     assert np.max(np.abs(out["tc"] - out["cuda"])) <= bound
-    # rank 16: the default engine is the tensor cores' (same launches, so
-    # the same fits up to the order of FP64 atomics in the MTTKRP)
+    # the default engine is the tensor cores' (same launches, so the same
+    # fits up to the order of FP64 atomics in the MTTKRP)
     assert np.max(np.abs(out["default"] - out["tc"])) <= bound
     if prec == "PRECISION_MIXED":
         assert np.max(np.abs(out["tc"] - out["fp64"])) <= 1e-5
