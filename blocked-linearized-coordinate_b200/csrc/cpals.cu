@@ -1170,16 +1170,18 @@ int plan_create(blco_tensor* t, int rank, double* const* d_factors, double* d_la
     if (st != BLCO_OK) { plan_free(p); return st; }
     // the stream copies the modes' schedules read (compressed fibres, or
     // heavy rows and cold stream), built now rather than inside the first
-    // iteration
+    // iteration; the modes' fibre builds share one scratch
+    FibScratch fsc;
     for (int n = 0; n < p->N && st == BLCO_OK; n++) {
         if (!t->resident) continue;
         const int k = mttkrp_select_kernel(t, n, R, p->sched[n].kernel, p->gather_dtype);
         if (k == BLCO_KERNEL_FIBRE &&
             (p->sched[n].kernel == BLCO_KERNEL_FIBRE || p->sched[n].kernel == BLCO_KERNEL_AUTO))
-            st = build_fibre_copy(t, n, p->s);
+            st = build_fibre_copy(t, n, p->s, &fsc);
         else if (k == BLCO_KERNEL_LVL2) // the heavy-row schedule's stream copies, likewise
             st = build_mode_copies(t, n, p->s);
     }
+    fib_scratch_free(fsc);
     if (st != BLCO_OK) { plan_free(p); return st; }
     // Descending mode length, ties in natural order (src/cpd_gpu.cu:137-139).
     for (int n = 0; n < p->N; n++) p->order[n] = n;

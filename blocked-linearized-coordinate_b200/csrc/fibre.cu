@@ -751,7 +751,38 @@ void fibre_free(FibreCopy& f)
     f = FibreCopy();
 }
 
-int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s)
+void fib_scratch_free(FibScratch& sc)
+{
+    cudaFree(sc.k0);
+    cudaFree(sc.k1);
+    cudaFree(sc.i0);
+    cudaFree(sc.i1);
+    cudaFree(sc.sa);
+    cudaFree(sc.sb);
+    cudaFree(sc.sums);
+    sc = FibScratch();
+}
+
+int fib_scratch_reserve(FibScratch& sc, uint64_t n)
+{
+    if (sc.k0 && sc.cap >= n) return BLCO_OK;
+    fib_scratch_free(sc);
+    cudaError_t e = cudaMalloc(&sc.k0, n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&sc.k1, n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&sc.i0, n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&sc.i1, n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&sc.sa, (n + 1) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&sc.sb, (n + 1) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&sc.sums, ((n + 1) / 4096 + 2) * 4);
+    if (e != cudaSuccess) {
+        fib_scratch_free(sc);
+        return cuda_fail(e, "fibre-copy scratch", __FILE__, __LINE__);
+    }
+    sc.cap = n;
+    return BLCO_OK;
+}
+
+int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s, FibScratch* sc)
 {
     FibreCopy& fc = t->fib[mode];
     if (fc.built) return BLCO_OK;
@@ -773,17 +804,11 @@ int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s)
     const int bits_t = __builtin_popcountll(L.mode_masks[mode]);
     const int bits_f = __builtin_popcountll(L.mode_masks[fm]);
 
-    uint64_t *k0 = nullptr, *k1 = nullptr, *i0 = nullptr, *i1 = nullptr;
-    uint32_t *sa = nullptr, *sb = nullptr, *sums = nullptr;
+    FibScratch own;
+    FibScratch& S = sc ? *sc : own;
     int st = BLCO_OK;
     auto cleanup = [&]() {
-        cudaFreeAsync(k0, s);
-        cudaFreeAsync(k1, s);
-        cudaFreeAsync(i0, s);
-        cudaFreeAsync(i1, s);
-        cudaFreeAsync(sa, s);
-        cudaFreeAsync(sb, s);
-        cudaFreeAsync(sums, s);
+        if (!sc) fib_scratch_free(own);
     };
 #define FB_CUDA(call)                                                          \
     do {                                                                       \
@@ -803,13 +828,9 @@ int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s)
             return st;                                                         \
         }                                                                      \
     } while (0)
-    FB_CUDA(cudaMallocAsync(&k0, n * 8, s));
-    FB_CUDA(cudaMallocAsync(&k1, n * 8, s));
-    FB_CUDA(cudaMallocAsync(&i0, n * 8, s));
-    FB_CUDA(cudaMallocAsync(&i1, n * 8, s));
-    FB_CUDA(cudaMallocAsync(&sa, (n + 1) * 4, s));
-    FB_CUDA(cudaMallocAsync(&sb, (n + 1) * 4, s));
-    FB_CUDA(cudaMallocAsync(&sums, ((n + 1) / 4096 + 2) * 4, s));
+    FB_TRY(fib_scratch_reserve(S, n));
+    uint64_t *k0 = S.k0, *k1 = S.k1, *i0 = S.i0, *i1 = S.i1;
+    uint32_t *sa = S.sa, *sb = S.sb, *sums = S.sums;
     const int grid = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)di.sm_count * 16);
     k_fib_keys<<<grid, 256, 0, s>>>(t->d_coords, n, L.mode_pos[mode], L.mode_masks[mode], L.mode_pos[fm],
                                     L.mode_masks[fm], bits_f, k0, i0);
@@ -845,10 +866,10 @@ int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s)
         const uint64_t np = pad4(nf);
         for (int m = 0; m < f.ninner; m++) {
             FB_CUDA(cudaMalloc(&f.d_fw[m], np * 4));
-            FB_CUDA(cudaMemsetAsync(f.d_fw[m], 0, np * 4, s));
+            FB_CUDA(cudaMemsetAsync(f.d_fw[m] + nf, 0, (np - nf) * 4, s)); // k_fib_write fills [0, nf)
         }
         FB_CUDA(cudaMalloc(&f.d_fv, np * 8));
-        FB_CUDA(cudaMemsetAsync(f.d_fv, 0, np * 8, s));
+        FB_CUDA(cudaMemsetAsync(f.d_fv + nf, 0, (np - nf) * 8, s));
         FB_CUDA(cudaMalloc(&f.d_fib, (f.nfib + 3) * 4));
         FB_CUDA(cudaMemsetAsync(f.d_fib, 0, (f.nfib + 3) * 4, s));
         FB_CUDA(cudaMalloc(&f.d_frows, (f.nrows_f + 2) * 4));
@@ -889,10 +910,10 @@ int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s)
         const uint64_t np = pad4(nl);
         for (int m = 0; m <= f.ninner; m++) {
             FB_CUDA(cudaMalloc(&f.d_lw[m], np * 4));
-            FB_CUDA(cudaMemsetAsync(f.d_lw[m], 0, np * 4, s));
+            FB_CUDA(cudaMemsetAsync(f.d_lw[m] + nl, 0, (np - nl) * 4, s)); // k_fib_write fills [0, nl)
         }
         FB_CUDA(cudaMalloc(&f.d_lv, np * 8));
-        FB_CUDA(cudaMemsetAsync(f.d_lv, 0, np * 8, s));
+        FB_CUDA(cudaMemsetAsync(f.d_lv + nl, 0, (np - nl) * 8, s));
         FB_CUDA(cudaMalloc(&f.d_lrows, (f.nrows_l + 2) * 4));
         FB_CUDA(cudaMemsetAsync(f.d_lrows, 0, (f.nrows_l + 2) * 4, s));
         FB_CUDA(cudaMalloc(&f.d_lctab, ((nl + FB_CHUNK - 1) / FB_CHUNK + 1) * 4));

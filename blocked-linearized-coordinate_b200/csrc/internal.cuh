@@ -253,7 +253,23 @@ int mttkrp_launch(const blco_tensor* t, const MttkrpArgs& a, cudaStream_t s);
 // fibre.cu: the compressed-fibre schedule (kernel id 4).
 bool fibre_eligible(const blco_tensor* t, int mode);
 int fibre_lanes(int rank, int dtype); // lanes per factor row, 0 = no kernel for this rank
-int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s);
+// Scratch of a fibre-copy build: sort keys and stream positions (a pair of
+// each for the radix sort's ping-pong), two flag/scan arrays and the scans'
+// block sums, 40 bytes per nonzero.  Taken with cudaMalloc, not from the
+// stream-ordered pool: the pool hands its memory back at every
+// synchronisation, so a build per mode mapped and unmapped all of it again
+// (about 90 ms per mode at 200M nonzeros, against a few ms here).  One
+// scratch serves the builds of all modes of a plan.
+struct FibScratch {
+    uint64_t *k0 = nullptr, *k1 = nullptr, *i0 = nullptr, *i1 = nullptr;
+    uint32_t *sa = nullptr, *sb = nullptr, *sums = nullptr;
+    uint64_t cap = 0; // nonzeros the buffers hold
+};
+int fib_scratch_reserve(FibScratch& sc, uint64_t n);
+void fib_scratch_free(FibScratch& sc); // waits for the device (cudaFree)
+// Builds the mode's copy once (no-op when built); sc = nullptr: a scratch of
+// its own, freed before it returns.
+int build_fibre_copy(blco_tensor* t, int mode, cudaStream_t s, FibScratch* sc = nullptr);
 // encode.cu: the mode's heavy-row and cold stream copies (HotTable), built
 // on first use by the heavy-row schedule (no-op when built, not resident,
 // or the mode has no heavy rows).
